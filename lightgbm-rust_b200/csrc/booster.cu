@@ -1,0 +1,535 @@
+// Device-resident boosting (Gbdt::train_one_iter, crates/lgbm-core/src/boosting.rs:957-1130),
+// the stand-alone objective gradients (RowObjective::gradients) and the
+// batched predictor (predict.rs:231), behind the C ABI of include/lgbm_b200.h.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "learner_impl.h"
+
+using namespace lgbm_b200;
+
+namespace lgbm_b200 {
+
+// objective/*.rs boost_from_score for the supported objectives (first iteration only).
+static double boost_from_score(const LgbmB200ObjectiveConfig& o, const std::vector<float>& label, int k) {
+  const size_t n = label.size();
+  if (o.objective == LGBM_B200_OBJ_BINARY) {  // binary.rs:129-154
+    double suml = 0.0;
+    for (size_t i = 0; i < n; ++i) suml += (double)(int32_t)(label[i] > 0.0f);
+    double pavg = suml / (double)n;
+    pavg = std::min(pavg, 1.0 - kEpsilon);
+    pavg = std::max(pavg, kEpsilon);
+    return std::log(pavg / ((double)1.0f - pavg)) / o.sigmoid;
+  }
+  if (o.objective == LGBM_B200_OBJ_REGRESSION) {  // regression.rs:123-139
+    double suml = 0.0;
+    for (size_t i = 0; i < n; ++i) suml += (double)label[i];
+    return suml / (double)n;
+  }
+  if (o.objective == LGBM_B200_OBJ_MULTICLASS) {  // multiclass.rs:97-124, :156-158
+    double c = 0.0;
+    for (size_t i = 0; i < n; ++i) c += (int32_t)label[i] == k ? 1.0 : 0.0;
+    return std::log(std::max(kEpsilon, c / (double)n));
+  }
+  return 0.0;
+}
+
+static Status launch_gradients(const LgbmB200ObjectiveConfig& o, const float* label, const double* score, int64_t n,
+                               float2* gh, float* g, float* h, int sms, cudaStream_t s) {
+  int blocks = std::max(1, (int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+  switch (o.objective) {
+    case LGBM_B200_OBJ_BINARY: k_grad_binary<<<blocks, 256, 0, s>>>(label, score, n, o.sigmoid, gh, g, h); break;
+    case LGBM_B200_OBJ_REGRESSION: k_grad_l2<<<blocks, 256, 0, s>>>(label, score, n, gh, g, h); break;
+    case LGBM_B200_OBJ_MULTICLASS:
+      k_grad_softmax<<<blocks, 256, 0, s>>>(label, score, n, o.num_class, gh, n, g, h);
+      break;
+    default: return Status(LGBM_B200_ERR_UNSUPPORTED, "objective not supported by the device gradients");
+  }
+  CU_LAUNCH();
+  return Status();
+}
+
+// Tree::shrink / add_bias / as_constant on the host copy (tree.rs:303-348).
+static void shrink(HostTree& t, double rate) {
+  for (int i = 0; i < t.num_leaves - 1; ++i) {
+    t.leaf_value[i] = maybe_round_to_zero_h(t.leaf_value[i] * rate);
+    t.internal_value[i] = maybe_round_to_zero_h(t.internal_value[i] * rate);
+  }
+  int last = t.num_leaves - 1;
+  t.leaf_value[last] = maybe_round_to_zero_h(t.leaf_value[last] * rate);
+}
+static void add_bias(HostTree& t, double v) {
+  for (int i = 0; i < t.num_leaves - 1; ++i) {
+    t.leaf_value[i] = maybe_round_to_zero_h(t.leaf_value[i] + v);
+    t.internal_value[i] = maybe_round_to_zero_h(t.internal_value[i] + v);
+  }
+  int last = t.num_leaves - 1;
+  t.leaf_value[last] = maybe_round_to_zero_h(t.leaf_value[last] + v);
+}
+static void as_constant(HostTree& t, double v, int32_t count) {
+  HostTree c;
+  c.num_leaves = 1;
+  c.leaf_parent = {-1};
+  c.leaf_value = {v};
+  c.leaf_weight = {0.0};
+  c.leaf_count = {count};
+  c.leaf_depth = {0};
+  c.cat_boundaries = {0};
+  c.cat_boundaries_inner = {0};
+  t = c;
+}
+
+}  // namespace lgbm_b200
+
+struct LgbmB200Booster {
+  LgbmB200Learner* L = nullptr;
+  LgbmB200BoostConfig cfg{};
+  int K = 1;
+  int64_t n = 0, nv = 0;
+  std::vector<float> label_h;
+  float* label_d = nullptr;
+  double* score = nullptr;        // [K x n]
+  double* valid_score = nullptr;  // [K x nv]
+  uint8_t* valid_bins = nullptr;
+  int32_t valid_stride = 0;
+  DeviceArena arena;
+  std::vector<double> init_scores;
+  std::vector<bool> class_need_train;
+  int iter = 0;
+  bool first = true;
+  // bagging (sample_strategy.rs)
+  bool bagging = false;
+  uint32_t* rng = nullptr;
+  uint8_t* in_bag = nullptr;
+  uint32_t* bag = nullptr;
+  uint32_t* oob = nullptr;
+  int32_t* counts = nullptr;
+  int32_t bag_cnt = 0, oob_cnt = 0;
+  bool need_re_bagging = true;
+  // column sampler (col_sampler.rs)
+  std::unique_ptr<Lcg> col_rand;
+  int32_t used_cnt_bytree = 0;
+  std::vector<HostTree> out_trees;
+  double* lv_dev = nullptr;  // [K x L] shrunk leaf values
+  ~LgbmB200Booster() { arena.free_all(); }
+};
+
+namespace lgbm_b200 {
+
+static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB200BoostConfig* cfg,
+                             const float* label, const uint8_t* valid_bins, int64_t nv) {
+  b->L = L;
+  b->cfg = *cfg;
+  b->K = L->K;
+  b->n = L->n;
+  b->nv = nv;
+  CU(cudaSetDevice(L->device));
+  const LgbmB200ObjectiveConfig& o = cfg->objective;
+  int want_k = o.objective == LGBM_B200_OBJ_MULTICLASS ? o.num_class : 1;
+  if (want_k != b->K)
+    return Status(LGBM_B200_ERR_INVALID_PARAMETER, "learner num_tree_slots must equal the objective's tree count");
+  if (o.objective == LGBM_B200_OBJ_LAMBDARANK)
+    return Status(LGBM_B200_ERR_UNSUPPORTED, "lambdarank in the device-resident booster");
+  const int64_t n = b->n;
+  b->label_h.assign(label, label + n);
+  DeviceArena& A = b->arena;
+  Status s;
+  if (!(s = A.alloc_n(&b->label_d, (size_t)n)).ok()) return s;
+  CU(cudaMemcpy(b->label_d, label, sizeof(float) * n, cudaMemcpyHostToDevice));
+  if (!(s = A.alloc_n(&b->score, (size_t)b->K * n)).ok()) return s;
+  CU(cudaMemset(b->score, 0, sizeof(double) * b->K * n));
+  if (nv > 0) {
+    b->valid_stride = L->stride;
+    if (!(s = A.alloc_n(&b->valid_bins, (size_t)nv * b->valid_stride)).ok()) return s;
+    std::vector<uint8_t> padded((size_t)nv * b->valid_stride, 0);
+    for (int64_t r = 0; r < nv; ++r)
+      std::memcpy(&padded[(size_t)r * b->valid_stride], valid_bins + (size_t)r * L->nf, (size_t)L->nf);
+    CU(cudaMemcpy(b->valid_bins, padded.data(), padded.size(), cudaMemcpyHostToDevice));
+    if (!(s = A.alloc_n(&b->valid_score, (size_t)b->K * nv)).ok()) return s;
+    CU(cudaMemset(b->valid_score, 0, sizeof(double) * b->K * nv));
+  }
+  if (!(s = A.alloc_n(&b->lv_dev, (size_t)b->K * L->L)).ok()) return s;
+  b->init_scores.assign(b->K, 0.0);
+  b->class_need_train.assign(b->K, true);
+  if (o.objective == LGBM_B200_OBJ_MULTICLASS) {
+    for (int k = 0; k < b->K; ++k) {
+      double c = 0.0;
+      for (int64_t i = 0; i < n; ++i) c += (int32_t)label[i] == k ? 1.0 : 0.0;
+      double p = std::fabs(c / (double)n);
+      b->class_need_train[k] = !(p <= kEpsilon || p >= 1.0 - kEpsilon);
+      if (!b->class_need_train[k])
+        return Status(LGBM_B200_ERR_UNSUPPORTED, "a class without rows (or with every row) in the device booster");
+    }
+  }
+  b->bagging = cfg->bagging_fraction < 1.0 && cfg->bagging_freq > 0;
+  if (b->bagging) {
+    int64_t nb = (n + 1023) / 1024;
+    std::vector<uint32_t> seeds((size_t)nb);
+    for (int64_t i = 0; i < nb; ++i) seeds[(size_t)i] = (uint32_t)(cfg->bagging_seed + (int32_t)i);
+    if (!(s = A.alloc_n(&b->rng, (size_t)nb)).ok()) return s;
+    CU(cudaMemcpy(b->rng, seeds.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
+    if (!(s = A.alloc_n(&b->in_bag, (size_t)n)).ok()) return s;
+    if (!(s = A.alloc_n(&b->bag, (size_t)n)).ok()) return s;
+    if (!(s = A.alloc_n(&b->oob, (size_t)n)).ok()) return s;
+    if (!(s = A.alloc_n(&b->counts, 2)).ok()) return s;
+    b->bag_cnt = (int32_t)n;
+  }
+  b->col_rand = std::make_unique<Lcg>(cfg->feature_fraction_seed);
+  int32_t total = L->nf;
+  b->used_cnt_bytree = cfg->feature_fraction < 1.0
+                           ? std::max(std::min(1, total), (int32_t)((double)total * cfg->feature_fraction + (double)0.5f))
+                           : total;
+  b->out_trees.resize(b->K);
+  return Status();
+}
+
+static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
+  LgbmB200Learner* L = b->L;
+  CU(cudaSetDevice(L->device));
+  cudaStream_t s = L->stream;
+  const int K = b->K;
+  const int64_t n = b->n;
+  const int sms = L->num_sms;
+  const int blocks = std::max(1, (int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+  std::vector<double> init(K, 0.0);
+  if (b->first && b->cfg.boost_from_average) {  // boosting.rs:480-509
+    for (int k = 0; k < K; ++k) {
+      double v = boost_from_score(b->cfg.objective, b->label_h, k);
+      if (std::fabs(v) > kEpsilon) {
+        k_add_const<<<blocks, 256, 0, s>>>(b->score + (size_t)k * n, n, v);
+        CU_LAUNCH();
+        if (b->nv > 0) {
+          k_add_const<<<blocks, 256, 0, s>>>(b->valid_score + (size_t)k * b->nv, b->nv, v);
+          CU_LAUNCH();
+        }
+        init[k] = v;
+      }
+    }
+    b->init_scores = init;
+  }
+  Status st = launch_gradients(b->cfg.objective, b->label_d, b->score, n, L->gh_all, nullptr, nullptr, sms, s);
+  if (!st.ok()) return st;
+  // bagging (sample_strategy.rs:280-320)
+  if (b->bagging && ((b->bag_cnt < n && b->iter % b->cfg.bagging_freq == 0) || b->need_re_bagging)) {
+    b->need_re_bagging = false;
+    int64_t nb = (n + 1023) / 1024;
+    k_bagging<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b->rng, n, b->cfg.bagging_fraction, b->in_bag);
+    CU_LAUNCH();
+    k_compact_bag<<<1, 1024, 0, s>>>(b->in_bag, n, b->bag, b->oob, b->counts, nullptr, 0);
+    CU_LAUNCH();
+    int32_t cnt[2];
+    CU(cudaMemcpyAsync(cnt, b->counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    b->bag_cnt = cnt[0];
+    b->oob_cnt = cnt[1];
+    int rc = lgbm_b200_learner_set_bagging(L, b->bag, b->bag_cnt, LGBM_B200_DEVICE);
+    if (rc != LGBM_B200_OK) return Status(rc, lgbm_b200_last_error());
+  }
+  // by-tree column samples, one per class tree (col_sampler.rs:88-96)
+  for (int k = 0; k < K; ++k) {
+    std::vector<uint8_t> used((size_t)L->nf, 1);
+    if (b->cfg.feature_fraction < 1.0) {
+      std::fill(used.begin(), used.end(), 0);
+      for (int32_t i : b->col_rand->sample(L->nf, b->used_cnt_bytree)) used[(size_t)i] = 1;
+    }
+    CU(cudaMemcpyAsync(L->slots_h[k].bytree, used.data(), used.size(), cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));
+  }
+  if (!(st = train(L, nullptr, nullptr, LGBM_B200_DEVICE)).ok()) return st;
+  // score updates (boosting.rs:1381-1408) with the shrunk leaf values
+  bool should_continue = false;
+  std::vector<double> lv((size_t)K * L->L, 0.0);
+  for (int k = 0; k < K; ++k) {
+    HostTree& t = b->out_trees[k];
+    t = L->trees[k];
+    if (t.num_leaves > 1) {
+      should_continue = true;
+      shrink(t, b->cfg.learning_rate);
+      for (int l = 0; l < t.num_leaves; ++l) lv[(size_t)k * L->L + l] = t.leaf_value[l];
+    }
+  }
+  CU(cudaMemcpyAsync(b->lv_dev, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice, s));
+  {
+    DCtx c = L->ctx;
+    k_add_leaf_outputs<<<dim3(std::max(1, sms * 4 / L->L + 1), L->L, K), 256, 0, s>>>(c, b->lv_dev, L->L, b->score, n);
+    CU_LAUNCH();
+    if (b->bagging && b->oob_cnt > 0) {
+      k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->oob_cnt + 255) / 256, sms * 8)), 1, K), 256, 0,
+                          s>>>(c, c.bins, c.stride, b->oob, b->oob_cnt, b->lv_dev, L->L, b->score, n);
+      CU_LAUNCH();
+    }
+    if (b->nv > 0) {
+      k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->nv + 255) / 256, sms * 8)), 1, K), 256, 0, s>>>(
+          c, b->valid_bins, b->valid_stride, nullptr, b->nv, b->lv_dev, L->L, b->valid_score, b->nv);
+      CU_LAUNCH();
+    }
+  }
+  CU(cudaStreamSynchronize(s));
+  for (int k = 0; k < K; ++k) {
+    HostTree& t = b->out_trees[k];
+    if (t.num_leaves > 1) {
+      if (std::fabs(b->init_scores[k]) > kEpsilon && b->first) add_bias(t, b->init_scores[k]);
+    } else if (b->first) {
+      as_constant(t, b->init_scores[k], (int32_t)n);
+    } else {
+      as_constant(t, 0.0, (int32_t)n);
+    }
+  }
+  b->first = false;
+  *stop = should_continue ? 0 : 1;
+  if (should_continue) b->iter += 1;
+  return Status();
+}
+
+// ---- stand-alone gradients with a cached per-device workspace -----------------------------
+struct GradWorkspace {
+  std::mutex mu;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  DeviceArena arena;
+  size_t cap = 0;
+  float* label = nullptr;
+  double* score = nullptr;
+  float* g = nullptr;
+  float* h = nullptr;
+};
+static GradWorkspace g_ws;
+
+}  // namespace lgbm_b200
+
+extern "C" {
+
+int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, const double* scores,
+                        int64_t num_data, const int32_t* query_boundaries, int32_t num_queries, float* grad,
+                        float* hess, int32_t location, int32_t device) {
+  (void)query_boundaries;
+  (void)num_queries;
+  if (!cfg || !label || !scores || !grad || !hess || num_data <= 0)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  const int k = cfg->objective == LGBM_B200_OBJ_MULTICLASS ? cfg->num_class : 1;
+  const size_t n = (size_t)num_data, nk = n * (size_t)k;
+  if (location == LGBM_B200_DEVICE) {
+    Status s = launch_gradients(*cfg, label, scores, num_data, nullptr, grad, hess, 148, 0);
+    if (!s.ok()) return fail(s);
+    cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+    return LGBM_B200_OK;
+  }
+  std::lock_guard<std::mutex> lock(g_ws.mu);
+  GradWorkspace& w = g_ws;
+  if (w.device != device) {
+    w.arena.free_all();
+    w.cap = 0;
+    if (w.stream) cudaStreamDestroy(w.stream);
+    if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(Status(LGBM_B200_ERR_CUDA, "stream"));
+    w.device = device;
+  }
+  if (w.cap < nk) {
+    w.arena.free_all();
+    Status s;
+    if (!(s = w.arena.alloc_n(&w.label, n)).ok() || !(s = w.arena.alloc_n(&w.score, nk)).ok() ||
+        !(s = w.arena.alloc_n(&w.g, nk)).ok() || !(s = w.arena.alloc_n(&w.h, nk)).ok()) {
+      w.cap = 0;
+      return fail(s);
+    }
+    w.cap = nk;
+  }
+  cudaStream_t s = w.stream;
+  cudaMemcpyAsync(w.label, label, sizeof(float) * n, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(w.score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
+  Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, 148, s);
+  if (!st.ok()) return fail(st);
+  cudaMemcpyAsync(grad, w.g, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hess, w.h, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_booster_create(LgbmB200Learner* learner, const LgbmB200BoostConfig* cfg, const float* label,
+                             const int32_t* query_boundaries, int32_t num_queries, const uint8_t* valid_bins,
+                             int64_t num_valid, LgbmB200Booster** out) {
+  (void)query_boundaries;
+  (void)num_queries;
+  if (!learner || !cfg || !label || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  auto b = std::make_unique<LgbmB200Booster>();
+  Status s = booster_create(b.get(), learner, cfg, label, valid_bins, valid_bins ? num_valid : 0);
+  if (!s.ok()) return fail(s);
+  *out = b.release();
+  return LGBM_B200_OK;
+}
+
+void lgbm_b200_booster_destroy(LgbmB200Booster* b) {
+  if (b) {
+    cudaSetDevice(b->L->device);
+    delete b;
+  }
+}
+
+int lgbm_b200_booster_train_iter(LgbmB200Booster* b, int32_t* stop, LgbmB200TreeView* out) {
+  if (!b || !stop) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  Status s = booster_iter(b, stop);
+  if (!s.ok()) return fail(s);
+  if (out)
+    for (int k = 0; k < b->K; ++k) b->out_trees[k].view(&out[k]);
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_booster_scores(LgbmB200Booster* b, int32_t which, double* out, int32_t location) {
+  if (!b || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  cudaSetDevice(b->L->device);
+  const double* src = which == 0 ? b->score : b->valid_score;
+  size_t cnt = (size_t)b->K * (which == 0 ? b->n : b->nv);
+  if (!src || cnt == 0) return LGBM_B200_OK;
+  cudaError_t e = cudaMemcpyAsync(out, src, sizeof(double) * cnt,
+                                  location == LGBM_B200_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                  b->L->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->L->stream);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_booster_init_scores(LgbmB200Booster* b, double* out) {
+  if (!b || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  for (int k = 0; k < b->K; ++k) out[k] = b->init_scores[k];
+  return LGBM_B200_OK;
+}
+
+}  // extern "C"
+
+// ---- forest / batched prediction ---------------------------------------------------------------
+struct LgbmB200Forest {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DeviceArena arena;
+  DForest f{};
+  int32_t ntpi = 1;
+  ~LgbmB200Forest() {
+    arena.free_all();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace lgbm_b200 {
+static Status forest_create(LgbmB200Forest* F, const LgbmB200TreeView* trees, int32_t nt, int32_t ntpi,
+                            int32_t device) {
+  F->device = device;
+  F->ntpi = std::max(1, ntpi);
+  CU(cudaSetDevice(device));
+  CU(cudaStreamCreateWithFlags(&F->stream, cudaStreamNonBlocking));
+  std::vector<int32_t> node_off, leaf_off, num_leaves, feature, left, right, cat_idx, cat_bnd{0};
+  std::vector<double> threshold, leaf_value;
+  std::vector<int8_t> dtype;
+  std::vector<uint32_t> cat_words;
+  for (int32_t t = 0; t < nt; ++t) {
+    const LgbmB200TreeView& v = trees[t];
+    node_off.push_back((int32_t)feature.size());
+    leaf_off.push_back((int32_t)leaf_value.size());
+    num_leaves.push_back(v.num_leaves);
+    int32_t cat_base = (int32_t)cat_bnd.size() - 1;
+    for (int32_t c = 0; c < v.num_cat; ++c) {
+      int32_t b0 = v.cat_boundaries[c], b1 = v.cat_boundaries[c + 1];
+      for (int32_t w = b0; w < b1; ++w) cat_words.push_back(v.cat_threshold[w]);
+      cat_bnd.push_back((int32_t)cat_words.size());
+    }
+    for (int32_t nd = 0; nd < v.num_leaves - 1; ++nd) {
+      feature.push_back(v.split_feature[nd]);
+      threshold.push_back(v.threshold[nd]);
+      dtype.push_back(v.decision_type[nd]);
+      left.push_back(v.left_child[nd]);
+      right.push_back(v.right_child[nd]);
+      cat_idx.push_back((v.decision_type[nd] & 1) ? cat_base + (int32_t)v.threshold[nd] : -1);
+    }
+    for (int32_t l = 0; l < v.num_leaves; ++l) leaf_value.push_back(v.leaf_value[l]);
+  }
+  DeviceArena& A = F->arena;
+  auto up = [&](auto& vec, auto** dst) -> Status {
+    Status s = A.alloc_n(dst, std::max<size_t>(vec.size(), 1));
+    if (!s.ok()) return s;
+    if (!vec.empty()) CU(cudaMemcpy(*dst, vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice));
+    return Status();
+  };
+  DForest& f = F->f;
+  f.num_trees = nt;
+  f.ntpi = F->ntpi;
+  Status s;
+  int32_t *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8;
+  double *d1, *d2;
+  int8_t* i8;
+  uint32_t* u1;
+  if (!(s = up(node_off, &a1)).ok() || !(s = up(leaf_off, &a2)).ok() || !(s = up(num_leaves, &a3)).ok() ||
+      !(s = up(feature, &a4)).ok() || !(s = up(left, &a5)).ok() || !(s = up(right, &a6)).ok() ||
+      !(s = up(cat_idx, &a7)).ok() || !(s = up(cat_bnd, &a8)).ok() || !(s = up(threshold, &d1)).ok() ||
+      !(s = up(leaf_value, &d2)).ok() || !(s = up(dtype, &i8)).ok() || !(s = up(cat_words, &u1)).ok())
+    return s;
+  f.node_off = a1;
+  f.leaf_off = a2;
+  f.num_leaves = a3;
+  f.feature = a4;
+  f.left = a5;
+  f.right = a6;
+  f.cat_idx = a7;
+  f.cat_bnd = a8;
+  f.threshold = d1;
+  f.leaf_value = d2;
+  f.dtype = i8;
+  f.cat_words = u1;
+  return Status();
+}
+}  // namespace lgbm_b200
+
+extern "C" {
+
+int lgbm_b200_forest_create(const LgbmB200TreeView* trees, int32_t num_trees, int32_t num_tree_per_iteration,
+                            int32_t device, LgbmB200Forest** out) {
+  if (!trees || num_trees < 0 || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  auto F = std::make_unique<LgbmB200Forest>();
+  Status s = forest_create(F.get(), trees, num_trees, num_tree_per_iteration, device);
+  if (!s.ok()) return fail(s);
+  *out = F.release();
+  return LGBM_B200_OK;
+}
+
+void lgbm_b200_forest_destroy(LgbmB200Forest* f) {
+  if (f) {
+    cudaSetDevice(f->device);
+    delete f;
+  }
+}
+
+int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t ncol, double* out,
+                      int32_t location) {
+  if (!F || !X || !out || nrow < 0 || ncol <= 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  if (nrow == 0) return LGBM_B200_OK;
+  cudaSetDevice(F->device);
+  cudaStream_t s = F->stream;
+  const float* Xd = X;
+  double* od = out;
+  float* xtmp = nullptr;
+  double* otmp = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (location == LGBM_B200_HOST) {
+    e = cudaMallocAsync(reinterpret_cast<void**>(&xtmp), sizeof(float) * nrow * ncol, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&otmp), sizeof(double) * nrow * F->ntpi, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(xtmp, X, sizeof(float) * nrow * ncol, cudaMemcpyHostToDevice, s);
+    Xd = xtmp;
+    od = otmp;
+  }
+  if (e == cudaSuccess) {
+    launch_predict(F->f, Xd, nrow, ncol, od, s);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && location == LGBM_B200_HOST)
+    e = cudaMemcpyAsync(out, otmp, sizeof(double) * nrow * F->ntpi, cudaMemcpyDeviceToHost, s);
+  if (xtmp) cudaFreeAsync(xtmp, s);
+  if (otmp) cudaFreeAsync(otmp, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+}  // extern "C"

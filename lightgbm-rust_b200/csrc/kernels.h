@@ -1,0 +1,59 @@
+// Kernel declarations and launch-shape constants shared by the kernel
+// translation units and the host driver.
+#pragma once
+#include "device_common.cuh"
+
+namespace lgbm_b200 {
+
+constexpr int kHistThreads = 512;
+constexpr int kMaxTileFeatures = 256;
+constexpr int kMaxTiles = 64;
+
+// Feature tiles of a histogram launch (blockIdx.y): tile k covers features
+// [f0[k], f0[k+1]) whose stored bins are [bin0[k], bin0[k+1]).
+struct DTileTable {
+  int32_t f0[kMaxTiles + 1];
+  int32_t bin0[kMaxTiles + 1];
+};
+
+struct ScanSmem {
+  double g[kMaxBins], h[kMaxBins];        // this leaf's feature view
+  double cg[kMaxBins], ch[kMaxBins];      // cumulative sums in scan order
+  int32_t cc[kMaxBins];                   // cumulative count estimates
+  int64_t ig[kMaxBins];                   // quantized view / cumulative
+  int32_t tpos[kMaxBins];                 // scan position -> t (-1: skipped default bin)
+  int32_t sorted[kMaxBins];               // categorical order
+  double key[kMaxBins];
+};
+
+__global__ void k_tree_init(DCtx c, const uint32_t* bag, int32_t n_used);
+template <int kMode>
+__global__ void k_hist_float(DCtx c, DTileTable tt);
+__global__ void k_hist_int(DCtx c, DTileTable tt, int32_t sub_rows);
+template <bool kInt>
+__global__ void k_scan(DCtx c);
+__global__ void k_partition(DCtx c);
+__global__ void k_leaf_sums(DCtx c, double* sums);
+__global__ void k_leaf_renew(DCtx c, const double* sums);
+__global__ void k_add_leaf_outputs(DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
+                                   int64_t score_stride);
+__global__ void k_add_tree_binned(DCtx c, const uint8_t* bins, int32_t stride, const uint32_t* rows, int64_t n,
+                                  const double* leaf_values, int32_t lv_stride, double* score, int64_t score_stride);
+
+// objective_kernels.cu
+__global__ void k_grad_binary(const float* label, const double* score, int64_t n, double sigmoid, float2* gh_out,
+                              float* g, float* h);
+__global__ void k_grad_l2(const float* label, const double* score, int64_t n, float2* gh_out, float* g, float* h);
+__global__ void k_grad_softmax(const float* label, const double* score, int64_t n, int32_t k, float2* gh_out,
+                               int64_t gh_stride, float* g, float* h);
+__global__ void k_interleave(const float* g, const float* h, int64_t n, float2* gh);
+__global__ void k_quant_absmax(const float2* gh, int64_t n, unsigned long long* maxbits, int32_t* counter,
+                               DSlotState* st, int32_t bins, int32_t const_hess, int32_t num_blocks);
+__global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv, int64_t start,
+                              const DSlotState* st, int32_t const_hess, int32_t stochastic, int32_t* packed);
+__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag);
+__global__ void k_compact_bag(const uint8_t* in_bag, int64_t n, uint32_t* bag, uint32_t* oob, int32_t* counts,
+                              int32_t* block_counts, int32_t num_blocks);
+__global__ void k_add_const(double* score, int64_t n, double v);
+
+}  // namespace lgbm_b200

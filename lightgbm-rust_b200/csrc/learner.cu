@@ -1,0 +1,668 @@
+// Host driver of the B200 tree learner and the C ABI of include/lgbm_b200.h.
+//
+// A learner handle owns the uploaded bin matrix and, per tree slot, every
+// device buffer the grow loop touches. One train call enqueues the whole
+// tree (init, then num_leaves-1 steps of histogram / scan / partition) on
+// the handle's stream without reading anything back until the tree is done
+// (optionally replayed from a captured CUDA graph), then copies the tree
+// arrays back and rebuilds the reference's Tree layout on the host.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "learner_impl.h"
+
+namespace lgbm_b200 {
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace lgbm_b200
+
+namespace lgbm_b200 {
+
+static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg, const uint8_t* bins, int64_t n,
+                            int32_t nf, const LgbmB200FeatureMeta* metas) {
+  h->cfg = *cfg;
+  if (n <= 0 || n > INT32_MAX) return Status(LGBM_B200_ERR_INVALID_DATA, "num_data must be in [1, 2^31-1]");
+  if (nf <= 0) return Status(LGBM_B200_ERR_INVALID_DATA, "no features");
+  if (cfg->num_leaves < 2 && cfg->num_leaves != 0) {
+  }
+  h->device = cfg->device;
+  CU(cudaSetDevice(h->device));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, h->device));
+  h->num_sms = prop.multiProcessorCount;
+  CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->n = n;
+  h->nf = nf;
+  h->K = std::max(1, cfg->num_tree_slots);
+  h->L = std::max(2, cfg->num_leaves);
+  h->stride = (nf + 15) / 16 * 16;
+  // features and histogram layout
+  int32_t pos = 0;
+  h->feats.resize(nf);
+  for (int32_t f = 0; f < nf; ++f) {
+    const LgbmB200FeatureMeta& m = metas[f];
+    DFeature& d = h->feats[f];
+    d.num_bin = m.num_bin;
+    d.most_freq_bin = m.most_freq_bin;
+    d.offset = m.most_freq_bin == 0 ? 1 : 0;
+    d.default_bin = m.default_bin;
+    d.missing_type = m.missing_type;
+    d.bin_type = m.bin_type;
+    d.monotone_type = m.monotone_type;
+    d.real_index = m.real_index;
+    d.penalty = m.penalty;
+    d.view_start = pos;
+    d.view_len = m.num_bin - d.offset;
+    if (d.view_len + 1 > kMaxBins || d.view_len < 0)
+      return Status(LGBM_B200_ERR_UNSUPPORTED, "feature " + std::to_string(f) + " stores more than 256 bins");
+    if (d.monotone_type != 0 && d.bin_type == 1)
+      return Status(LGBM_B200_ERR_INVALID_PARAMETER,
+                    "The output cannot be monotone with respect to categorical features");
+    pos += d.view_len;
+  }
+  h->total_bins = pos;
+  bool use_monotone = false;
+  for (auto& f : h->feats) use_monotone |= f.monotone_type != 0;
+  // feature tiles: each tile's shared histogram fits the budget
+  const int mode = cfg->hist_precision;
+  if (mode < 0 || mode > 2) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "hist_precision");
+  const size_t cell = mode == LGBM_B200_HIST_QUANT ? 4 : 16;
+  const size_t budget = mode == LGBM_B200_HIST_QUANT ? 96 * 1024 : 200 * 1024;
+  h->ntiles = 0;
+  h->tiles.f0[0] = 0;
+  h->tiles.bin0[0] = 0;
+  {
+    int32_t cur_bins = 0, cur_f = 0;
+    for (int32_t f = 0; f < nf; ++f) {
+      int32_t vl = h->feats[f].view_len;
+      if (cur_f > 0 && ((size_t)(cur_bins + vl) * cell > budget || cur_f >= kMaxTileFeatures)) {
+        h->ntiles++;
+        if (h->ntiles >= kMaxTiles) return Status(LGBM_B200_ERR_UNSUPPORTED, "too many histogram feature tiles");
+        h->tiles.f0[h->ntiles] = f;
+        h->tiles.bin0[h->ntiles] = h->feats[f].view_start;
+        cur_bins = 0;
+        cur_f = 0;
+      }
+      cur_bins += vl;
+      cur_f += 1;
+    }
+    h->ntiles++;
+    h->tiles.f0[h->ntiles] = nf;
+    h->tiles.bin0[h->ntiles] = h->total_bins;
+    size_t maxbins = 0;
+    for (int t = 0; t < h->ntiles; ++t) maxbins = std::max(maxbins, (size_t)(h->tiles.bin0[t + 1] - h->tiles.bin0[t]));
+    h->hist_smem = maxbins * cell;
+  }
+  if (mode == LGBM_B200_HIST_QUANT) {
+    int32_t half = std::max(1, cfg->num_grad_quant_bins / 2);
+    int64_t lim = std::min<int64_t>(32767 / half, 65535 / std::max(1, cfg->num_grad_quant_bins));
+    h->sub_rows = (int32_t)std::min<int64_t>(8192, lim);
+    if (cfg->num_grad_quant_bins < 2 || cfg->num_grad_quant_bins > 64)
+      return Status(LGBM_B200_ERR_UNSUPPORTED, "num_grad_quant_bins must be in [2, 64]");
+  }
+  // kernel attributes and grid sizes
+  if (mode == LGBM_B200_HIST_F64)
+    CU(cudaFuncSetAttribute(k_hist_float<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+  else if (mode == LGBM_B200_HIST_F32C)
+    CU(cudaFuncSetAttribute(k_hist_float<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+  else
+    CU(cudaFuncSetAttribute(k_hist_int, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+  h->scan_smem = 2 * sizeof(ScanSmem);
+  CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
+  CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
+  int per_sm = 1;
+  if (mode == LGBM_B200_HIST_F64)
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_float<0>, kHistThreads, h->hist_smem));
+  else if (mode == LGBM_B200_HIST_F32C)
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_float<1>, kHistThreads, h->hist_smem));
+  else
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_int, kHistThreads, h->hist_smem));
+  per_sm = std::max(1, per_sm);
+  h->hist_grid = std::max(1, h->num_sms * per_sm / std::max(1, h->ntiles));
+  h->part_grid = h->num_sms * 4;
+  int32_t rpb = cfg->hist_rows_per_block > 0 ? cfg->hist_rows_per_block : 2048;
+
+  // device buffers
+  DeviceArena& A = h->arena;
+  uint8_t* bins_d;
+  Status s = A.alloc_n(&bins_d, (size_t)n * h->stride);
+  if (!s.ok()) return s;
+  {
+    // host copy with the padded row stride, uploaded once
+    std::vector<uint8_t> padded((size_t)n * h->stride, 0);
+    for (int64_t r = 0; r < n; ++r) std::memcpy(&padded[(size_t)r * h->stride], bins + (size_t)r * nf, (size_t)nf);
+    CU(cudaMemcpy(bins_d, padded.data(), padded.size(), cudaMemcpyHostToDevice));
+  }
+  DFeature* feats_d;
+  if (!(s = A.alloc_n(&feats_d, (size_t)nf)).ok()) return s;
+  CU(cudaMemcpy(feats_d, h->feats.data(), sizeof(DFeature) * nf, cudaMemcpyHostToDevice));
+  const int K = h->K, L = h->L;
+  const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+  const size_t max_tiles = ((size_t)n + 2047) / 2048 + 1;
+  h->slots_h.resize(K);
+  for (int k = 0; k < K; ++k) {
+    DSlot& d = h->slots_h[k];
+    std::memset(&d, 0, sizeof(d));
+#define ALLOC(ptr, count)                                  \
+  if (!(s = A.alloc_n(&(ptr), (size_t)(count))).ok()) return s;
+    ALLOC(d.st, 1);
+    ALLOC(d.idx[0], n);
+    ALLOC(d.idx[1], n);
+    ALLOC(d.leaf_begin, L);
+    ALLOC(d.leaf_count, L);
+    ALLOC(d.leaf_side, L);
+    ALLOC(d.buf_of, L);
+    ALLOC(d.best, L);
+    ALLOC(d.splittable, (size_t)L * nf);
+    ALLOC(d.cmin, L);
+    ALLOC(d.cmax, L);
+    {
+      double* hp;
+      ALLOC(hp, cells * L);
+      d.hist = hp;
+    }
+    ALLOC(d.feat_res, 2 * (size_t)nf);
+    ALLOC(d.feat_ok, 4 * (size_t)nf);
+    ALLOC(d.tile_status, max_tiles);
+    d.gh = nullptr;  // set below from the contiguous [K x n] buffer
+    if (mode == LGBM_B200_HIST_QUANT) ALLOC(d.packed, n);
+    ALLOC(d.bytree, nf);
+    ALLOC(d.root_partials, 2 * kRootBlocks);
+    ALLOC(d.root_ipartials, kRootBlocks);
+    ALLOC(d.root_counter, 1);
+    DTree& t = d.tree;
+    ALLOC(t.split_feature_inner, L);
+    ALLOC(t.split_feature, L);
+    ALLOC(t.split_gain, L);
+    ALLOC(t.threshold_in_bin, L);
+    ALLOC(t.decision_type, L);
+    ALLOC(t.left_child, L);
+    ALLOC(t.right_child, L);
+    ALLOC(t.leaf_parent, L);
+    ALLOC(t.leaf_value, L);
+    ALLOC(t.leaf_weight, L);
+    ALLOC(t.leaf_count, L);
+    ALLOC(t.leaf_depth, L);
+    ALLOC(t.internal_value, L);
+    ALLOC(t.internal_weight, L);
+    ALLOC(t.internal_count, L);
+    ALLOC(t.cat_bits, (size_t)L * kCatWords);
+    ALLOC(t.node_gain, L);
+    CU(cudaMemset(d.st, 0, sizeof(DSlotState)));
+    CU(cudaMemset(d.tile_status, 0, max_tiles * sizeof(unsigned long long)));
+    CU(cudaMemset(d.root_counter, 0, sizeof(int32_t)));
+    CU(cudaMemset(d.bytree, 1, nf));
+  }
+  if (!(s = A.alloc_n(&h->gh_all, (size_t)K * n)).ok()) return s;
+  for (int k = 0; k < K; ++k) h->slots_h[k].gh = h->gh_all + (size_t)k * n;
+  DSlot* slots_d;
+  if (!(s = A.alloc_n(&slots_d, (size_t)K)).ok()) return s;
+  CU(cudaMemcpy(slots_d, h->slots_h.data(), sizeof(DSlot) * K, cudaMemcpyHostToDevice));
+  if (!(s = A.alloc_n(&h->bag, (size_t)n)).ok()) return s;
+  if (!(s = A.alloc_n(&h->leaf_sums, (size_t)K * L * 2)).ok()) return s;
+  if (!(s = A.alloc_n(&h->leaf_values_dev, (size_t)K * L)).ok()) return s;
+  if (mode == LGBM_B200_HIST_QUANT) {
+    if (!(s = A.alloc_n(&h->maxbits, 2)).ok()) return s;
+    if (!(s = A.alloc_n(&h->quant_counter, 1)).ok()) return s;
+    CU(cudaMemset(h->maxbits, 0, 2 * sizeof(unsigned long long)));
+    CU(cudaMemset(h->quant_counter, 0, sizeof(int32_t)));
+    // learner/quant.rs:364-398: per-block MT19937 tables (the block layout
+    // follows the reference's thread count)
+    if (cfg->stochastic_rounding) {
+      size_t nt = (size_t)std::max(1, cfg->quant_num_threads);
+      size_t nb = std::max<size_t>(1, std::min(nt, ((size_t)n + 511) / 512));
+      size_t bs = (size_t)n;
+      if (nb > 1) bs = (((size_t)n + nb - 1) / nb + 31) / 32 * 32;
+      std::vector<double> g(n), hh(n);
+      for (size_t b = 0; b < nb; ++b) {
+        size_t st = b * bs, en = std::min((size_t)n, st + bs);
+        Mt19937 ge((uint32_t)(cfg->seed + (int32_t)b));
+        Mt19937 he((uint32_t)(cfg->seed + (int32_t)b + (int32_t)nt));
+        for (size_t i = st; i < en; ++i) {
+          g[i] = ge.uniform01();
+          hh[i] = he.uniform01();
+        }
+      }
+      if (!(s = A.alloc_n(&h->grv, (size_t)n)).ok()) return s;
+      if (!(s = A.alloc_n(&h->hrv, (size_t)n)).ok()) return s;
+      CU(cudaMemcpy(h->grv, g.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+      CU(cudaMemcpy(h->hrv, hh.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    h->start_eng = std::make_unique<Mt19937>((uint32_t)cfg->seed);
+  }
+  // context
+  DCtx& c = h->ctx;
+  c.bins = bins_d;
+  c.num_data = n;
+  c.stride = h->stride;
+  c.num_features = nf;
+  c.total_bins = h->total_bins;
+  c.hist_mode = mode;
+  c.bagging = 0;
+  c.feats = feats_d;
+  DParams& p = c.p;
+  p.lambda_l1 = cfg->lambda_l1;
+  p.lambda_l2 = cfg->lambda_l2;
+  p.max_delta_step = cfg->max_delta_step;
+  p.path_smooth = cfg->path_smooth;
+  p.min_data_in_leaf = cfg->min_data_in_leaf;
+  p.min_sum_hessian_in_leaf = cfg->min_sum_hessian_in_leaf;
+  p.min_gain_to_split = cfg->min_gain_to_split;
+  p.max_cat_to_onehot = cfg->max_cat_to_onehot;
+  p.max_cat_threshold = cfg->max_cat_threshold;
+  p.cat_l2 = cfg->cat_l2;
+  p.cat_smooth = cfg->cat_smooth;
+  p.min_data_per_group = cfg->min_data_per_group;
+  p.num_leaves = L;
+  p.max_depth = cfg->max_depth;
+  p.monotone_penalty = cfg->monotone_penalty;
+  p.use_monotone = use_monotone ? 1 : 0;
+  c.slots = slots_d;
+  c.num_slots = K;
+  c.rows_per_block = rpb;
+  h->n_used = (int32_t)n;
+  h->st_h.resize(K);
+  h->trees.resize(K);
+  h->timing = false;
+  for (int i = 0; i < 4 * (h->L - 1); ++i) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    h->ev.push_back(e);
+  }
+  return Status();
+}
+
+// Enqueue one whole tree (every slot) on the stream: init, the split steps
+// and leaf renewal. Nothing here reads device memory back.
+static Status enqueue_tree(LgbmB200Learner* h) {
+  const DCtx& c = h->ctx;
+  const int K = h->K, L = h->L;
+  const int mode = h->cfg.hist_precision;
+  cudaStream_t s = h->stream;
+  dim3 init_grid(h->root_grid, 1, K);
+  k_tree_init<<<init_grid, 256, 0, s>>>(c, h->bagging ? h->bag : nullptr, h->n_used);
+  CU_LAUNCH();
+  dim3 hist_grid(h->hist_grid, h->ntiles, K);
+  dim3 scan_grid(h->nf, 1, K);
+  dim3 part_grid(h->part_grid, 1, K);
+  for (int step = 0; step < L - 1; ++step) {
+    cudaEvent_t* ev = h->timing ? &h->ev[(size_t)4 * step] : nullptr;
+    if (ev) CU(cudaEventRecord(ev[0], s));
+    if (mode == LGBM_B200_HIST_F64)
+      k_hist_float<0><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+    else if (mode == LGBM_B200_HIST_F32C)
+      k_hist_float<1><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+    else
+      k_hist_int<<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+    CU_LAUNCH();
+    if (ev) CU(cudaEventRecord(ev[1], s));
+    if (mode == LGBM_B200_HIST_QUANT) k_scan<true><<<scan_grid, 64, h->scan_smem, s>>>(c);
+    else k_scan<false><<<scan_grid, 64, h->scan_smem, s>>>(c);
+    CU_LAUNCH();
+    if (ev) CU(cudaEventRecord(ev[2], s));
+    k_partition<<<part_grid, 256, 0, s>>>(c);
+    CU_LAUNCH();
+    if (ev) CU(cudaEventRecord(ev[3], s));
+  }
+  if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
+    CU(cudaMemsetAsync(h->leaf_sums, 0, sizeof(double) * K * L * 2, s));
+    k_leaf_sums<<<dim3(8, L, K), 256, 0, s>>>(c, h->leaf_sums);
+    CU_LAUNCH();
+    k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
+    CU_LAUNCH();
+  }
+  h->last_launches = 1 + 3 * (L - 1) + ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
+  return Status();
+}
+
+static Status run_tree(LgbmB200Learner* h) {
+  cudaStream_t s = h->stream;
+  const bool graph = h->cfg.use_cuda_graph != 0 && !h->timing;
+  const int key = (h->bagging ? 1 : 0);
+  if (!graph) return enqueue_tree(h);
+  if (h->graph_exec == nullptr || h->graph_key != key) {
+    if (h->graph_exec) {
+      cudaGraphExecDestroy(h->graph_exec);
+      h->graph_exec = nullptr;
+    }
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    Status st = enqueue_tree(h);
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (!st.ok()) return st;
+    if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    CU(cudaGraphInstantiate(&h->graph_exec, g, 0));
+    cudaGraphDestroy(g);
+    h->graph_key = key;
+  }
+  CU(cudaGraphLaunch(h->graph_exec, s));
+  return Status();
+}
+
+// Copies one slot's device tree back and rebuilds the reference's arrays.
+static Status read_tree(LgbmB200Learner* h, int k) {
+  const DSlot& d = h->slots_h[k];
+  const DSlotState& st = h->st_h[k];
+  HostTree& t = h->trees[k];
+  const int nl = std::max(1, st.num_leaves_cur);
+  const int nn = nl - 1;
+  t.num_leaves = nl;
+  auto get = [&](auto& vec, const auto* src, int count) -> Status {
+    vec.resize((size_t)std::max(count, 0));
+    if (count > 0)
+      CU(cudaMemcpyAsync(vec.data(), src, sizeof(vec[0]) * count, cudaMemcpyDeviceToHost, h->stream));
+    return Status();
+  };
+  Status s;
+  if (!(s = get(t.split_feature_inner, d.tree.split_feature_inner, nn)).ok()) return s;
+  if (!(s = get(t.split_feature, d.tree.split_feature, nn)).ok()) return s;
+  if (!(s = get(t.split_gain, d.tree.split_gain, nn)).ok()) return s;
+  if (!(s = get(t.threshold_in_bin, d.tree.threshold_in_bin, nn)).ok()) return s;
+  if (!(s = get(t.decision_type, d.tree.decision_type, nn)).ok()) return s;
+  if (!(s = get(t.left_child, d.tree.left_child, nn)).ok()) return s;
+  if (!(s = get(t.right_child, d.tree.right_child, nn)).ok()) return s;
+  if (!(s = get(t.leaf_parent, d.tree.leaf_parent, nl)).ok()) return s;
+  if (!(s = get(t.leaf_value, d.tree.leaf_value, nl)).ok()) return s;
+  if (!(s = get(t.leaf_weight, d.tree.leaf_weight, nl)).ok()) return s;
+  if (!(s = get(t.leaf_count, d.tree.leaf_count, nl)).ok()) return s;
+  if (!(s = get(t.leaf_depth, d.tree.leaf_depth, nl)).ok()) return s;
+  if (!(s = get(t.internal_value, d.tree.internal_value, nn)).ok()) return s;
+  if (!(s = get(t.internal_weight, d.tree.internal_weight, nn)).ok()) return s;
+  if (!(s = get(t.internal_count, d.tree.internal_count, nn)).ok()) return s;
+  if (!(s = get(t.cat_bits, d.tree.cat_bits, nn * kCatWords)).ok()) return s;
+  if (!(s = get(t.node_gain, d.tree.node_gain, nn)).ok()) return s;
+  CU(cudaStreamSynchronize(h->stream));
+  // real-valued thresholds and category bitsets (learner/mod.rs:1132-1165)
+  t.threshold.assign((size_t)nn, 0.0);
+  t.num_cat = 0;
+  t.cat_boundaries.assign(1, 0);
+  t.cat_boundaries_inner.assign(1, 0);
+  t.cat_threshold.clear();
+  t.cat_threshold_inner.clear();
+  for (int node = 0; node < nn; ++node) {
+    int inner = t.split_feature_inner[node];
+    if (t.decision_type[node] & 1) {
+      std::vector<uint32_t> bi, bc;
+      for (int b = 0; b < kMaxBins; ++b) {
+        if ((t.cat_bits[(size_t)node * kCatWords + b / 32] >> (b % 32)) & 1u) {
+          size_t w = (size_t)(b / 32);
+          if (bi.size() < w + 1) bi.resize(w + 1, 0);
+          bi[w] |= 1u << (b % 32);
+          int32_t cat = (inner < (int)h->bin_to_cat.size() && b < (int)h->bin_to_cat[inner].size())
+                            ? h->bin_to_cat[inner][b]
+                            : b;
+          if (cat >= 0) {
+            size_t wc = (size_t)(cat / 32);
+            if (bc.size() < wc + 1) bc.resize(wc + 1, 0);
+            bc[wc] |= 1u << (cat % 32);
+          }
+        }
+      }
+      t.threshold[node] = (double)t.threshold_in_bin[node];
+      t.cat_boundaries.push_back(t.cat_boundaries.back() + (int32_t)bc.size());
+      t.cat_threshold.insert(t.cat_threshold.end(), bc.begin(), bc.end());
+      t.cat_boundaries_inner.push_back(t.cat_boundaries_inner.back() + (int32_t)bi.size());
+      t.cat_threshold_inner.insert(t.cat_threshold_inner.end(), bi.begin(), bi.end());
+      t.num_cat += 1;
+    } else {
+      uint32_t tb = t.threshold_in_bin[node];
+      t.threshold[node] = (inner < (int)h->upper_bounds.size() && tb < h->upper_bounds[inner].size())
+                              ? h->upper_bounds[inner][tb]
+                              : (double)tb;
+    }
+  }
+  return Status();
+}
+
+Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location) {
+  CU(cudaSetDevice(h->device));
+  const int K = h->K;
+  const int64_t n = h->n;
+  cudaStream_t s = h->stream;
+  // gradients into the interleaved per-slot buffers
+  if (grad) {
+    if (location == LGBM_B200_HOST) {
+      if (!h->score_scratch) {
+        Status st = h->arena.alloc(reinterpret_cast<void**>(&h->score_scratch), sizeof(float) * 2 * n);
+        if (!st.ok()) return st;
+      }
+      float* tmp = reinterpret_cast<float*>(h->score_scratch);
+      for (int k = 0; k < K; ++k) {
+        CU(cudaMemcpyAsync(tmp, grad + (size_t)k * n, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(tmp + n, hess + (size_t)k * n, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        k_interleave<<<h->num_sms * 4, 256, 0, s>>>(tmp, tmp + n, n, const_cast<float2*>(h->slots_h[k].gh));
+        CU_LAUNCH();
+      }
+    } else {
+      for (int k = 0; k < K; ++k) {
+        k_interleave<<<h->num_sms * 4, 256, 0, s>>>(grad + (size_t)k * n, hess + (size_t)k * n, n,
+                                                    const_cast<float2*>(h->slots_h[k].gh));
+        CU_LAUNCH();
+      }
+    }
+  }
+  if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT) {
+    for (int k = 0; k < K; ++k) {
+      int blocks = h->num_sms * 4;
+      k_quant_absmax<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->maxbits, h->quant_counter, h->slots_h[k].st,
+                                            h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks);
+      CU_LAUNCH();
+      int64_t start = h->start_eng->uniform_int(0, (int32_t)n);
+      k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, start, h->slots_h[k].st,
+                                           h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
+                                           h->slots_h[k].packed);
+      CU_LAUNCH();
+    }
+  }
+  h->last_ms[0] = h->last_ms[1] = h->last_ms[2] = h->last_ms[3] = 0;
+  Status st = run_tree(h);
+  if (!st.ok()) return st;
+  for (int k = 0; k < K; ++k)
+    CU(cudaMemcpyAsync(&h->st_h[k], h->slots_h[k].st, sizeof(DSlotState), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (h->timing) {  // per-kernel-family device time of this tree
+    for (int step = 0; step < h->L - 1; ++step) {
+      cudaEvent_t* ev = &h->ev[(size_t)4 * step];
+      float a, b, d;
+      CU(cudaEventElapsedTime(&a, ev[0], ev[1]));
+      CU(cudaEventElapsedTime(&b, ev[1], ev[2]));
+      CU(cudaEventElapsedTime(&d, ev[2], ev[3]));
+      h->last_ms[0] += a;
+      h->last_ms[1] += b;
+      h->last_ms[2] += d;
+    }
+  }
+  h->last_hist_rows = 0;
+  for (int k = 0; k < K; ++k) {
+    const DSlotState& ss = h->st_h[k];
+    h->last_hist_rows += ss.hist_rows;
+    if (ss.status == kStatusTimeout) return Status(LGBM_B200_ERR_TIMEOUT, "device-side wait timed out (partition)");
+    if (ss.status == kStatusEmptyChild)
+      return Status(LGBM_B200_ERR_INVALID_PARAMETER, "Check failed: (best_split_info.left_count) > (0)");
+    if (!(st = read_tree(h, k)).ok()) return st;
+  }
+  return Status();
+}
+
+}  // namespace lgbm_b200
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+extern "C" {
+
+const char* lgbm_b200_last_error(void) { return g_last_error.c_str(); }
+const char* lgbm_b200_version(void) { return "lgbm_b200 0.1 (sm_100a)"; }
+
+int lgbm_b200_dataset_create(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams* params,
+                             LgbmB200Dataset** out) {
+  if (!X || !params || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  auto d = std::make_unique<Dataset>();
+  Status s = build_dataset(X, n, ncol, *params, *d);
+  if (!s.ok()) return fail(s);
+  *out = reinterpret_cast<LgbmB200Dataset*>(d.release());
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_dataset_create_valid(const float* X, int64_t n, int32_t ncol, const LgbmB200Dataset* ref,
+                                   LgbmB200Dataset** out) {
+  if (!X || !ref || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  auto d = std::make_unique<Dataset>();
+  Status s = build_valid_dataset(X, n, ncol, *reinterpret_cast<const Dataset*>(ref), *d);
+  if (!s.ok()) return fail(s);
+  *out = reinterpret_cast<LgbmB200Dataset*>(d.release());
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out) {
+  if (!ds || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  reinterpret_cast<Dataset*>(ds)->fill_view(out);
+  return LGBM_B200_OK;
+}
+
+void lgbm_b200_dataset_free(LgbmB200Dataset* ds) { delete reinterpret_cast<Dataset*>(ds); }
+
+int lgbm_b200_learner_create(const LgbmB200LearnerConfig* cfg, const uint8_t* bins, int64_t num_data,
+                             int32_t num_features, const LgbmB200FeatureMeta* metas, const double* upper_bounds,
+                             const int64_t* ub_offsets, const int32_t* bin_to_cat, const int64_t* cat_offsets,
+                             LgbmB200Learner** out) {
+  if (!cfg || !bins || !metas || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  auto h = std::make_unique<LgbmB200Learner>();
+  Status s = setup_learner(h.get(), cfg, bins, num_data, num_features, metas);
+  if (!s.ok()) return fail(s);
+  h->upper_bounds.resize(num_features);
+  h->bin_to_cat.resize(num_features);
+  for (int32_t f = 0; f < num_features; ++f) {
+    if (upper_bounds && ub_offsets)
+      h->upper_bounds[f].assign(upper_bounds + ub_offsets[f], upper_bounds + ub_offsets[f + 1]);
+    if (bin_to_cat && cat_offsets) h->bin_to_cat[f].assign(bin_to_cat + cat_offsets[f], bin_to_cat + cat_offsets[f + 1]);
+  }
+  *out = h.release();
+  return LGBM_B200_OK;
+}
+
+void lgbm_b200_learner_destroy(LgbmB200Learner* h) {
+  if (h) {
+    cudaSetDevice(h->device);
+    delete h;
+  }
+}
+
+int lgbm_b200_learner_set_bagging(LgbmB200Learner* h, const uint32_t* used, int64_t num_used, int32_t location) {
+  if (!h) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null handle"));
+  if (cudaSetDevice(h->device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  if (!used) {
+    h->bagging = false;
+    h->n_used = (int32_t)h->n;
+    h->ctx.bagging = 0;
+    return LGBM_B200_OK;
+  }
+  if (num_used < 0 || num_used > h->n) return fail(Status(LGBM_B200_ERR_INVALID_DATA, "bag size"));
+  cudaError_t e = cudaMemcpyAsync(h->bag, used, sizeof(uint32_t) * (size_t)num_used,
+                                  location == LGBM_B200_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  h->stream);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  h->bagging = true;
+  h->n_used = (int32_t)num_used;
+  h->ctx.bagging = num_used < h->n ? 1 : 0;
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_set_feature_mask(LgbmB200Learner* h, int32_t slot, const uint8_t* is_used) {
+  if (!h || slot < 0 || slot >= h->K) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "slot"));
+  cudaSetDevice(h->device);
+  std::vector<uint8_t> m((size_t)h->nf, 1);
+  if (is_used)
+    for (int32_t f = 0; f < h->nf; ++f) m[f] = is_used[f] ? 1 : 0;
+  cudaError_t e = cudaMemcpyAsync(h->slots_h[slot].bytree, m.data(), (size_t)h->nf, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location,
+                            LgbmB200TreeView* out) {
+  if (!h || !grad || !hess) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  Status s = lgbm_b200::train(h, grad, hess, location);
+  if (!s.ok()) return fail(s);
+  if (out)
+    for (int k = 0; k < h->K; ++k) h->trees[k].view(&out[k]);
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const double* leaf_values,
+                                       int32_t num_leaves, double* score, int32_t location) {
+  if (!h || !leaf_values || !score || slot < 0 || slot >= h->K)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  cudaSetDevice(h->device);
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  const int L = h->L;
+  std::vector<double> lv((size_t)L, 0.0);
+  for (int l = 0; l < std::min(num_leaves, L); ++l) lv[l] = leaf_values[l];
+  double* lvd = h->leaf_values_dev + (size_t)slot * L;
+  cudaError_t e = cudaMemcpyAsync(lvd, lv.data(), sizeof(double) * L, cudaMemcpyHostToDevice, s);
+  double* sc = score;
+  double* tmp = nullptr;
+  if (e == cudaSuccess && location == LGBM_B200_HOST) {
+    e = cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(double) * n, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, score, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    sc = tmp;
+  }
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  // launch only over this slot: grid.z = 1 with a context whose slots start at `slot`
+  DCtx c = h->ctx;
+  c.slots = h->ctx.slots + slot;
+  k_add_leaf_outputs<<<dim3(std::max(1, h->num_sms * 4 / L + 1), L, 1), 256, 0, s>>>(c, lvd, 0, sc, 0);
+  e = cudaGetLastError();
+  if (e == cudaSuccess && tmp) {
+    e = cudaMemcpyAsync(score, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(tmp, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* leaf_begin, int32_t* leaf_count,
+                                    uint32_t* indices) {
+  if (!h || slot < 0 || slot >= h->K) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "slot"));
+  cudaSetDevice(h->device);
+  const DSlot& d = h->slots_h[slot];
+  const int nl = std::max(1, h->st_h[slot].num_leaves_cur);
+  std::vector<int32_t> side((size_t)nl), beg((size_t)nl), cnt((size_t)nl);
+  cudaStream_t s = h->stream;
+  cudaMemcpyAsync(beg.data(), d.leaf_begin, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(cnt.data(), d.leaf_count, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(side.data(), d.leaf_side, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "readback"));
+  for (int l = 0; l < nl; ++l) {
+    if (leaf_begin) leaf_begin[l] = beg[l];
+    if (leaf_count) leaf_count[l] = cnt[l];
+    if (indices && cnt[l] > 0)
+      cudaMemcpyAsync(indices + beg[l], d.idx[side[l]] + beg[l], sizeof(uint32_t) * cnt[l], cudaMemcpyDeviceToHost, s);
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "readback"));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_rows, int32_t* launches) {
+  if (!h) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null handle"));
+  if (ms)
+    for (int i = 0; i < 4; ++i) ms[i] = h->last_ms[i];
+  if (hist_rows) *hist_rows = h->last_hist_rows;
+  if (launches) *launches = h->last_launches;
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_set_timing(LgbmB200Learner* h, int32_t enabled) {
+  if (!h) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null handle"));
+  h->timing = enabled != 0;
+  return LGBM_B200_OK;
+}
+
+}  // extern "C"

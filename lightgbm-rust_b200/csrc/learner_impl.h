@@ -1,0 +1,248 @@
+// Host-side internals of the learner handle shared by the CUDA translation
+// units (learner.cu, booster.cu).
+#pragma once
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "lgbm_b200_internal.h"
+#include "predict.h"
+
+namespace lgbm_b200 {
+
+
+#define CU(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return Status(LGBM_B200_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+#define CU_LAUNCH()                                                                              \
+  do {                                                                                           \
+    cudaError_t e_ = cudaGetLastError();                                                         \
+    if (e_ != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+inline int fail(const Status& s) {
+  set_last_error(s.msg);
+  return s.code;
+}
+
+// ------------------------------------------------------------------------------------------
+// host RNGs used by the learner (learner/quant.rs random tables; col_sampler.rs)
+// ------------------------------------------------------------------------------------------
+struct Mt19937 {  // crates/lgbm-core/src/mt19937.rs (libstdc++ mt19937)
+  uint32_t state[624];
+  int idx;
+  explicit Mt19937(uint32_t seed) {
+    state[0] = seed;
+    for (int i = 1; i < 624; ++i) state[i] = 1812433253u * (state[i - 1] ^ (state[i - 1] >> 30)) + (uint32_t)i;
+    idx = 624;
+  }
+  uint32_t next_u32() {
+    if (idx >= 624) {
+      for (int k = 0; k < 624; ++k) {
+        uint32_t y = (state[k] & 0x80000000u) | (state[(k + 1) % 624] & 0x7fffffffu);
+        state[k] = state[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+      }
+      idx = 0;
+    }
+    uint32_t z = state[idx++];
+    z ^= z >> 11;
+    z ^= (z << 7) & 0x9d2c5680u;
+    z ^= (z << 15) & 0xefc60000u;
+    z ^= z >> 18;
+    return z;
+  }
+  double uniform01() {
+    const double R = 4294967296.0;
+    double sum = (double)next_u32();
+    sum += (double)next_u32() * R;
+    double ret = sum / (R * R);
+    if (ret >= 1.0) {
+      uint64_t bits = 0x3FEFFFFFFFFFFFFFull;
+      std::memcpy(&ret, &bits, 8);
+    }
+    return ret * (1.0 - 0.0) + 0.0;
+  }
+  int32_t uniform_int(int32_t a, int32_t b) {
+    uint32_t range = (uint32_t)((int64_t)b - (int64_t)a + 1);
+    uint64_t product = (uint64_t)next_u32() * (uint64_t)range;
+    uint32_t low = (uint32_t)product;
+    if (low < range) {
+      uint32_t threshold = (uint32_t)(-range) % range;
+      while (low < threshold) {
+        product = (uint64_t)next_u32() * (uint64_t)range;
+        low = (uint32_t)product;
+      }
+    }
+    return (int32_t)((int64_t)(product >> 32) + (int64_t)a);
+  }
+};
+
+struct Lcg {  // crates/lgbm-core/src/random.rs
+  uint32_t x;
+  explicit Lcg(int32_t seed) : x((uint32_t)seed) {}
+  int32_t rand_int16() { x = x * 214013u + 2531011u; return (int32_t)((x >> 16) & 0x7FFF); }
+  int32_t rand_int32() { x = x * 214013u + 2531011u; return (int32_t)(x & 0x7FFFFFFF); }
+  int32_t next_int(int32_t lo, int32_t hi) { return rand_int32() % (hi - lo) + lo; }
+  float next_float() { return (float)rand_int16() / 32768.0f; }
+  std::vector<int32_t> sample(int32_t n, int32_t k) {
+    std::vector<int32_t> ret;
+    if (k > n || k <= 0) return ret;
+    if (k == n) {
+      for (int32_t i = 0; i < n; ++i) ret.push_back(i);
+    } else if (k > 1 && (double)k > ((double)n / std::log2((double)k))) {
+      for (int32_t i = 0; i < n; ++i) {
+        double prob = (double)((size_t)k - ret.size()) / (double)(n - i);
+        if ((double)next_float() < prob) ret.push_back(i);
+      }
+    } else {
+      std::vector<char> seen((size_t)n, 0);
+      for (int32_t r = n - k; r < n; ++r) {
+        int32_t v = next_int(0, r + 1);
+        if (seen[(size_t)v]) seen[(size_t)r] = 1;
+        else seen[(size_t)v] = 1;
+      }
+      for (int32_t i = 0; i < n; ++i)
+        if (seen[(size_t)i]) ret.push_back(i);
+    }
+    return ret;
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// device memory
+// ------------------------------------------------------------------------------------------
+struct DeviceArena {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  Status alloc(void** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(p, n);
+    if (e != cudaSuccess)
+      return Status(LGBM_B200_ERR_CUDA, "cudaMalloc(" + std::to_string(n) + "): " + cudaGetErrorString(e));
+    ptrs.push_back(*p);
+    bytes += n;
+    return Status();
+  }
+  template <class T>
+  Status alloc_n(T** p, size_t n) {
+    return alloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  }
+  void free_all() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+struct HostTree {  // the reference's Tree arrays for one trained tree
+  int32_t num_leaves = 1;
+  std::vector<int32_t> split_feature_inner, split_feature, left_child, right_child, leaf_parent, leaf_count,
+      leaf_depth, internal_count, cat_boundaries, cat_boundaries_inner;
+  std::vector<float> split_gain;
+  std::vector<uint32_t> threshold_in_bin, cat_threshold, cat_threshold_inner, cat_bits;
+  std::vector<double> threshold, leaf_value, leaf_weight, internal_value, internal_weight, node_gain;
+  std::vector<int8_t> decision_type;
+  int32_t num_cat = 0;
+  void view(LgbmB200TreeView* v) const {
+    v->num_leaves = num_leaves;
+    v->split_feature_inner = split_feature_inner.data();
+    v->split_feature = split_feature.data();
+    v->split_gain = split_gain.data();
+    v->threshold_in_bin = threshold_in_bin.data();
+    v->threshold = threshold.data();
+    v->decision_type = decision_type.data();
+    v->left_child = left_child.data();
+    v->right_child = right_child.data();
+    v->leaf_parent = leaf_parent.data();
+    v->leaf_value = leaf_value.data();
+    v->leaf_weight = leaf_weight.data();
+    v->leaf_count = leaf_count.data();
+    v->leaf_depth = leaf_depth.data();
+    v->internal_value = internal_value.data();
+    v->internal_weight = internal_weight.data();
+    v->internal_count = internal_count.data();
+    v->num_cat = num_cat;
+    v->cat_boundaries = cat_boundaries.data();
+    v->cat_threshold = cat_threshold.data();
+    v->cat_boundaries_inner = cat_boundaries_inner.data();
+    v->cat_threshold_inner = cat_threshold_inner.data();
+  }
+};
+
+}  // namespace lgbm_b200
+
+using namespace lgbm_b200;
+
+struct LgbmB200Learner {
+  LgbmB200LearnerConfig cfg{};
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  DeviceArena arena;
+  int64_t n = 0;
+  int32_t nf = 0, stride = 0, total_bins = 0, K = 1, L = 2;
+  std::vector<DFeature> feats;
+  std::vector<std::vector<double>> upper_bounds;
+  std::vector<std::vector<int32_t>> bin_to_cat;
+  DCtx ctx{};
+  DTileTable tiles{};
+  int ntiles = 1;
+  size_t hist_smem = 0, scan_smem = 0;
+  int hist_grid = 148, part_grid = 592, root_grid = kRootBlocks;
+  int32_t sub_rows = 8192;
+  std::vector<DSlot> slots_h;
+  float2* gh_all = nullptr;  // [K x n] interleaved gradients of every slot
+  // quantization
+  double* grv = nullptr;
+  double* hrv = nullptr;
+  std::unique_ptr<Mt19937> start_eng;
+  unsigned long long* maxbits = nullptr;
+  int32_t* quant_counter = nullptr;
+  // bagging
+  uint32_t* bag = nullptr;
+  int32_t n_used = 0;
+  bool bagging = false;
+  // leaf renewal scratch [K][L][2]
+  double* leaf_sums = nullptr;
+  double* leaf_values_dev = nullptr;  // [K][L] for add_leaf_outputs
+  double* score_scratch = nullptr;
+  // readback
+  std::vector<DSlotState> st_h;
+  std::vector<HostTree> trees;
+  std::vector<int32_t> tmp_i32;
+  // timing
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;
+  double last_ms[4] = {0, 0, 0, 0};
+  int64_t last_hist_rows = 0;
+  int32_t last_launches = 0;
+  // captured tree growth
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_key = -1;
+  ~LgbmB200Learner() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto e : ev) cudaEventDestroy(e);
+    arena.free_all();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+
+namespace lgbm_b200 {
+// One tree per slot from the given gradients (class-major [K x n]); NULL
+// gradients reuse the slots' interleaved buffers filled by the caller.
+Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
+}  // namespace lgbm_b200
+
+namespace lgbm_b200 {
+inline double maybe_round_to_zero_h(double v) {  // tree.rs:22-29
+  return (v >= -(double)1e-35f && v <= (double)1e-35f) ? 0.0 : v;
+}
+}  // namespace lgbm_b200

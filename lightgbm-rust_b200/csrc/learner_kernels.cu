@@ -1,0 +1,1387 @@
+// The tree learner's sm_100a kernels. One tree (or one tree per class slot,
+// grown in lockstep) is grown entirely on the device: every kernel reads
+// the current leaf, counts and split from the slot's control block, so the
+// per-split launches need no host round trip and can be captured in a CUDA
+// graph.
+//
+// Per split step (learner/mod.rs:653-666):
+//   k_hist       histogram of the smaller leaf      (multi_val_bin.rs:556-703)
+//   k_scan       fix / subtract / threshold scan per feature, then in the
+//                last CTA: best split per leaf, best leaf, Tree::split
+//                bookkeeping and the partition LUT  (learner/mod.rs:816-1225,
+//                split.rs, histogram.rs:42-85, tree.rs:254-297)
+//   k_partition  stable-by-leaf row split with decoupled look-back, then the
+//                smaller/larger choice and before_find_best_split
+//                (partition.rs:107-174, learner/mod.rs:1200-1208, :712-731)
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace lgbm_b200 {
+
+// =====================================================================================
+// tree init: DataPartition::init, root sums and the root LeafSplits
+// (learner/mod.rs:572-648, partition.rs:202-218)
+// =====================================================================================
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ bool before_find_best_split(const DCtx& c, DSlot& s, int32_t left, int32_t right) {
+  const DParams& p = c.p;
+  if (p.max_depth > 0 && s.tree.leaf_depth[left] >= p.max_depth) {
+    s.best[left].gain = -INFINITY;
+    if (right >= 0) s.best[right].gain = -INFINITY;
+    return false;
+  }
+  int32_t nl = left >= 0 ? s.leaf_count[left] : 0;
+  int32_t nr = right >= 0 ? s.leaf_count[right] : 0;
+  int32_t min2 = p.min_data_in_leaf * 2;
+  if (nr < min2 && nl < min2) {
+    s.best[left].gain = -INFINITY;
+    if (right >= 0) s.best[right].gain = -INFINITY;
+    return false;
+  }
+  return true;
+}
+
+// Grid (kRootBlocks, 1, slots), 256 threads.
+__global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, int32_t n_used) {
+  DSlot& s = c.slots[blockIdx.z];
+  const int64_t n = n_used;
+  const int tid = threadIdx.x;
+  // positions -> rows (identity, or the in-bag rows)
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + tid; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s.idx[0][i] = bag ? bag[i] : (uint32_t)i;
+  // zero histogram buffer 0 (the root's)
+  size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+  double* h0 = reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h0[i] = 0.0;
+
+  // deterministic partial sums over this block's contiguous chunk
+  int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  double sg = 0.0, sh = 0.0;
+  long long si = 0;
+  if (c.hist_mode == LGBM_B200_HIST_QUANT) {
+    for (int64_t i = b0 + tid; i < b1; i += blockDim.x) {
+      // quant.rs:452-477: the bag variant sums packed values by position
+      int64_t r = (c.bagging) ? i : (int64_t)(bag ? bag[i] : (uint32_t)i);
+      int32_t v = s.packed[r];
+      int64_t gq = (int64_t)(v >> 16), hq = (int64_t)(v & 0xFFFF);
+      si += (long long)((uint64_t)(gq << 32) + (uint64_t)hq);
+      int32_t w = s.packed[bag ? bag[i] : (uint32_t)i];
+      if (c.bagging) {  // f32 scales (quant.rs:467-477)
+        sg += (double)((float)(w >> 16) * (float)s.st->grad_scale);
+        sh += (double)((float)(w & 0xFFFF) * (float)s.st->hess_scale);
+      } else {
+        sg += (double)(w >> 16) * s.st->grad_scale;
+        sh += (double)(w & 0xFFFF) * s.st->hess_scale;
+      }
+    }
+  } else {
+    for (int64_t i = b0 + tid; i < b1; i += blockDim.x) {
+      float2 v = s.gh[bag ? bag[i] : (uint32_t)i];
+      sg += (double)v.x;
+      sh += (double)v.y;
+    }
+  }
+  __shared__ double red_g[8], red_h[8];
+  __shared__ long long red_i[8];
+  sg = warp_sum_d(sg);
+  sh = warp_sum_d(sh);
+  si = warp_sum_ll(si);
+  if ((tid & 31) == 0) {
+    red_g[tid >> 5] = sg;
+    red_h[tid >> 5] = sh;
+    red_i[tid >> 5] = si;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (tid == 0) {
+    double a = 0, b = 0;
+    long long d = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += red_g[w];
+      b += red_h[w];
+      d += red_i[w];
+    }
+    s.root_partials[blockIdx.x] = a;
+    s.root_partials[kRootBlocks + blockIdx.x] = b;
+    s.root_ipartials[blockIdx.x] = d;
+    __threadfence();
+    last = atomicAdd(s.root_counter, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const DParams& p = c.p;
+  DSlotState* st = s.st;
+  // per-leaf state
+  for (int l = tid; l < p.num_leaves; l += blockDim.x) {
+    s.best[l].feature = -1;
+    s.best[l].inner = -1;
+    s.best[l].gain = -INFINITY;
+    s.cmin[l] = -1.7976931348623157e308;
+    s.cmax[l] = 1.7976931348623157e308;
+    s.buf_of[l] = l;
+    s.leaf_begin[l] = 0;
+    s.leaf_count[l] = 0;
+    s.leaf_side[l] = 0;
+  }
+  for (int f = tid; f < c.num_features; f += blockDim.x) s.splittable[f] = 1;
+  __syncthreads();
+  if (tid != 0) return;
+  *s.root_counter = 0;
+  double a = 0, b = 0;
+  long long d = 0;
+  for (int k = 0; k < (int)gridDim.x; ++k) {
+    a += s.root_partials[k];
+    b += s.root_partials[kRootBlocks + k];
+    d += s.root_ipartials[k];
+  }
+  s.leaf_count[0] = (int32_t)n;
+  st->num_used = (int32_t)n;
+  st->num_leaves_cur = 1;
+  st->done = 0;
+  st->status = kStatusOk;
+  st->num_cat = 0;
+  st->scan_counter = 0;
+  st->part_ticket = 0;
+  st->hist_rows = 0;
+  st->smaller.leaf = 0;
+  st->smaller.num_data = (int32_t)n;
+  st->smaller.sum_gradients = a;
+  st->smaller.sum_hessians = b;
+  st->smaller.int_sum = (int64_t)d;
+  st->larger.leaf = -1;
+  st->larger.num_data = 0;
+  st->left_leaf = 0;
+  st->right_leaf = -1;
+  DTree& t = s.tree;
+  t.leaf_parent[0] = -1;
+  t.leaf_value[0] = maybe_round_to_zero(root_output(a, b, p, (int32_t)n));
+  t.leaf_weight[0] = 0.0;
+  t.leaf_count[0] = 0;
+  t.leaf_depth[0] = 0;
+  st->need_find = before_find_best_split(c, s, 0, -1) ? 1 : 0;
+}
+
+// =====================================================================================
+// histogram of the smaller leaf (multi_val_bin.rs:556-703, :710-791)
+// =====================================================================================
+struct LeafRows {
+  const uint32_t* idx;  // position -> row
+  int64_t begin, count;
+};
+
+__device__ __forceinline__ bool hist_setup(const DCtx& c, DSlot& s, LeafRows& lr, int64_t& r0, int64_t& r1) {
+  DSlotState* st = s.st;
+  if (st->done || !st->need_find) return false;
+  int32_t leaf = st->smaller.leaf;
+  lr.count = s.leaf_count[leaf];
+  lr.begin = s.leaf_begin[leaf];
+  lr.idx = s.idx[s.leaf_side[leaf]];
+  int64_t per = c.rows_per_block;
+  int64_t active = min((int64_t)gridDim.x, (lr.count + per - 1) / per);
+  if ((int64_t)blockIdx.x >= active) return false;
+  int64_t chunk = (lr.count + active - 1) / active;
+  r0 = (int64_t)blockIdx.x * chunk;
+  r1 = min(lr.count, r0 + chunk);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) st->hist_rows += lr.count;
+  return r0 < r1;
+}
+
+// Feature tile of a histogram launch: features [f0, f1), stored bins [bin0, bin0 + nbins).
+__device__ __forceinline__ void tile_of(const DTileTable& tt, int tile, int& f0, int& f1, int& bin0, int& nbins) {
+  f0 = tt.f0[tile];
+  f1 = tt.f0[tile + 1];
+  bin0 = tt.bin0[tile];
+  nbins = tt.bin0[tile + 1] - bin0;
+}
+
+// FP64 (kMode 0) and FP32-compensated (kMode 1) histograms: each thread takes
+// (row, 4-feature word) units; shared-memory atomics, then one global merge.
+template <int kMode>
+__global__ void __launch_bounds__(kHistThreads) k_hist_float(DCtx c, DTileTable tt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DSlot& s = c.slots[blockIdx.z];
+  LeafRows lr;
+  int64_t r0, r1;
+  if (!hist_setup(c, s, lr, r0, r1)) return;
+  int f0, f1, bin0, nbins;
+  tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
+  __shared__ int32_t vstart[kMaxTileFeatures];
+  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+  // kMode 0: double2 (g, h) per bin; kMode 1: float4 (g_hi, g_lo, h_hi, h_lo)
+  if (kMode == 0) {
+    double2* sh = reinterpret_cast<double2*>(smem_raw);
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = make_double2(0.0, 0.0);
+  } else {
+    float4* sh = reinterpret_cast<float4*>(smem_raw);
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const int nfeat = f1 - f0;
+  const int wpr = (nfeat + 3) >> 2;  // 4-byte words per row in this tile
+  const int64_t units = (r1 - r0) * wpr;
+  const uint32_t* idx = lr.idx + lr.begin;
+  const float2* gh = s.gh;  // interleaved (g, h)
+  for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
+    int64_t pos = r0 + u / wpr;
+    int w = (int)(u % wpr);
+    uint32_t row = idx[pos];
+    float2 v = gh[row];
+    uint32_t word = *reinterpret_cast<const uint32_t*>(c.bins + (size_t)row * c.stride + f0 + 4 * w);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int fl = 4 * w + k;
+      uint32_t raw = (word >> (8 * k)) & 0xFFu;
+      if (fl < nfeat && raw != 0u) {
+        int b = vstart[fl] + (int)raw;
+        if (kMode == 0) {
+          double2* sh = reinterpret_cast<double2*>(smem_raw);
+          atomicAdd(&sh[b].x, (double)v.x);
+          atomicAdd(&sh[b].y, (double)v.y);
+        } else {
+          float4* sh = reinterpret_cast<float4*>(smem_raw);
+          // TwoSum of the value the atomic replaced and the addend: the
+          // rounding error goes to the low word.
+          float og = atomicAdd(&sh[b].x, v.x);
+          float sg = __fadd_rn(og, v.x);
+          float bg = __fsub_rn(sg, og);
+          float eg = __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(v.x, bg));
+          atomicAdd(&sh[b].y, eg);
+          float oh = atomicAdd(&sh[b].z, v.y);
+          float sh2 = __fadd_rn(oh, v.y);
+          float bh = __fsub_rn(sh2, oh);
+          float eh = __fadd_rn(__fsub_rn(oh, __fsub_rn(sh2, bh)), __fsub_rn(v.y, bh));
+          atomicAdd(&sh[b].w, eh);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double* out = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+    double g, h;
+    if (kMode == 0) {
+      double2 v = reinterpret_cast<double2*>(smem_raw)[i];
+      g = v.x;
+      h = v.y;
+    } else {
+      float4 v = reinterpret_cast<float4*>(smem_raw)[i];
+      g = (double)v.x + (double)v.y;
+      h = (double)v.z + (double)v.w;
+    }
+    if (g != 0.0 || h != 0.0) {
+      atomicAdd(out + 2 * (size_t)(bin0 + i), g);
+      atomicAdd(out + 2 * (size_t)(bin0 + i) + 1, h);
+    }
+  }
+}
+template __global__ void k_hist_float<0>(DCtx, DTileTable);
+template __global__ void k_hist_float<1>(DCtx, DTileTable);
+
+// Quantized histogram: per-row packed (g << 16) + h added into int32 shared
+// cells (int16 gradient / hessian halves), flushed every `sub_rows` rows
+// into the global packed int64 histogram (int32 halves), so no half overflows.
+__global__ void __launch_bounds__(kHistThreads) k_hist_int(DCtx c, DTileTable tt, int32_t sub_rows) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int32_t* sh = reinterpret_cast<int32_t*>(smem_raw);
+  DSlot& s = c.slots[blockIdx.z];
+  LeafRows lr;
+  int64_t r0, r1;
+  if (!hist_setup(c, s, lr, r0, r1)) return;
+  int f0, f1, bin0, nbins;
+  tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
+  __shared__ int32_t vstart[kMaxTileFeatures];
+  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int nfeat = f1 - f0;
+  const int wpr = (nfeat + 3) >> 2;
+  const uint32_t* idx = lr.idx + lr.begin;
+  unsigned long long* out = reinterpret_cast<unsigned long long*>(s.hist) +
+                            (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
+  for (int64_t q0 = r0; q0 < r1; q0 += sub_rows) {
+    int64_t q1 = min(r1, q0 + sub_rows);
+    int64_t units = (q1 - q0) * wpr;
+    for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
+      int64_t pos = q0 + u / wpr;
+      int w = (int)(u % wpr);
+      uint32_t row = idx[pos];
+      int32_t v = s.packed[row];
+      uint32_t word = *reinterpret_cast<const uint32_t*>(c.bins + (size_t)row * c.stride + f0 + 4 * w);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        int fl = 4 * w + k;
+        uint32_t raw = (word >> (8 * k)) & 0xFFu;
+        if (fl < nfeat && raw != 0u) atomicAdd(&sh[vstart[fl] + (int)raw], v);
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+      int32_t cell = sh[i];
+      if (cell != 0) {
+        int64_t hq = (int64_t)(cell & 0xFFFF);
+        int64_t gq = (int64_t)((cell - (int32_t)hq) >> 16);
+        atomicAdd(out + bin0 + i, (unsigned long long)((uint64_t)(gq << 32) + (uint64_t)hq));
+        sh[i] = 0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// =====================================================================================
+// split scan (split.rs:246-891 and :930-1400) — one CTA of two warps per
+// (feature, slot): warp 0 the smaller leaf, warp 1 the larger leaf.
+// =====================================================================================
+
+
+struct LeafCtx {
+  double sum_g, sum_h;  // sum_h includes 2*kEpsilon (FP forms)
+  int64_t int_sum;
+  double gs, hs;
+  int32_t num_data;
+  double parent_output;
+  bool mc;
+  double cmin, cmax;
+};
+
+// Warp-wide argmax with the scan's tie rule: larger gain, then smaller position.
+__device__ __forceinline__ void warp_best(double& gain, int32_t& pos) {
+  for (int o = 16; o > 0; o >>= 1) {
+    double og = __shfl_xor_sync(0xffffffffu, gain, o);
+    int32_t op = __shfl_xor_sync(0xffffffffu, pos, o);
+    if (og > gain || (og == gain && op < pos)) {
+      gain = og;
+      pos = op;
+    }
+  }
+}
+__device__ __forceinline__ int32_t warp_min_i(int32_t v) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One direction of FindBestThresholdSequentially (split.rs:676-891), FP64
+// form. Lane 0 forms the cumulative sums in the reference's order; all lanes
+// then evaluate the candidates; the break / skip / strict-greater rules
+// pick the same threshold as the sequential loop.
+template <bool kInt>
+__device__ bool scan_dir(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc, double min_gain_shift,
+                         bool reverse, bool skip_default, bool na_as_missing, DSplit& out) {
+  const int lane = threadIdx.x & 31;
+  const int offset = m.offset;
+  const double cnt_factor =
+      kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
+  int32_t npos = 0;
+  if (lane == 0) {
+    if (reverse) {
+      double ag = 0.0, ah = kEpsilon;
+      int32_t acnt = 0;
+      int64_t ai = 0;
+      for (int32_t t = m.num_bin - 1 - offset - (int32_t)na_as_missing; t >= 1 - offset; --t) {
+        if (skip_default && t + offset == m.default_bin) continue;
+        if (kInt) {
+          ai = (int64_t)((uint64_t)ai + (uint64_t)sm.ig[t]);
+          sm.cc[npos] = round_int((double)int_hess(ai) * cnt_factor);
+          reinterpret_cast<int64_t*>(sm.ch)[npos] = ai;
+        } else {
+          double hs = sm.h[t];
+          ag += sm.g[t];
+          ah += hs;
+          acnt += round_int(hs * cnt_factor);
+          sm.cg[npos] = ag;
+          sm.ch[npos] = ah;
+          sm.cc[npos] = acnt;
+        }
+        sm.tpos[npos] = t;
+        ++npos;
+      }
+    } else {
+      double ag = 0.0, ah = kEpsilon;
+      int32_t acnt = 0;
+      int64_t ai = 0;
+      int32_t t = 0;
+      if (na_as_missing && offset == 1) {
+        if (kInt) {
+          ai = lc.int_sum;
+          for (int32_t i = 0; i < m.num_bin - offset; ++i) ai = (int64_t)((uint64_t)ai - (uint64_t)sm.ig[i]);
+        } else {
+          ag = lc.sum_g;
+          ah = lc.sum_h - kEpsilon;
+          acnt = lc.num_data;
+          for (int32_t i = 0; i < m.num_bin - offset; ++i) {
+            double hs = sm.h[i];
+            ag -= sm.g[i];
+            ah -= hs;
+            acnt -= round_int(hs * cnt_factor);
+          }
+        }
+        t = -1;
+      }
+      for (; t <= m.num_bin - 2 - offset; ++t) {
+        if (skip_default && t + offset == m.default_bin) continue;
+        if (kInt) {
+          if (t >= 0) ai = (int64_t)((uint64_t)ai + (uint64_t)sm.ig[t]);
+          sm.cc[npos] = round_int((double)int_hess(ai) * cnt_factor);
+          reinterpret_cast<int64_t*>(sm.ch)[npos] = ai;
+        } else {
+          if (t >= 0) {
+            ag += sm.g[t];
+            ah += sm.h[t];
+            acnt += round_int(sm.h[t] * cnt_factor);
+          }
+          sm.cg[npos] = ag;
+          sm.ch[npos] = ah;
+          sm.cc[npos] = acnt;
+        }
+        sm.tpos[npos] = t;
+        ++npos;
+      }
+    }
+  }
+  npos = __shfl_sync(0xffffffffu, npos, 0);
+  __syncwarp();
+  const int32_t min_data = p.min_data_in_leaf;
+  const double min_hess = p.min_sum_hessian_in_leaf;
+  // pass 1: first break position
+  int32_t brk = INT32_MAX;
+  for (int32_t k = lane; k < npos; k += 32) {
+    int32_t cnt_acc = sm.cc[k];
+    double hacc, hrest;
+    if (kInt) {
+      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[k];
+      hacc = (double)int_hess(acc) * lc.hs;
+      hrest = (double)int_hess((int64_t)((uint64_t)lc.int_sum - (uint64_t)acc)) * lc.hs;
+    } else {
+      hacc = sm.ch[k];
+      hrest = lc.sum_h - hacc;
+    }
+    bool skip1 = cnt_acc < min_data || hacc < min_hess;
+    if (!skip1 && (lc.num_data - cnt_acc < min_data || hrest < min_hess)) brk = min(brk, k);
+  }
+  brk = warp_min_i(brk);
+  // pass 2: gains of the candidates before the break
+  double best_gain = -INFINITY;
+  int32_t best_k = INT32_MAX;
+  bool splittable = false;
+  for (int32_t k = lane; k < min(npos, brk); k += 32) {
+    int32_t cnt_acc = sm.cc[k];
+    double ga, ha, gr, hr;  // accumulated side, rest side
+    if (kInt) {
+      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[k];
+      int64_t rest = (int64_t)((uint64_t)lc.int_sum - (uint64_t)acc);
+      ha = (double)int_hess(acc) * lc.hs;
+      hr = (double)int_hess(rest) * lc.hs;
+      if (cnt_acc < min_data || ha < min_hess) continue;
+      ga = (double)int_grad(acc) * lc.gs;
+      gr = (double)int_grad(rest) * lc.gs;
+      ha += kEpsilon;
+      hr += kEpsilon;
+    } else {
+      ha = sm.ch[k];
+      if (cnt_acc < min_data || ha < min_hess) continue;
+      ga = sm.cg[k];
+      hr = lc.sum_h - ha;
+      gr = lc.sum_g - ga;
+    }
+    int32_t rest_cnt = lc.num_data - cnt_acc;
+    double gain = reverse ? split_gain(gr, hr, ga, ha, p, rest_cnt, cnt_acc, lc.parent_output, lc.mc, lc.cmin,
+                                       lc.cmax, m.monotone_type)
+                          : split_gain(ga, ha, gr, hr, p, cnt_acc, rest_cnt, lc.parent_output, lc.mc, lc.cmin,
+                                       lc.cmax, m.monotone_type);
+    if (gain <= min_gain_shift) continue;
+    splittable = true;
+    if (gain > best_gain) {  // NaN never becomes best
+      best_gain = gain;
+      best_k = k;
+    }
+  }
+  splittable = __any_sync(0xffffffffu, splittable);
+  warp_best(best_gain, best_k);
+  // a basic constraint with min > max never accepts a best threshold (split.rs:765-771)
+  if (lc.mc && lc.cmin > lc.cmax) best_k = INT32_MAX;
+  if (lane == 0 && splittable && best_k != INT32_MAX && best_gain > out.gain + min_gain_shift) {
+    int32_t t = sm.tpos[best_k];
+    double slg, slh;  // best left sums
+    int32_t left_count;
+    int64_t left_int = 0;
+    if (kInt) {
+      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[best_k];
+      left_int = reverse ? (int64_t)((uint64_t)lc.int_sum - (uint64_t)acc) : acc;
+      int64_t right_int = (int64_t)((uint64_t)lc.int_sum - (uint64_t)left_int);
+      double lg = (double)int_grad(left_int) * lc.gs, lh = (double)int_hess(left_int) * lc.hs;
+      double rg = (double)int_grad(right_int) * lc.gs, rh = (double)int_hess(right_int) * lc.hs;
+      int32_t lcnt = round_int((double)int_hess(left_int) * cnt_factor);
+      int32_t rcnt = round_int((double)int_hess(right_int) * cnt_factor);
+      out.threshold = (uint32_t)(reverse ? t - 1 + offset : t + offset);
+      double lo = leaf_output(lg, lh, p, lcnt, lc.parent_output);
+      double ro = leaf_output(rg, rh, p, rcnt, lc.parent_output);
+      out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
+      out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
+      out.left_count = lcnt;
+      out.right_count = rcnt;
+      out.left_sum_gradient = lg;
+      out.left_sum_hessian = lh;
+      out.right_sum_gradient = rg;
+      out.right_sum_hessian = rh;
+      out.left_sum_gh = left_int;
+      out.right_sum_gh = right_int;
+    } else {
+      if (reverse) {
+        slg = lc.sum_g - sm.cg[best_k];
+        slh = lc.sum_h - sm.ch[best_k];
+        left_count = lc.num_data - sm.cc[best_k];
+        out.threshold = (uint32_t)(t - 1 + offset);
+      } else {
+        slg = sm.cg[best_k];
+        slh = sm.ch[best_k];
+        left_count = sm.cc[best_k];
+        out.threshold = (uint32_t)(t + offset);
+      }
+      double lo = leaf_output(slg, slh, p, left_count, lc.parent_output);
+      double ro = leaf_output(lc.sum_g - slg, lc.sum_h - slh, p, lc.num_data - left_count, lc.parent_output);
+      out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
+      out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
+      out.left_count = left_count;
+      out.left_sum_gradient = slg;
+      out.left_sum_hessian = slh - kEpsilon;
+      out.right_count = lc.num_data - left_count;
+      out.right_sum_gradient = lc.sum_g - slg;
+      out.right_sum_hessian = lc.sum_h - slh - kEpsilon;
+    }
+    out.gain = best_gain - min_gain_shift;
+    out.default_left = reverse ? 1 : 0;
+  }
+  __syncwarp();
+  return splittable;
+}
+
+// split.rs:448-670 / :1194-1400 categorical threshold search, in lane 0
+// (the candidate lists are at most a few dozen bins; the stable sort is a
+// rank sort done by the whole warp).
+template <bool kInt>
+__device__ bool scan_categorical(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc, DSplit& out) {
+  const int lane = threadIdx.x & 31;
+  const int offset = m.offset;
+  const int bin_start = 1 - offset, bin_end = m.num_bin - offset;
+  const bool use_onehot = m.num_bin <= p.max_cat_to_onehot;
+  const double gs = lc.gs, hs = lc.hs;
+  double sum_gradient = kInt ? (double)int_grad(lc.int_sum) * gs : lc.sum_g;
+  double sum_hessian = kInt ? (double)int_hess(lc.int_sum) * hs : lc.sum_h;
+  const double cnt_factor = kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
+  auto G = [&](int t) { return kInt ? (double)int_grad(sm.ig[t]) * gs : sm.g[t]; };
+  auto H = [&](int t) { return kInt ? (double)int_hess(sm.ig[t]) * hs : sm.h[t]; };
+  auto CNT = [&](int t) {
+    return kInt ? round_int((double)int_hess(sm.ig[t]) * cnt_factor) : round_int(sm.h[t] * cnt_factor);
+  };
+  int32_t used_bin = 0;
+  if (!use_onehot) {
+    // bins with enough data, then a stable sort by sum_grad / (sum_hess + cat_smooth)
+    if (lane == 0) {
+      for (int i = bin_start; i < bin_end; ++i)
+        if ((double)CNT(i) >= p.cat_smooth) sm.tpos[used_bin++] = i;
+    }
+    used_bin = __shfl_sync(0xffffffffu, used_bin, 0);
+    __syncwarp();
+    for (int k = lane; k < used_bin; k += 32) {
+      int i = sm.tpos[k];
+      sm.key[k] = G(i) / (H(i) + p.cat_smooth);
+    }
+    __syncwarp();
+    for (int k = lane; k < used_bin; k += 32) {
+      double kk = sm.key[k];
+      int rank = 0;
+      for (int j = 0; j < used_bin; ++j) {
+        double kj = sm.key[j];
+        if (kj < kk || (j < k && !(kk < kj) && !(kj < kk))) ++rank;
+      }
+      sm.sorted[rank] = sm.tpos[k];
+    }
+    __syncwarp();
+  }
+  bool is_splittable = false;
+  if (lane == 0) {
+    out.default_left = 0;
+    double gain_shift = use_smoothing(p) ? leaf_gain_given_output(sum_gradient, sum_hessian, p, lc.parent_output)
+                                         : leaf_gain(sum_gradient, sum_hessian, p, lc.num_data, 0.0);
+    double min_gain_shift = gain_shift + p.min_gain_to_split;
+    DParams pc = p;
+    double best_gain = -INFINITY;
+    int32_t best_left_count = 0, best_threshold = -1, best_dir = 1;
+    double best_slg = 0.0, best_slh = 0.0;
+    int64_t best_left_int = 0;
+    if (use_onehot) {
+      for (int t = bin_start; t < bin_end; ++t) {
+        int32_t cnt = CNT(t);
+        double grad = G(t), hess = H(t);
+        if (cnt < p.min_data_in_leaf || hess < p.min_sum_hessian_in_leaf) continue;
+        int32_t other_count = lc.num_data - cnt;
+        if (other_count < p.min_data_in_leaf) continue;
+        double soh, sog;
+        if (kInt) {
+          int64_t other = (int64_t)((uint64_t)lc.int_sum - (uint64_t)sm.ig[t]);
+          soh = (double)int_hess(other) * hs;
+          if (soh < p.min_sum_hessian_in_leaf) continue;
+          sog = (double)int_grad(other) * gs;
+        } else {
+          soh = sum_hessian - hess - kEpsilon;
+          if (soh < p.min_sum_hessian_in_leaf) continue;
+          sog = sum_gradient - grad;
+        }
+        double gain = split_gain(sog, soh, grad, kInt ? hess : hess + kEpsilon, pc, other_count, cnt, lc.parent_output,
+                                 lc.mc, lc.cmin, lc.cmax, 0);
+        if (gain <= min_gain_shift) continue;
+        is_splittable = true;
+        if (gain > best_gain) {
+          best_threshold = t;
+          best_slg = grad;
+          best_slh = kInt ? hess : hess + kEpsilon;
+          best_left_count = cnt;
+          best_left_int = kInt ? sm.ig[t] : 0;
+          best_gain = gain;
+        }
+      }
+    } else {
+      pc.lambda_l2 += p.cat_l2;
+      int32_t max_num_cat = min(p.max_cat_threshold, (used_bin + 1) / 2);
+      for (int d = 0; d < 2; ++d) {
+        int32_t dir = d == 0 ? 1 : -1;
+        int32_t start_pos = d == 0 ? 0 : used_bin - 1;
+        int32_t cnt_cur_group = 0, left_count = 0;
+        double slg = 0.0, slh = kEpsilon;
+        int64_t sl_int = 0;
+        for (int32_t i = 0; i < used_bin && i < max_num_cat; ++i) {
+          int t = sm.sorted[start_pos];
+          start_pos += dir;
+          int32_t cnt = CNT(t);
+          double srh, srg, slh_eff;
+          if (kInt) {
+            sl_int = (int64_t)((uint64_t)sl_int + (uint64_t)sm.ig[t]);
+            left_count += cnt;
+            cnt_cur_group += cnt;
+            slh_eff = (double)int_hess(sl_int) * hs;
+            if (left_count < p.min_data_in_leaf || slh_eff < p.min_sum_hessian_in_leaf) continue;
+            int32_t right_count = lc.num_data - left_count;
+            if (right_count < p.min_data_in_leaf || right_count < p.min_data_per_group) break;
+            int64_t sr_int = (int64_t)((uint64_t)lc.int_sum - (uint64_t)sl_int);
+            srh = (double)int_hess(sr_int) * hs;
+            if (srh < p.min_sum_hessian_in_leaf) break;
+            if (cnt_cur_group < p.min_data_per_group) continue;
+            cnt_cur_group = 0;
+            double slg_i = (double)int_grad(sl_int) * gs;
+            srg = (double)int_grad(sr_int) * gs;
+            double gain = split_gain(slg_i, slh_eff, srg, srh, pc, left_count, right_count, lc.parent_output, lc.mc,
+                                     lc.cmin, lc.cmax, 0);
+            if (gain <= min_gain_shift) continue;
+            is_splittable = true;
+            if (gain > best_gain) {
+              best_left_int = sl_int;
+              best_threshold = i;
+              best_gain = gain;
+              best_dir = dir;
+            }
+          } else {
+            slg += G(t);
+            slh += H(t);
+            left_count += cnt;
+            cnt_cur_group += cnt;
+            if (left_count < p.min_data_in_leaf || slh < p.min_sum_hessian_in_leaf) continue;
+            int32_t right_count = lc.num_data - left_count;
+            if (right_count < p.min_data_in_leaf || right_count < p.min_data_per_group) break;
+            srh = sum_hessian - slh;
+            if (srh < p.min_sum_hessian_in_leaf) break;
+            if (cnt_cur_group < p.min_data_per_group) continue;
+            cnt_cur_group = 0;
+            srg = sum_gradient - slg;
+            double gain = split_gain(slg, slh, srg, srh, pc, left_count, right_count, lc.parent_output, lc.mc, lc.cmin,
+                                     lc.cmax, 0);
+            if (gain <= min_gain_shift) continue;
+            is_splittable = true;
+            if (gain > best_gain) {
+              best_left_count = left_count;
+              best_slg = slg;
+              best_slh = slh;
+              best_threshold = i;
+              best_gain = gain;
+              best_dir = dir;
+            }
+          }
+        }
+      }
+    }
+    if (is_splittable) {
+      if (kInt) {
+        int64_t left = best_left_int;
+        int64_t right = (int64_t)((uint64_t)lc.int_sum - (uint64_t)left);
+        double lg = (double)int_grad(left) * gs, lh = (double)int_hess(left) * hs;
+        double rg = (double)int_grad(right) * gs, rh = (double)int_hess(right) * hs;
+        int32_t lcnt = round_int((double)int_hess(left) * cnt_factor);
+        int32_t rcnt = round_int((double)int_hess(right) * cnt_factor);
+        double lo = leaf_output(lg, lh, pc, lcnt, lc.parent_output);
+        double ro = leaf_output(rg, rh, pc, rcnt, lc.parent_output);
+        out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
+        out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
+        out.left_count = lcnt;
+        out.right_count = rcnt;
+        out.left_sum_gradient = lg;
+        out.left_sum_hessian = lh;
+        out.right_sum_gradient = rg;
+        out.right_sum_hessian = rh;
+        out.left_sum_gh = left;
+        out.right_sum_gh = right;
+      } else {
+        double lo = leaf_output(best_slg, best_slh, pc, best_left_count, lc.parent_output);
+        double ro = leaf_output(sum_gradient - best_slg, sum_hessian - best_slh, pc, lc.num_data - best_left_count,
+                                lc.parent_output);
+        out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
+        out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
+        out.left_count = best_left_count;
+        out.left_sum_gradient = best_slg;
+        out.left_sum_hessian = best_slh - kEpsilon;
+        out.right_count = lc.num_data - best_left_count;
+        out.right_sum_gradient = sum_gradient - best_slg;
+        out.right_sum_hessian = sum_hessian - best_slh - kEpsilon;
+      }
+      out.monotone_type = 0;
+      out.gain = best_gain - min_gain_shift;
+      for (int w = 0; w < kCatWords; ++w) out.cat_bits[w] = 0;
+      int32_t ncat = 0;
+      if (use_onehot) {
+        uint32_t b = (uint32_t)(best_threshold + offset);
+        out.cat_bits[b >> 5] |= 1u << (b & 31);
+        ncat = 1;
+      } else {
+        for (int32_t i = 0; i <= best_threshold; ++i) {
+          uint32_t b = (uint32_t)((best_dir == 1 ? sm.sorted[i] : sm.sorted[used_bin - 1 - i]) + offset);
+          out.cat_bits[b >> 5] |= 1u << (b & 31);
+          ++ncat;
+        }
+      }
+      out.num_cat = ncat;
+    }
+  }
+  is_splittable = __shfl_sync(0xffffffffu, (int)is_splittable, 0) != 0;
+  __syncwarp();
+  return is_splittable;
+}
+
+// find_best_threshold (split.rs:246-271, :930-950) for one leaf and feature.
+template <bool kInt>
+__device__ bool find_best_threshold_warp(ScanSmem& sm, const DFeature& m, const DParams& p, LeafCtx lc, DSplit& out) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    out.default_left = 1;
+    out.gain = -INFINITY;
+    out.num_cat = 0;
+    out.monotone_type = 0;
+  }
+  if (!kInt) lc.sum_h = lc.sum_h + 2.0 * kEpsilon;
+  bool ok;
+  if (m.bin_type == 1) {
+    ok = scan_categorical<kInt>(sm, m, p, lc, out);
+  } else {
+    if (lane == 0) out.monotone_type = m.monotone_type;
+    double sg = kInt ? (double)int_grad(lc.int_sum) * lc.gs : lc.sum_g;
+    double sh = kInt ? (double)int_hess(lc.int_sum) * lc.hs : lc.sum_h;
+    double min_gain_shift = leaf_gain(sg, sh, p, lc.num_data, lc.parent_output) + p.min_gain_to_split;
+    __syncwarp();
+    if (m.num_bin > 2 && m.missing_type != 0) {
+      if (m.missing_type == 1) {
+        ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, true, false, out);
+        ok |= scan_dir<kInt>(sm, m, p, lc, min_gain_shift, false, true, false, out);
+      } else {
+        ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, false, true, out);
+        ok |= scan_dir<kInt>(sm, m, p, lc, min_gain_shift, false, false, true, out);
+      }
+    } else {
+      ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, false, false, out);
+      if (lane == 0 && m.missing_type == 2) out.default_left = 0;
+    }
+  }
+  if (lane == 0) out.gain *= m.penalty;
+  __syncwarp();
+  return ok;
+}
+
+__device__ double monotone_split_gain_penalty(int32_t depth, double penalization) {  // constraints.rs:852-861
+  double d = (double)depth;
+  if (penalization >= d + 1.0) return kEpsilon;
+  if (penalization <= 1.0) return 1.0 - penalization / pow(2.0, d) + kEpsilon;
+  return 1.0 - pow(2.0, penalization - 1.0 - d) + kEpsilon;
+}
+
+__device__ __forceinline__ bool split_better(const DSplit& a, const DSplit& b) {
+  return better_than(a.gain, a.feature, b.gain, b.feature);
+}
+
+// The selected split is applied to the tree (tree.rs:240-297) and the
+// partition LUT is written; runs in one thread.
+__device__ void apply_split(const DCtx& c, DSlot& s, int32_t bl) {
+  DSlotState* st = s.st;
+  const DParams& p = c.p;
+  DTree& t = s.tree;
+  const DSplit& info = s.best[bl];
+  const DFeature& m = c.feats[info.inner];
+  int32_t R = st->num_leaves_cur;
+  int32_t node = R - 1;
+  bool numerical = m.bin_type == 0;
+  int32_t parent = t.leaf_parent[bl];
+  if (parent >= 0) {
+    if (t.left_child[parent] == ~bl) t.left_child[parent] = node;
+    else t.right_child[parent] = node;
+  }
+  t.split_feature_inner[node] = info.inner;
+  t.split_feature[node] = info.feature;
+  t.split_gain[node] = (float)(info.gain + p.min_gain_to_split);
+  t.node_gain[node] = info.gain;
+  t.left_child[node] = ~bl;
+  t.right_child[node] = ~R;
+  t.leaf_parent[bl] = node;
+  t.leaf_parent[R] = node;
+  t.internal_weight[node] = info.left_sum_hessian + info.right_sum_hessian;
+  t.internal_value[node] = t.leaf_value[bl];
+  t.leaf_value[bl] = isnan(info.left_output) ? 0.0 : info.left_output;
+  t.leaf_weight[bl] = info.left_sum_hessian;
+  t.leaf_value[R] = isnan(info.right_output) ? 0.0 : info.right_output;
+  t.leaf_weight[R] = info.right_sum_hessian;
+  int32_t d = t.leaf_depth[bl] + 1;
+  t.leaf_depth[bl] = d;
+  t.leaf_depth[R] = d;
+  int8_t dt = 0;
+  bool default_left = numerical ? info.default_left != 0 : false;
+  if (default_left) dt |= 2;
+  dt = (int8_t)((dt & 3) | (m.missing_type << 2));
+  if (!numerical) dt |= 1;
+  t.decision_type[node] = dt;
+  t.threshold_in_bin[node] = numerical ? info.threshold : (uint32_t)st->num_cat;
+  for (int w = 0; w < kCatWords; ++w) t.cat_bits[node * kCatWords + w] = numerical ? 0u : info.cat_bits[w];
+  if (!numerical) st->num_cat += 1;
+  // basic monotone constraints (constraints.rs:467-480)
+  if (p.use_monotone) {
+    s.cmin[R] = s.cmin[bl];
+    s.cmax[R] = s.cmax[bl];
+    if (numerical) {
+      double mid = (info.left_output + info.right_output) / 2.0;
+      if (info.monotone_type < 0) {
+        s.cmin[bl] = mid < s.cmin[bl] ? s.cmin[bl] : mid;
+        s.cmax[R] = s.cmax[R] < mid ? s.cmax[R] : mid;
+      } else if (info.monotone_type > 0) {
+        s.cmax[bl] = s.cmax[bl] < mid ? s.cmax[bl] : mid;
+        s.cmin[R] = mid < s.cmin[R] ? s.cmin[R] : mid;
+      }
+    }
+  }
+  // partition LUT over stored group values (learner/mod.rs:1313-1329)
+  int32_t ntb = m.view_len + 1;
+  for (int32_t raw = 0; raw < kMaxBins; ++raw) {
+    uint8_t left = 0;
+    if (raw < ntb) {
+      uint32_t b = decode_bin((uint32_t)raw, m);
+      if (numerical) {
+        bool miss = (m.missing_type == 1 && b == (uint32_t)m.default_bin) ||
+                    (m.missing_type == 2 && b == (uint32_t)(m.num_bin - 1));
+        left = miss ? (uint8_t)default_left : (uint8_t)(b <= info.threshold);
+      } else {
+        auto bit = [&](uint32_t v) { return (info.cat_bits[v >> 5] >> (v & 31)) & 1u; };
+        if (b == (uint32_t)m.most_freq_bin) left = (uint8_t)(m.most_freq_bin > 0 && bit(b));
+        else left = (uint8_t)bit(b);
+      }
+    }
+    st->lut[raw] = left;
+  }
+  st->split_leaf = bl;
+  st->new_leaf = R;
+  st->split_inner = info.inner;
+  st->num_leaves_cur = R + 1;
+  st->part_ticket = 0;
+  st->part_epoch += 1;
+}
+
+template <bool kInt>
+__global__ void __launch_bounds__(64) k_scan(DCtx c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScanSmem* sms = reinterpret_cast<ScanSmem*>(smem_raw);
+  DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  if (st->done) return;
+  const int f = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const DFeature m = c.feats[f];
+  const DParams& p = c.p;
+  const int32_t nf = c.num_features;
+  const bool have_larger = st->larger.leaf >= 0;
+  const bool need = st->need_find != 0;
+  const int32_t L = st->left_leaf;
+  bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
+  if (used) {
+    ScanSmem& sm = sms[warp];
+    ScanSmem& sm0 = sms[0];
+    const DLeafSplits sl = st->smaller;
+    const int len = m.view_len;
+    const size_t sbase = (size_t)s.buf_of[sl.leaf] * c.total_bins + m.view_start;
+    // load the smaller leaf's view, fix the most frequent bin (histogram.rs:42-56)
+    if (warp == 0) {
+      if (kInt) {
+        const int64_t* hs = reinterpret_cast<const int64_t*>(s.hist) + sbase;
+        for (int i = lane; i < len; i += 32) sm0.ig[i] = hs[i];
+        __syncwarp();
+        if (lane == 0 && m.most_freq_bin > 0) {
+          int64_t acc = sl.int_sum;
+          for (int i = 0; i < m.num_bin; ++i)
+            if (i != m.most_freq_bin) acc = (int64_t)((uint64_t)acc - (uint64_t)sm0.ig[i]);
+          sm0.ig[m.most_freq_bin] = acc;
+          reinterpret_cast<int64_t*>(s.hist)[sbase + m.most_freq_bin] = acc;
+        }
+      } else {
+        const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
+        for (int i = lane; i < len; i += 32) {
+          sm0.g[i] = hs[2 * i];
+          sm0.h[i] = hs[2 * i + 1];
+        }
+        __syncwarp();
+        if (lane == 0 && m.most_freq_bin > 0) {
+          double g = sl.sum_gradients, h = sl.sum_hessians;
+          for (int i = 0; i < m.num_bin; ++i) {
+            if (i != m.most_freq_bin) {
+              g -= sm0.g[i];
+              h -= sm0.h[i];
+            }
+          }
+          sm0.g[m.most_freq_bin] = g;
+          sm0.h[m.most_freq_bin] = h;
+          double* w = reinterpret_cast<double*>(s.hist) + 2 * (sbase + m.most_freq_bin);
+          w[0] = g;
+          w[1] = h;
+        }
+      }
+    }
+    __syncthreads();
+    if (warp == 1 && have_larger) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
+      const DLeafSplits ll = st->larger;
+      const size_t lbase = (size_t)s.buf_of[ll.leaf] * c.total_bins + m.view_start;
+      if (kInt) {
+        int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
+        for (int i = lane; i < len; i += 32) {
+          int64_t v = (int64_t)((uint64_t)lh[i] - (uint64_t)sm0.ig[i]);
+          sm.ig[i] = v;
+          lh[i] = v;
+        }
+      } else {
+        double* lh = reinterpret_cast<double*>(s.hist) + 2 * lbase;
+        for (int i = lane; i < len; i += 32) {
+          double g = lh[2 * i] - sm0.g[i], h = lh[2 * i + 1] - sm0.h[i];
+          sm.g[i] = g;
+          sm.h[i] = h;
+          lh[2 * i] = g;
+          lh[2 * i + 1] = h;
+        }
+      }
+    }
+    __syncwarp();
+    if (warp == 0 || have_larger) {
+      const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
+      LeafCtx lc;
+      lc.sum_g = ls.sum_gradients;
+      lc.sum_h = ls.sum_hessians;
+      lc.int_sum = ls.int_sum;
+      lc.gs = st->grad_scale;
+      lc.hs = st->hess_scale;
+      lc.num_data = ls.num_data;
+      // learner/mod.rs:1303-1309 parent output
+      lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
+                                                  : ls.weight;
+      lc.mc = p.use_monotone != 0;
+      lc.cmin = s.cmin[ls.leaf];
+      lc.cmax = s.cmax[ls.leaf];
+      DSplit& out = s.feat_res[warp * nf + f];
+      bool ok = find_best_threshold_warp<kInt>(sm, m, p, lc, out);
+      if (lane == 0) {
+        out.feature = m.real_index;
+        out.inner = f;
+        s.feat_ok[warp * nf + f] = ok ? 1 : 0;
+      }
+    }
+  }
+  // last CTA of this slot: best split per leaf, best leaf, tree bookkeeping
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&st->scan_counter, 1) == nf - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (need) {
+    // warp w reduces leaf side w (0 smaller, 1 larger)
+    if (warp == 0 || have_larger) {
+      const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
+      double pen = monotone_split_gain_penalty(s.tree.leaf_depth[ls.leaf], p.monotone_penalty);
+      double bg = -INFINITY;
+      int32_t bfeat = -1, bf = -1;
+      for (int ff = lane; ff < nf; ff += 32) {
+        bool u = s.bytree[ff] && (!have_larger || s.splittable[L * nf + ff]);
+        if (!u) continue;
+        DSplit& r = s.feat_res[warp * nf + ff];
+        double g = r.gain;
+        if (r.monotone_type != 0) g *= pen;
+        if (better_than(g, r.feature, bg, bfeat)) {
+          bg = g;
+          bfeat = r.feature;
+          bf = ff;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        double og = __shfl_xor_sync(0xffffffffu, bg, o);
+        int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
+        int32_t off = __shfl_xor_sync(0xffffffffu, bf, o);
+        if (better_than(og, ofe, bg, bfeat)) {
+          bg = og;
+          bfeat = ofe;
+          bf = off;
+        }
+      }
+      // splittable flags of this leaf (learner/mod.rs:842-849, :1066-1086)
+      uint8_t* spl_new = s.feat_ok + 2 * nf + warp * nf;  // staged, applied after both reads
+      for (int ff = lane; ff < nf; ff += 32) {
+        bool u = s.bytree[ff] && (!have_larger || s.splittable[L * nf + ff]);
+        spl_new[ff] = u ? s.feat_ok[warp * nf + ff] : 0;
+      }
+      if (lane == 0) {
+        DSplit& dst = s.best[ls.leaf];
+        if (bf >= 0) {
+          dst = s.feat_res[warp * nf + bf];
+          dst.gain = bg;
+        } else {
+          dst.feature = -1;
+          dst.inner = -1;
+          dst.gain = -INFINITY;
+        }
+      }
+    }
+    __syncthreads();
+    for (int ff = threadIdx.x; ff < nf; ff += blockDim.x) {
+      s.splittable[st->smaller.leaf * nf + ff] = s.feat_ok[2 * nf + ff];
+      if (have_larger) s.splittable[st->larger.leaf * nf + ff] = s.feat_ok[3 * nf + ff];
+    }
+  }
+  __syncthreads();
+  if (warp != 0) return;
+  // best leaf (learner/mod.rs:698-706): larger gain, smaller feature, smaller leaf
+  double bg = -INFINITY;
+  int32_t bfeat = -1, bl = INT32_MAX;
+  for (int l = lane; l < p.num_leaves; l += 32) {
+    const DSplit& r = s.best[l];
+    if (bl == INT32_MAX || better_than(r.gain, r.feature, bg, bfeat)) {
+      bg = r.gain;
+      bfeat = r.feature;
+      bl = l;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double og = __shfl_xor_sync(0xffffffffu, bg, o);
+    int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
+    int32_t ol = __shfl_xor_sync(0xffffffffu, bl, o);
+    bool take = false;
+    if (ol != INT32_MAX) {
+      if (bl == INT32_MAX) take = true;
+      else if (better_than(og, ofe, bg, bfeat)) take = true;
+      else if (!better_than(bg, bfeat, og, ofe) && ol < bl) take = true;
+    }
+    if (take) {
+      bg = og;
+      bfeat = ofe;
+      bl = ol;
+    }
+  }
+  if (lane == 0) {
+    st->scan_counter = 0;
+    if (!(bg > 0.0)) {
+      st->done = 1;
+    } else {
+      apply_split(c, s, bl);
+    }
+  }
+}
+template __global__ void k_scan<false>(DCtx);
+template __global__ void k_scan<true>(DCtx);
+
+// =====================================================================================
+// partition (partition.rs:107-174): out-of-place split of the leaf's rows into
+// the other index buffer; left rows keep their order, right rows are written
+// from the end (reversed). Tiles are claimed in order and chained with a
+// decoupled look-back on the running left count.
+// =====================================================================================
+constexpr int kPartThreads = 256;
+constexpr int kPartItems = 8;
+constexpr int kPartTile = kPartThreads * kPartItems;
+constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
+constexpr uint32_t kEpochMask = 0x7FFFFFFFu;
+constexpr unsigned long long kValueMask = (1ull << 31) - 1;
+
+// status word: flag (2 bits) | epoch (31 bits) | left count (31 bits)
+__device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsigned long long flag, uint64_t v) {
+  return flag | ((unsigned long long)(epoch & kEpochMask) << 31) | (v & kValueMask);
+}
+
+__device__ void partition_finalize(const DCtx& c, DSlot& s, int32_t total_left) {
+  DSlotState* st = s.st;
+  int32_t L = st->split_leaf, R = st->new_leaf;
+  int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
+  int32_t side = s.leaf_side[L];
+  int32_t nl = total_left, nr = cnt - total_left;
+  s.leaf_count[L] = nl;
+  s.leaf_begin[R] = begin + nl;
+  s.leaf_count[R] = nr;
+  s.leaf_side[L] = 1 - side;
+  s.leaf_side[R] = 1 - side;
+  DTree& t = s.tree;
+  int32_t node = R - 1;
+  t.leaf_count[L] = nl;
+  t.leaf_count[R] = nr;
+  t.internal_count[node] = nl + nr;
+  const DSplit& info = s.best[L];
+  DLeafSplits ls{L, nl, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
+  DLeafSplits rs{R, nr, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
+  if (nl < nr) {
+    if (nl <= 0) st->status = kStatusEmptyChild;
+    st->smaller = ls;
+    st->larger = rs;
+  } else {
+    if (nr <= 0) st->status = kStatusEmptyChild;
+    st->smaller = rs;
+    st->larger = ls;
+  }
+  if (st->status != kStatusOk) {
+    st->done = 1;
+    return;
+  }
+  // HistogramPool::Move: the parent's buffer goes to the larger leaf, the
+  // fresh buffer R (zeroed by this kernel) to the smaller one.
+  if (st->larger.leaf == L) {
+    s.buf_of[R] = R;
+  } else {
+    s.buf_of[R] = s.buf_of[L];
+    s.buf_of[L] = R;
+  }
+  st->left_leaf = L;
+  st->right_leaf = R;
+  st->need_find = before_find_best_split(c, s, L, R) ? 1 : 0;
+}
+
+// Grid (G, 1, slots), kPartThreads threads.
+__global__ void __launch_bounds__(kPartThreads) k_partition(DCtx c) {
+  DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  if (st->done) return;
+  __shared__ uint8_t lut[kMaxBins];
+  __shared__ int32_t warp_tot[kPartThreads / 32];
+  __shared__ int32_t s_tile, s_prefix;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t L = st->split_leaf;
+  const int32_t R = st->new_leaf;
+  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
+  const int32_t side = s.leaf_side[L];
+  const uint32_t epoch = st->part_epoch;
+  const int32_t inner = st->split_inner;
+  // zero the fresh histogram buffer R for the next smaller leaf
+  {
+    size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+    double* h = reinterpret_cast<double*>(s.hist) + (size_t)R * cells;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h[i] = 0.0;
+  }
+  if (cnt == 0) {
+    if (blockIdx.x == 0 && tid == 0) partition_finalize(c, s, 0);
+    return;
+  }
+  for (int i = tid; i < kMaxBins; i += blockDim.x) lut[i] = st->lut[i];
+  const uint32_t* in = s.idx[side] + begin;
+  uint32_t* out = s.idx[1 - side] + begin;
+  const int32_t ntiles = (cnt + kPartTile - 1) / kPartTile;
+  const uint8_t* col = c.bins + inner;
+  __syncthreads();
+  while (true) {
+    if (tid == 0) s_tile = atomicAdd(&st->part_ticket, 1);
+    __syncthreads();
+    const int32_t tile = s_tile;
+    if (tile >= ntiles) break;
+    const int32_t t0 = tile * kPartTile;
+    uint32_t rows[kPartItems];
+    uint32_t flags = 0;
+    int32_t nleft = 0;
+#pragma unroll
+    for (int k = 0; k < kPartItems; ++k) {
+      int32_t pos = t0 + tid * kPartItems + k;
+      if (pos < cnt) {
+        uint32_t r = in[pos];
+        rows[k] = r;
+        uint32_t raw = col[(size_t)r * c.stride];
+        if (lut[raw]) {
+          flags |= 1u << k;
+          ++nleft;
+        }
+      }
+    }
+    // block exclusive scan of per-thread left counts
+    int32_t incl = nleft;
+    for (int o = 1; o < 32; o <<= 1) {
+      int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    int32_t wbase = 0, tile_left = 0;
+    for (int w = 0; w < kPartThreads / 32; ++w) {
+      if (w < warp) wbase += warp_tot[w];
+      tile_left += warp_tot[w];
+    }
+    const int32_t excl = wbase + incl - nleft;
+    // decoupled look-back on the left count
+    if (tid == 0) {
+      unsigned long long* stat = s.tile_status;
+      if (tile == 0) {
+        atomicExch(&stat[0], pack_status(epoch, kFlagInc, (uint64_t)tile_left));
+        s_prefix = 0;
+      } else {
+        atomicExch(&stat[tile], pack_status(epoch, kFlagAgg, (uint64_t)tile_left));
+        int64_t acc = 0;
+        int32_t pred = tile - 1;
+        int spins = 0;
+        while (pred >= 0) {
+          unsigned long long v = atomicAdd(&stat[pred], 0ull);
+          uint32_t ve = (uint32_t)((v >> 31) & kEpochMask);
+          unsigned long long flag = v & (3ull << 62);
+          if (ve != (epoch & kEpochMask) || flag == 0) {
+            if (++spins > kSpinLimit) {
+              st->status = kStatusTimeout;
+              st->done = 1;
+              break;
+            }
+            __nanosleep(32);
+            continue;
+          }
+          acc += (int64_t)(v & kValueMask);
+          if (flag == kFlagInc) break;
+          --pred;
+        }
+        atomicExch(&stat[tile], pack_status(epoch, kFlagInc, (uint64_t)(acc + tile_left)));
+        s_prefix = (int32_t)acc;
+      }
+    }
+    __syncthreads();
+    const int32_t prefix = s_prefix;
+    // scatter: left rows ascending from begin, right rows descending from the end
+    int32_t lrank = prefix + excl;
+#pragma unroll
+    for (int k = 0; k < kPartItems; ++k) {
+      int32_t pos = t0 + tid * kPartItems + k;
+      if (pos < cnt) {
+        if (flags & (1u << k)) {
+          out[lrank++] = rows[k];
+        } else {
+          int32_t rrank = pos - lrank;  // rights before this row
+          out[cnt - 1 - rrank] = rows[k];
+        }
+      }
+    }
+    if (tile == ntiles - 1 && tid == 0) partition_finalize(c, s, prefix + tile_left);
+    __syncthreads();
+  }
+}
+
+// =====================================================================================
+// leaf renewal from FP64 gradient sums (learner/mod.rs:736-747) and the
+// score updates (partition.rs:306-319; tree.rs:605-711 binned routing)
+// =====================================================================================
+// Grid (G, num_leaves, slots): block (x, leaf) sums a chunk of the leaf's rows.
+__global__ void __launch_bounds__(256) k_leaf_sums(DCtx c, double* sums /*[slots][leaves][2]*/) {
+  DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  int32_t leaf = blockIdx.y;
+  if (leaf >= st->num_leaves_cur) return;
+  int32_t begin = s.leaf_begin[leaf], cnt = s.leaf_count[leaf];
+  const uint32_t* idx = s.idx[s.leaf_side[leaf]] + begin;
+  double g = 0.0, h = 0.0;
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    float2 v = s.gh[idx[i]];
+    g += (double)v.x;
+    h += (double)v.y;
+  }
+  g = warp_sum_d(g);
+  h = warp_sum_d(h);
+  if ((threadIdx.x & 31) == 0) {
+    double* o = sums + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
+    atomicAdd(o, g);
+    atomicAdd(o + 1, h);
+  }
+}
+
+__global__ void k_leaf_renew(DCtx c, const double* sums) {
+  DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  for (int32_t leaf = threadIdx.x; leaf < st->num_leaves_cur; leaf += blockDim.x) {
+    const double* o = sums + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
+    s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(o[0], o[1], c.p, s.leaf_count[leaf]));
+  }
+}
+
+// score[row] += leaf_value[leaf] * scale over each leaf's rows.
+// Grid (G, num_leaves, slots).
+__global__ void __launch_bounds__(256) k_add_leaf_outputs(DCtx c, const double* leaf_values, int32_t lv_stride,
+                                                          double* score, int64_t score_stride) {
+  DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  int32_t leaf = blockIdx.y;
+  if (leaf >= st->num_leaves_cur) return;
+  double v = leaf_values[(size_t)blockIdx.z * lv_stride + leaf];
+  int32_t begin = s.leaf_begin[leaf], cnt = s.leaf_count[leaf];
+  const uint32_t* idx = s.idx[s.leaf_side[leaf]] + begin;
+  double* sc = score + (size_t)blockIdx.z * score_stride;
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) sc[idx[i]] += v;
+}
+
+// Binned tree walk (tree.rs:588-633) for rows `rows` (or 0..n): score += leaf value.
+__global__ void __launch_bounds__(256) k_add_tree_binned(DCtx c, const uint8_t* bins, int32_t stride,
+                                                         const uint32_t* rows, int64_t n, const double* leaf_values,
+                                                         int32_t lv_stride, double* score, int64_t score_stride) {
+  DSlot& s = c.slots[blockIdx.z];
+  const DTree& t = s.tree;
+  int32_t nl = s.st->num_leaves_cur;
+  const double* lv = leaf_values + (size_t)blockIdx.z * lv_stride;
+  double* sc = score + (size_t)blockIdx.z * score_stride;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = rows ? (int64_t)rows[i] : i;
+    int32_t node = 0;
+    if (nl > 1) {
+      while (node >= 0) {
+        int32_t inner = t.split_feature_inner[node];
+        const DFeature& m = c.feats[inner];
+        uint32_t b = decode_bin(bins[(size_t)r * stride + inner], m);
+        int8_t dt = t.decision_type[node];
+        if (dt & 1) {
+          const uint32_t* bits = t.cat_bits + node * kCatWords;
+          bool left = b < (uint32_t)kMaxBins && ((bits[b >> 5] >> (b & 31)) & 1u);
+          node = left ? t.left_child[node] : t.right_child[node];
+          continue;
+        }
+        int32_t mt = (dt >> 2) & 3;
+        bool is_default = (mt == 1 && b == (uint32_t)m.default_bin) || (mt == 2 && b == (uint32_t)(m.num_bin - 1));
+        bool left = is_default ? (dt & 2) != 0 : b <= t.threshold_in_bin[node];
+        node = left ? t.left_child[node] : t.right_child[node];
+      }
+      node = ~node;
+    }
+    sc[r] += lv[node];
+  }
+}
+
+}  // namespace lgbm_b200

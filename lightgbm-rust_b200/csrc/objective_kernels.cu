@@ -1,0 +1,205 @@
+// Objective gradients, quantized gradients and bagging on the device.
+//   k_grad_binary   objective/binary.rs:101-127
+//   k_grad_l2       objective/regression.rs:209-224 (L2, no weights)
+//   k_grad_softmax  objective/multiclass.rs:16-30, :126-154
+//   k_quant_*       learner/quant.rs:411-448 (DiscretizeGradients)
+//   k_bagging       sample_strategy.rs:280-320 (one LCG per 1024-row block)
+// Each kernel can write the learner's interleaved (g, h) buffer directly.
+#include "kernels.h"
+
+namespace lgbm_b200 {
+
+__global__ void __launch_bounds__(256) k_grad_binary(const float* label, const double* score, int64_t n,
+                                                     double sigmoid, float2* gh_out, float* g, float* h) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double lab = label[i] > 0.0f ? 1.0 : -1.0;
+    double response = -lab * sigmoid / ((double)1.0f + exp(lab * sigmoid * score[i]));
+    double ar = fabs(response);
+    float gv = (float)(response * 1.0);
+    float hv = (float)(ar * (sigmoid - ar) * 1.0);
+    if (gh_out) gh_out[i] = make_float2(gv, hv);
+    if (g) {
+      g[i] = gv;
+      h[i] = hv;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_grad_l2(const float* label, const double* score, int64_t n, float2* gh_out,
+                                                 float* g, float* h) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float gv = (float)(score[i] - (double)label[i]);
+    if (gh_out) gh_out[i] = make_float2(gv, 1.0f);
+    if (g) {
+      g[i] = gv;
+      h[i] = 1.0f;
+    }
+  }
+}
+
+// One row per thread; scores / outputs are class-major [k x n].
+__global__ void __launch_bounds__(256) k_grad_softmax(const float* label, const double* score, int64_t n, int32_t k,
+                                                      float2* gh_out, int64_t gh_stride, float* g, float* h) {
+  const double factor = (double)k / (double)((float)k - 1.0f);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double wmax = score[i];
+    for (int c = 1; c < k; ++c) {
+      double v = score[(int64_t)c * n + i];
+      wmax = v < wmax ? wmax : v;
+    }
+    double wsum = 0.0;
+    for (int c = 0; c < k; ++c) wsum += exp(score[(int64_t)c * n + i] - wmax);
+    int32_t li = (int32_t)label[i];
+    for (int c = 0; c < k; ++c) {
+      double p = exp(score[(int64_t)c * n + i] - wmax) / wsum;
+      double gg = li == c ? p - (double)1.0f : p;
+      double hh = factor * p * ((double)1.0f - p);
+      if (gh_out) gh_out[(int64_t)c * gh_stride + i] = make_float2((float)gg, (float)hh);
+      if (g) {
+        g[(int64_t)c * n + i] = (float)gg;
+        h[(int64_t)c * n + i] = (float)hh;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_interleave(const float* g, const float* h, int64_t n, float2* gh) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    gh[i] = make_float2(g[i], h[i]);
+}
+
+// max |g| and |h| (order-independent, exact); the last block derives the
+// scales exactly as quant.rs:429-430 does.
+__global__ void __launch_bounds__(256) k_quant_absmax(const float2* gh, int64_t n, unsigned long long* maxbits,
+                                                      int32_t* counter, DSlotState* st, int32_t bins,
+                                                      int32_t const_hess, int32_t num_blocks) {
+  double mg = 0.0, mh = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float2 v = gh[i];
+    mg = fmax(mg, fabs((double)v.x));
+    mh = fmax(mh, fabs((double)v.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+    mh = fmax(mh, __shfl_xor_sync(0xffffffffu, mh, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&maxbits[0], (unsigned long long)__double_as_longlong(mg));
+    atomicMax(&maxbits[1], (unsigned long long)__double_as_longlong(mh));
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(counter, 1) == num_blocks - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double max_g = __longlong_as_double((long long)atomicAdd(&maxbits[0], 0ull));
+  double max_h = __longlong_as_double((long long)atomicAdd(&maxbits[1], 0ull));
+  st->grad_scale = max_g / (double)(bins / 2);
+  st->hess_scale = const_hess ? max_h : max_h / (double)bins;
+  maxbits[0] = 0;
+  maxbits[1] = 0;
+  *counter = 0;
+}
+
+// quant.rs:355-359 static_cast<int8_t>(double) as x86-64 compiles it.
+__device__ __forceinline__ int32_t to_i8(double x) {
+  int32_t t = (isnan(x) || !(x >= -2147483648.0 && x < 2147483648.0)) ? INT32_MIN : (int32_t)x;
+  return (int32_t)(int8_t)t;
+}
+
+// quant.rs:434-447; packed[i] = (g << 16) + (h as u8).
+__global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n, const double* grv,
+                                                     const double* hrv, int64_t start, const DSlotState* st,
+                                                     int32_t const_hess, int32_t stochastic, int32_t* packed) {
+  const double inv_g = 1.0 / st->grad_scale;
+  const double inv_h = 1.0 / st->hess_scale;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float2 v = gh[i];
+    double g = (double)v.x;
+    double rg = 0.5, rh = 0.5;
+    if (stochastic) {
+      int64_t pos = (i + start) % n;
+      rg = grv[pos];
+      rh = hrv[pos];
+    }
+    int32_t gq = g >= 0.0 ? to_i8(g * inv_g + rg) : to_i8(g * inv_g - rg);
+    int32_t hq = const_hess ? 1 : to_i8((double)v.y * inv_h + rh);
+    packed[i] = gq * 65536 + (int32_t)(uint8_t)hq;
+  }
+}
+
+// sample_strategy.rs:280-320: rows of block b draw from the LCG `state[b]`
+// (Random(bagging_seed + b)) in row order; r < fraction keeps the row.
+// One thread per 1024-row block; block_counts receives each block's in-bag count.
+__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag) {
+  int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t r0 = b * 1024;
+  if (r0 >= n) return;
+  int64_t r1 = min(n, r0 + 1024);
+  uint32_t x = rng_state[b];
+  for (int64_t r = r0; r < r1; ++r) {
+    x = x * 214013u + 2531011u;
+    float f = (float)((x >> 16) & 0x7FFF) / 32768.0f;
+    in_bag[r] = (double)f < fraction ? 1 : 0;
+  }
+  rng_state[b] = x;
+}
+
+// Ascending in-bag rows and the out-of-bag rows. A single CTA walks the
+// 1024-row blocks in order: each warp ballots 32 rows at a time.
+__global__ void __launch_bounds__(1024) k_compact_bag(const uint8_t* in_bag, int64_t n, uint32_t* bag, uint32_t* oob,
+                                                      int32_t* counts, int32_t* block_counts, int32_t num_blocks) {
+  __shared__ int32_t warp_in[32], warp_out[32];
+  __shared__ int32_t base_in, base_out;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    base_in = 0;
+    base_out = 0;
+  }
+  __syncthreads();
+  for (int64_t r0 = 0; r0 < n; r0 += blockDim.x) {
+    int64_t r = r0 + tid;
+    bool valid = r < n;
+    bool in = valid && in_bag[r];
+    unsigned bi = __ballot_sync(0xffffffffu, in);
+    unsigned bo = __ballot_sync(0xffffffffu, valid && !in);
+    if (lane == 0) {
+      warp_in[warp] = __popc(bi);
+      warp_out[warp] = __popc(bo);
+    }
+    __syncthreads();
+    int32_t pi = 0, po = 0, ti = 0, to = 0;
+    for (int w = 0; w < 32; ++w) {
+      if (w < warp) {
+        pi += warp_in[w];
+        po += warp_out[w];
+      }
+      ti += warp_in[w];
+      to += warp_out[w];
+    }
+    unsigned below = (1u << lane) - 1u;
+    if (in) bag[base_in + pi + __popc(bi & below)] = (uint32_t)r;
+    else if (valid) oob[base_out + po + __popc(bo & below)] = (uint32_t)r;
+    __syncthreads();
+    if (tid == 0) {
+      base_in += ti;
+      base_out += to;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    counts[0] = base_in;
+    counts[1] = base_out;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_add_const(double* score, int64_t n, double v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    score[i] += v;
+}
+
+}  // namespace lgbm_b200
