@@ -202,6 +202,18 @@ int lgbm_b200_learner_set_timing(LgbmB200Learner* h, int32_t enabled);
  * [histogram, scan, partition, other]; rows histogrammed; kernels launched. */
 int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_rows, int32_t* launches);
 
+/* Diagnostics for the parity tests. lgbm_b200_learner_histogram runs the
+ * learner's histogram kernel over `rows` (NULL: every row) of slot `slot`'s
+ * gradients from the last train call (quantized form: its packed values) and
+ * writes the histogram in the learner's layout: per inner feature its
+ * num_bin - offset stored bins, FP64 [g, h] pairs (F64 / F32C forms) or packed
+ * (g << 32) + h int64 sums (quantized form). lgbm_b200_learner_quantized
+ * returns the last packed quantized gradients and [grad_scale, hess_scale]
+ * (learner/quant.rs:411-448). These replace no reference call. */
+int lgbm_b200_learner_histogram(LgbmB200Learner* h, int32_t slot, const uint32_t* rows, int64_t num_rows,
+                                void* out);
+int lgbm_b200_learner_quantized(LgbmB200Learner* h, int32_t slot, int64_t* packed, double* scales);
+
 /* ------------------------------------------------------------------------
  * Objective gradients: RowObjective::gradients (objective/mod.rs:52) for
  * binary (binary.rs:101), L2 (regression.rs:209), softmax (multiclass.rs:126)

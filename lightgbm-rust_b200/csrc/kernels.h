@@ -26,7 +26,7 @@ struct ScanSmem {
   double key[kMaxBins];
 };
 
-__global__ void k_tree_init(DCtx c, const uint32_t* bag, int32_t n_used);
+__global__ void k_tree_init(DCtx c, const uint32_t* bag, const int32_t* n_used);
 template <int kMode>
 __global__ void k_hist_float(DCtx c, DTileTable tt);
 __global__ void k_hist_int(DCtx c, DTileTable tt, int32_t sub_rows);

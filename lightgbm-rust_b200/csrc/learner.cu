@@ -79,7 +79,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     int32_t cur_bins = 0, cur_f = 0;
     for (int32_t f = 0; f < nf; ++f) {
       int32_t vl = h->feats[f].view_len;
-      if (cur_f > 0 && ((size_t)(cur_bins + vl) * cell > budget || cur_f >= kMaxTileFeatures)) {
+      // tiles start at a multiple of 4 features: the kernels load 4 stored bins per 32-bit word
+      if (cur_f > 0 && (f % 4) == 0 &&
+          ((size_t)(cur_bins + 4 * kMaxBins) * cell > budget || cur_f + 4 > kMaxTileFeatures)) {
         h->ntiles++;
         if (h->ntiles >= kMaxTiles) return Status(LGBM_B200_ERR_UNSUPPORTED, "too many histogram feature tiles");
         h->tiles.f0[h->ntiles] = f;
@@ -203,6 +205,11 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   if (!(s = A.alloc_n(&slots_d, (size_t)K)).ok()) return s;
   CU(cudaMemcpy(slots_d, h->slots_h.data(), sizeof(DSlot) * K, cudaMemcpyHostToDevice));
   if (!(s = A.alloc_n(&h->bag, (size_t)n)).ok()) return s;
+  if (!(s = A.alloc_n(&h->n_used_dev, 1)).ok()) return s;
+  {
+    int32_t nn = (int32_t)n;
+    CU(cudaMemcpy(h->n_used_dev, &nn, sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   if (!(s = A.alloc_n(&h->leaf_sums, (size_t)K * L * 2)).ok()) return s;
   if (!(s = A.alloc_n(&h->leaf_values_dev, (size_t)K * L)).ok()) return s;
   if (mode == LGBM_B200_HIST_QUANT) {
@@ -284,7 +291,7 @@ static Status enqueue_tree(LgbmB200Learner* h) {
   const int mode = h->cfg.hist_precision;
   cudaStream_t s = h->stream;
   dim3 init_grid(h->root_grid, 1, K);
-  k_tree_init<<<init_grid, 256, 0, s>>>(c, h->bagging ? h->bag : nullptr, h->n_used);
+  k_tree_init<<<init_grid, 256, 0, s>>>(c, h->bagging ? h->bag : nullptr, h->n_used_dev);
   CU_LAUNCH();
   dim3 hist_grid(h->hist_grid, h->ntiles, K);
   dim3 scan_grid(h->nf, 1, K);
@@ -322,7 +329,7 @@ static Status enqueue_tree(LgbmB200Learner* h) {
 static Status run_tree(LgbmB200Learner* h) {
   cudaStream_t s = h->stream;
   const bool graph = h->cfg.use_cuda_graph != 0 && !h->timing;
-  const int key = (h->bagging ? 1 : 0);
+  const int key = (h->bagging ? 1 : 0) + 2 * h->ctx.bagging;
   if (!graph) return enqueue_tree(h);
   if (h->graph_exec == nullptr || h->graph_key != key) {
     if (h->graph_exec) {
@@ -488,6 +495,45 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
   return Status();
 }
 
+// The learner's histogram kernel over an arbitrary row subset of the
+// slot's current gradients (quantized: its current packed values), for the
+// parity tests. Rows (host, in the given order) stand in for leaf 0.
+Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int64_t nrows, void* out) {
+  CU(cudaSetDevice(h->device));
+  cudaStream_t s = h->stream;
+  const DSlot& d = h->slots_h[slot];
+  const int64_t cnt = rows ? nrows : h->n;
+  std::vector<uint32_t> r((size_t)cnt);
+  for (int64_t i = 0; i < cnt; ++i) r[(size_t)i] = rows ? rows[i] : (uint32_t)i;
+  CU(cudaMemcpyAsync(d.idx[0], r.data(), sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice, s));
+  int32_t zero = 0, c32 = (int32_t)cnt;
+  CU(cudaMemcpyAsync(d.leaf_begin, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d.leaf_count, &c32, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d.leaf_side, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d.buf_of, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  DSlotState ss;
+  CU(cudaMemcpyAsync(&ss, d.st, sizeof(ss), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  ss.done = 0;
+  ss.need_find = 1;
+  ss.smaller.leaf = 0;
+  CU(cudaMemcpyAsync(d.st, &ss, sizeof(ss), cudaMemcpyHostToDevice, s));
+  const int mode = h->cfg.hist_precision;
+  const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+  CU(cudaMemsetAsync(d.hist, 0, cells * 8, s));
+  // one slot only: a context whose slot array starts at `slot`
+  DCtx c = h->ctx;
+  c.slots = h->ctx.slots + slot;
+  dim3 grid(h->hist_grid, h->ntiles, 1);
+  if (mode == LGBM_B200_HIST_F64) k_hist_float<0><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+  else if (mode == LGBM_B200_HIST_F32C) k_hist_float<1><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+  else k_hist_int<<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+  CU_LAUNCH();
+  CU(cudaMemcpyAsync(out, d.hist, cells * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return Status();
+}
+
 }  // namespace lgbm_b200
 
 // ==========================================================================================
@@ -559,12 +605,20 @@ int lgbm_b200_learner_set_bagging(LgbmB200Learner* h, const uint32_t* used, int6
     h->bagging = false;
     h->n_used = (int32_t)h->n;
     h->ctx.bagging = 0;
+    int32_t nn = (int32_t)h->n;
+    cudaError_t e0 = cudaMemcpyAsync(h->n_used_dev, &nn, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
+    if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(h->stream);
+    if (e0 != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e0)));
     return LGBM_B200_OK;
   }
   if (num_used < 0 || num_used > h->n) return fail(Status(LGBM_B200_ERR_INVALID_DATA, "bag size"));
   cudaError_t e = cudaMemcpyAsync(h->bag, used, sizeof(uint32_t) * (size_t)num_used,
                                   location == LGBM_B200_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                                   h->stream);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  int32_t nu = (int32_t)num_used;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->n_used_dev, &nu, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   h->bagging = true;
   h->n_used = (int32_t)num_used;
@@ -656,6 +710,36 @@ int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_
     for (int i = 0; i < 4; ++i) ms[i] = h->last_ms[i];
   if (hist_rows) *hist_rows = h->last_hist_rows;
   if (launches) *launches = h->last_launches;
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_histogram(LgbmB200Learner* h, int32_t slot, const uint32_t* rows, int64_t num_rows,
+                                void* out) {
+  if (!h || slot < 0 || slot >= h->K || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  Status st = lgbm_b200::histogram_of_rows(h, slot, rows, num_rows, out);
+  if (!st.ok()) return fail(st);
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_quantized(LgbmB200Learner* h, int32_t slot, int64_t* packed, double* scales) {
+  if (!h || slot < 0 || slot >= h->K) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  if (h->cfg.hist_precision != LGBM_B200_HIST_QUANT)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "the learner does not quantize gradients"));
+  cudaSetDevice(h->device);
+  std::vector<int32_t> v((size_t)h->n);
+  DSlotState ss;
+  cudaMemcpyAsync(v.data(), h->slots_h[slot].packed, sizeof(int32_t) * h->n, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(&ss, h->slots_h[slot].st, sizeof(ss), cudaMemcpyDeviceToHost, h->stream);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "readback"));
+  for (int64_t i = 0; i < h->n; ++i) {
+    int64_t hq = (int64_t)(v[i] & 0xFFFF);
+    int64_t gq = (int64_t)((v[i] - (int32_t)hq) >> 16);
+    if (packed) packed[i] = (int64_t)((uint64_t)(gq << 32) + (uint64_t)hq);
+  }
+  if (scales) {
+    scales[0] = ss.grad_scale;
+    scales[1] = ss.hess_scale;
+  }
   return LGBM_B200_OK;
 }
 

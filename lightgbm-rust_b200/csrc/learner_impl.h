@@ -207,6 +207,7 @@ struct LgbmB200Learner {
   int32_t* quant_counter = nullptr;
   // bagging
   uint32_t* bag = nullptr;
+  int32_t* n_used_dev = nullptr;  // in-bag row count read by k_tree_init
   int32_t n_used = 0;
   bool bagging = false;
   // leaf renewal scratch [K][L][2]
@@ -239,6 +240,7 @@ namespace lgbm_b200 {
 // One tree per slot from the given gradients (class-major [K x n]); NULL
 // gradients reuse the slots' interleaved buffers filled by the caller.
 Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
+Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int64_t nrows, void* out);
 }  // namespace lgbm_b200
 
 namespace lgbm_b200 {

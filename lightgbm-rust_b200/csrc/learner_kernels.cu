@@ -50,9 +50,9 @@ __device__ bool before_find_best_split(const DCtx& c, DSlot& s, int32_t left, in
 }
 
 // Grid (kRootBlocks, 1, slots), 256 threads.
-__global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, int32_t n_used) {
+__global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, const int32_t* n_used) {
   DSlot& s = c.slots[blockIdx.z];
-  const int64_t n = n_used;
+  const int64_t n = *n_used;
   const int tid = threadIdx.x;
   // positions -> rows (identity, or the in-bag rows)
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + tid; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -216,7 +216,11 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_float(DCtx c, DTileTable 
   int f0, f1, bin0, nbins;
   tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
   __shared__ int32_t vstart[kMaxTileFeatures];
-  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+  __shared__ uint32_t vlen[kMaxTileFeatures];
+  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+    vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+    vlen[f - f0] = (uint32_t)c.feats[f].view_len;
+  }
   // kMode 0: double2 (g, h) per bin; kMode 1: float4 (g_hi, g_lo, h_hi, h_lo)
   if (kMode == 0) {
     double2* sh = reinterpret_cast<double2*>(smem_raw);
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_float(DCtx c, DTileTable 
     for (int k = 0; k < 4; ++k) {
       int fl = 4 * w + k;
       uint32_t raw = (word >> (8 * k)) & 0xFFu;
-      if (fl < nfeat && raw != 0u) {
+      if (fl < nfeat && raw != 0u && raw <= vlen[fl]) {
         int b = vstart[fl] + (int)raw;
         if (kMode == 0) {
           double2* sh = reinterpret_cast<double2*>(smem_raw);
@@ -300,7 +304,11 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_int(DCtx c, DTileTable tt
   int f0, f1, bin0, nbins;
   tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
   __shared__ int32_t vstart[kMaxTileFeatures];
-  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+  __shared__ uint32_t vlen[kMaxTileFeatures];
+  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+    vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
+    vlen[f - f0] = (uint32_t)c.feats[f].view_len;
+  }
   for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
   __syncthreads();
   const int nfeat = f1 - f0;
@@ -321,7 +329,7 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_int(DCtx c, DTileTable tt
       for (int k = 0; k < 4; ++k) {
         int fl = 4 * w + k;
         uint32_t raw = (word >> (8 * k)) & 0xFFu;
-        if (fl < nfeat && raw != 0u) atomicAdd(&sh[vstart[fl] + (int)raw], v);
+        if (fl < nfeat && raw != 0u && raw <= vlen[fl]) atomicAdd(&sh[vstart[fl] + (int)raw], v);
       }
     }
     __syncthreads();

@@ -266,6 +266,24 @@ class Learner:
                                                         _ptr(cnt, C.c_int32), _ptr(idx, C.c_uint32)))
         return beg, cnt, idx
 
+    def histogram(self, rows=None, slot=0):
+        """The learner's histogram kernel over `rows` (diagnostics)."""
+        total = int(np.sum(self.binned["num_bin"] - (self.binned["most_freq_bin"] == 0)))
+        quant = self.p["hist_precision"] == "quantized"
+        out = np.zeros(total if quant else 2 * total, np.int64 if quant else np.float64)
+        r = None if rows is None else np.ascontiguousarray(rows, dtype=np.uint32)
+        L.check(L.lib().lgbm_b200_learner_histogram(self.handle, slot, _ptr(r, C.c_uint32) if r is not None else None,
+                                                    0 if r is None else len(r), out.ctypes.data))
+        return out
+
+    def quantized(self, slot=0):
+        n = self.binned["num_data"]
+        packed = np.zeros(n, np.int64)
+        scales = np.zeros(2, np.float64)
+        L.check(L.lib().lgbm_b200_learner_quantized(self.handle, slot, _ptr(packed, C.c_int64),
+                                                    _ptr(scales, C.c_double)))
+        return packed, scales
+
     def set_timing(self, on):
         L.check(L.lib().lgbm_b200_learner_set_timing(self.handle, int(bool(on))))
 

@@ -1,0 +1,271 @@
+"""Parity of the CUDA tree-learning path with the CPU oracle, through the C ABI.
+
+Tolerances:
+  - bins, per-bin integer sums, leaf row sets, tree structure: exact;
+  - FP64 histogram sums: 1e-12 relative to the oracle's single-threaded
+    row-order sums (atomics reorder the additions);
+  - split gains / leaf values: 1e-10 / 1e-9 relative;
+  - quantized form: integer histograms and trees exact.
+"""
+import numpy as np
+import pytest
+
+from conftest import binned_dataset
+
+pytestmark = pytest.mark.gpu
+
+
+def _binary_data(n, f=28, seed=0, nan_frac=0.0):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    z = X[:, 0] + X[:, 1] * X[:, 2] - 0.5 * X[:, 3] ** 2 + 0.3 * rng.standard_normal(n)
+    y = (rng.random(n) < 1 / (1 + np.exp(-z))).astype(np.float32)
+    if nan_frac:
+        X[rng.random(X.shape) < nan_frac] = np.nan
+    return X, y
+
+
+def _grads(orc, p, y, scores=None):
+    if scores is None:
+        scores = np.zeros(len(y))
+    return orc.gradients(p, y, scores)
+
+
+def assert_same_tree(a, b, leaf_rtol=1e-9, gain_rtol=1e-6, check_inner=True):
+    assert a["num_leaves"] == b["num_leaves"], (a["num_leaves"], b["num_leaves"])
+    for k in ("split_feature", "threshold_in_bin", "decision_type", "left_child", "right_child", "leaf_count",
+              "internal_count", "leaf_depth"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+    for k in ("leaf_value", "leaf_weight", "internal_value", "internal_weight"):
+        np.testing.assert_allclose(a[k], b[k], rtol=leaf_rtol, atol=1e-12, err_msg=k)
+    np.testing.assert_allclose(a["split_gain"], b["split_gain"], rtol=gain_rtol, err_msg="split_gain")
+
+
+@pytest.mark.parametrize("form", ["f64", "f32c"])
+def test_histogram_float_forms(lgb, orc, form):
+    X, y = _binary_data(60000, seed=1, nan_frac=0.02)
+    params = {"objective": "binary", "hist_precision": form}
+    ds = binned_dataset(lgb, X, y, params)
+    b = ds.binned()
+    p = lgb.resolve_params(params)
+    g, h = _grads(orc, p, y, np.random.default_rng(2).standard_normal(len(y)) * 0.5)
+    learner = lgb.Learner(ds, params)
+    learner.train(g, h)  # loads the gradients into the learner
+    rng = np.random.default_rng(3)
+    for rows in (None, np.sort(rng.choice(len(y), 20000, replace=False)).astype(np.uint32),
+                 np.sort(rng.choice(len(y), 37, replace=False)).astype(np.uint32)):
+        got = learner.histogram(rows)
+        want = orc.hist(b, rows, g, h)
+        scale = np.maximum(np.abs(want), 1e-300)
+        err = np.max(np.abs(got - want) / np.maximum(scale, np.abs(want).max() * 1e-16 + 1e-300))
+        tol = 1e-12 if form == "f64" else 1e-7
+        assert err < tol, (form, err)
+
+
+def test_quantized_gradients_and_histogram_exact(lgb, orc):
+    X, y = _binary_data(50000, seed=4)
+    params = {"objective": "binary", "use_quantized_grad": True, "num_grad_quant_bins": 4, "num_threads": 8,
+              "seed": 7}
+    ds = binned_dataset(lgb, X, y, params)
+    b = ds.binned()
+    p = lgb.resolve_params(params)
+    g, h = _grads(orc, p, y, np.random.default_rng(5).standard_normal(len(y)))
+    learner = lgb.Learner(ds, params)
+    learner.train(g, h)
+    packed, scales = learner.quantized()
+    # the oracle's discretizer after one call with the same seed / thread count
+    import ctypes as C
+
+    want = np.zeros(len(y), np.int64)
+    ws = np.zeros(2)
+    orc.lib().oracle_discretize(4, int(p["seed"]), 0, 1, len(y), 8, 1,
+                                g.ctypes.data_as(C.POINTER(C.c_float)), h.ctypes.data_as(C.POINTER(C.c_float)),
+                                want.ctypes.data_as(C.POINTER(C.c_int64)), ws.ctypes.data_as(C.POINTER(C.c_double)))
+    assert list(scales) == list(ws)
+    assert np.array_equal(packed, want)
+    rows = np.sort(np.random.default_rng(6).choice(len(y), 12345, replace=False)).astype(np.uint32)
+    got = learner.histogram(rows)
+    total = int(np.sum(b["num_bin"] - (b["most_freq_bin"] == 0)))
+    exp = np.zeros(total, np.int64)
+    d = orc.Data(b)
+    orc.lib().oracle_hist(C.byref(d.s), rows.ctypes.data_as(C.POINTER(C.c_uint32)), len(rows), None, None,
+                          want.ctypes.data_as(C.POINTER(C.c_int64)), None, exp.ctypes.data_as(C.POINTER(C.c_int64)))
+    assert np.array_equal(got, exp)
+
+
+def _tree_pair(lgb, orc, X, y, params, grad_scores=None, categorical=None, bag=None, mask=None):
+    ds = binned_dataset(lgb, X, y, params, categorical=categorical)
+    b = ds.binned()
+    p = lgb.resolve_params(params)
+    g, h = _grads(orc, p, y, grad_scores)
+    learner = lgb.Learner(ds, params)
+    if bag is not None:
+        learner.set_bagging(bag)
+    if mask is not None:
+        learner.set_feature_mask(0, mask)
+    gt = learner.train(g, h)[0]
+    om = orc.train_trees(p, b, g, h, bag=bag, bytree=None if mask is None else mask.reshape(1, -1))
+    return gt, om.trees[0], learner, om, b
+
+
+@pytest.mark.parametrize("num_leaves", [2, 31, 255])
+def test_single_tree_f64(lgb, orc, num_leaves):
+    X, y = _binary_data(20000, seed=10)
+    params = {"objective": "binary", "num_leaves": num_leaves, "min_data_in_leaf": 20}
+    gt, ot, learner, om, b = _tree_pair(lgb, orc, X, y, params)
+    assert_same_tree(gt, ot)
+    # leaf row sets are exact
+    beg, cnt, idx = learner.partition(0, gt["num_leaves"])
+    obeg, ocnt, oidx = orc.partition(om, ot["num_leaves"], len(y))
+    for leaf in range(gt["num_leaves"]):
+        a = np.sort(idx[beg[leaf]: beg[leaf] + cnt[leaf]])
+        o = oidx[obeg[leaf]: obeg[leaf] + ocnt[leaf]]
+        assert np.array_equal(a, o), leaf
+
+
+def test_single_tree_nan_missing_and_regularisation(lgb, orc):
+    X, y = _binary_data(30000, seed=11, nan_frac=0.05)
+    params = {"objective": "binary", "num_leaves": 63, "min_data_in_leaf": 10, "lambda_l1": 0.5,
+              "lambda_l2": 2.0, "max_delta_step": 0.7, "min_gain_to_split": 0.01}
+    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
+    assert_same_tree(gt, ot)
+
+
+def test_single_tree_path_smooth_and_depth(lgb, orc):
+    X, y = _binary_data(20000, seed=12)
+    params = {"objective": "binary", "num_leaves": 63, "max_depth": 5, "path_smooth": 3.0}
+    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
+    assert_same_tree(gt, ot)
+
+
+def test_single_tree_categorical(lgb, orc):
+    rng = np.random.default_rng(13)
+    n = 30000
+    X = rng.standard_normal((n, 6)).astype(np.float32)
+    p = 1.0 / np.arange(1, 31) ** 1.2
+    p /= p.sum()
+    X[:, 4] = rng.choice(30, n, p=p)
+    X[:, 5] = rng.integers(0, 3, n)
+    eff = rng.standard_normal(30)
+    y = (X[:, 0] + eff[X[:, 4].astype(int)] + 0.5 * (X[:, 5] == 1) + 0.3 * rng.standard_normal(n) > 0)
+    params = {"objective": "binary", "num_leaves": 31, "max_cat_to_onehot": 4, "min_data_per_group": 50,
+              "cat_smooth": 5.0}
+    gt, ot, *_ = _tree_pair(lgb, orc, X, y.astype(np.float32), params, categorical=[4, 5])
+    assert gt["num_cat"] > 0
+    assert_same_tree(gt, ot)
+    assert np.array_equal(gt["cat_boundaries"], ot["cat_boundaries"])
+    assert np.array_equal(gt["cat_threshold"], ot["cat_threshold"])
+
+
+def test_single_tree_bagging_and_feature_mask(lgb, orc):
+    X, y = _binary_data(25000, seed=14, nan_frac=0.03)
+    rng = np.random.default_rng(15)
+    bag = np.sort(rng.choice(len(y), 18000, replace=False)).astype(np.uint32)
+    mask = (rng.random(X.shape[1]) < 0.7).astype(np.uint8)
+    params = {"objective": "regression", "num_leaves": 127}
+    gt, ot, *_ = _tree_pair(lgb, orc, X, rng.standard_normal(len(y)).astype(np.float32), params, bag=bag, mask=mask)
+    assert_same_tree(gt, ot)
+    assert set(gt["split_feature"]) <= set(np.nonzero(mask)[0])
+
+
+def test_single_tree_monotone(lgb, orc):
+    X, y = _binary_data(20000, seed=16)
+    mono = [1, -1, 0, 0] + [0] * 24
+    params = {"objective": "binary", "num_leaves": 31, "monotone_constraints": mono, "monotone_penalty": 0.5}
+    ds = binned_dataset(lgb, X, y, params)
+    b = ds.binned()
+    p = lgb.resolve_params(params)
+    g, h = orc.gradients(p, y, np.zeros(len(y)))
+    learner = lgb.Learner(ds, params)
+    gt = learner.train(g, h)[0]
+    ot = orc.train_trees(p, b, g, h, monotone=mono).trees[0]
+    assert_same_tree(gt, ot)
+
+
+@pytest.mark.parametrize("renew", [False, True])
+def test_single_tree_quantized_exact(lgb, orc, renew):
+    X, y = _binary_data(40000, seed=17)
+    params = {"objective": "binary", "num_leaves": 127, "use_quantized_grad": True, "num_threads": 16,
+              "quant_train_renew_leaf": renew}
+    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
+    if renew:  # leaf outputs re-fit from FP64 gradient sums (summation order differs)
+        assert_same_tree(gt, ot, leaf_rtol=1e-12)
+    else:
+        assert_same_tree(gt, ot, leaf_rtol=0.0, gain_rtol=0.0)
+
+
+def test_multiclass_slots_in_lockstep(lgb, orc):
+    rng = np.random.default_rng(18)
+    n = 15000
+    X = rng.standard_normal((n, 10)).astype(np.float32)
+    y = np.argmax(X[:, :3] + 0.5 * rng.standard_normal((n, 3)), axis=1).astype(np.float32)
+    params = {"objective": "multiclass", "num_class": 3, "num_leaves": 31}
+    ds = binned_dataset(lgb, X, y, params)
+    b = ds.binned()
+    p = lgb.resolve_params(params)
+    scores = rng.standard_normal(3 * n) * 0.3
+    g, h = orc.gradients(p, y, scores)
+    learner = lgb.Learner(ds, params, num_tree_slots=3)
+    gts = learner.train(g, h)
+    om = orc.train_trees(p, b, g, h, num_trees=3)
+    for k in range(3):
+        assert_same_tree(gts[k], om.trees[k])
+
+
+def test_gradients(lgb, orc):
+    rng = np.random.default_rng(19)
+    n = 100000
+    s = rng.standard_normal(n) * 3
+    yb = (rng.random(n) < 0.4).astype(np.float32)
+    for params, y, sc in (({"objective": "binary"}, yb, s), ({"objective": "regression"}, rng.standard_normal(n), s),
+                          ({"objective": "multiclass", "num_class": 4}, rng.integers(0, 4, n).astype(np.float32),
+                           rng.standard_normal(4 * n))):
+        p = lgb.resolve_params(params)
+        g, h = lgb.gradients(params, y, sc)
+        og, oh = orc.gradients(p, y, sc)
+        # exp is not correctly rounded on either side: allow one f32 ulp
+        for a, o in ((g, og), (h, oh)):
+            ulps = np.abs(a.view(np.int32).astype(np.int64) - o.view(np.int32).astype(np.int64))
+            assert ulps.max() <= 1, (params, ulps.max())
+            assert np.mean(ulps == 0) > 0.99
+
+
+def test_boosting_matches_oracle(lgb, orc):
+    X, y = _binary_data(12000, seed=20)
+    Xv, yv = _binary_data(3000, seed=21)
+    params = {"objective": "binary", "num_leaves": 31, "learning_rate": 0.1, "min_data_in_leaf": 20}
+    rounds = 30
+    ds = lgb.Dataset(X, y, params=params)
+    dv = lgb.Dataset(Xv, yv, params=params, reference=ds)
+    bst = lgb.train(params, ds, rounds, valid_sets=[dv])
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, rounds, valid_binned=dv.binned())
+    assert bst.num_trees() == len(om.trees)
+    same = 0
+    for a, o in zip(bst.trees, om.trees):
+        if not (np.array_equal(a["split_feature"], o["split_feature"])
+                and np.array_equal(a["threshold_in_bin"], o["threshold_in_bin"])):
+            break
+        np.testing.assert_allclose(a["leaf_value"], o["leaf_value"], rtol=1e-7, atol=1e-12)
+        same += 1
+    assert same >= 10, same
+    auc_g = orc.auc(yv, bst.scores(valid=True)[0])
+    auc_o = orc.auc(yv, om.scores(valid=True)[0])
+    assert abs(auc_g - auc_o) < 1e-4
+    # batched prediction of the GPU model on raw features equals its binned valid scores
+    raw = bst.predict(Xv, raw_score=True)
+    np.testing.assert_allclose(raw, bst.scores(valid=True)[0], rtol=1e-12, atol=1e-12)
+
+
+def test_predict_matches_oracle(lgb, orc):
+    X, y = _binary_data(8000, seed=22, nan_frac=0.05)
+    params = {"objective": "binary", "num_leaves": 15}
+    ds = lgb.Dataset(X, y, params=params)
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, 20)
+    bst = lgb.Booster(params)
+    bst.trees = [dict(t, leaf_parent=np.zeros(t["num_leaves"], np.int32),
+                      cat_boundaries_inner=np.zeros(1, np.int32), cat_threshold_inner=np.zeros(0, np.uint32))
+                 for t in om.trees]
+    Xt, _ = _binary_data(5000, seed=23, nan_frac=0.05)
+    got = bst.predict(Xt, raw_score=True)
+    want = om.predict_raw(Xt)[:, 0]
+    assert np.array_equal(got, want)
