@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 tree-learning path on the binary 10M-row workload.
+
+Workload (seeded synthetic data, no public dataset): binary objective,
+10,000,000 train + 1,000,000 held-out rows x 28 features (21 N(0,1) + 7
+heavy-tailed products / ratios), max_bin 255, 255 leaves, learning rate 0.1,
+500 rounds. A step is one boosting iteration (gradients, one tree grown on
+the device, score updates of the training and held-out rows).
+
+The line reports seconds per 500 rounds of the headline form (quantized
+int8 gradients with int16/int32 histograms), the held-out AUC after 500
+rounds of every form (FP64, FP32-compensated, quantized), the histogram
+kernel's achieved HBM bandwidth against the measured peak, an end-to-end
+figure through the C ABI with pinned host buffers, and the CPU oracle timed
+on the host's cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lightgbm-rust_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), max_bin 255, 255 leaves, lr 0.1, 500 rounds"
+METRIC = "s per 500 rounds (quantized hist, equal AUC to FP64) + hist GB/s"
+ROUNDS = 500
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _auc(y, s):
+    """AUC with tied scores sharing credit (metric.rs:701-731)."""
+    order = np.argsort(-s, kind="mergesort")
+    y = y[order]
+    s = s[order]
+    pos = (y > 0).astype(np.float64)
+    neg = 1.0 - pos
+    starts = np.r_[0, np.nonzero(np.diff(s))[0] + 1]
+    cp = np.add.reduceat(pos, starts)
+    cn = np.add.reduceat(neg, starts)
+    before = np.cumsum(cp) - cp
+    acc = float(np.sum(cn * (cp * 0.5 + before)))
+    tp = float(pos.sum())
+    return acc / (tp * (len(s) - tp)) if 0 < tp < len(s) else 1.0
+
+
+def _barrier():
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+def _max_over_ranks(v):
+    import torch
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return v
+
+
+def hist_bytes_per_row(nf, form):
+    """Algorithmic bytes one histogram row costs: its bin row, its gradient
+    pair (8 B f32 g/h, or the 4 B packed quantized pair) and its u32 row index."""
+    return nf * 1 + (4 if form == "quantized" else 8) + 4
+
+
+def run_form(lgb, data, ds, dv, form, args, device):
+    params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8,
+                  use_cuda_graph=True)
+    bst = lgb.Booster(params, ds, dv)
+    L = bst.learner
+    for _ in range(args.warmup):
+        bst.update()
+    _barrier()
+    L.record(0)
+    clocks = Clocks(device)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        bst.update()
+    L.record(1)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ms = L.elapsed(0, 1) / args.steps
+    # histogram kernel timing over the same number of steps, events around every launch
+    L.set_timing(True)
+    hist_ms = scan_ms = part_ms = 0.0
+    rows = 0
+    launches = 0
+    for _ in range(args.steps):
+        bst.update()
+        t, r, nl = L.last_timing()
+        hist_ms += t[0]
+        scan_ms += t[1]
+        part_ms += t[2]
+        rows += r
+        launches = nl
+    L.set_timing(False)
+    done = args.warmup + 2 * args.steps
+    for _ in range(max(0, args.rounds - done)):
+        if bst.update():
+            break
+    auc = _auc(data["y_valid"], bst.scores(valid=True)[0])
+    nf = ds.binned()["num_features"]
+    hist_launches = args.steps * (int(params["num_leaves"]) - 1)
+    hist_bytes = rows * hist_bytes_per_row(nf, form)
+    return {
+        "ms_per_step": ms, "wall_ms_per_step": 1000 * wall / args.steps, "s_per_500": ms * ROUNDS / 1000.0,
+        "auc": auc, "hist_ms_per_launch": hist_ms / hist_launches, "hist_gbs": hist_bytes / (hist_ms / 1000) / 1e9,
+        "hist_bytes_per_launch": hist_bytes / hist_launches, "hist_rows_per_tree": rows / args.steps,
+        "scan_ms_per_step": scan_ms / args.steps, "partition_ms_per_step": part_ms / args.steps,
+        "hist_ms_per_step": hist_ms / args.steps, "kernel_launches_per_tree": launches, "clocks": clk,
+        "num_trees": bst.num_trees(), "nf": nf,
+    }
+
+
+def run_e2e(lgb, data, ds, form, args, device):
+    """The drop-in call sequence with host buffers: RowObjective::gradients,
+    SerialTreeLearner::train and add_leaf_outputs through the C ABI, with
+    pinned host memory and every host<->device copy inside the timed region."""
+    import ctypes as C
+
+    import torch
+
+    from lgbm_b200 import _lib as LL
+    from lgbm_b200.basic import objective_config, resolve_params
+
+    params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8)
+    p = resolve_params(params)
+    learner = lgb.Learner(ds, params)
+    n = len(data["y"])
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+    label = pin(n, torch.float32)
+    label[:] = data["y"]
+    score = pin(n, torch.float64)
+    pavg = min(max(float(np.mean(data["y"] > 0)), 1e-15), 1 - 1e-15)
+    score[:] = np.log(pavg / (1 - pavg))
+    g = pin(n, torch.float32)
+    h = pin(n, torch.float32)
+    oc = objective_config(p)
+    lr = float(p["learning_rate"])
+
+    def step():
+        LL.check(LL.lib().lgbm_b200_gradients(C.byref(oc), label.ctypes.data, score.ctypes.data, n, None, 0,
+                                              g.ctypes.data, h.ctypes.data, LL.HOST, device))
+        t = learner.train(g, h)[0]
+        lv = np.where(np.abs(t["leaf_value"] * lr) <= np.float32(1e-35), 0.0, t["leaf_value"] * lr)
+        learner.add_leaf_outputs(0, lv, score)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    ms = 1000 * (time.perf_counter() - t0) / args.steps
+    return {"value": ms * ROUNDS / 1000.0, "unit": "s/500 rounds", "ms_per_step": ms,
+            # gradients: label + scores in, g/h out; train: g/h in; add_leaf_outputs: scores in and out
+            "h2d_bytes_per_step": n * (4 + 8) + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
+
+
+def run_cpu_baseline(lgb, form, sample_scale, iters):
+    """The oracle (the reference's CPU learner restated) on the host cores, on
+    a bounded sample of the workload; seconds per 500 rounds scaled to the
+    full row count."""
+    from lgbm_b200 import synthetic
+    from oracle import oracle as orc
+
+    d = synthetic.make(2, scale=sample_scale)
+    threads = os.cpu_count() or 8
+    params = dict(d["params"], hist_precision=form, num_threads=threads)
+    p = lgb.resolve_params(params)
+    ds = lgb.Dataset(d["X"], d["y"], params=params)
+    b = ds.binned()
+    t0 = time.perf_counter()
+    orc.train(p, b, d["y"], 1)
+    t1 = time.perf_counter()
+    orc.train(p, b, d["y"], 1 + iters)
+    t2 = time.perf_counter()
+    per_iter = ((t2 - t1) - (t1 - t0)) / iters
+    per_iter = max(per_iter, (t2 - t1) / (1 + iters))
+    rows = len(d["y"])
+    scale = 10_000_000 / rows
+    return {"value": per_iter * scale * ROUNDS, "unit": "s/500 rounds", "cores": threads, "kind": "port",
+            "sample": f"{rows} rows of the same generator, {iters} timed iterations ({form} form, "
+                      f"{threads} threads), per-iteration time scaled by {scale:.0f}x rows and x{ROUNDS} rounds"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--forms", default="quantized,f32c,f64")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--rounds", type=int, default=ROUNDS, help="rounds trained per form (AUC after these)")
+    ap.add_argument("--param", action="append", default=[], help="extra training parameter k=v (launch-shape sweeps)")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import lgbm_b200 as lgb
+
+        sample = 0.1 * args.scale
+        iters = max(1, min(args.steps, 3))
+        t0 = time.perf_counter()
+        cb = run_cpu_baseline(lgb, "quantized", sample, iters)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s/500 rounds",
+                "n_gpus": args.gpus, "steps": iters, "warmup": 1, "ms_per_step": cb["value"] / ROUNDS * 1000,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "form": "quantized",
+                                                "sample_rows": int(10_000_000 * sample)},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "s/500 rounds", "h2d_bytes_per_step": 0,
+                                             "d2h_bytes_per_step": 0},
+                "wall_s": time.perf_counter() - t0}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import lgbm_b200 as lgb
+    from lgbm_b200 import synthetic
+
+    data = synthetic.make(2, scale=args.scale)
+    for kv in args.param:
+        k, v = kv.split("=", 1)
+        try:
+            data["params"][k] = json.loads(v)
+        except ValueError:
+            data["params"][k] = v
+    forms = [f for f in args.forms.split(",") if f]
+    ds = lgb.Dataset(data["X"], data["y"], params=data["params"]).construct()
+    dv = lgb.Dataset(data["X_valid"], data["y_valid"], params=data["params"], reference=ds).construct()
+    res = {}
+    for form in forms:
+        res[form] = run_form(lgb, data, ds, dv, form, args, local_rank)
+    head = "quantized" if "quantized" in res else forms[0]
+    r = res[head]
+    ms = _max_over_ranks(r["ms_per_step"])
+    value = ms * ROUNDS / 1000.0 / world
+    e2e = None if args.no_e2e else run_e2e(lgb, data, ds, head, args, local_rank)
+    cpu = None if (args.no_cpu or rank != 0) else run_cpu_baseline(lgb, head, 0.1 * args.scale, 3)
+    peak, peak_kind = _peaks()
+    achieved = r["hist_gbs"]
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "s/500 rounds", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8" if head == "quantized" else ("f32" if head == "f32c" else "f64"),
+        "data": "synthetic (seeded generator with the workload's shapes and distributions)",
+        "config": {"workload": WORKLOAD, "form": head, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (bin matrix 320 MB, gradients 80 MB)", "rows": len(data["y"]),
+                   "held_out_rows": len(data["y_valid"])},
+        "forms": {k: {"s_per_500_rounds": v["s_per_500"], "ms_per_step": v["ms_per_step"], "auc": v["auc"],
+                      "hist_gbs": v["hist_gbs"], "hist_ms_per_step": v["hist_ms_per_step"],
+                      "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
+                      "hist_rows_per_tree": v["hist_rows_per_tree"]} for k, v in res.items()},
+        "roofline": {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]},
+        "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 5),
+        "clocks": r["clocks"],
+    }
+    if "f64" in res and head in res:
+        line["speedup_vs_f64"] = res["f64"]["ms_per_step"] / res[head]["ms_per_step"]
+        line["auc_delta_vs_f64"] = res[head]["auc"] - res["f64"]["auc"]
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -198,6 +198,10 @@ int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* l
 /* Per-kernel timing: when enabled, every split step of the next train calls
  * is bracketed by CUDA events on the learner's stream (no extra syncs). */
 int lgbm_b200_learner_set_timing(LgbmB200Learner* h, int32_t enabled);
+/* Timing marks: record event `mark` (0..15) on the learner's stream; the
+ * elapsed device time between two recorded marks, in ms. */
+int lgbm_b200_learner_record(LgbmB200Learner* h, int32_t mark);
+int lgbm_b200_learner_elapsed(LgbmB200Learner* h, int32_t a, int32_t b, double* ms);
 /* Device time of the last train call summed per kernel family, ms:
  * [histogram, scan, partition, other]; rows histogrammed; kernels launched. */
 int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_rows, int32_t* launches);

@@ -110,6 +110,8 @@ struct DSlot {
   int32_t* leaf_side;      // which idx buffer holds the leaf's rows
   int32_t* buf_of;         // histogram buffer of each leaf
   DSplit* best;            // best_split_per_leaf [num_leaves]
+  double* bgain;           // best[l].gain and best[l].feature, compact for the best-leaf argmax
+  int32_t* bfeat;
   uint8_t* splittable;     // [num_leaves][num_features]
   double* cmin;            // basic monotone constraint per leaf
   double* cmax;
@@ -127,9 +129,11 @@ struct DSlot {
 };
 
 constexpr int kRootBlocks = 296;
+constexpr int kMaxSlots = 16;  // tree slots grown together (slot structs travel as kernel parameters)
 
 struct DCtx {
   const uint8_t* bins;  // row-major, row stride `stride` bytes
+  const uint8_t* colbins;  // column-major copy [num_features x num_data]
   int64_t num_data;
   int32_t stride;
   int32_t num_features;
@@ -138,7 +142,7 @@ struct DCtx {
   int32_t bagging;     // 1 when the in-bag rows are a strict subset
   const DFeature* feats;
   DParams p;
-  DSlot* slots;
+  DSlot slots[kMaxSlots];  // by value: read from the constant bank
   int32_t num_slots;
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
 };

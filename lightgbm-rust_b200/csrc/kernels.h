@@ -8,6 +8,7 @@ namespace lgbm_b200 {
 constexpr int kHistThreads = 512;
 constexpr int kMaxTileFeatures = 256;
 constexpr int kMaxTiles = 64;
+constexpr int kMaxLaneGroups = 6;  // 32-feature groups per histogram tile (int32 cells)
 
 // Feature tiles of a histogram launch (blockIdx.y): tile k covers features
 // [f0[k], f0[k+1]) whose stored bins are [bin0[k], bin0[k+1]).
@@ -26,18 +27,18 @@ struct ScanSmem {
   double key[kMaxBins];
 };
 
-__global__ void k_tree_init(DCtx c, const uint32_t* bag, const int32_t* n_used);
+__global__ void k_tree_init(const __grid_constant__ DCtx c, const uint32_t* bag, const int32_t* n_used);
 template <int kMode>
-__global__ void k_hist_float(DCtx c, DTileTable tt);
-__global__ void k_hist_int(DCtx c, DTileTable tt, int32_t sub_rows);
+__global__ void k_hist_lane(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows);
 template <bool kInt>
-__global__ void k_scan(DCtx c);
-__global__ void k_partition(DCtx c);
-__global__ void k_leaf_sums(DCtx c, double* sums);
-__global__ void k_leaf_renew(DCtx c, const double* sums);
-__global__ void k_add_leaf_outputs(DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
+__global__ void k_scan(const __grid_constant__ DCtx c);
+__global__ void k_partition(const __grid_constant__ DCtx c);
+__global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
+__global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* sums);
+__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums);
+__global__ void k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
                                    int64_t score_stride);
-__global__ void k_add_tree_binned(DCtx c, const uint8_t* bins, int32_t stride, const uint32_t* rows, int64_t n,
+__global__ void k_add_tree_binned(const __grid_constant__ DCtx c, const uint8_t* bins, int32_t stride, const uint32_t* rows, int64_t n,
                                   const double* leaf_values, int32_t lv_stride, double* score, int64_t score_stride);
 
 // objective_kernels.cu

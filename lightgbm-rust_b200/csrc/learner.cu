@@ -38,8 +38,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   h->n = n;
   h->nf = nf;
   h->K = std::max(1, cfg->num_tree_slots);
+  if (h->K > kMaxSlots) return Status(LGBM_B200_ERR_UNSUPPORTED, "more than 16 trees grown together");
   h->L = std::max(2, cfg->num_leaves);
-  h->stride = (nf + 15) / 16 * 16;
+  h->stride = (nf + 31) / 32 * 32;
   // features and histogram layout
   int32_t pos = 0;
   h->feats.resize(nf);
@@ -67,37 +68,24 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   h->total_bins = pos;
   bool use_monotone = false;
   for (auto& f : h->feats) use_monotone |= f.monotone_type != 0;
-  // feature tiles: each tile's shared histogram fits the budget
+  // feature tiles: groups of 32 features (lane l of a warp owns feature
+  // f0 + 32g + l); int32 cells allow up to kMaxLaneGroups groups per tile,
+  // FP64 / FP32-pair cells (16 bytes) one group
   const int mode = cfg->hist_precision;
   if (mode < 0 || mode > 2) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "hist_precision");
   const size_t cell = mode == LGBM_B200_HIST_QUANT ? 4 : 16;
-  const size_t budget = mode == LGBM_B200_HIST_QUANT ? 96 * 1024 : 200 * 1024;
-  h->ntiles = 0;
-  h->tiles.f0[0] = 0;
-  h->tiles.bin0[0] = 0;
+  const int groups_per_tile = mode == LGBM_B200_HIST_QUANT ? kMaxLaneGroups : 1;
   {
-    int32_t cur_bins = 0, cur_f = 0;
-    for (int32_t f = 0; f < nf; ++f) {
-      int32_t vl = h->feats[f].view_len;
-      // tiles start at a multiple of 4 features: the kernels load 4 stored bins per 32-bit word
-      if (cur_f > 0 && (f % 4) == 0 &&
-          ((size_t)(cur_bins + 4 * kMaxBins) * cell > budget || cur_f + 4 > kMaxTileFeatures)) {
-        h->ntiles++;
-        if (h->ntiles >= kMaxTiles) return Status(LGBM_B200_ERR_UNSUPPORTED, "too many histogram feature tiles");
-        h->tiles.f0[h->ntiles] = f;
-        h->tiles.bin0[h->ntiles] = h->feats[f].view_start;
-        cur_bins = 0;
-        cur_f = 0;
-      }
-      cur_bins += vl;
-      cur_f += 1;
+    const int ngroups = (nf + 31) / 32;
+    h->ntiles = (ngroups + groups_per_tile - 1) / groups_per_tile;
+    if (h->ntiles > kMaxTiles) return Status(LGBM_B200_ERR_UNSUPPORTED, "too many histogram feature tiles");
+    for (int t = 0; t <= h->ntiles; ++t) {
+      int f = std::min(nf, t * groups_per_tile * 32);
+      h->tiles.f0[t] = f;
+      h->tiles.bin0[t] = f < nf ? h->feats[f].view_start : h->total_bins;
     }
-    h->ntiles++;
-    h->tiles.f0[h->ntiles] = nf;
-    h->tiles.bin0[h->ntiles] = h->total_bins;
-    size_t maxbins = 0;
-    for (int t = 0; t < h->ntiles; ++t) maxbins = std::max(maxbins, (size_t)(h->tiles.bin0[t + 1] - h->tiles.bin0[t]));
-    h->hist_smem = maxbins * cell;
+    int max_groups = std::min(ngroups, groups_per_tile);
+    h->hist_smem = (size_t)max_groups * kMaxBins * 32 * cell;
   }
   if (mode == LGBM_B200_HIST_QUANT) {
     int32_t half = std::max(1, cfg->num_grad_quant_bins / 2);
@@ -108,21 +96,21 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   // kernel attributes and grid sizes
   if (mode == LGBM_B200_HIST_F64)
-    CU(cudaFuncSetAttribute(k_hist_float<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+    CU(cudaFuncSetAttribute(k_hist_lane<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
   else if (mode == LGBM_B200_HIST_F32C)
-    CU(cudaFuncSetAttribute(k_hist_float<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+    CU(cudaFuncSetAttribute(k_hist_lane<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
   else
-    CU(cudaFuncSetAttribute(k_hist_int, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+    CU(cudaFuncSetAttribute(k_hist_lane<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
   h->scan_smem = 2 * sizeof(ScanSmem);
   CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   int per_sm = 1;
   if (mode == LGBM_B200_HIST_F64)
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_float<0>, kHistThreads, h->hist_smem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<0>, kHistThreads, h->hist_smem));
   else if (mode == LGBM_B200_HIST_F32C)
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_float<1>, kHistThreads, h->hist_smem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<1>, kHistThreads, h->hist_smem));
   else
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_int, kHistThreads, h->hist_smem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<2>, kHistThreads, h->hist_smem));
   per_sm = std::max(1, per_sm);
   h->hist_grid = std::max(1, h->num_sms * per_sm / std::max(1, h->ntiles));
   h->part_grid = h->num_sms * 4;
@@ -139,6 +127,11 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     for (int64_t r = 0; r < n; ++r) std::memcpy(&padded[(size_t)r * h->stride], bins + (size_t)r * nf, (size_t)nf);
     CU(cudaMemcpy(bins_d, padded.data(), padded.size(), cudaMemcpyHostToDevice));
   }
+  uint8_t* colbins_d;
+  if (!(s = A.alloc_n(&colbins_d, (size_t)n * nf)).ok()) return s;
+  k_transpose_bins<<<h->num_sms * 8, 256>>>(bins_d, n, h->stride, nf, colbins_d);
+  CU(cudaGetLastError());
+  CU(cudaDeviceSynchronize());
   DFeature* feats_d;
   if (!(s = A.alloc_n(&feats_d, (size_t)nf)).ok()) return s;
   CU(cudaMemcpy(feats_d, h->feats.data(), sizeof(DFeature) * nf, cudaMemcpyHostToDevice));
@@ -159,6 +152,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     ALLOC(d.leaf_side, L);
     ALLOC(d.buf_of, L);
     ALLOC(d.best, L);
+    ALLOC(d.bgain, L);
+    ALLOC(d.bfeat, L);
     ALLOC(d.splittable, (size_t)L * nf);
     ALLOC(d.cmin, L);
     ALLOC(d.cmax, L);
@@ -201,9 +196,6 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   if (!(s = A.alloc_n(&h->gh_all, (size_t)K * n)).ok()) return s;
   for (int k = 0; k < K; ++k) h->slots_h[k].gh = h->gh_all + (size_t)k * n;
-  DSlot* slots_d;
-  if (!(s = A.alloc_n(&slots_d, (size_t)K)).ok()) return s;
-  CU(cudaMemcpy(slots_d, h->slots_h.data(), sizeof(DSlot) * K, cudaMemcpyHostToDevice));
   if (!(s = A.alloc_n(&h->bag, (size_t)n)).ok()) return s;
   if (!(s = A.alloc_n(&h->n_used_dev, 1)).ok()) return s;
   {
@@ -244,6 +236,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   // context
   DCtx& c = h->ctx;
   c.bins = bins_d;
+  c.colbins = colbins_d;
   c.num_data = n;
   c.stride = h->stride;
   c.num_features = nf;
@@ -268,7 +261,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   p.max_depth = cfg->max_depth;
   p.monotone_penalty = cfg->monotone_penalty;
   p.use_monotone = use_monotone ? 1 : 0;
-  c.slots = slots_d;
+  for (int k = 0; k < K; ++k) c.slots[k] = h->slots_h[k];
   c.num_slots = K;
   c.rows_per_block = rpb;
   h->n_used = (int32_t)n;
@@ -280,6 +273,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     CU(cudaEventCreate(&e));
     h->ev.push_back(e);
   }
+  for (int i = 0; i < 16; ++i) CU(cudaEventCreate(&h->marks[i]));
   return Status();
 }
 
@@ -298,22 +292,22 @@ static Status enqueue_tree(LgbmB200Learner* h) {
   dim3 part_grid(h->part_grid, 1, K);
   for (int step = 0; step < L - 1; ++step) {
     cudaEvent_t* ev = h->timing ? &h->ev[(size_t)4 * step] : nullptr;
-    if (ev) CU(cudaEventRecord(ev[0], s));
+    if (ev) CU(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal));
     if (mode == LGBM_B200_HIST_F64)
-      k_hist_float<0><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+      k_hist_lane<0><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
     else if (mode == LGBM_B200_HIST_F32C)
-      k_hist_float<1><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
+      k_hist_lane<1><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
     else
-      k_hist_int<<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+      k_hist_lane<2><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
     CU_LAUNCH();
-    if (ev) CU(cudaEventRecord(ev[1], s));
+    if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
     if (mode == LGBM_B200_HIST_QUANT) k_scan<true><<<scan_grid, 64, h->scan_smem, s>>>(c);
     else k_scan<false><<<scan_grid, 64, h->scan_smem, s>>>(c);
     CU_LAUNCH();
-    if (ev) CU(cudaEventRecord(ev[2], s));
+    if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
     k_partition<<<part_grid, 256, 0, s>>>(c);
     CU_LAUNCH();
-    if (ev) CU(cudaEventRecord(ev[3], s));
+    if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
     CU(cudaMemsetAsync(h->leaf_sums, 0, sizeof(double) * K * L * 2, s));
@@ -328,8 +322,8 @@ static Status enqueue_tree(LgbmB200Learner* h) {
 
 static Status run_tree(LgbmB200Learner* h) {
   cudaStream_t s = h->stream;
-  const bool graph = h->cfg.use_cuda_graph != 0 && !h->timing;
-  const int key = (h->bagging ? 1 : 0) + 2 * h->ctx.bagging;
+  const bool graph = h->cfg.use_cuda_graph != 0;
+  const int key = (h->bagging ? 1 : 0) + 2 * h->ctx.bagging + 4 * (h->timing ? 1 : 0);
   if (!graph) return enqueue_tree(h);
   if (h->graph_exec == nullptr || h->graph_key != key) {
     if (h->graph_exec) {
@@ -523,11 +517,12 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   CU(cudaMemsetAsync(d.hist, 0, cells * 8, s));
   // one slot only: a context whose slot array starts at `slot`
   DCtx c = h->ctx;
-  c.slots = h->ctx.slots + slot;
+  c.slots[0] = h->ctx.slots[slot];
   dim3 grid(h->hist_grid, h->ntiles, 1);
-  if (mode == LGBM_B200_HIST_F64) k_hist_float<0><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
-  else if (mode == LGBM_B200_HIST_F32C) k_hist_float<1><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles);
-  else k_hist_int<<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+  if (mode == LGBM_B200_HIST_F64) k_hist_lane<0><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+  else if (mode == LGBM_B200_HIST_F32C)
+    k_hist_lane<1><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+  else k_hist_lane<2><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
   CU_LAUNCH();
   CU(cudaMemcpyAsync(out, d.hist, cells * 8, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
@@ -670,7 +665,7 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   // launch only over this slot: grid.z = 1 with a context whose slots start at `slot`
   DCtx c = h->ctx;
-  c.slots = h->ctx.slots + slot;
+  c.slots[0] = h->ctx.slots[slot];
   k_add_leaf_outputs<<<dim3(std::max(1, h->num_sms * 4 / L + 1), L, 1), 256, 0, s>>>(c, lvd, 0, sc, 0);
   e = cudaGetLastError();
   if (e == cudaSuccess && tmp) {
@@ -740,6 +735,25 @@ int lgbm_b200_learner_quantized(LgbmB200Learner* h, int32_t slot, int64_t* packe
     scales[0] = ss.grad_scale;
     scales[1] = ss.hess_scale;
   }
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_record(LgbmB200Learner* h, int32_t mark) {
+  if (!h || mark < 0 || mark >= 16) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "mark"));
+  cudaSetDevice(h->device);
+  cudaError_t e = cudaEventRecord(h->marks[mark], h->stream);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_elapsed(LgbmB200Learner* h, int32_t a, int32_t b, double* ms) {
+  if (!h || a < 0 || a >= 16 || b < 0 || b >= 16 || !ms) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "mark"));
+  cudaSetDevice(h->device);
+  float t = 0.f;
+  cudaError_t e = cudaEventSynchronize(h->marks[b]);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, h->marks[a], h->marks[b]);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  *ms = t;
   return LGBM_B200_OK;
 }
 

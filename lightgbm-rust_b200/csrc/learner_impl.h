@@ -221,6 +221,7 @@ struct LgbmB200Learner {
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> ev;
+  cudaEvent_t marks[16] = {};  // caller-placed timing marks on the learner's stream
   double last_ms[4] = {0, 0, 0, 0};
   int64_t last_hist_rows = 0;
   int32_t last_launches = 0;
@@ -230,6 +231,8 @@ struct LgbmB200Learner {
   ~LgbmB200Learner() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto e : ev) cudaEventDestroy(e);
+    for (auto e : marks)
+      if (e) cudaEventDestroy(e);
     arena.free_all();
     if (stream) cudaStreamDestroy(stream);
   }

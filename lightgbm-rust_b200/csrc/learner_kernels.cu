@@ -15,6 +15,7 @@
 //                (partition.rs:107-174, learner/mod.rs:1200-1208, :712-731)
 #include "device_common.cuh"
 #include "kernels.h"
+#include "scan_warp.cuh"
 
 namespace lgbm_b200 {
 
@@ -31,11 +32,15 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
   return v;
 }
 
-__device__ bool before_find_best_split(const DCtx& c, DSlot& s, int32_t left, int32_t right) {
+__device__ bool before_find_best_split(const DCtx& c, const DSlot& s, int32_t left, int32_t right) {
   const DParams& p = c.p;
   if (p.max_depth > 0 && s.tree.leaf_depth[left] >= p.max_depth) {
     s.best[left].gain = -INFINITY;
-    if (right >= 0) s.best[right].gain = -INFINITY;
+    s.bgain[left] = -INFINITY;
+    if (right >= 0) {
+      s.best[right].gain = -INFINITY;
+      s.bgain[right] = -INFINITY;
+    }
     return false;
   }
   int32_t nl = left >= 0 ? s.leaf_count[left] : 0;
@@ -43,15 +48,19 @@ __device__ bool before_find_best_split(const DCtx& c, DSlot& s, int32_t left, in
   int32_t min2 = p.min_data_in_leaf * 2;
   if (nr < min2 && nl < min2) {
     s.best[left].gain = -INFINITY;
-    if (right >= 0) s.best[right].gain = -INFINITY;
+    s.bgain[left] = -INFINITY;
+    if (right >= 0) {
+      s.best[right].gain = -INFINITY;
+      s.bgain[right] = -INFINITY;
+    }
     return false;
   }
   return true;
 }
 
 // Grid (kRootBlocks, 1, slots), 256 threads.
-__global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, const int32_t* n_used) {
-  DSlot& s = c.slots[blockIdx.z];
+__global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx c, const uint32_t* bag, const int32_t* n_used) {
+  const DSlot& s = c.slots[blockIdx.z];
   const int64_t n = *n_used;
   const int tid = threadIdx.x;
   // positions -> rows (identity, or the in-bag rows)
@@ -126,6 +135,8 @@ __global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, 
     s.best[l].feature = -1;
     s.best[l].inner = -1;
     s.best[l].gain = -INFINITY;
+    s.bgain[l] = -INFINITY;
+    s.bfeat[l] = -1;
     s.cmin[l] = -1.7976931348623157e308;
     s.cmax[l] = 1.7976931348623157e308;
     s.buf_of[l] = l;
@@ -162,7 +173,7 @@ __global__ void __launch_bounds__(256) k_tree_init(DCtx c, const uint32_t* bag, 
   st->larger.num_data = 0;
   st->left_leaf = 0;
   st->right_leaf = -1;
-  DTree& t = s.tree;
+  const DTree& t = s.tree;
   t.leaf_parent[0] = -1;
   t.leaf_value[0] = maybe_round_to_zero(root_output(a, b, p, (int32_t)n));
   t.leaf_weight[0] = 0.0;
@@ -179,7 +190,7 @@ struct LeafRows {
   int64_t begin, count;
 };
 
-__device__ __forceinline__ bool hist_setup(const DCtx& c, DSlot& s, LeafRows& lr, int64_t& r0, int64_t& r1) {
+__device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, LeafRows& lr, int64_t& r0, int64_t& r1) {
   DSlotState* st = s.st;
   if (st->done || !st->need_find) return false;
   int32_t leaf = st->smaller.leaf;
@@ -204,147 +215,169 @@ __device__ __forceinline__ void tile_of(const DTileTable& tt, int tile, int& f0,
   nbins = tt.bin0[tile + 1] - bin0;
 }
 
-// FP64 (kMode 0) and FP32-compensated (kMode 1) histograms: each thread takes
-// (row, 4-feature word) units; shared-memory atomics, then one global merge.
+// Histogram of the smaller leaf's rows over one feature tile, in a bin-major
+// shared layout: feature f0 + 32g + lane keeps its cell of stored value `raw`
+// at cells[g][raw][lane], so in every warp-wide atomic the 32 lanes touch 32
+// different banks. A warp walks its rows 32 at a time: lane l loads row
+// index and gradient of row l, then every row is broadcast by shuffle and
+// each lane adds it into its own feature's cell.
+//   kMode 0: FP64 g / h cells (the reference's sums, reordered by atomics)
+//   kMode 1: FP32 (hi, lo) pairs per value, the rounding error of every
+//            add kept in lo (TwoSum), merged in FP64 when flushed
+//   kMode 2: int32 cells holding (g << 16) + h of quantized gradients,
+//            flushed every `sub_rows` rows into packed int64 sums
 template <int kMode>
-__global__ void __launch_bounds__(kHistThreads) k_hist_float(DCtx c, DTileTable tt) {
+__global__ void __launch_bounds__(kHistThreads) k_hist_lane(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  DSlot& s = c.slots[blockIdx.z];
+  const DSlot& s = c.slots[blockIdx.z];
   LeafRows lr;
   int64_t r0, r1;
   if (!hist_setup(c, s, lr, r0, r1)) return;
   int f0, f1, bin0, nbins;
   tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
-  __shared__ int32_t vstart[kMaxTileFeatures];
-  __shared__ uint32_t vlen[kMaxTileFeatures];
-  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
-    vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
-    vlen[f - f0] = (uint32_t)c.feats[f].view_len;
-  }
-  // kMode 0: double2 (g, h) per bin; kMode 1: float4 (g_hi, g_lo, h_hi, h_lo)
-  if (kMode == 0) {
-    double2* sh = reinterpret_cast<double2*>(smem_raw);
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = make_double2(0.0, 0.0);
-  } else {
-    float4* sh = reinterpret_cast<float4*>(smem_raw);
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  __syncthreads();
-  const int nfeat = f1 - f0;
-  const int wpr = (nfeat + 3) >> 2;  // 4-byte words per row in this tile
-  const int64_t units = (r1 - r0) * wpr;
-  const uint32_t* idx = lr.idx + lr.begin;
-  const float2* gh = s.gh;  // interleaved (g, h)
-  for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
-    int64_t pos = r0 + u / wpr;
-    int w = (int)(u % wpr);
-    uint32_t row = idx[pos];
-    float2 v = gh[row];
-    uint32_t word = *reinterpret_cast<const uint32_t*>(c.bins + (size_t)row * c.stride + f0 + 4 * w);
+  (void)nbins;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int ngroups = (f1 - f0 + 31) >> 5;
+  constexpr int kCellWords = kMode == 2 ? 1 : (kMode == 0 ? 4 : 4);  // 32-bit words per cell
+  const int group_cells = kMaxBins * 32;
+  // per-lane feature facts for each group
+  int32_t vlen_g[kMaxLaneGroups], vstart_g[kMaxLaneGroups];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      int fl = 4 * w + k;
-      uint32_t raw = (word >> (8 * k)) & 0xFFu;
-      if (fl < nfeat && raw != 0u && raw <= vlen[fl]) {
-        int b = vstart[fl] + (int)raw;
-        if (kMode == 0) {
-          double2* sh = reinterpret_cast<double2*>(smem_raw);
-          atomicAdd(&sh[b].x, (double)v.x);
-          atomicAdd(&sh[b].y, (double)v.y);
+  for (int g = 0; g < kMaxLaneGroups; ++g) {
+    int f = f0 + 32 * g + lane;
+    bool ok = g < ngroups && f < f1;
+    vlen_g[g] = ok ? c.feats[f].view_len : 0;
+    vstart_g[g] = ok ? c.feats[f].view_start : 0;
+  }
+  uint32_t* cells = reinterpret_cast<uint32_t*>(smem_raw);
+  const int total_words = ngroups * group_cells * kCellWords;
+  for (int i = threadIdx.x; i < total_words; i += blockDim.x) cells[i] = 0u;
+  __syncthreads();
+  const uint32_t* idx = lr.idx + lr.begin;
+  const uint8_t* bins = c.bins + f0 + lane;
+  const size_t stride = (size_t)c.stride;
+  double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
+  unsigned long long* outi = reinterpret_cast<unsigned long long*>(s.hist) +
+                             (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
+  // Flush the tile's cells into the leaf histogram (cells of stored value 0,
+  // the most frequent bin, are outside every feature view). Thread t always
+  // handles lane (t % 32) of a row, i.e. its own feature of each group.
+  auto flush = [&]() {
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < kMaxLaneGroups; ++g) {
+      if (g >= ngroups) break;
+      const int vl = vlen_g[g];
+      const size_t vs = (size_t)vstart_g[g];
+      for (int raw = 1 + warp; raw <= vl; raw += nwarps) {
+        const int k = raw * 32 + lane;
+        const size_t dst = vs + raw - 1;
+        if (kMode == 2) {
+          int32_t* ic = reinterpret_cast<int32_t*>(cells) + g * group_cells;
+          int32_t cell = ic[k];
+          if (cell != 0) {
+            int64_t hq = (int64_t)(cell & 0xFFFF);
+            int64_t gq = (int64_t)((cell - (int32_t)hq) >> 16);
+            atomicAdd(outi + dst, (unsigned long long)((uint64_t)(gq << 32) + (uint64_t)hq));
+            ic[k] = 0;
+          }
         } else {
-          float4* sh = reinterpret_cast<float4*>(smem_raw);
-          // TwoSum of the value the atomic replaced and the addend: the
-          // rounding error goes to the low word.
-          float og = atomicAdd(&sh[b].x, v.x);
-          float sg = __fadd_rn(og, v.x);
-          float bg = __fsub_rn(sg, og);
-          float eg = __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(v.x, bg));
-          atomicAdd(&sh[b].y, eg);
-          float oh = atomicAdd(&sh[b].z, v.y);
-          float sh2 = __fadd_rn(oh, v.y);
-          float bh = __fsub_rn(sh2, oh);
-          float eh = __fadd_rn(__fsub_rn(oh, __fsub_rn(sh2, bh)), __fsub_rn(v.y, bh));
-          atomicAdd(&sh[b].w, eh);
+          const uint32_t* base = cells + g * group_cells * 4;
+          double gv, hv;
+          if (kMode == 0) {
+            const double* d = reinterpret_cast<const double*>(base);
+            gv = d[k];
+            hv = d[group_cells + k];
+          } else {
+            const float* fl = reinterpret_cast<const float*>(base);
+            gv = (double)fl[k] + (double)fl[group_cells + k];
+            hv = (double)fl[2 * group_cells + k] + (double)fl[3 * group_cells + k];
+          }
+          if (gv != 0.0 || hv != 0.0) {
+            atomicAdd(outf + 2 * dst, gv);
+            atomicAdd(outf + 2 * dst + 1, hv);
+          }
         }
       }
     }
-  }
-  __syncthreads();
-  double* out = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
-  for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
-    double g, h;
-    if (kMode == 0) {
-      double2 v = reinterpret_cast<double2*>(smem_raw)[i];
-      g = v.x;
-      h = v.y;
-    } else {
-      float4 v = reinterpret_cast<float4*>(smem_raw)[i];
-      g = (double)v.x + (double)v.y;
-      h = (double)v.z + (double)v.w;
-    }
-    if (g != 0.0 || h != 0.0) {
-      atomicAdd(out + 2 * (size_t)(bin0 + i), g);
-      atomicAdd(out + 2 * (size_t)(bin0 + i) + 1, h);
-    }
-  }
-}
-template __global__ void k_hist_float<0>(DCtx, DTileTable);
-template __global__ void k_hist_float<1>(DCtx, DTileTable);
-
-// Quantized histogram: per-row packed (g << 16) + h added into int32 shared
-// cells (int16 gradient / hessian halves), flushed every `sub_rows` rows
-// into the global packed int64 histogram (int32 halves), so no half overflows.
-__global__ void __launch_bounds__(kHistThreads) k_hist_int(DCtx c, DTileTable tt, int32_t sub_rows) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  int32_t* sh = reinterpret_cast<int32_t*>(smem_raw);
-  DSlot& s = c.slots[blockIdx.z];
-  LeafRows lr;
-  int64_t r0, r1;
-  if (!hist_setup(c, s, lr, r0, r1)) return;
-  int f0, f1, bin0, nbins;
-  tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
-  __shared__ int32_t vstart[kMaxTileFeatures];
-  __shared__ uint32_t vlen[kMaxTileFeatures];
-  for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
-    vstart[f - f0] = c.feats[f].view_start - bin0 - 1;
-    vlen[f - f0] = (uint32_t)c.feats[f].view_len;
-  }
-  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh[i] = 0;
-  __syncthreads();
-  const int nfeat = f1 - f0;
-  const int wpr = (nfeat + 3) >> 2;
-  const uint32_t* idx = lr.idx + lr.begin;
-  unsigned long long* out = reinterpret_cast<unsigned long long*>(s.hist) +
-                            (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
-  for (int64_t q0 = r0; q0 < r1; q0 += sub_rows) {
-    int64_t q1 = min(r1, q0 + sub_rows);
-    int64_t units = (q1 - q0) * wpr;
-    for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
-      int64_t pos = q0 + u / wpr;
-      int w = (int)(u % wpr);
-      uint32_t row = idx[pos];
-      int32_t v = s.packed[row];
-      uint32_t word = *reinterpret_cast<const uint32_t*>(c.bins + (size_t)row * c.stride + f0 + 4 * w);
+    __syncthreads();
+  };
+  const int64_t span = kMode == 2 ? (int64_t)sub_rows : (r1 - r0);
+  for (int64_t q0 = r0; q0 < r1; q0 += span) {
+    const int64_t q1 = min(r1, q0 + span);
+    for (int64_t p0 = q0 + (int64_t)warp * 32; p0 < q1; p0 += (int64_t)nwarps * 32) {
+      const int nrow = (int)min((int64_t)32, q1 - p0);
+      uint32_t my_row = lane < nrow ? idx[p0 + lane] : 0u;
+      int32_t my_q = 0;
+      float my_g = 0.f, my_h = 0.f;
+      if (lane < nrow) {
+        if (kMode == 2) {
+          my_q = s.packed[my_row];
+        } else {
+          float2 v = s.gh[my_row];
+          my_g = v.x;
+          my_h = v.y;
+        }
+      }
+      // 8 rows at a time: broadcast their row / gradient, load each lane's
+      // stored value of the 8 rows (independent loads), then 8 atomics. A
+      // stored value indexes cells [0, 256) of the lane's own column, so no
+      // value can address outside the tile; values past the feature's bins
+      // land in cells the flush ignores.
+      for (int j0 = 0; j0 < nrow; j0 += 8) {
+        uint32_t rr[8];
+        int32_t qv[8];
+        float gv[8], hv[8];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        int fl = 4 * w + k;
-        uint32_t raw = (word >> (8 * k)) & 0xFFu;
-        if (fl < nfeat && raw != 0u && raw <= vlen[fl]) atomicAdd(&sh[vstart[fl] + (int)raw], v);
+        for (int u = 0; u < 8; ++u) {
+          const int src = (j0 + u) & 31;
+          rr[u] = __shfl_sync(0xffffffffu, my_row, src);
+          if (kMode == 2) {
+            qv[u] = __shfl_sync(0xffffffffu, my_q, src);
+          } else {
+            gv[u] = __shfl_sync(0xffffffffu, my_g, src);
+            hv[u] = __shfl_sync(0xffffffffu, my_h, src);
+          }
+        }
+#pragma unroll
+        for (int g = 0; g < kMaxLaneGroups; ++g) {
+          if (g >= ngroups) break;
+          const bool live = vlen_g[g] > 0;
+          uint32_t raw[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            raw[u] = (live && j0 + u < nrow) ? (uint32_t)bins[(size_t)rr[u] * stride + 32 * g] : 0u;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (raw[u] == 0u) continue;
+            const int k = (int)raw[u] * 32 + lane;
+            if (kMode == 2) {
+              atomicAdd(reinterpret_cast<int32_t*>(cells) + g * group_cells + k, qv[u]);
+            } else if (kMode == 0) {
+              double* d = reinterpret_cast<double*>(cells + g * group_cells * 4);
+              atomicAdd(d + k, (double)gv[u]);
+              atomicAdd(d + group_cells + k, (double)hv[u]);
+            } else {
+              float* fl = reinterpret_cast<float*>(cells + g * group_cells * 4);
+              float og = atomicAdd(fl + k, gv[u]);
+              float sg = __fadd_rn(og, gv[u]);
+              float bg = __fsub_rn(sg, og);
+              atomicAdd(fl + group_cells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv[u], bg)));
+              float oh = atomicAdd(fl + 2 * group_cells + k, hv[u]);
+              float s2 = __fadd_rn(oh, hv[u]);
+              float bh = __fsub_rn(s2, oh);
+              atomicAdd(fl + 3 * group_cells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv[u], bh)));
+            }
+          }
+        }
       }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
-      int32_t cell = sh[i];
-      if (cell != 0) {
-        int64_t hq = (int64_t)(cell & 0xFFFF);
-        int64_t gq = (int64_t)((cell - (int32_t)hq) >> 16);
-        atomicAdd(out + bin0 + i, (unsigned long long)((uint64_t)(gq << 32) + (uint64_t)hq));
-        sh[i] = 0;
-      }
-    }
-    __syncthreads();
+    flush();
   }
 }
+template __global__ void k_hist_lane<0>(const __grid_constant__ DCtx, DTileTable, int32_t);
+template __global__ void k_hist_lane<1>(const __grid_constant__ DCtx, DTileTable, int32_t);
+template __global__ void k_hist_lane<2>(const __grid_constant__ DCtx, DTileTable, int32_t);
 
 // =====================================================================================
 // split scan (split.rs:246-891 and :930-1400) — one CTA of two warps per
@@ -378,206 +411,11 @@ __device__ __forceinline__ int32_t warp_min_i(int32_t v) {
   return v;
 }
 
-// One direction of FindBestThresholdSequentially (split.rs:676-891), FP64
-// form. Lane 0 forms the cumulative sums in the reference's order; all lanes
-// then evaluate the candidates; the break / skip / strict-greater rules
-// pick the same threshold as the sequential loop.
-template <bool kInt>
-__device__ bool scan_dir(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc, double min_gain_shift,
-                         bool reverse, bool skip_default, bool na_as_missing, DSplit& out) {
-  const int lane = threadIdx.x & 31;
-  const int offset = m.offset;
-  const double cnt_factor =
-      kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
-  int32_t npos = 0;
-  if (lane == 0) {
-    if (reverse) {
-      double ag = 0.0, ah = kEpsilon;
-      int32_t acnt = 0;
-      int64_t ai = 0;
-      for (int32_t t = m.num_bin - 1 - offset - (int32_t)na_as_missing; t >= 1 - offset; --t) {
-        if (skip_default && t + offset == m.default_bin) continue;
-        if (kInt) {
-          ai = (int64_t)((uint64_t)ai + (uint64_t)sm.ig[t]);
-          sm.cc[npos] = round_int((double)int_hess(ai) * cnt_factor);
-          reinterpret_cast<int64_t*>(sm.ch)[npos] = ai;
-        } else {
-          double hs = sm.h[t];
-          ag += sm.g[t];
-          ah += hs;
-          acnt += round_int(hs * cnt_factor);
-          sm.cg[npos] = ag;
-          sm.ch[npos] = ah;
-          sm.cc[npos] = acnt;
-        }
-        sm.tpos[npos] = t;
-        ++npos;
-      }
-    } else {
-      double ag = 0.0, ah = kEpsilon;
-      int32_t acnt = 0;
-      int64_t ai = 0;
-      int32_t t = 0;
-      if (na_as_missing && offset == 1) {
-        if (kInt) {
-          ai = lc.int_sum;
-          for (int32_t i = 0; i < m.num_bin - offset; ++i) ai = (int64_t)((uint64_t)ai - (uint64_t)sm.ig[i]);
-        } else {
-          ag = lc.sum_g;
-          ah = lc.sum_h - kEpsilon;
-          acnt = lc.num_data;
-          for (int32_t i = 0; i < m.num_bin - offset; ++i) {
-            double hs = sm.h[i];
-            ag -= sm.g[i];
-            ah -= hs;
-            acnt -= round_int(hs * cnt_factor);
-          }
-        }
-        t = -1;
-      }
-      for (; t <= m.num_bin - 2 - offset; ++t) {
-        if (skip_default && t + offset == m.default_bin) continue;
-        if (kInt) {
-          if (t >= 0) ai = (int64_t)((uint64_t)ai + (uint64_t)sm.ig[t]);
-          sm.cc[npos] = round_int((double)int_hess(ai) * cnt_factor);
-          reinterpret_cast<int64_t*>(sm.ch)[npos] = ai;
-        } else {
-          if (t >= 0) {
-            ag += sm.g[t];
-            ah += sm.h[t];
-            acnt += round_int(sm.h[t] * cnt_factor);
-          }
-          sm.cg[npos] = ag;
-          sm.ch[npos] = ah;
-          sm.cc[npos] = acnt;
-        }
-        sm.tpos[npos] = t;
-        ++npos;
-      }
-    }
-  }
-  npos = __shfl_sync(0xffffffffu, npos, 0);
-  __syncwarp();
-  const int32_t min_data = p.min_data_in_leaf;
-  const double min_hess = p.min_sum_hessian_in_leaf;
-  // pass 1: first break position
-  int32_t brk = INT32_MAX;
-  for (int32_t k = lane; k < npos; k += 32) {
-    int32_t cnt_acc = sm.cc[k];
-    double hacc, hrest;
-    if (kInt) {
-      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[k];
-      hacc = (double)int_hess(acc) * lc.hs;
-      hrest = (double)int_hess((int64_t)((uint64_t)lc.int_sum - (uint64_t)acc)) * lc.hs;
-    } else {
-      hacc = sm.ch[k];
-      hrest = lc.sum_h - hacc;
-    }
-    bool skip1 = cnt_acc < min_data || hacc < min_hess;
-    if (!skip1 && (lc.num_data - cnt_acc < min_data || hrest < min_hess)) brk = min(brk, k);
-  }
-  brk = warp_min_i(brk);
-  // pass 2: gains of the candidates before the break
-  double best_gain = -INFINITY;
-  int32_t best_k = INT32_MAX;
-  bool splittable = false;
-  for (int32_t k = lane; k < min(npos, brk); k += 32) {
-    int32_t cnt_acc = sm.cc[k];
-    double ga, ha, gr, hr;  // accumulated side, rest side
-    if (kInt) {
-      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[k];
-      int64_t rest = (int64_t)((uint64_t)lc.int_sum - (uint64_t)acc);
-      ha = (double)int_hess(acc) * lc.hs;
-      hr = (double)int_hess(rest) * lc.hs;
-      if (cnt_acc < min_data || ha < min_hess) continue;
-      ga = (double)int_grad(acc) * lc.gs;
-      gr = (double)int_grad(rest) * lc.gs;
-      ha += kEpsilon;
-      hr += kEpsilon;
-    } else {
-      ha = sm.ch[k];
-      if (cnt_acc < min_data || ha < min_hess) continue;
-      ga = sm.cg[k];
-      hr = lc.sum_h - ha;
-      gr = lc.sum_g - ga;
-    }
-    int32_t rest_cnt = lc.num_data - cnt_acc;
-    double gain = reverse ? split_gain(gr, hr, ga, ha, p, rest_cnt, cnt_acc, lc.parent_output, lc.mc, lc.cmin,
-                                       lc.cmax, m.monotone_type)
-                          : split_gain(ga, ha, gr, hr, p, cnt_acc, rest_cnt, lc.parent_output, lc.mc, lc.cmin,
-                                       lc.cmax, m.monotone_type);
-    if (gain <= min_gain_shift) continue;
-    splittable = true;
-    if (gain > best_gain) {  // NaN never becomes best
-      best_gain = gain;
-      best_k = k;
-    }
-  }
-  splittable = __any_sync(0xffffffffu, splittable);
-  warp_best(best_gain, best_k);
-  // a basic constraint with min > max never accepts a best threshold (split.rs:765-771)
-  if (lc.mc && lc.cmin > lc.cmax) best_k = INT32_MAX;
-  if (lane == 0 && splittable && best_k != INT32_MAX && best_gain > out.gain + min_gain_shift) {
-    int32_t t = sm.tpos[best_k];
-    double slg, slh;  // best left sums
-    int32_t left_count;
-    int64_t left_int = 0;
-    if (kInt) {
-      int64_t acc = reinterpret_cast<int64_t*>(sm.ch)[best_k];
-      left_int = reverse ? (int64_t)((uint64_t)lc.int_sum - (uint64_t)acc) : acc;
-      int64_t right_int = (int64_t)((uint64_t)lc.int_sum - (uint64_t)left_int);
-      double lg = (double)int_grad(left_int) * lc.gs, lh = (double)int_hess(left_int) * lc.hs;
-      double rg = (double)int_grad(right_int) * lc.gs, rh = (double)int_hess(right_int) * lc.hs;
-      int32_t lcnt = round_int((double)int_hess(left_int) * cnt_factor);
-      int32_t rcnt = round_int((double)int_hess(right_int) * cnt_factor);
-      out.threshold = (uint32_t)(reverse ? t - 1 + offset : t + offset);
-      double lo = leaf_output(lg, lh, p, lcnt, lc.parent_output);
-      double ro = leaf_output(rg, rh, p, rcnt, lc.parent_output);
-      out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
-      out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
-      out.left_count = lcnt;
-      out.right_count = rcnt;
-      out.left_sum_gradient = lg;
-      out.left_sum_hessian = lh;
-      out.right_sum_gradient = rg;
-      out.right_sum_hessian = rh;
-      out.left_sum_gh = left_int;
-      out.right_sum_gh = right_int;
-    } else {
-      if (reverse) {
-        slg = lc.sum_g - sm.cg[best_k];
-        slh = lc.sum_h - sm.ch[best_k];
-        left_count = lc.num_data - sm.cc[best_k];
-        out.threshold = (uint32_t)(t - 1 + offset);
-      } else {
-        slg = sm.cg[best_k];
-        slh = sm.ch[best_k];
-        left_count = sm.cc[best_k];
-        out.threshold = (uint32_t)(t + offset);
-      }
-      double lo = leaf_output(slg, slh, p, left_count, lc.parent_output);
-      double ro = leaf_output(lc.sum_g - slg, lc.sum_h - slh, p, lc.num_data - left_count, lc.parent_output);
-      out.left_output = lc.mc ? clampc(lo, lc.cmin, lc.cmax) : lo;
-      out.right_output = lc.mc ? clampc(ro, lc.cmin, lc.cmax) : ro;
-      out.left_count = left_count;
-      out.left_sum_gradient = slg;
-      out.left_sum_hessian = slh - kEpsilon;
-      out.right_count = lc.num_data - left_count;
-      out.right_sum_gradient = lc.sum_g - slg;
-      out.right_sum_hessian = lc.sum_h - slh - kEpsilon;
-    }
-    out.gain = best_gain - min_gain_shift;
-    out.default_left = reverse ? 1 : 0;
-  }
-  __syncwarp();
-  return splittable;
-}
-
 // split.rs:448-670 / :1194-1400 categorical threshold search, in lane 0
 // (the candidate lists are at most a few dozen bins; the stable sort is a
 // rank sort done by the whole warp).
 template <bool kInt>
-__device__ bool scan_categorical(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc, DSplit& out) {
+__device__ __noinline__ bool scan_categorical(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc, DSplit& out) {
   const int lane = threadIdx.x & 31;
   const int offset = m.offset;
   const int bin_start = 1 - offset, bin_end = m.num_bin - offset;
@@ -801,19 +639,45 @@ __device__ bool find_best_threshold_warp(ScanSmem& sm, const DFeature& m, const 
     double sg = kInt ? (double)int_grad(lc.int_sum) * lc.gs : lc.sum_g;
     double sh = kInt ? (double)int_hess(lc.int_sum) * lc.hs : lc.sum_h;
     double min_gain_shift = leaf_gain(sg, sh, p, lc.num_data, lc.parent_output) + p.min_gain_to_split;
-    __syncwarp();
-    if (m.num_bin > 2 && m.missing_type != 0) {
-      if (m.missing_type == 1) {
-        ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, true, false, out);
-        ok |= scan_dir<kInt>(sm, m, p, lc, min_gain_shift, false, true, false, out);
-      } else {
-        ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, false, true, out);
-        ok |= scan_dir<kInt>(sm, m, p, lc, min_gain_shift, false, false, true, out);
+    double cnt_factor =
+        kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
+    LaneBins v;
+    int32_t ce[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      int t = lane * kPer + j;
+      v.g[j] = v.h[j] = 0.0;
+      v.q[j] = 0;
+      ce[j] = 0;
+      if (t < m.view_len) {
+        if (kInt) {
+          v.q[j] = sm.ig[t];
+        } else {
+          v.g[j] = sm.g[t];
+          v.h[j] = sm.h[t];
+          ce[j] = round_int(v.h[j] * cnt_factor);
+        }
       }
-    } else {
-      ok = scan_dir<kInt>(sm, m, p, lc, min_gain_shift, true, false, false, out);
-      if (lane == 0 && m.missing_type == 2) out.default_left = 0;
     }
+    __syncwarp();
+    auto run = [&](bool rev, bool sd, bool na) {
+      ScanBest r = scan_direction<kInt>(v, ce, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data,
+                                        lc.parent_output, lc.mc, lc.cmin, lc.cmax, min_gain_shift, cnt_factor, rev,
+                                        sd, na);
+      if (lane == 0)
+        apply_direction<kInt>(r, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data, lc.parent_output,
+                              lc.mc, lc.cmin, lc.cmax, min_gain_shift, cnt_factor, rev, out);
+      __syncwarp();
+      return r.splittable;
+    };
+    // split.rs:426-439: the directions scanned and their missing-value rules
+    const bool two = m.num_bin > 2 && m.missing_type != 0;
+    const bool skip_default = two && m.missing_type == 1;
+    const bool na_missing = two && m.missing_type == 2;
+    ok = false;
+#pragma unroll 1
+    for (int d = 0; d < (two ? 2 : 1); ++d) ok |= run(d == 0, skip_default, na_missing);
+    if (!two && lane == 0 && m.missing_type == 2) out.default_left = 0;
   }
   if (lane == 0) out.gain *= m.penalty;
   __syncwarp();
@@ -831,12 +695,38 @@ __device__ __forceinline__ bool split_better(const DSplit& a, const DSplit& b) {
   return better_than(a.gain, a.feature, b.gain, b.feature);
 }
 
-// The selected split is applied to the tree (tree.rs:240-297) and the
-// partition LUT is written; runs in one thread.
-__device__ void apply_split(const DCtx& c, DSlot& s, int32_t bl) {
+// Partition LUT over stored group values (learner/mod.rs:1313-1329): one
+// goes-left flag per value a row of the split feature can hold; warp-parallel.
+__device__ void write_partition_lut(const DCtx& c, const DSlot& s, int32_t bl) {
+  const int lane = threadIdx.x & 31;
+  const DSplit& info = s.best[bl];
+  const DFeature& m = c.feats[info.inner];
+  const bool numerical = m.bin_type == 0;
+  const bool default_left = numerical ? info.default_left != 0 : false;
+  const int32_t ntb = m.view_len + 1;
+  for (int32_t raw = lane; raw < kMaxBins; raw += 32) {
+    uint8_t left = 0;
+    if (raw < ntb) {
+      uint32_t b = decode_bin((uint32_t)raw, m);
+      if (numerical) {
+        bool miss = (m.missing_type == 1 && b == (uint32_t)m.default_bin) ||
+                    (m.missing_type == 2 && b == (uint32_t)(m.num_bin - 1));
+        left = miss ? (uint8_t)default_left : (uint8_t)(b <= info.threshold);
+      } else {
+        auto bit = [&](uint32_t v) { return (info.cat_bits[v >> 5] >> (v & 31)) & 1u; };
+        if (b == (uint32_t)m.most_freq_bin) left = (uint8_t)(m.most_freq_bin > 0 && bit(b));
+        else left = (uint8_t)bit(b);
+      }
+    }
+    s.st->lut[raw] = left;
+  }
+}
+
+// The selected split is applied to the tree (tree.rs:240-297); one thread.
+__device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
-  DTree& t = s.tree;
+  const DTree& t = s.tree;
   const DSplit& info = s.best[bl];
   const DFeature& m = c.feats[info.inner];
   int32_t R = st->num_leaves_cur;
@@ -888,24 +778,6 @@ __device__ void apply_split(const DCtx& c, DSlot& s, int32_t bl) {
       }
     }
   }
-  // partition LUT over stored group values (learner/mod.rs:1313-1329)
-  int32_t ntb = m.view_len + 1;
-  for (int32_t raw = 0; raw < kMaxBins; ++raw) {
-    uint8_t left = 0;
-    if (raw < ntb) {
-      uint32_t b = decode_bin((uint32_t)raw, m);
-      if (numerical) {
-        bool miss = (m.missing_type == 1 && b == (uint32_t)m.default_bin) ||
-                    (m.missing_type == 2 && b == (uint32_t)(m.num_bin - 1));
-        left = miss ? (uint8_t)default_left : (uint8_t)(b <= info.threshold);
-      } else {
-        auto bit = [&](uint32_t v) { return (info.cat_bits[v >> 5] >> (v & 31)) & 1u; };
-        if (b == (uint32_t)m.most_freq_bin) left = (uint8_t)(m.most_freq_bin > 0 && bit(b));
-        else left = (uint8_t)bit(b);
-      }
-    }
-    st->lut[raw] = left;
-  }
   st->split_leaf = bl;
   st->new_leaf = R;
   st->split_inner = info.inner;
@@ -915,10 +787,10 @@ __device__ void apply_split(const DCtx& c, DSlot& s, int32_t bl) {
 }
 
 template <bool kInt>
-__global__ void __launch_bounds__(64) k_scan(DCtx c) {
+__global__ void __launch_bounds__(64) k_scan(const __grid_constant__ DCtx c) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScanSmem* sms = reinterpret_cast<ScanSmem*>(smem_raw);
-  DSlot& s = c.slots[blockIdx.z];
+  const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
   const int f = blockIdx.x;
@@ -942,12 +814,18 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
         const int64_t* hs = reinterpret_cast<const int64_t*>(s.hist) + sbase;
         for (int i = lane; i < len; i += 32) sm0.ig[i] = hs[i];
         __syncwarp();
-        if (lane == 0 && m.most_freq_bin > 0) {
-          int64_t acc = sl.int_sum;
-          for (int i = 0; i < m.num_bin; ++i)
-            if (i != m.most_freq_bin) acc = (int64_t)((uint64_t)acc - (uint64_t)sm0.ig[i]);
-          sm0.ig[m.most_freq_bin] = acc;
-          reinterpret_cast<int64_t*>(s.hist)[sbase + m.most_freq_bin] = acc;
+        if (m.most_freq_bin > 0) {  // exact: any summation order
+          int64_t part = 0;
+          for (int i = lane; i < m.num_bin; i += 32)
+            if (i != m.most_freq_bin) part = (int64_t)((uint64_t)part + (uint64_t)sm0.ig[i]);
+          for (int o = 16; o > 0; o >>= 1)
+            part = (int64_t)((uint64_t)part + (uint64_t)__shfl_xor_sync(0xffffffffu, part, o));
+          int64_t acc = (int64_t)((uint64_t)sl.int_sum - (uint64_t)part);
+          __syncwarp();
+          if (lane == 0) {
+            sm0.ig[m.most_freq_bin] = acc;
+            reinterpret_cast<int64_t*>(s.hist)[sbase + m.most_freq_bin] = acc;
+          }
         }
       } else {
         const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
@@ -956,19 +834,31 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
           sm0.h[i] = hs[2 * i + 1];
         }
         __syncwarp();
-        if (lane == 0 && m.most_freq_bin > 0) {
-          double g = sl.sum_gradients, h = sl.sum_hessians;
-          for (int i = 0; i < m.num_bin; ++i) {
-            if (i != m.most_freq_bin) {
-              g -= sm0.g[i];
-              h -= sm0.h[i];
-            }
+        if (m.most_freq_bin > 0) {  // sequential subtraction in bin order, as a lane carry chain
+          double g8[kPer], h8[kPer];
+#pragma unroll
+          for (int j = 0; j < kPer; ++j) {
+            int t = lane * kPer + j;
+            g8[j] = t < len ? sm0.g[t] : 0.0;
+            h8[j] = t < len ? sm0.h[t] : 0.0;
           }
-          sm0.g[m.most_freq_bin] = g;
-          sm0.h[m.most_freq_bin] = h;
-          double* w = reinterpret_cast<double*>(s.hist) + 2 * (sbase + m.most_freq_bin);
-          w[0] = g;
-          w[1] = h;
+          double g = sl.sum_gradients, h = sl.sum_hessians;
+          int32_t unused = 0;
+          carry_chain(false, 0, (m.num_bin - 1) / kPer, g, h, unused, [&](int j, double& x, double& y, int32_t&) {
+            int t = lane * kPer + j;
+            if (t < m.num_bin && t != m.most_freq_bin) {
+              x -= g8[j];
+              y -= h8[j];
+            }
+          });
+          __syncwarp();
+          if (lane == 0) {
+            sm0.g[m.most_freq_bin] = g;
+            sm0.h[m.most_freq_bin] = h;
+            double* w = reinterpret_cast<double*>(s.hist) + 2 * (sbase + m.most_freq_bin);
+            w[0] = g;
+            w[1] = h;
+          }
         }
       }
     }
@@ -1033,7 +923,7 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
     // warp w reduces leaf side w (0 smaller, 1 larger)
     if (warp == 0 || have_larger) {
       const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
-      double pen = monotone_split_gain_penalty(s.tree.leaf_depth[ls.leaf], p.monotone_penalty);
+      double pen = p.use_monotone ? monotone_split_gain_penalty(s.tree.leaf_depth[ls.leaf], p.monotone_penalty) : 1.0;
       double bg = -INFINITY;
       int32_t bfeat = -1, bf = -1;
       for (int ff = lane; ff < nf; ff += 32) {
@@ -1074,6 +964,8 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
           dst.inner = -1;
           dst.gain = -INFINITY;
         }
+        s.bgain[ls.leaf] = dst.gain;
+        s.bfeat[ls.leaf] = dst.feature;
       }
     }
     __syncthreads();
@@ -1088,10 +980,11 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
   double bg = -INFINITY;
   int32_t bfeat = -1, bl = INT32_MAX;
   for (int l = lane; l < p.num_leaves; l += 32) {
-    const DSplit& r = s.best[l];
-    if (bl == INT32_MAX || better_than(r.gain, r.feature, bg, bfeat)) {
-      bg = r.gain;
-      bfeat = r.feature;
+    double g = s.bgain[l];
+    int32_t fe = s.bfeat[l];
+    if (bl == INT32_MAX || better_than(g, fe, bg, bfeat)) {
+      bg = g;
+      bfeat = fe;
       bl = l;
     }
   }
@@ -1111,17 +1004,22 @@ __global__ void __launch_bounds__(64) k_scan(DCtx c) {
       bl = ol;
     }
   }
+  if (!(bg > 0.0)) {
+    if (lane == 0) {
+      st->scan_counter = 0;
+      st->done = 1;
+    }
+    return;
+  }
+  write_partition_lut(c, s, bl);
+  __syncwarp();
   if (lane == 0) {
     st->scan_counter = 0;
-    if (!(bg > 0.0)) {
-      st->done = 1;
-    } else {
-      apply_split(c, s, bl);
-    }
+    apply_split(c, s, bl);
   }
 }
-template __global__ void k_scan<false>(DCtx);
-template __global__ void k_scan<true>(DCtx);
+template __global__ void k_scan<false>(const __grid_constant__ DCtx);
+template __global__ void k_scan<true>(const __grid_constant__ DCtx);
 
 // =====================================================================================
 // partition (partition.rs:107-174): out-of-place split of the leaf's rows into
@@ -1141,7 +1039,7 @@ __device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsign
   return flag | ((unsigned long long)(epoch & kEpochMask) << 31) | (v & kValueMask);
 }
 
-__device__ void partition_finalize(const DCtx& c, DSlot& s, int32_t total_left) {
+__device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t total_left) {
   DSlotState* st = s.st;
   int32_t L = st->split_leaf, R = st->new_leaf;
   int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
@@ -1152,7 +1050,7 @@ __device__ void partition_finalize(const DCtx& c, DSlot& s, int32_t total_left) 
   s.leaf_count[R] = nr;
   s.leaf_side[L] = 1 - side;
   s.leaf_side[R] = 1 - side;
-  DTree& t = s.tree;
+  const DTree& t = s.tree;
   int32_t node = R - 1;
   t.leaf_count[L] = nl;
   t.leaf_count[R] = nr;
@@ -1187,8 +1085,8 @@ __device__ void partition_finalize(const DCtx& c, DSlot& s, int32_t total_left) 
 }
 
 // Grid (G, 1, slots), kPartThreads threads.
-__global__ void __launch_bounds__(kPartThreads) k_partition(DCtx c) {
-  DSlot& s = c.slots[blockIdx.z];
+__global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
+  const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
   __shared__ uint8_t lut[kMaxBins];
@@ -1215,7 +1113,7 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(DCtx c) {
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
   const int32_t ntiles = (cnt + kPartTile - 1) / kPartTile;
-  const uint8_t* col = c.bins + inner;
+  const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
   __syncthreads();
   while (true) {
     if (tid == 0) s_tile = atomicAdd(&st->part_ticket, 1);
@@ -1232,7 +1130,7 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(DCtx c) {
       if (pos < cnt) {
         uint32_t r = in[pos];
         rows[k] = r;
-        uint32_t raw = col[(size_t)r * c.stride];
+        uint32_t raw = col[r];
         if (lut[raw]) {
           flags |= 1u << k;
           ++nleft;
@@ -1306,13 +1204,21 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(DCtx c) {
   }
 }
 
+// Column-major copy of the bin matrix (the partition reads one feature of the
+// rows of a leaf, which are ascending, so neighbouring rows share sectors).
+__global__ void __launch_bounds__(256) k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf,
+                                                        uint8_t* colbins) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    for (int32_t f = 0; f < nf; ++f) colbins[(size_t)f * n + r] = bins[(size_t)r * stride + f];
+}
+
 // =====================================================================================
 // leaf renewal from FP64 gradient sums (learner/mod.rs:736-747) and the
 // score updates (partition.rs:306-319; tree.rs:605-711 binned routing)
 // =====================================================================================
 // Grid (G, num_leaves, slots): block (x, leaf) sums a chunk of the leaf's rows.
-__global__ void __launch_bounds__(256) k_leaf_sums(DCtx c, double* sums /*[slots][leaves][2]*/) {
-  DSlot& s = c.slots[blockIdx.z];
+__global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* sums /*[slots][leaves][2]*/) {
+  const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   int32_t leaf = blockIdx.y;
   if (leaf >= st->num_leaves_cur) return;
@@ -1333,8 +1239,8 @@ __global__ void __launch_bounds__(256) k_leaf_sums(DCtx c, double* sums /*[slots
   }
 }
 
-__global__ void k_leaf_renew(DCtx c, const double* sums) {
-  DSlot& s = c.slots[blockIdx.z];
+__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums) {
+  const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   for (int32_t leaf = threadIdx.x; leaf < st->num_leaves_cur; leaf += blockDim.x) {
     const double* o = sums + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
@@ -1344,9 +1250,9 @@ __global__ void k_leaf_renew(DCtx c, const double* sums) {
 
 // score[row] += leaf_value[leaf] * scale over each leaf's rows.
 // Grid (G, num_leaves, slots).
-__global__ void __launch_bounds__(256) k_add_leaf_outputs(DCtx c, const double* leaf_values, int32_t lv_stride,
+__global__ void __launch_bounds__(256) k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride,
                                                           double* score, int64_t score_stride) {
-  DSlot& s = c.slots[blockIdx.z];
+  const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   int32_t leaf = blockIdx.y;
   if (leaf >= st->num_leaves_cur) return;
@@ -1358,10 +1264,10 @@ __global__ void __launch_bounds__(256) k_add_leaf_outputs(DCtx c, const double* 
 }
 
 // Binned tree walk (tree.rs:588-633) for rows `rows` (or 0..n): score += leaf value.
-__global__ void __launch_bounds__(256) k_add_tree_binned(DCtx c, const uint8_t* bins, int32_t stride,
+__global__ void __launch_bounds__(256) k_add_tree_binned(const __grid_constant__ DCtx c, const uint8_t* bins, int32_t stride,
                                                          const uint32_t* rows, int64_t n, const double* leaf_values,
                                                          int32_t lv_stride, double* score, int64_t score_stride) {
-  DSlot& s = c.slots[blockIdx.z];
+  const DSlot& s = c.slots[blockIdx.z];
   const DTree& t = s.tree;
   int32_t nl = s.st->num_leaves_cur;
   const double* lv = leaf_values + (size_t)blockIdx.z * lv_stride;

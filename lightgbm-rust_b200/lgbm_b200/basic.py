@@ -284,6 +284,16 @@ class Learner:
                                                     _ptr(scales, C.c_double)))
         return packed, scales
 
+    def record(self, mark):
+        """Record timing mark `mark` (0..15) on the learner's CUDA stream."""
+        L.check(L.lib().lgbm_b200_learner_record(self.handle, int(mark)))
+
+    def elapsed(self, a, b):
+        """Device milliseconds between two recorded marks."""
+        ms = C.c_double()
+        L.check(L.lib().lgbm_b200_learner_elapsed(self.handle, int(a), int(b), C.byref(ms)))
+        return ms.value
+
     def set_timing(self, on):
         L.check(L.lib().lgbm_b200_learner_set_timing(self.handle, int(bool(on))))
 

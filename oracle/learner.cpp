@@ -6,6 +6,8 @@
 // Scope: dense single-feature groups (u8 values), row-wise layout, no
 // forced splits / CEGB / linear trees / extra trees / interaction
 // constraints; bagging without subset; basic monotone constraints.
+#include <omp.h>
+
 #include <algorithm>
 #include <memory>
 #include <stdexcept>
@@ -56,13 +58,12 @@ void SerialTreeLearner::set_bagging_data(const uint32_t* used, size_t n_used) { 
   }
 }
 
-// multi_val_bin.rs:644-648 (per row, per column: out[bin] += [g, h]) at one
-// thread; `rows == nullptr` walks every row.
-void SerialTreeLearner::build_hist(const uint32_t* rows, size_t n, const float* grad, const float* hess,
-                                   double* out) const {
-  std::fill(out, out + 2 * total_bins_, 0.0);
+// multi_val_bin.rs:644-648 (per row, per column: out[bin] += [g, h]);
+// `rows == nullptr` walks every row.
+void SerialTreeLearner::build_hist_block(const uint32_t* rows, size_t k0, size_t k1, const float* grad,
+                                         const float* hess, double* out) const {
   int32_t nf = d_->num_features;
-  for (size_t k = 0; k < n; ++k) {
+  for (size_t k = k0; k < k1; ++k) {
     size_t r = rows ? rows[k] : k;
     double g = (double)grad[r], h = (double)hess[r];
     const uint8_t* row = d_->bins + r * (size_t)nf;
@@ -76,10 +77,63 @@ void SerialTreeLearner::build_hist(const uint32_t* rows, size_t n, const float* 
   }
 }
 
+// multi_val_bin.rs:556-611 construct: rows split into Threading::BlockInfo
+// blocks (min block size from multi_val_bin.rs:348-351), each summed in row
+// order, blocks added in block order (HistMerge) — equal to the reference
+// at the same thread count.
+void SerialTreeLearner::build_hist(const uint32_t* rows, size_t n, const float* grad, const float* hess,
+                                   double* out) const {
+  std::fill(out, out + 2 * total_bins_, 0.0);
+  size_t threads = (size_t)std::max(cfg_.num_threads, 1);
+  size_t nblock = 1, bsize = n;
+  if (threads > 1) {
+    size_t mv_bins = total_bins_ + (size_t)d_->num_features;  // + each group's slot 0
+    int32_t mbs = (int32_t)((double)(0.3f * (float)mv_bins) / ((double)d_->num_features + kZeroThreshold));
+    size_t min_block = (size_t)std::min(std::max(mbs + 1, 32), 1024);
+    block_info(threads, n, min_block, &nblock, &bsize);
+  }
+  if (nblock == 1) {
+    build_hist_block(rows, 0, n, grad, hess, out);
+    return;
+  }
+  std::vector<std::vector<double>> bufs(nblock - 1, std::vector<double>(2 * total_bins_, 0.0));
+#pragma omp parallel for schedule(static, 1) num_threads((int)threads)
+  for (long b = 0; b < (long)nblock; ++b) {
+    size_t s = std::min((size_t)b * bsize, n), e = std::min(s + bsize, n);
+    build_hist_block(rows, s, e, grad, hess, b == 0 ? out : bufs[(size_t)b - 1].data());
+  }
+  for (auto& src : bufs)
+    for (size_t i = 0; i < 2 * total_bins_; ++i) out[i] += src[i];
+}
+
 // multi_val_bin.rs:763-791 construct_int (wrapping packed sums).
 void SerialTreeLearner::build_hist_int(const uint32_t* rows, size_t n, const int64_t* packed, int64_t* out) const {
   std::fill(out, out + total_bins_, 0);
   int32_t nf = d_->num_features;
+  int threads = std::max(cfg_.num_threads, 1);
+  if (threads > 1 && n > 4096) {  // integer sums: any block split gives the same result
+    std::vector<std::vector<int64_t>> bufs((size_t)threads, std::vector<int64_t>(total_bins_, 0));
+#pragma omp parallel num_threads(threads)
+    {
+      int t = omp_get_thread_num();
+      size_t s = n * (size_t)t / (size_t)threads, e = n * (size_t)(t + 1) / (size_t)threads;
+      int64_t* o = bufs[(size_t)t].data();
+      for (size_t k = s; k < e; ++k) {
+        size_t r = rows ? rows[k] : k;
+        uint64_t v = (uint64_t)packed[r];
+        const uint8_t* row = d_->bins + r * (size_t)nf;
+        for (int32_t f = 0; f < nf; ++f) {
+          uint32_t raw = row[f];
+          if (raw == 0) continue;
+          size_t ti = view_start_[f] + raw - 1;
+          o[ti] = (int64_t)((uint64_t)o[ti] + v);
+        }
+      }
+    }
+    for (auto& b : bufs)
+      for (size_t i = 0; i < total_bins_; ++i) out[i] = (int64_t)((uint64_t)out[i] + (uint64_t)b[i]);
+    return;
+  }
   for (size_t k = 0; k < n; ++k) {
     size_t r = rows ? rows[k] : k;
     uint64_t v = (uint64_t)packed[r];
@@ -202,10 +256,16 @@ void SerialTreeLearner::find_best_splits(const Tree& tree, const float* grad, co
 
   SplitInfo s_best, l_best;
   std::vector<bool> s_spl = s_spl_init;
+  // per-feature searches are independent (learner/mod.rs:954-1057); the
+  // reduction below walks the features in order
+  std::vector<SplitInfo> s_res(nf), l_res(nf);
+  std::vector<char> s_okv(nf, 0), l_okv(nf, 0);
+#pragma omp parallel for schedule(dynamic) num_threads(std::max(cfg_.num_threads, 1))
   for (int32_t f = 0; f < nf; ++f) {
     if (!is_used[f]) continue;
     const FeatureMeta& meta = d_->metas[f];
-    SplitInfo s_split, l_split;
+    SplitInfo& s_split = s_res[f];
+    SplitInfo& l_split = l_res[f];
     bool s_ok, l_ok = false;
     if (cfg_.quantized) {
       int64_t* hist = s_ibuf.data() + view_start_[f];
@@ -234,14 +294,21 @@ void SerialTreeLearner::find_best_splits(const Tree& tree, const float* grad, co
     s_split.feature_inner = f;
     l_split.feature = meta.real_index;
     l_split.feature_inner = f;
+    s_okv[f] = s_ok;
+    l_okv[f] = l_ok;
+  }
+  for (int32_t f = 0; f < nf; ++f) {
+    if (!is_used[f]) continue;
+    SplitInfo& s_split = s_res[f];
+    SplitInfo& l_split = l_res[f];
     // finish_split (learner/mod.rs:1283-1300): the monotone depth penalty.
     if (s_split.monotone_type != 0) s_split.gain *= s_pen;
     if (s_split.better_than(s_best)) s_best = s_split;
-    s_spl[f] = s_ok;
+    s_spl[f] = s_okv[f] != 0;
     if (larger_.leaf >= 0) {
       if (l_split.monotone_type != 0) l_split.gain *= l_pen;
       if (l_split.better_than(l_best)) l_best = l_split;
-      l_spl[f] = l_ok;
+      l_spl[f] = l_okv[f] != 0;
     }
   }
   best_split_per_leaf_[sm_leaf] = s_best;

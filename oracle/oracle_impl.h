@@ -126,6 +126,8 @@ class SerialTreeLearner {
   std::vector<size_t> view_start_;
   size_t total_bins_ = 0;
   void build_hist(const uint32_t* rows, size_t n, const float* grad, const float* hess, double* out) const;
+  void build_hist_block(const uint32_t* rows, size_t k0, size_t k1, const float* grad, const float* hess,
+                        double* out) const;
   void build_hist_int(const uint32_t* rows, size_t n, const int64_t* packed, int64_t* out) const;
   size_t partition_split(int32_t leaf, int32_t inner, const std::vector<bool>& lut, int32_t right_leaf);
 
