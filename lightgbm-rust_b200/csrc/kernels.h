@@ -6,9 +6,9 @@
 namespace lgbm_b200 {
 
 constexpr int kHistThreads = 512;
-constexpr int kMaxTileFeatures = 256;
+constexpr int kHistTileRows = kHistThreads;  // rows staged per histogram tile: one per thread
 constexpr int kMaxTiles = 64;
-constexpr int kMaxLaneGroups = 6;  // 32-feature groups per histogram tile (int32 cells)
+constexpr int kMaxLaneGroups = 4;  // 32-feature groups per histogram tile (int32 cells)
 
 // Feature tiles of a histogram launch (blockIdx.y): tile k covers features
 // [f0[k], f0[k+1]) whose stored bins are [bin0[k], bin0[k+1]).
@@ -17,19 +17,33 @@ struct DTileTable {
   int32_t bin0[kMaxTiles + 1];
 };
 
+constexpr int kScanThreads = 256;  // one thread per stored bin of a feature view
+
 struct ScanSmem {
   double g[kMaxBins], h[kMaxBins];        // this leaf's feature view
   double cg[kMaxBins], ch[kMaxBins];      // cumulative sums in scan order
   int32_t cc[kMaxBins];                   // cumulative count estimates
-  int64_t ig[kMaxBins];                   // quantized view / cumulative
-  int32_t tpos[kMaxBins];                 // scan position -> t (-1: skipped default bin)
+  int32_t ce[kMaxBins];                   // count estimate of each bin
+  int64_t ig[kMaxBins];                   // quantized view
+  int64_t cq[kMaxBins];                   // quantized cumulative sums in scan order
+  int32_t tpos[kMaxBins];                 // categorical: bins with enough data
   int32_t sorted[kMaxBins];               // categorical order
   double key[kMaxBins];
+  double eg, eh;                          // the extra candidate t = -1
+  int32_t ec, brk, ok;
+  int64_t eq;
+  double wgain[kScanThreads / 32];        // per-warp best candidates
+  int32_t wt[kScanThreads / 32];
 };
 
 __global__ void k_tree_init(const __grid_constant__ DCtx c, const uint32_t* bag, const int32_t* n_used);
-template <int kMode>
-__global__ void k_hist_lane(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows);
+template <int kMode, int kNG>
+__global__ void k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows);
+// dynamic shared memory, kernel and launch of the histogram for a form and groups per tile
+size_t hist_smem_bytes(int mode, int ng);
+const void* hist_kernel(int mode, int ng);
+void launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                 int32_t sub_rows);
 template <bool kInt>
 __global__ void k_scan(const __grid_constant__ DCtx c);
 __global__ void k_partition(const __grid_constant__ DCtx c);

@@ -84,8 +84,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
       h->tiles.f0[t] = f;
       h->tiles.bin0[t] = f < nf ? h->feats[f].view_start : h->total_bins;
     }
-    int max_groups = std::min(ngroups, groups_per_tile);
-    h->hist_smem = (size_t)max_groups * kMaxBins * 32 * cell;
+    h->hist_ng = std::min(ngroups, groups_per_tile);
+    h->hist_smem = hist_smem_bytes(mode, h->hist_ng);
   }
   if (mode == LGBM_B200_HIST_QUANT) {
     int32_t half = std::max(1, cfg->num_grad_quant_bins / 2);
@@ -95,26 +95,17 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
       return Status(LGBM_B200_ERR_UNSUPPORTED, "num_grad_quant_bins must be in [2, 64]");
   }
   // kernel attributes and grid sizes
-  if (mode == LGBM_B200_HIST_F64)
-    CU(cudaFuncSetAttribute(k_hist_lane<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
-  else if (mode == LGBM_B200_HIST_F32C)
-    CU(cudaFuncSetAttribute(k_hist_lane<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
-  else
-    CU(cudaFuncSetAttribute(k_hist_lane<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
-  h->scan_smem = 2 * sizeof(ScanSmem);
+  const void* hk = hist_kernel(mode, h->hist_ng);
+  CU(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+  h->scan_smem = sizeof(ScanSmem);
   CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   int per_sm = 1;
-  if (mode == LGBM_B200_HIST_F64)
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<0>, kHistThreads, h->hist_smem));
-  else if (mode == LGBM_B200_HIST_F32C)
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<1>, kHistThreads, h->hist_smem));
-  else
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist_lane<2>, kHistThreads, h->hist_smem));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, kHistThreads, h->hist_smem));
   per_sm = std::max(1, per_sm);
   h->hist_grid = std::max(1, h->num_sms * per_sm / std::max(1, h->ntiles));
   h->part_grid = h->num_sms * 4;
-  int32_t rpb = cfg->hist_rows_per_block > 0 ? cfg->hist_rows_per_block : 2048;
+  int32_t rpb = cfg->hist_rows_per_block > 0 ? cfg->hist_rows_per_block : 512;
 
   // device buffers
   DeviceArena& A = h->arena;
@@ -288,21 +279,16 @@ static Status enqueue_tree(LgbmB200Learner* h) {
   k_tree_init<<<init_grid, 256, 0, s>>>(c, h->bagging ? h->bag : nullptr, h->n_used_dev);
   CU_LAUNCH();
   dim3 hist_grid(h->hist_grid, h->ntiles, K);
-  dim3 scan_grid(h->nf, 1, K);
+  dim3 scan_grid(h->nf, 2, K);
   dim3 part_grid(h->part_grid, 1, K);
   for (int step = 0; step < L - 1; ++step) {
     cudaEvent_t* ev = h->timing ? &h->ev[(size_t)4 * step] : nullptr;
     if (ev) CU(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal));
-    if (mode == LGBM_B200_HIST_F64)
-      k_hist_lane<0><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
-    else if (mode == LGBM_B200_HIST_F32C)
-      k_hist_lane<1><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
-    else
-      k_hist_lane<2><<<hist_grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+    launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows);
     CU_LAUNCH();
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
-    if (mode == LGBM_B200_HIST_QUANT) k_scan<true><<<scan_grid, 64, h->scan_smem, s>>>(c);
-    else k_scan<false><<<scan_grid, 64, h->scan_smem, s>>>(c);
+    if (mode == LGBM_B200_HIST_QUANT) k_scan<true><<<scan_grid, kScanThreads, h->scan_smem, s>>>(c);
+    else k_scan<false><<<scan_grid, kScanThreads, h->scan_smem, s>>>(c);
     CU_LAUNCH();
     if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
     k_partition<<<part_grid, 256, 0, s>>>(c);
@@ -519,10 +505,7 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
   dim3 grid(h->hist_grid, h->ntiles, 1);
-  if (mode == LGBM_B200_HIST_F64) k_hist_lane<0><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
-  else if (mode == LGBM_B200_HIST_F32C)
-    k_hist_lane<1><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
-  else k_hist_lane<2><<<grid, kHistThreads, h->hist_smem, s>>>(c, h->tiles, h->sub_rows);
+  launch_hist(mode, h->hist_ng, grid, h->hist_smem, s, c, h->tiles, h->sub_rows);
   CU_LAUNCH();
   CU(cudaMemcpyAsync(out, d.hist, cells * 8, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));

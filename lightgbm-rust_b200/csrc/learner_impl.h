@@ -194,6 +194,7 @@ struct LgbmB200Learner {
   DCtx ctx{};
   DTileTable tiles{};
   int ntiles = 1;
+  int hist_ng = 1;  // 32-feature groups per histogram tile
   size_t hist_smem = 0, scan_smem = 0;
   int hist_grid = 148, part_grid = 592, root_grid = kRootBlocks;
   int32_t sub_rows = 8192;

@@ -215,19 +215,22 @@ __device__ __forceinline__ void tile_of(const DTileTable& tt, int tile, int& f0,
   nbins = tt.bin0[tile + 1] - bin0;
 }
 
-// Histogram of the smaller leaf's rows over one feature tile, in a bin-major
-// shared layout: feature f0 + 32g + lane keeps its cell of stored value `raw`
-// at cells[g][raw][lane], so in every warp-wide atomic the 32 lanes touch 32
-// different banks. A warp walks its rows 32 at a time: lane l loads row
-// index and gradient of row l, then every row is broadcast by shuffle and
-// each lane adds it into its own feature's cell.
+// Histogram of the smaller leaf's rows over one feature tile of kNG groups of
+// 32 features. The CTA walks its rows in tiles of kHistTileRows (one row per
+// thread): a thread loads its row index, its gradient pair and the row's
+// 32 x kNG bin bytes (16-byte vector loads of the row-major matrix) into
+// registers one tile ahead, so the gathers of the next tile are in flight
+// while the current tile is accumulated. A tile is staged in shared memory
+// and accumulated in a bin-major layout: feature f0 + 32g + lane keeps its
+// cell of stored value `raw` at cells[g][raw][lane], so in every warp-wide
+// atomic the 32 lanes touch 32 different banks.
 //   kMode 0: FP64 g / h cells (the reference's sums, reordered by atomics)
 //   kMode 1: FP32 (hi, lo) pairs per value, the rounding error of every
 //            add kept in lo (TwoSum), merged in FP64 when flushed
 //   kMode 2: int32 cells holding (g << 16) + h of quantized gradients,
-//            flushed every `sub_rows` rows into packed int64 sums
-template <int kMode>
-__global__ void __launch_bounds__(kHistThreads) k_hist_lane(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+//            flushed at least every `sub_rows` rows into packed int64 sums
+template <int kMode, int kNG>
+__global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const DSlot& s = c.slots[blockIdx.z];
   LeafRows lr;
@@ -236,44 +239,50 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_lane(const __grid_constan
   int f0, f1, bin0, nbins;
   tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
   (void)nbins;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int ngroups = (f1 - f0 + 31) >> 5;
-  constexpr int kCellWords = kMode == 2 ? 1 : (kMode == 0 ? 4 : 4);  // 32-bit words per cell
-  const int group_cells = kMaxBins * 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kHistThreads / 32;
+  constexpr int kRowsPerWarp = kHistTileRows / kWarps;
+  constexpr int kCellBytes = kMode == 2 ? 4 : 16;
+  constexpr int kGroupCells = kMaxBins * 32;
+  constexpr int kRowBytes = 32 * kNG;
+  const int ngroups = (f1 - f0 + 31) >> 5;  // <= kNG
+  unsigned char* cells = smem_raw;
+  uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)kNG * kGroupCells * kCellBytes);
+  int32_t* sq = reinterpret_cast<int32_t*>(sbins + kHistTileRows * 2 * kNG);
+  float2* sgh = reinterpret_cast<float2*>(sq);
   // per-lane feature facts for each group
-  int32_t vlen_g[kMaxLaneGroups], vstart_g[kMaxLaneGroups];
+  int32_t vlen_g[kNG], vstart_g[kNG];
 #pragma unroll
-  for (int g = 0; g < kMaxLaneGroups; ++g) {
+  for (int g = 0; g < kNG; ++g) {
     int f = f0 + 32 * g + lane;
     bool ok = g < ngroups && f < f1;
     vlen_g[g] = ok ? c.feats[f].view_len : 0;
     vstart_g[g] = ok ? c.feats[f].view_start : 0;
   }
-  uint32_t* cells = reinterpret_cast<uint32_t*>(smem_raw);
-  const int total_words = ngroups * group_cells * kCellWords;
-  for (int i = threadIdx.x; i < total_words; i += blockDim.x) cells[i] = 0u;
-  __syncthreads();
+  {
+    uint4* z = reinterpret_cast<uint4*>(cells);
+    const int n16 = ngroups * kGroupCells * kCellBytes / 16;
+    for (int i = threadIdx.x; i < n16; i += kHistThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
   const uint32_t* idx = lr.idx + lr.begin;
-  const uint8_t* bins = c.bins + f0 + lane;
   const size_t stride = (size_t)c.stride;
   double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
   unsigned long long* outi = reinterpret_cast<unsigned long long*>(s.hist) +
                              (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
-  // Flush the tile's cells into the leaf histogram (cells of stored value 0,
-  // the most frequent bin, are outside every feature view). Thread t always
-  // handles lane (t % 32) of a row, i.e. its own feature of each group.
+  // Flush the cells into the leaf histogram (cells of stored value 0, the
+  // most frequent bin, are outside every feature view). Thread t handles
+  // lane t % 32 of a value row, i.e. its own feature of each group.
   auto flush = [&]() {
-    __syncthreads();
 #pragma unroll
-    for (int g = 0; g < kMaxLaneGroups; ++g) {
+    for (int g = 0; g < kNG; ++g) {
       if (g >= ngroups) break;
       const int vl = vlen_g[g];
       const size_t vs = (size_t)vstart_g[g];
-      for (int raw = 1 + warp; raw <= vl; raw += nwarps) {
+      for (int raw = 1 + warp; raw <= vl; raw += kWarps) {
         const int k = raw * 32 + lane;
         const size_t dst = vs + raw - 1;
         if (kMode == 2) {
-          int32_t* ic = reinterpret_cast<int32_t*>(cells) + g * group_cells;
+          int32_t* ic = reinterpret_cast<int32_t*>(cells) + g * kGroupCells;
           int32_t cell = ic[k];
           if (cell != 0) {
             int64_t hq = (int64_t)(cell & 0xFFFF);
@@ -282,16 +291,16 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_lane(const __grid_constan
             ic[k] = 0;
           }
         } else {
-          const uint32_t* base = cells + g * group_cells * 4;
+          const unsigned char* base = cells + (size_t)g * kGroupCells * 16;
           double gv, hv;
           if (kMode == 0) {
             const double* d = reinterpret_cast<const double*>(base);
             gv = d[k];
-            hv = d[group_cells + k];
+            hv = d[kGroupCells + k];
           } else {
             const float* fl = reinterpret_cast<const float*>(base);
-            gv = (double)fl[k] + (double)fl[group_cells + k];
-            hv = (double)fl[2 * group_cells + k] + (double)fl[3 * group_cells + k];
+            gv = (double)fl[k] + (double)fl[kGroupCells + k];
+            hv = (double)fl[2 * kGroupCells + k] + (double)fl[3 * kGroupCells + k];
           }
           if (gv != 0.0 || hv != 0.0) {
             atomicAdd(outf + 2 * dst, gv);
@@ -300,84 +309,133 @@ __global__ void __launch_bounds__(kHistThreads) k_hist_lane(const __grid_constan
         }
       }
     }
-    __syncthreads();
   };
-  const int64_t span = kMode == 2 ? (int64_t)sub_rows : (r1 - r0);
-  for (int64_t q0 = r0; q0 < r1; q0 += span) {
-    const int64_t q1 = min(r1, q0 + span);
-    for (int64_t p0 = q0 + (int64_t)warp * 32; p0 < q1; p0 += (int64_t)nwarps * 32) {
-      const int nrow = (int)min((int64_t)32, q1 - p0);
-      uint32_t my_row = lane < nrow ? idx[p0 + lane] : 0u;
-      int32_t my_q = 0;
-      float my_g = 0.f, my_h = 0.f;
-      if (lane < nrow) {
+  // registers of the next tile: this thread's row of it
+  uint32_t nrow = 0;
+  int32_t nq = 0;
+  float2 ngh = make_float2(0.f, 0.f);
+  uint4 nb[2 * kNG];
+  auto fetch = [&](int64_t pos) {
+    const bool live = pos < r1;
+    nrow = live ? __ldg(idx + pos) : 0u;
+    if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
+    else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
+    const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
+#pragma unroll
+    for (int k = 0; k < 2 * kNG; ++k)
+      nb[k] = (live && (k >> 1) < ngroups) ? __ldg(src + k) : make_uint4(0u, 0u, 0u, 0u);
+  };
+  fetch(r0 + threadIdx.x);
+  int32_t since_flush = 0;
+  __syncthreads();
+  for (int64_t t0 = r0; t0 < r1; t0 += kHistTileRows) {
+    const int tile_rows = (int)min((int64_t)kHistTileRows, r1 - t0);
+    // stage this tile (the previous tile's accumulation has finished)
+#pragma unroll
+    for (int k = 0; k < 2 * kNG; ++k) sbins[threadIdx.x * 2 * kNG + k] = nb[k];
+    if (kMode == 2) sq[threadIdx.x] = nq;
+    else sgh[threadIdx.x] = ngh;
+    __syncthreads();
+    // the next tile's gathers run while this one is accumulated
+    if (t0 + kHistTileRows < r1) fetch(t0 + kHistTileRows + threadIdx.x);
+    const unsigned char* sb = reinterpret_cast<const unsigned char*>(sbins);
+    const int rw0 = warp * kRowsPerWarp;
+    const int rw1 = min(rw0 + kRowsPerWarp, tile_rows);
+    for (int r = rw0; r < rw1; r += 4) {
+      uint32_t raw[4][kNG];
+      int32_t qv[4];
+      float gv[4], hv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = r + u < rw1;
         if (kMode == 2) {
-          my_q = s.packed[my_row];
+          qv[u] = ok ? sq[r + u] : 0;
         } else {
-          float2 v = s.gh[my_row];
-          my_g = v.x;
-          my_h = v.y;
+          float2 v = ok ? sgh[r + u] : make_float2(0.f, 0.f);
+          gv[u] = v.x;
+          hv[u] = v.y;
         }
+#pragma unroll
+        for (int g = 0; g < kNG; ++g)
+          raw[u][g] = (ok && g < ngroups) ? (uint32_t)sb[(size_t)(r + u) * kRowBytes + 32 * g + lane] : 0u;
       }
-      // 8 rows at a time: broadcast their row / gradient, load each lane's
-      // stored value of the 8 rows (independent loads), then 8 atomics. A
-      // stored value indexes cells [0, 256) of the lane's own column, so no
-      // value can address outside the tile; values past the feature's bins
-      // land in cells the flush ignores.
-      for (int j0 = 0; j0 < nrow; j0 += 8) {
-        uint32_t rr[8];
-        int32_t qv[8];
-        float gv[8], hv[8];
+      // A stored value indexes cells [0, 256) of the lane's own column, so no
+      // value can address outside the group; values past the feature's bins
+      // (lanes past the last feature read padding zeros) land in cells the
+      // flush ignores.
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int src = (j0 + u) & 31;
-          rr[u] = __shfl_sync(0xffffffffu, my_row, src);
+      for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int g = 0; g < kNG; ++g) {
+          if (raw[u][g] == 0u) continue;
+          const int k = (int)raw[u][g] * 32 + lane;
           if (kMode == 2) {
-            qv[u] = __shfl_sync(0xffffffffu, my_q, src);
+            atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + k, qv[u]);
+          } else if (kMode == 0) {
+            double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
+            atomicAdd(d + k, (double)gv[u]);
+            atomicAdd(d + kGroupCells + k, (double)hv[u]);
           } else {
-            gv[u] = __shfl_sync(0xffffffffu, my_g, src);
-            hv[u] = __shfl_sync(0xffffffffu, my_h, src);
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < kMaxLaneGroups; ++g) {
-          if (g >= ngroups) break;
-          const bool live = vlen_g[g] > 0;
-          uint32_t raw[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u)
-            raw[u] = (live && j0 + u < nrow) ? (uint32_t)bins[(size_t)rr[u] * stride + 32 * g] : 0u;
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            if (raw[u] == 0u) continue;
-            const int k = (int)raw[u] * 32 + lane;
-            if (kMode == 2) {
-              atomicAdd(reinterpret_cast<int32_t*>(cells) + g * group_cells + k, qv[u]);
-            } else if (kMode == 0) {
-              double* d = reinterpret_cast<double*>(cells + g * group_cells * 4);
-              atomicAdd(d + k, (double)gv[u]);
-              atomicAdd(d + group_cells + k, (double)hv[u]);
-            } else {
-              float* fl = reinterpret_cast<float*>(cells + g * group_cells * 4);
-              float og = atomicAdd(fl + k, gv[u]);
-              float sg = __fadd_rn(og, gv[u]);
-              float bg = __fsub_rn(sg, og);
-              atomicAdd(fl + group_cells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv[u], bg)));
-              float oh = atomicAdd(fl + 2 * group_cells + k, hv[u]);
-              float s2 = __fadd_rn(oh, hv[u]);
-              float bh = __fsub_rn(s2, oh);
-              atomicAdd(fl + 3 * group_cells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv[u], bh)));
-            }
+            float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
+            float og = atomicAdd(fl + k, gv[u]);
+            float sg = __fadd_rn(og, gv[u]);
+            float bg = __fsub_rn(sg, og);
+            atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv[u], bg)));
+            float oh = atomicAdd(fl + 2 * kGroupCells + k, hv[u]);
+            float s2 = __fadd_rn(oh, hv[u]);
+            float bh = __fsub_rn(s2, oh);
+            atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv[u], bh)));
           }
         }
       }
     }
-    flush();
+    since_flush += tile_rows;
+    __syncthreads();
+    // int32 cells hold at most sub_rows rows before their 16-bit halves could wrap
+    if (kMode == 2 && t0 + kHistTileRows < r1 && since_flush + kHistTileRows > sub_rows) {
+      flush();
+      since_flush = 0;
+      __syncthreads();
+    }
+  }
+  flush();
+}
+
+#define LGBM_B200_HIST_INST(M, G) \
+  template __global__ void k_hist<M, G>(const __grid_constant__ DCtx, DTileTable, int32_t);
+LGBM_B200_HIST_INST(0, 1)
+LGBM_B200_HIST_INST(1, 1)
+LGBM_B200_HIST_INST(2, 1)
+LGBM_B200_HIST_INST(2, 2)
+LGBM_B200_HIST_INST(2, 3)
+LGBM_B200_HIST_INST(2, 4)
+#undef LGBM_B200_HIST_INST
+
+size_t hist_smem_bytes(int mode, int ng) {
+  const size_t cell = mode == 2 ? 4 : 16;
+  return (size_t)ng * kMaxBins * 32 * cell + (size_t)kHistTileRows * 32 * ng + (size_t)kHistTileRows * 8;
+}
+
+const void* hist_kernel(int mode, int ng) {
+  if (mode == 0) return reinterpret_cast<const void*>(&k_hist<0, 1>);
+  if (mode == 1) return reinterpret_cast<const void*>(&k_hist<1, 1>);
+  switch (ng) {
+    case 1: return reinterpret_cast<const void*>(&k_hist<2, 1>);
+    case 2: return reinterpret_cast<const void*>(&k_hist<2, 2>);
+    case 3: return reinterpret_cast<const void*>(&k_hist<2, 3>);
+    default: return reinterpret_cast<const void*>(&k_hist<2, 4>);
   }
 }
-template __global__ void k_hist_lane<0>(const __grid_constant__ DCtx, DTileTable, int32_t);
-template __global__ void k_hist_lane<1>(const __grid_constant__ DCtx, DTileTable, int32_t);
-template __global__ void k_hist_lane<2>(const __grid_constant__ DCtx, DTileTable, int32_t);
+
+void launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                 int32_t sub_rows) {
+  if (mode == 0) k_hist<0, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+  else if (mode == 1) k_hist<1, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+  else if (ng == 1) k_hist<2, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+  else if (ng == 2) k_hist<2, 2><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+  else if (ng == 3) k_hist<2, 3><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+  else k_hist<2, 4><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+}
 
 // =====================================================================================
 // split scan (split.rs:246-891 and :930-1400) — one CTA of two warps per
@@ -620,11 +678,250 @@ __device__ __noinline__ bool scan_categorical(ScanSmem& sm, const DFeature& m, c
   return is_splittable;
 }
 
-// find_best_threshold (split.rs:246-271, :930-950) for one leaf and feature.
+// One direction of FindBestThresholdSequentially (split.rs:676-891 and
+// :995-1190) over the view in `sm`, by the whole CTA. Warp 0 forms the
+// cumulative sums in the reference's order (FP64: a lane carry chain, one
+// add per visited bin in scan order; packed integers: any order is exact);
+// then thread t evaluates candidate t and the CTA reduces the first break
+// and the best gain with the sequential loop's rules. Thread 0 applies the
+// winner to `out`. Returns whether any candidate was splittable.
 template <bool kInt>
-__device__ bool find_best_threshold_warp(ScanSmem& sm, const DFeature& m, const DParams& p, LeafCtx lc, DSplit& out) {
-  const int lane = threadIdx.x & 31;
+__device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc,
+                                     double min_gain_shift, double cnt_factor, bool reverse, bool skip_default,
+                                     bool na_as_missing, DSplit& out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int offset = m.offset;
+  const int len = m.view_len;
+  int32_t t_lo, t_hi;
+  if (reverse) {
+    t_hi = m.num_bin - 1 - offset - (int32_t)na_as_missing;
+    t_lo = 1 - offset;
+  } else {
+    t_lo = 0;
+    t_hi = m.num_bin - 2 - offset;
+  }
+  const int32_t skip_t = skip_default ? m.default_bin - offset : INT32_MIN;
+  auto visited = [&](int t) { return t >= t_lo && t <= t_hi && t != skip_t && t < len; };
+  // extra candidate t = -1 (forward with NaN missing and no stored bin 0)
+  const bool first_extra = !reverse && na_as_missing && offset == 1;
+  const int32_t nstored = m.num_bin - offset;
+  const int khi = len > 0 ? (len - 1) / kPer : -1;
+  if (warp == 0) {
+    if (!kInt) {
+      double a = 0.0, b = kEpsilon;
+      int32_t c = 0;
+      if (first_extra) {  // split.rs:787-800: the leaf sums minus every stored bin, ascending
+        a = lc.sum_g;
+        b = lc.sum_h - kEpsilon;
+        c = lc.num_data;
+        carry_chain(false, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
+          int t = lane * kPer + j;
+          if (t < nstored && t < len) {
+            x -= sm.g[t];
+            y -= sm.h[t];
+            z -= sm.ce[t];
+          }
+        });
+        if (lane == 0) {
+          sm.eg = a;
+          sm.eh = b;
+          sm.ec = c;
+        }
+      }
+      carry_chain(reverse, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
+        int t = lane * kPer + j;
+        if (visited(t)) {
+          x += sm.g[t];
+          y += sm.h[t];
+          z += sm.ce[t];
+          sm.cg[t] = x;
+          sm.ch[t] = y;
+          sm.cc[t] = z;
+        }
+      });
+    } else {
+      // exact packed sums: lane-local part in scan order plus a warp scan of lane totals
+      int64_t loc = 0;
+      for (int jj = 0; jj < kPer; ++jj) {
+        int j = reverse ? kPer - 1 - jj : jj;
+        int t = lane * kPer + j;
+        if (visited(t)) {
+          loc = (int64_t)((uint64_t)loc + (uint64_t)sm.ig[t]);
+          sm.cq[t] = loc;
+        }
+      }
+      int64_t incl = loc;
+      for (int o = 1; o < 32; o <<= 1) {
+        int64_t other = reverse ? __shfl_down_sync(0xffffffffu, incl, o) : __shfl_up_sync(0xffffffffu, incl, o);
+        bool ok = reverse ? lane + o < 32 : lane >= o;
+        if (ok) incl = (int64_t)((uint64_t)incl + (uint64_t)other);
+      }
+      int64_t base = 0;
+      if (first_extra) {
+        int64_t all = 0;
+        for (int j = 0; j < kPer; ++j) {
+          int t = lane * kPer + j;
+          if (t < nstored && t < len) all = (int64_t)((uint64_t)all + (uint64_t)sm.ig[t]);
+        }
+        for (int o = 16; o > 0; o >>= 1)
+          all = (int64_t)((uint64_t)all + (uint64_t)__shfl_xor_sync(0xffffffffu, all, o));
+        base = (int64_t)((uint64_t)lc.int_sum - (uint64_t)all);
+        if (lane == 0) {
+          sm.eq = base;
+          sm.ec = round_int((double)int_hess(base) * cnt_factor);
+        }
+      }
+      const int64_t add = (int64_t)((uint64_t)base + (uint64_t)incl - (uint64_t)loc);
+      for (int j = 0; j < kPer; ++j) {
+        int t = lane * kPer + j;
+        if (visited(t)) {
+          int64_t v = (int64_t)((uint64_t)add + (uint64_t)sm.cq[t]);
+          sm.cq[t] = v;
+          sm.cc[t] = round_int((double)int_hess(v) * cnt_factor);
+        }
+      }
+    }
+    if (lane == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
+  }
+  __syncthreads();
+  const int32_t min_data = p.min_data_in_leaf;
+  const double min_hess = p.min_sum_hessian_in_leaf;
+  // accumulated side's values of candidate t (t = -1: the extra candidate)
+  auto acc = [&](int t, double& ag, double& ah, int32_t& ac, int64_t& aq) {
+    if (t < 0) {
+      ag = sm.eg;
+      ah = sm.eh;
+      ac = sm.ec;
+      aq = sm.eq;
+    } else {
+      ag = kInt ? 0.0 : sm.cg[t];
+      ah = kInt ? 0.0 : sm.ch[t];
+      ac = sm.cc[t];
+      aq = kInt ? sm.cq[t] : 0;
+    }
+  };
+  auto sides = [&](double ah, int64_t aq, double& ha, double& hr) {
+    if (kInt) {
+      ha = (double)int_hess(aq) * lc.hs;
+      hr = (double)int_hess((int64_t)((uint64_t)lc.int_sum - (uint64_t)aq)) * lc.hs;
+    } else {
+      ha = ah;
+      hr = lc.sum_h - ah;
+    }
+  };
+  // thread 0 also owns the extra candidate
+  const int ncand = (tid == 0 && first_extra) ? 2 : 1;
+  // pass 1: the first break in scan order
+  {
+    int32_t brk = reverse ? INT32_MIN : INT32_MAX;
+#pragma unroll 1
+    for (int k = 0; k < ncand; ++k) {
+      const int t = k == 0 ? tid : -1;
+      if (t >= 0 && !visited(t)) continue;
+      double ag, ah, ha, hr;
+      int32_t ac;
+      int64_t aq;
+      acc(t, ag, ah, ac, aq);
+      sides(ah, aq, ha, hr);
+      bool skip1 = ac < min_data || ha < min_hess;
+      if (!skip1 && (lc.num_data - ac < min_data || hr < min_hess)) brk = reverse ? max(brk, t) : min(brk, t);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      int32_t ob = __shfl_xor_sync(0xffffffffu, brk, o);
+      brk = reverse ? max(brk, ob) : min(brk, ob);
+    }
+    if (lane == 0 && brk != (reverse ? INT32_MIN : INT32_MAX)) {
+      if (reverse) atomicMax(&sm.brk, brk);
+      else atomicMin(&sm.brk, brk);
+    }
+  }
+  __syncthreads();
+  const int32_t brk = sm.brk;
+  // pass 2: gains of the candidates before the break
+  double best_gain = -INFINITY;
+  int32_t best_t = INT32_MIN;
+  bool splittable = false;
+#pragma unroll 1
+  for (int k = 0; k < ncand; ++k) {
+    const int t = k == 0 ? tid : -1;
+    if (t >= 0 && !visited(t)) continue;
+    if (t >= 0 ? (reverse ? t <= brk : t >= brk) : !(brk > -1)) continue;
+    double ag, ah, ha, hr;
+    int32_t ac;
+    int64_t aq;
+    acc(t, ag, ah, ac, aq);
+    sides(ah, aq, ha, hr);
+    if (ac < min_data || ha < min_hess) continue;
+    double ga, gr;
+    if (kInt) {
+      int64_t rest = (int64_t)((uint64_t)lc.int_sum - (uint64_t)aq);
+      ga = (double)int_grad(aq) * lc.gs;
+      gr = (double)int_grad(rest) * lc.gs;
+      ha += kEpsilon;
+      hr += kEpsilon;
+    } else {
+      ga = ag;
+      gr = lc.sum_g - ag;
+    }
+    int32_t rc = lc.num_data - ac;
+    double gain = reverse ? split_gain(gr, hr, ga, ha, p, rc, ac, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
+                                       m.monotone_type)
+                          : split_gain(ga, ha, gr, hr, p, ac, rc, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
+                                       m.monotone_type);
+    if (gain <= min_gain_shift) continue;
+    splittable = true;
+    if (gain > best_gain || (gain == best_gain && best_t != INT32_MIN && (reverse ? t > best_t : t < best_t))) {
+      best_gain = gain;
+      best_t = t;
+    }
+  }
+  warp_pick(reverse, best_gain, best_t);
   if (lane == 0) {
+    sm.wgain[warp] = best_gain;
+    sm.wt[warp] = best_t;
+  }
+  const bool any = __syncthreads_or(splittable) != 0;
+  if (tid == 0) {
+    double bg = -INFINITY;
+    int32_t bt = INT32_MIN;
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+      double og = sm.wgain[w];
+      int32_t ot = sm.wt[w];
+      if (og > bg || (og == bg && ot != INT32_MIN && (bt == INT32_MIN || (reverse ? ot > bt : ot < bt)))) {
+        bg = og;
+        bt = ot;
+      }
+    }
+    ScanBest r;
+    r.splittable = any;
+    r.gain = bg;
+    r.t = bt;
+    r.acc_g = r.acc_h = 0.0;
+    r.acc_c = 0;
+    r.acc_q = 0;
+    if (bt != INT32_MIN) {
+      double ag, ah;
+      int32_t ac;
+      int64_t aq;
+      acc(bt, ag, ah, ac, aq);
+      r.acc_g = ag;
+      r.acc_h = ah;
+      r.acc_c = ac;
+      r.acc_q = aq;
+    }
+    apply_direction<kInt>(r, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data, lc.parent_output,
+                          lc.mc, lc.cmin, lc.cmax, min_gain_shift, cnt_factor, reverse, out);
+  }
+  __syncthreads();
+  return any;
+}
+
+// find_best_threshold (split.rs:246-271, :930-950) for one leaf and feature,
+// by the whole CTA; the view is in `sm` (g/h, or ig for the quantized form).
+template <bool kInt>
+__device__ bool find_best_threshold_block(ScanSmem& sm, const DFeature& m, const DParams& p, LeafCtx lc, DSplit& out) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
     out.default_left = 1;
     out.gain = -INFINITY;
     out.num_cat = 0;
@@ -633,54 +930,35 @@ __device__ bool find_best_threshold_warp(ScanSmem& sm, const DFeature& m, const 
   if (!kInt) lc.sum_h = lc.sum_h + 2.0 * kEpsilon;
   bool ok;
   if (m.bin_type == 1) {
-    ok = scan_categorical<kInt>(sm, m, p, lc, out);
+    __syncthreads();
+    if (tid < 32) {
+      bool r = scan_categorical<kInt>(sm, m, p, lc, out);
+      if (tid == 0) sm.ok = r ? 1 : 0;
+    }
+    __syncthreads();
+    ok = sm.ok != 0;
   } else {
-    if (lane == 0) out.monotone_type = m.monotone_type;
+    if (tid == 0) out.monotone_type = m.monotone_type;
     double sg = kInt ? (double)int_grad(lc.int_sum) * lc.gs : lc.sum_g;
     double sh = kInt ? (double)int_hess(lc.int_sum) * lc.hs : lc.sum_h;
     double min_gain_shift = leaf_gain(sg, sh, p, lc.num_data, lc.parent_output) + p.min_gain_to_split;
     double cnt_factor =
         kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
-    LaneBins v;
-    int32_t ce[kPer];
-#pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      int t = lane * kPer + j;
-      v.g[j] = v.h[j] = 0.0;
-      v.q[j] = 0;
-      ce[j] = 0;
-      if (t < m.view_len) {
-        if (kInt) {
-          v.q[j] = sm.ig[t];
-        } else {
-          v.g[j] = sm.g[t];
-          v.h[j] = sm.h[t];
-          ce[j] = round_int(v.h[j] * cnt_factor);
-        }
-      }
-    }
-    __syncwarp();
-    auto run = [&](bool rev, bool sd, bool na) {
-      ScanBest r = scan_direction<kInt>(v, ce, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data,
-                                        lc.parent_output, lc.mc, lc.cmin, lc.cmax, min_gain_shift, cnt_factor, rev,
-                                        sd, na);
-      if (lane == 0)
-        apply_direction<kInt>(r, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data, lc.parent_output,
-                              lc.mc, lc.cmin, lc.cmax, min_gain_shift, cnt_factor, rev, out);
-      __syncwarp();
-      return r.splittable;
-    };
+    if (!kInt && tid < m.view_len) sm.ce[tid] = round_int(sm.h[tid] * cnt_factor);
+    __syncthreads();
     // split.rs:426-439: the directions scanned and their missing-value rules
     const bool two = m.num_bin > 2 && m.missing_type != 0;
     const bool skip_default = two && m.missing_type == 1;
     const bool na_missing = two && m.missing_type == 2;
     ok = false;
 #pragma unroll 1
-    for (int d = 0; d < (two ? 2 : 1); ++d) ok |= run(d == 0, skip_default, na_missing);
-    if (!two && lane == 0 && m.missing_type == 2) out.default_left = 0;
+    for (int d = 0; d < (two ? 2 : 1); ++d)
+      ok |= scan_direction_block<kInt>(sm, m, p, lc, min_gain_shift, cnt_factor, d == 0, skip_default, na_missing,
+                                        out);
+    if (!two && tid == 0 && m.missing_type == 2) out.default_left = 0;
   }
-  if (lane == 0) out.gain *= m.penalty;
-  __syncwarp();
+  if (tid == 0) out.gain *= m.penalty;
+  __syncthreads();
   return ok;
 }
 
@@ -787,74 +1065,73 @@ __device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl) {
 }
 
 template <bool kInt>
-__global__ void __launch_bounds__(64) k_scan(const __grid_constant__ DCtx c) {
+__global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ DCtx c) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ScanSmem* sms = reinterpret_cast<ScanSmem*>(smem_raw);
+  ScanSmem& sm = *reinterpret_cast<ScanSmem*>(smem_raw);
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
   const int f = blockIdx.x;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int side = blockIdx.y;  // 0: the smaller leaf, 1: the larger leaf
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const DFeature m = c.feats[f];
   const DParams& p = c.p;
   const int32_t nf = c.num_features;
   const bool have_larger = st->larger.leaf >= 0;
   const bool need = st->need_find != 0;
   const int32_t L = st->left_leaf;
-  bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
-  if (used) {
-    ScanSmem& sm = sms[warp];
-    ScanSmem& sm0 = sms[0];
+  const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
+  if (used && (side == 0 || have_larger)) {
     const DLeafSplits sl = st->smaller;
     const int len = m.view_len;
     const size_t sbase = (size_t)s.buf_of[sl.leaf] * c.total_bins + m.view_start;
-    // load the smaller leaf's view, fix the most frequent bin (histogram.rs:42-56)
-    if (warp == 0) {
-      if (kInt) {
-        const int64_t* hs = reinterpret_cast<const int64_t*>(s.hist) + sbase;
-        for (int i = lane; i < len; i += 32) sm0.ig[i] = hs[i];
+    // the smaller leaf's view with its most frequent bin fixed (histogram.rs:42-56)
+    if (kInt) {
+      const int64_t* hs = reinterpret_cast<const int64_t*>(s.hist) + sbase;
+      if (tid < len) sm.ig[tid] = hs[tid];
+    } else {
+      const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
+      if (tid < len) {
+        sm.g[tid] = hs[2 * tid];
+        sm.h[tid] = hs[2 * tid + 1];
+      }
+    }
+    __syncthreads();
+    if (m.most_freq_bin > 0 && warp == 0) {
+      if (kInt) {  // exact: any summation order
+        int64_t part = 0;
+        for (int i = lane; i < m.num_bin; i += 32)
+          if (i != m.most_freq_bin) part = (int64_t)((uint64_t)part + (uint64_t)sm.ig[i]);
+        for (int o = 16; o > 0; o >>= 1)
+          part = (int64_t)((uint64_t)part + (uint64_t)__shfl_xor_sync(0xffffffffu, part, o));
+        int64_t fixed = (int64_t)((uint64_t)sl.int_sum - (uint64_t)part);
         __syncwarp();
-        if (m.most_freq_bin > 0) {  // exact: any summation order
-          int64_t part = 0;
-          for (int i = lane; i < m.num_bin; i += 32)
-            if (i != m.most_freq_bin) part = (int64_t)((uint64_t)part + (uint64_t)sm0.ig[i]);
-          for (int o = 16; o > 0; o >>= 1)
-            part = (int64_t)((uint64_t)part + (uint64_t)__shfl_xor_sync(0xffffffffu, part, o));
-          int64_t acc = (int64_t)((uint64_t)sl.int_sum - (uint64_t)part);
-          __syncwarp();
-          if (lane == 0) {
-            sm0.ig[m.most_freq_bin] = acc;
-            reinterpret_cast<int64_t*>(s.hist)[sbase + m.most_freq_bin] = acc;
-          }
+        if (lane == 0) {
+          sm.ig[m.most_freq_bin] = fixed;
+          if (side == 0) reinterpret_cast<int64_t*>(s.hist)[sbase + m.most_freq_bin] = fixed;
         }
-      } else {
-        const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
-        for (int i = lane; i < len; i += 32) {
-          sm0.g[i] = hs[2 * i];
-          sm0.h[i] = hs[2 * i + 1];
-        }
-        __syncwarp();
-        if (m.most_freq_bin > 0) {  // sequential subtraction in bin order, as a lane carry chain
-          double g8[kPer], h8[kPer];
+      } else {  // sequential subtraction in bin order, as a lane carry chain
+        double g8[kPer], h8[kPer];
 #pragma unroll
-          for (int j = 0; j < kPer; ++j) {
-            int t = lane * kPer + j;
-            g8[j] = t < len ? sm0.g[t] : 0.0;
-            h8[j] = t < len ? sm0.h[t] : 0.0;
+        for (int j = 0; j < kPer; ++j) {
+          int t = lane * kPer + j;
+          g8[j] = t < len ? sm.g[t] : 0.0;
+          h8[j] = t < len ? sm.h[t] : 0.0;
+        }
+        double g = sl.sum_gradients, h = sl.sum_hessians;
+        int32_t unused = 0;
+        carry_chain(false, 0, (m.num_bin - 1) / kPer, g, h, unused, [&](int j, double& x, double& y, int32_t&) {
+          int t = lane * kPer + j;
+          if (t < m.num_bin && t != m.most_freq_bin) {
+            x -= g8[j];
+            y -= h8[j];
           }
-          double g = sl.sum_gradients, h = sl.sum_hessians;
-          int32_t unused = 0;
-          carry_chain(false, 0, (m.num_bin - 1) / kPer, g, h, unused, [&](int j, double& x, double& y, int32_t&) {
-            int t = lane * kPer + j;
-            if (t < m.num_bin && t != m.most_freq_bin) {
-              x -= g8[j];
-              y -= h8[j];
-            }
-          });
-          __syncwarp();
-          if (lane == 0) {
-            sm0.g[m.most_freq_bin] = g;
-            sm0.h[m.most_freq_bin] = h;
+        });
+        __syncwarp();
+        if (lane == 0) {
+          sm.g[m.most_freq_bin] = g;
+          sm.h[m.most_freq_bin] = h;
+          if (side == 0) {
             double* w = reinterpret_cast<double*>(s.hist) + 2 * (sbase + m.most_freq_bin);
             w[0] = g;
             w[1] = h;
@@ -863,50 +1140,45 @@ __global__ void __launch_bounds__(64) k_scan(const __grid_constant__ DCtx c) {
       }
     }
     __syncthreads();
-    if (warp == 1 && have_larger) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
-      const DLeafSplits ll = st->larger;
-      const size_t lbase = (size_t)s.buf_of[ll.leaf] * c.total_bins + m.view_start;
-      if (kInt) {
-        int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
-        for (int i = lane; i < len; i += 32) {
-          int64_t v = (int64_t)((uint64_t)lh[i] - (uint64_t)sm0.ig[i]);
-          sm.ig[i] = v;
-          lh[i] = v;
-        }
-      } else {
-        double* lh = reinterpret_cast<double*>(s.hist) + 2 * lbase;
-        for (int i = lane; i < len; i += 32) {
-          double g = lh[2 * i] - sm0.g[i], h = lh[2 * i + 1] - sm0.h[i];
-          sm.g[i] = g;
-          sm.h[i] = h;
-          lh[2 * i] = g;
-          lh[2 * i + 1] = h;
+    if (side == 1) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
+      const size_t lbase = (size_t)s.buf_of[st->larger.leaf] * c.total_bins + m.view_start;
+      if (tid < len) {
+        if (kInt) {
+          int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
+          int64_t v = (int64_t)((uint64_t)lh[tid] - (uint64_t)sm.ig[tid]);
+          sm.ig[tid] = v;
+          lh[tid] = v;
+        } else {
+          double* lh = reinterpret_cast<double*>(s.hist) + 2 * lbase;
+          double g = lh[2 * tid] - sm.g[tid], h = lh[2 * tid + 1] - sm.h[tid];
+          sm.g[tid] = g;
+          sm.h[tid] = h;
+          lh[2 * tid] = g;
+          lh[2 * tid + 1] = h;
         }
       }
+      __syncthreads();
     }
-    __syncwarp();
-    if (warp == 0 || have_larger) {
-      const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
-      LeafCtx lc;
-      lc.sum_g = ls.sum_gradients;
-      lc.sum_h = ls.sum_hessians;
-      lc.int_sum = ls.int_sum;
-      lc.gs = st->grad_scale;
-      lc.hs = st->hess_scale;
-      lc.num_data = ls.num_data;
-      // learner/mod.rs:1303-1309 parent output
-      lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
-                                                  : ls.weight;
-      lc.mc = p.use_monotone != 0;
-      lc.cmin = s.cmin[ls.leaf];
-      lc.cmax = s.cmax[ls.leaf];
-      DSplit& out = s.feat_res[warp * nf + f];
-      bool ok = find_best_threshold_warp<kInt>(sm, m, p, lc, out);
-      if (lane == 0) {
-        out.feature = m.real_index;
-        out.inner = f;
-        s.feat_ok[warp * nf + f] = ok ? 1 : 0;
-      }
+    const DLeafSplits ls = side == 0 ? st->smaller : st->larger;
+    LeafCtx lc;
+    lc.sum_g = ls.sum_gradients;
+    lc.sum_h = ls.sum_hessians;
+    lc.int_sum = ls.int_sum;
+    lc.gs = st->grad_scale;
+    lc.hs = st->hess_scale;
+    lc.num_data = ls.num_data;
+    // learner/mod.rs:1303-1309 parent output
+    lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
+                                                : ls.weight;
+    lc.mc = p.use_monotone != 0;
+    lc.cmin = s.cmin[ls.leaf];
+    lc.cmax = s.cmax[ls.leaf];
+    DSplit& out = s.feat_res[side * nf + f];
+    bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
+    if (tid == 0) {
+      out.feature = m.real_index;
+      out.inner = f;
+      s.feat_ok[side * nf + f] = ok ? 1 : 0;
     }
   }
   // last CTA of this slot: best split per leaf, best leaf, tree bookkeeping
@@ -914,14 +1186,14 @@ __global__ void __launch_bounds__(64) k_scan(const __grid_constant__ DCtx c) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    last = atomicAdd(&st->scan_counter, 1) == nf - 1;
+    last = atomicAdd(&st->scan_counter, 1) == 2 * nf - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   if (need) {
     // warp w reduces leaf side w (0 smaller, 1 larger)
-    if (warp == 0 || have_larger) {
+    if (warp == 0 || (warp == 1 && have_larger)) {
       const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
       double pen = p.use_monotone ? monotone_split_gain_penalty(s.tree.leaf_depth[ls.leaf], p.monotone_penalty) : 1.0;
       double bg = -INFINITY;
@@ -1151,36 +1423,58 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
       tile_left += warp_tot[w];
     }
     const int32_t excl = wbase + incl - nleft;
-    // decoupled look-back on the left count
-    if (tid == 0) {
+    // decoupled look-back on the left count: warp 0 reads 32 predecessors at a
+    // time and sums back to the nearest one whose inclusive prefix is posted
+    if (warp == 0) {
       unsigned long long* stat = s.tile_status;
       if (tile == 0) {
-        atomicExch(&stat[0], pack_status(epoch, kFlagInc, (uint64_t)tile_left));
-        s_prefix = 0;
+        if (lane == 0) {
+          atomicExch(&stat[0], pack_status(epoch, kFlagInc, (uint64_t)tile_left));
+          s_prefix = 0;
+        }
       } else {
-        atomicExch(&stat[tile], pack_status(epoch, kFlagAgg, (uint64_t)tile_left));
+        if (lane == 0) atomicExch(&stat[tile], pack_status(epoch, kFlagAgg, (uint64_t)tile_left));
         int64_t acc = 0;
-        int32_t pred = tile - 1;
+        int32_t base = tile - 1;
         int spins = 0;
-        while (pred >= 0) {
-          unsigned long long v = atomicAdd(&stat[pred], 0ull);
-          uint32_t ve = (uint32_t)((v >> 31) & kEpochMask);
-          unsigned long long flag = v & (3ull << 62);
-          if (ve != (epoch & kEpochMask) || flag == 0) {
-            if (++spins > kSpinLimit) {
-              st->status = kStatusTimeout;
-              st->done = 1;
+        while (true) {
+          const int32_t pred = base - lane;
+          bool valid = true, inc = true;
+          uint64_t val = 0;
+          if (pred >= 0) {
+            unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(&stat[pred]);
+            uint32_t ve = (uint32_t)((v >> 31) & kEpochMask);
+            unsigned long long flag = v & (3ull << 62);
+            valid = ve == (epoch & kEpochMask) && flag != 0;
+            inc = flag == kFlagInc;
+            val = v & kValueMask;
+          }
+          const unsigned inc_mask = __ballot_sync(0xffffffffu, valid && inc);
+          const unsigned bad_mask = __ballot_sync(0xffffffffu, !valid);
+          const int first_inc = inc_mask ? __ffs(inc_mask) - 1 : 32;
+          const unsigned need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
+          if (bad_mask & need) {
+            if (++spins > kSpinLimit) {  // give up: the prefix 0 keeps every write in the leaf's range
+              if (lane == 0) {
+                st->status = kStatusTimeout;
+                st->done = 1;
+              }
+              acc = 0;
               break;
             }
             __nanosleep(32);
             continue;
           }
-          acc += (int64_t)(v & kValueMask);
-          if (flag == kFlagInc) break;
-          --pred;
+          int64_t part = lane <= first_inc ? (int64_t)val : 0;
+          for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+          acc += part;
+          if (first_inc < 32) break;
+          base -= 32;
         }
-        atomicExch(&stat[tile], pack_status(epoch, kFlagInc, (uint64_t)(acc + tile_left)));
-        s_prefix = (int32_t)acc;
+        if (lane == 0) {
+          atomicExch(&stat[tile], pack_status(epoch, kFlagInc, (uint64_t)(acc + tile_left)));
+          s_prefix = (int32_t)acc;
+        }
       }
     }
     __syncthreads();
