@@ -281,6 +281,22 @@ void lgbm_b200_forest_destroy(LgbmB200Forest* f);
 int lgbm_b200_predict(LgbmB200Forest* f, const float* X, int64_t nrow, int32_t ncol, double* out,
                       int32_t location);
 
+/* lgbm_b200_predict with HOST buffers (X and out in host memory) that
+ * allocates no device memory; it has no counterpart in the reference. It is
+ * for callers that cannot allocate while they predict: a serving process
+ * whose free device memory is held by another allocator, or a
+ * latency-bound thread that must not wait on allocation or on the
+ * synchronisation that freeing memory can bring. Rows and scores go
+ * through one 16 MiB array in device memory compiled into the library, in
+ * chunks of rows; a row needing more than 16 MiB - 256 bytes of staging
+ * (4 x ncol + 8 x num_tree_per_iteration) is rejected with
+ * LGBM_B200_ERR_INVALID_PARAMETER. The array is shared by every call on a
+ * device: calls that overlap in time on one device race on it and must be
+ * serialised by the caller. The first call on a device resolves the array's
+ * address (cudaGetSymbolAddress); make it before capturing any stream on
+ * that device. Results equal lgbm_b200_predict's. */
+int lgbm_b200_predict_noalloc(LgbmB200Forest* f, const float* X, int64_t nrow, int32_t ncol, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -533,3 +533,12 @@ int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t n
 }
 
 }  // extern "C"
+
+namespace lgbm_b200 {
+void forest_parts(const LgbmB200Forest* F, int* device, cudaStream_t* stream, const DForest** f, int32_t* ntpi) {
+  *device = F->device;
+  *stream = F->stream;
+  *f = &F->f;
+  *ntpi = F->ntpi;
+}
+}  // namespace lgbm_b200

@@ -22,4 +22,8 @@ struct DForest {
 
 void launch_predict(const DForest& f, const float* X, int64_t nrow, int32_t ncol, double* out, cudaStream_t s);
 
+// Device, stream, flat layout and trees per iteration of a forest made by
+// lgbm_b200_forest_create.
+void forest_parts(const LgbmB200Forest* F, int* device, cudaStream_t* stream, const DForest** f, int32_t* ntpi);
+
 }  // namespace lgbm_b200

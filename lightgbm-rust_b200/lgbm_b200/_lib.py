@@ -118,6 +118,7 @@ SIGNATURES = {
     "lgbm_b200_forest_create": (C.c_int, [P(TreeView), i32, i32, i32, P(C.c_void_p)]),
     "lgbm_b200_forest_destroy": (None, [C.c_void_p]),
     "lgbm_b200_predict": (C.c_int, [C.c_void_p, C.c_void_p, i64, i32, C.c_void_p, i32]),
+    "lgbm_b200_predict_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, i64, i32, C.c_void_p]),
 }
 
 _lib = None
