@@ -68,15 +68,16 @@ struct DSlotState {
   int32_t status;
   int32_t need_find;       // before_find_best_split of (left_leaf, right_leaf)
   int32_t left_leaf, right_leaf;
-  int32_t split_leaf, new_leaf, split_inner;  // the split the partition applies
-  int32_t scan_counter, part_ticket, part_done;
+  int32_t scan_counter;
+  int32_t part_ticket;     // next row tile of the running partition
+  int32_t part_done;       // partition CTAs finished
+  int32_t part_left;       // rows sent left (posted by the last tile)
   uint32_t part_epoch;
   int32_t num_used;        // in-bag rows
   int32_t num_cat;         // categorical splits so far
   int32_t use_indices_root;
   double grad_scale, hess_scale;  // quantized gradients
   DLeafSplits smaller, larger;
-  uint8_t lut[kMaxBins];   // partition: goes-left per stored group value
   int64_t hist_rows;       // rows histogrammed in this tree (statistics)
 };
 

@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->num_cat = 0;
   st->scan_counter = 0;
   st->part_ticket = 0;
+  st->part_done = 0;
   st->hist_rows = 0;
   st->smaller.leaf = 0;
   st->smaller.num_data = (int32_t)n;
@@ -974,15 +975,14 @@ __device__ __forceinline__ bool split_better(const DSplit& a, const DSplit& b) {
 }
 
 // Partition LUT over stored group values (learner/mod.rs:1313-1329): one
-// goes-left flag per value a row of the split feature can hold; warp-parallel.
-__device__ void write_partition_lut(const DCtx& c, const DSlot& s, int32_t bl) {
-  const int lane = threadIdx.x & 31;
-  const DSplit& info = s.best[bl];
+// goes-left flag per value a row of the split feature can hold; thread t
+// of the CTA writes value t.
+__device__ void build_partition_lut(const DCtx& c, const DSplit& info, uint8_t* lut) {
   const DFeature& m = c.feats[info.inner];
   const bool numerical = m.bin_type == 0;
   const bool default_left = numerical ? info.default_left != 0 : false;
   const int32_t ntb = m.view_len + 1;
-  for (int32_t raw = lane; raw < kMaxBins; raw += 32) {
+  for (int32_t raw = threadIdx.x; raw < kMaxBins; raw += blockDim.x) {
     uint8_t left = 0;
     if (raw < ntb) {
       uint32_t b = decode_bin((uint32_t)raw, m);
@@ -996,18 +996,17 @@ __device__ void write_partition_lut(const DCtx& c, const DSlot& s, int32_t bl) {
         else left = (uint8_t)bit(b);
       }
     }
-    s.st->lut[raw] = left;
+    lut[raw] = left;
   }
 }
 
 // The selected split is applied to the tree (tree.rs:240-297); one thread.
-__device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl) {
+__device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
   const DTree& t = s.tree;
   const DSplit& info = s.best[bl];
   const DFeature& m = c.feats[info.inner];
-  int32_t R = st->num_leaves_cur;
   int32_t node = R - 1;
   bool numerical = m.bin_type == 0;
   int32_t parent = t.leaf_parent[bl];
@@ -1056,12 +1055,7 @@ __device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl) {
       }
     }
   }
-  st->split_leaf = bl;
-  st->new_leaf = R;
-  st->split_inner = info.inner;
   st->num_leaves_cur = R + 1;
-  st->part_ticket = 0;
-  st->part_epoch += 1;
 }
 
 template <bool kInt>
@@ -1071,6 +1065,11 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
+  // the partition that follows claims its row tiles from this counter
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    st->part_ticket = 0;
+    st->part_done = 0;
+  }
   const int f = blockIdx.x;
   const int side = blockIdx.y;  // 0: the smaller leaf, 1: the larger leaf
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1181,114 +1180,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
       s.feat_ok[side * nf + f] = ok ? 1 : 0;
     }
   }
-  // last CTA of this slot: best split per leaf, best leaf, tree bookkeeping
-  __shared__ bool last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(&st->scan_counter, 1) == 2 * nf - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  if (need) {
-    // warp w reduces leaf side w (0 smaller, 1 larger)
-    if (warp == 0 || (warp == 1 && have_larger)) {
-      const DLeafSplits ls = warp == 0 ? st->smaller : st->larger;
-      double pen = p.use_monotone ? monotone_split_gain_penalty(s.tree.leaf_depth[ls.leaf], p.monotone_penalty) : 1.0;
-      double bg = -INFINITY;
-      int32_t bfeat = -1, bf = -1;
-      for (int ff = lane; ff < nf; ff += 32) {
-        bool u = s.bytree[ff] && (!have_larger || s.splittable[L * nf + ff]);
-        if (!u) continue;
-        DSplit& r = s.feat_res[warp * nf + ff];
-        double g = r.gain;
-        if (r.monotone_type != 0) g *= pen;
-        if (better_than(g, r.feature, bg, bfeat)) {
-          bg = g;
-          bfeat = r.feature;
-          bf = ff;
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        double og = __shfl_xor_sync(0xffffffffu, bg, o);
-        int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
-        int32_t off = __shfl_xor_sync(0xffffffffu, bf, o);
-        if (better_than(og, ofe, bg, bfeat)) {
-          bg = og;
-          bfeat = ofe;
-          bf = off;
-        }
-      }
-      // splittable flags of this leaf (learner/mod.rs:842-849, :1066-1086)
-      uint8_t* spl_new = s.feat_ok + 2 * nf + warp * nf;  // staged, applied after both reads
-      for (int ff = lane; ff < nf; ff += 32) {
-        bool u = s.bytree[ff] && (!have_larger || s.splittable[L * nf + ff]);
-        spl_new[ff] = u ? s.feat_ok[warp * nf + ff] : 0;
-      }
-      if (lane == 0) {
-        DSplit& dst = s.best[ls.leaf];
-        if (bf >= 0) {
-          dst = s.feat_res[warp * nf + bf];
-          dst.gain = bg;
-        } else {
-          dst.feature = -1;
-          dst.inner = -1;
-          dst.gain = -INFINITY;
-        }
-        s.bgain[ls.leaf] = dst.gain;
-        s.bfeat[ls.leaf] = dst.feature;
-      }
-    }
-    __syncthreads();
-    for (int ff = threadIdx.x; ff < nf; ff += blockDim.x) {
-      s.splittable[st->smaller.leaf * nf + ff] = s.feat_ok[2 * nf + ff];
-      if (have_larger) s.splittable[st->larger.leaf * nf + ff] = s.feat_ok[3 * nf + ff];
-    }
-  }
-  __syncthreads();
-  if (warp != 0) return;
-  // best leaf (learner/mod.rs:698-706): larger gain, smaller feature, smaller leaf
-  double bg = -INFINITY;
-  int32_t bfeat = -1, bl = INT32_MAX;
-  for (int l = lane; l < p.num_leaves; l += 32) {
-    double g = s.bgain[l];
-    int32_t fe = s.bfeat[l];
-    if (bl == INT32_MAX || better_than(g, fe, bg, bfeat)) {
-      bg = g;
-      bfeat = fe;
-      bl = l;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    double og = __shfl_xor_sync(0xffffffffu, bg, o);
-    int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
-    int32_t ol = __shfl_xor_sync(0xffffffffu, bl, o);
-    bool take = false;
-    if (ol != INT32_MAX) {
-      if (bl == INT32_MAX) take = true;
-      else if (better_than(og, ofe, bg, bfeat)) take = true;
-      else if (!better_than(bg, bfeat, og, ofe) && ol < bl) take = true;
-    }
-    if (take) {
-      bg = og;
-      bfeat = ofe;
-      bl = ol;
-    }
-  }
-  if (!(bg > 0.0)) {
-    if (lane == 0) {
-      st->scan_counter = 0;
-      st->done = 1;
-    }
-    return;
-  }
-  write_partition_lut(c, s, bl);
-  __syncwarp();
-  if (lane == 0) {
-    st->scan_counter = 0;
-    apply_split(c, s, bl);
-  }
 }
 template __global__ void k_scan<false>(const __grid_constant__ DCtx);
 template __global__ void k_scan<true>(const __grid_constant__ DCtx);
@@ -1311,9 +1202,8 @@ __device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsign
   return flag | ((unsigned long long)(epoch & kEpochMask) << 31) | (v & kValueMask);
 }
 
-__device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t total_left) {
+__device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left) {
   DSlotState* st = s.st;
-  int32_t L = st->split_leaf, R = st->new_leaf;
   int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
   int32_t side = s.leaf_side[L];
   int32_t nl = total_left, nr = cnt - total_left;
@@ -1356,7 +1246,184 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t total_
   st->need_find = before_find_best_split(c, s, L, R) ? 1 : 0;
 }
 
-// Grid (G, 1, slots), kPartThreads threads.
+// Decision state a partition CTA derives from the scan results.
+struct SplitDecision {
+  double side_bg[2];     // best (penalized) gain of the smaller / larger new leaf
+  int32_t side_feat[2];  // its real feature, -1 none
+  int32_t side_bf[2];    // its inner feature, -1 none
+  double wbg[kPartThreads / 32];
+  int32_t wfeat[kPartThreads / 32], wleaf[kPartThreads / 32];
+  int32_t bl;            // the leaf to split, -1: the tree is finished
+};
+
+// Best split of a new leaf over its features and its per-feature splittable
+// flags (learner/mod.rs:842-849, :1066-1086); one warp.
+__device__ void new_leaf_best(const DCtx& c, const DSlot& s, int side, int32_t leaf, bool have_larger, int32_t Lft,
+                              double& bg, int32_t& bfeat, int32_t& bf) {
+  const int lane = threadIdx.x & 31;
+  const DParams& p = c.p;
+  const int32_t nf = c.num_features;
+  double pen = p.use_monotone ? monotone_split_gain_penalty(s.tree.leaf_depth[leaf], p.monotone_penalty) : 1.0;
+  bg = -INFINITY;
+  bfeat = -1;
+  bf = -1;
+  for (int ff = lane; ff < nf; ff += 32) {
+    bool u = s.bytree[ff] && (!have_larger || s.splittable[Lft * nf + ff]);
+    if (!u) continue;
+    const DSplit& r = s.feat_res[side * nf + ff];
+    double g = r.gain;
+    if (r.monotone_type != 0) g *= pen;
+    if (better_than(g, r.feature, bg, bfeat)) {
+      bg = g;
+      bfeat = r.feature;
+      bf = ff;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double og = __shfl_xor_sync(0xffffffffu, bg, o);
+    int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
+    int32_t off = __shfl_xor_sync(0xffffffffu, bf, o);
+    if (better_than(og, ofe, bg, bfeat)) {
+      bg = og;
+      bfeat = ofe;
+      bf = off;
+    }
+  }
+}
+
+// Leaf argmax rule of best_leaf (learner/mod.rs:698-706): larger gain, then
+// smaller feature, then smaller leaf.
+__device__ __forceinline__ bool leaf_takes(double og, int32_t ofe, int32_t ol, double bg, int32_t bfeat, int32_t bl) {
+  if (ol == INT32_MAX) return false;
+  if (bl == INT32_MAX) return true;
+  if (better_than(og, ofe, bg, bfeat)) return true;
+  return !better_than(bg, bfeat, og, ofe) && ol < bl;
+}
+
+// Split decision of this step, computed by every partition CTA: the best
+// split of the two new leaves (warps 0, 1), the best of the other leaves
+// (warps 2..), then the best leaf (thread 0).
+__device__ void decide_split(const DCtx& c, const DSlot& s, SplitDecision& d) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const DSlotState* st = s.st;
+  const bool need = st->need_find != 0;
+  const int32_t S = st->smaller.leaf, G = st->larger.leaf, Lft = st->left_leaf;
+  const bool have_larger = G >= 0;
+  const int32_t NL = c.p.num_leaves;
+  if (warp < 2) {
+    double bg = -INFINITY;
+    int32_t bfeat = -1, bf = -1;
+    if (need && (warp == 0 || have_larger)) new_leaf_best(c, s, warp, warp == 0 ? S : G, have_larger, Lft, bg, bfeat, bf);
+    if (lane == 0) {
+      d.side_bg[warp] = bf >= 0 ? bg : -INFINITY;
+      d.side_feat[warp] = bf >= 0 ? bfeat : -1;
+      d.side_bf[warp] = bf;
+    }
+  } else {
+    double bg = -INFINITY;
+    int32_t bfeat = -1, bl = INT32_MAX;
+    for (int32_t l = tid - 64; l < NL; l += kPartThreads - 64) {
+      if (need && (l == S || l == G)) continue;
+      double g = s.bgain[l];
+      int32_t fe = s.bfeat[l];
+      if (leaf_takes(g, fe, l, bg, bfeat, bl)) {
+        bg = g;
+        bfeat = fe;
+        bl = l;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double og = __shfl_xor_sync(0xffffffffu, bg, o);
+      int32_t ofe = __shfl_xor_sync(0xffffffffu, bfeat, o);
+      int32_t ol = __shfl_xor_sync(0xffffffffu, bl, o);
+      if (leaf_takes(og, ofe, ol, bg, bfeat, bl)) {
+        bg = og;
+        bfeat = ofe;
+        bl = ol;
+      }
+    }
+    if (lane == 0) {
+      d.wbg[warp] = bg;
+      d.wfeat[warp] = bfeat;
+      d.wleaf[warp] = bl;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double bg = -INFINITY;
+    int32_t bfeat = -1, bl = INT32_MAX;
+    auto offer = [&](double g, int32_t fe, int32_t l) {
+      if (leaf_takes(g, fe, l, bg, bfeat, bl)) {
+        bg = g;
+        bfeat = fe;
+        bl = l;
+      }
+    };
+    for (int w = 2; w < kPartThreads / 32; ++w) offer(d.wbg[w], d.wfeat[w], d.wleaf[w]);
+    if (need) {
+      offer(d.side_bg[0], d.side_feat[0], S);
+      if (have_larger) offer(d.side_bg[1], d.side_feat[1], G);
+    }
+    d.bl = (bl != INT32_MAX && bg > 0.0) ? bl : -1;
+  }
+  __syncthreads();
+}
+
+// End of a split step, by the last CTA of the launch to finish: the new
+// leaves' best splits and splittable flags are stored, the split is applied
+// to the tree (tree.rs:240-297) and the children's ranges, smaller / larger
+// choice and before_find_best_split are recorded. Every other CTA of the
+// launch has exited, so none of them reads the state changed here.
+__device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& d, int32_t bl, int32_t R,
+                            int32_t total_left) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  DSlotState* st = s.st;
+  const int32_t nf = c.num_features;
+  const bool need = st->need_find != 0;
+  const int32_t S = st->smaller.leaf, G = st->larger.leaf, Lft = st->left_leaf;
+  const bool have_larger = G >= 0;
+  __syncthreads();
+  if (need) {
+    for (int ff = tid; ff < nf; ff += blockDim.x) {
+      bool u = s.bytree[ff] && (!have_larger || s.splittable[Lft * nf + ff]);
+      uint8_t ns = u ? s.feat_ok[ff] : 0;
+      uint8_t ng = u ? s.feat_ok[nf + ff] : 0;
+      s.splittable[S * nf + ff] = ns;
+      if (have_larger) s.splittable[G * nf + ff] = ng;
+    }
+    if (warp < 2 && (warp == 0 || have_larger)) {
+      const int32_t leaf = warp == 0 ? S : G;
+      const int32_t bf = d.side_bf[warp];
+      DSplit& dst = s.best[leaf];
+      if (bf >= 0) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&s.feat_res[warp * nf + bf]);
+        uint32_t* w = reinterpret_cast<uint32_t*>(&dst);
+        for (int i = lane; i < (int)(sizeof(DSplit) / 4); i += 32) w[i] = src[i];
+        __syncwarp();
+        if (lane == 0) {
+          dst.gain = d.side_bg[warp];
+          s.bgain[leaf] = d.side_bg[warp];
+          s.bfeat[leaf] = dst.feature;
+        }
+      } else if (lane == 0) {
+        dst.feature = -1;
+        dst.inner = -1;
+        dst.gain = -INFINITY;
+        s.bgain[leaf] = -INFINITY;
+        s.bfeat[leaf] = -1;
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    apply_split(c, s, bl, R);
+    partition_finalize(c, s, bl, R, total_left);
+    st->part_epoch += 1;
+  }
+}
+
+// Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
+// step's split decision and the goes-left LUT, then claims row tiles.
 __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
@@ -1364,29 +1431,53 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   __shared__ uint8_t lut[kMaxBins];
   __shared__ int32_t warp_tot[kPartThreads / 32];
   __shared__ int32_t s_tile, s_prefix;
+  __shared__ SplitDecision dec;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int32_t L = st->split_leaf;
-  const int32_t R = st->new_leaf;
+  const int32_t R = st->num_leaves_cur;
+  const uint32_t epoch = st->part_epoch;
+  decide_split(c, s, dec);
+  const int32_t L = dec.bl;
+  if (L < 0) {
+    if (blockIdx.x == 0 && tid == 0) st->done = 1;
+    return;
+  }
+  const int32_t nf = c.num_features;
+  const DSplit& info = (st->need_find && L == st->smaller.leaf)   ? s.feat_res[dec.side_bf[0]]
+                       : (st->need_find && L == st->larger.leaf) ? s.feat_res[nf + dec.side_bf[1]]
+                                                                  : s.best[L];
+  const int32_t inner = info.inner;
+  build_partition_lut(c, info, lut);
   const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
   const int32_t side = s.leaf_side[L];
-  const uint32_t epoch = st->part_epoch;
-  const int32_t inner = st->split_inner;
   // zero the fresh histogram buffer R for the next smaller leaf
   {
     size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
     double* h = reinterpret_cast<double*>(s.hist) + (size_t)R * cells;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h[i] = 0.0;
   }
+  __syncthreads();
+  __shared__ bool s_last;
+  // the last CTA to exit ends the step
+  auto exit_step = [&]() {
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      s_last = atomicAdd(&st->part_done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      finish_step(c, s, dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+    }
+  };
   if (cnt == 0) {
-    if (blockIdx.x == 0 && tid == 0) partition_finalize(c, s, 0);
+    exit_step();
     return;
   }
-  for (int i = tid; i < kMaxBins; i += blockDim.x) lut[i] = st->lut[i];
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
   const int32_t ntiles = (cnt + kPartTile - 1) / kPartTile;
   const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
-  __syncthreads();
   while (true) {
     if (tid == 0) s_tile = atomicAdd(&st->part_ticket, 1);
     __syncthreads();
@@ -1493,9 +1584,10 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
         }
       }
     }
-    if (tile == ntiles - 1 && tid == 0) partition_finalize(c, s, prefix + tile_left);
+    if (tile == ntiles - 1 && tid == 0) st->part_left = prefix + tile_left;
     __syncthreads();
   }
+  exit_step();
 }
 
 // Column-major copy of the bin matrix (the partition reads one feature of the
