@@ -7,6 +7,9 @@ namespace lgbm_b200 {
 
 constexpr int kHistThreads = 512;
 constexpr int kHistTileRows = kHistThreads;  // rows staged per histogram tile: one per thread
+constexpr int kHistCluster = 8;              // CTAs per quantized histogram cluster (one reduction per cluster)
+// CTAs per histogram cluster of a form: the float forms' CTAs fill an SM each and flush alone
+__host__ __device__ constexpr int hist_cluster(int mode) { return mode == 2 ? kHistCluster : 1; }
 constexpr int kMaxTiles = 64;
 constexpr int kMaxLaneGroups = 4;  // 32-feature groups per histogram tile (int32 cells)
 

@@ -100,10 +100,19 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   h->scan_smem = sizeof(ScanSmem);
   CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
-  int per_sm = 1;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, kHistThreads, h->hist_smem));
-  per_sm = std::max(1, per_sm);
-  h->hist_grid = std::max(1, h->num_sms * per_sm / std::max(1, h->ntiles));
+  {
+    // the histogram runs in clusters (of hist_cluster(mode) CTAs): as many
+    // clusters as fit on the device at once, shared among the feature tiles
+    cudaLaunchConfig_t lc = {};
+    const int cl = hist_cluster(mode);
+    lc.gridDim = dim3(cl * 64, 1, 1);
+    lc.blockDim = dim3(kHistThreads, 1, 1);
+    lc.dynamicSmemBytes = h->hist_smem;
+    int clusters = 0;
+    CU(cudaOccupancyMaxActiveClusters(&clusters, hk, &lc));
+    if (clusters < 1) return Status(LGBM_B200_ERR_CUDA, "histogram cluster does not fit on the device");
+    h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
+  }
   h->part_grid = h->num_sms * 4;
   int32_t rpb = cfg->hist_rows_per_block > 0 ? cfg->hist_rows_per_block : 512;
 

@@ -13,6 +13,8 @@
 //   k_partition  stable-by-leaf row split with decoupled look-back, then the
 //                smaller/larger choice and before_find_best_split
 //                (partition.rs:107-174, learner/mod.rs:1200-1208, :712-731)
+#include <cooperative_groups.h>
+
 #include "device_common.cuh"
 #include "kernels.h"
 #include "scan_warp.cuh"
@@ -191,6 +193,11 @@ struct LeafRows {
   int64_t begin, count;
 };
 
+// Rows [r0, r1) of the smaller leaf for this CTA. CTAs are used in whole
+// clusters of kCl so that every CTA of a used cluster takes part in
+// the cluster's reduction (its row range may be empty); returns false for
+// CTAs of unused clusters and when no histogram is needed.
+template <int kCl>
 __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, LeafRows& lr, int64_t& r0, int64_t& r1) {
   DSlotState* st = s.st;
   if (st->done || !st->need_find) return false;
@@ -200,12 +207,13 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, LeafRo
   lr.idx = s.idx[s.leaf_side[leaf]];
   int64_t per = c.rows_per_block;
   int64_t active = min((int64_t)gridDim.x, (lr.count + per - 1) / per);
+  active = (active + kCl - 1) / kCl * kCl;
   if ((int64_t)blockIdx.x >= active) return false;
   int64_t chunk = (lr.count + active - 1) / active;
-  r0 = (int64_t)blockIdx.x * chunk;
+  r0 = min(lr.count, (int64_t)blockIdx.x * chunk);
   r1 = min(lr.count, r0 + chunk);
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) st->hist_rows += lr.count;
-  return r0 < r1;
+  return true;
 }
 
 // Feature tile of a histogram launch: features [f0, f1), stored bins [bin0, bin0 + nbins).
@@ -224,25 +232,37 @@ __device__ __forceinline__ void tile_of(const DTileTable& tt, int tile, int& f0,
 // while the current tile is accumulated. A tile is staged in shared memory
 // and accumulated in a bin-major layout: feature f0 + 32g + lane keeps its
 // cell of stored value `raw` at cells[g][raw][lane], so in every warp-wide
-// atomic the 32 lanes touch 32 different banks.
+// atomic the 32 lanes touch 32 different banks. Stored value 0 (the most
+// frequent bin) and the zero padding of short rows land in cells[g][0],
+// which no feature view contains.
 //   kMode 0: FP64 g / h cells (the reference's sums, reordered by atomics)
 //   kMode 1: FP32 (hi, lo) pairs per value, the rounding error of every
 //            add kept in lo (TwoSum), merged in FP64 when flushed
 //   kMode 2: int32 cells holding (g << 16) + h of quantized gradients,
 //            flushed at least every `sub_rows` rows into packed int64 sums
+// The quantized form runs in clusters of kHistCluster CTAs: at the end every
+// CTA reduces one slice of the cells over the cluster's shared memories
+// (distributed shared memory) and adds it to the leaf histogram, so a
+// cluster issues one global atomic per cell instead of one per CTA. The
+// float forms (one 148 KB CTA per SM) flush each CTA's own cells.
 template <int kMode, int kNG>
-__global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+__global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kHistThreads, 2)
+    k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+  namespace cg = cooperative_groups;
+  constexpr int kCl = hist_cluster(kMode);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const DSlot& s = c.slots[blockIdx.z];
   LeafRows lr;
   int64_t r0, r1;
-  if (!hist_setup(c, s, lr, r0, r1)) return;
+  if (!hist_setup<kCl>(c, s, lr, r0, r1)) return;
+  cg::cluster_group cluster = cg::this_cluster();
   int f0, f1, bin0, nbins;
   tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
   (void)nbins;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kHistThreads / 32;
   constexpr int kRowsPerWarp = kHistTileRows / kWarps;
+  static_assert(kRowsPerWarp == 32, "one staged row per lane of a warp");
   constexpr int kCellBytes = kMode == 2 ? 4 : 16;
   constexpr int kGroupCells = kMaxBins * 32;
   constexpr int kRowBytes = 32 * kNG;
@@ -251,14 +271,12 @@ __global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant_
   uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)kNG * kGroupCells * kCellBytes);
   int32_t* sq = reinterpret_cast<int32_t*>(sbins + kHistTileRows * 2 * kNG);
   float2* sgh = reinterpret_cast<float2*>(sq);
-  // per-lane feature facts for each group
-  int32_t vlen_g[kNG], vstart_g[kNG];
-#pragma unroll
-  for (int g = 0; g < kNG; ++g) {
-    int f = f0 + 32 * g + lane;
-    bool ok = g < ngroups && f < f1;
-    vlen_g[g] = ok ? c.feats[f].view_len : 0;
-    vstart_g[g] = ok ? c.feats[f].view_start : 0;
+  __shared__ int32_t s_vlen[32 * kNG], s_vstart[32 * kNG];
+  for (int i = threadIdx.x; i < 32 * kNG; i += kHistThreads) {
+    const int f = f0 + i;
+    const bool ok = (i >> 5) < ngroups && f < f1;
+    s_vlen[i] = ok ? c.feats[f].view_len : 0;
+    s_vstart[i] = ok ? c.feats[f].view_start : 0;
   }
   {
     uint4* z = reinterpret_cast<uint4*>(cells);
@@ -270,45 +288,42 @@ __global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant_
   double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
   unsigned long long* outi = reinterpret_cast<unsigned long long*>(s.hist) +
                              (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
-  // Flush the cells into the leaf histogram (cells of stored value 0, the
-  // most frequent bin, are outside every feature view). Thread t handles
-  // lane t % 32 of a value row, i.e. its own feature of each group.
-  auto flush = [&]() {
-#pragma unroll
-    for (int g = 0; g < kNG; ++g) {
-      if (g >= ngroups) break;
-      const int vl = vlen_g[g];
-      const size_t vs = (size_t)vstart_g[g];
-      for (int raw = 1 + warp; raw <= vl; raw += kWarps) {
-        const int k = raw * 32 + lane;
-        const size_t dst = vs + raw - 1;
-        if (kMode == 2) {
-          int32_t* ic = reinterpret_cast<int32_t*>(cells) + g * kGroupCells;
-          int32_t cell = ic[k];
-          if (cell != 0) {
-            int64_t hq = (int64_t)(cell & 0xFFFF);
-            int64_t gq = (int64_t)((cell - (int32_t)hq) >> 16);
-            atomicAdd(outi + dst, (unsigned long long)((uint64_t)(gq << 32) + (uint64_t)hq));
-            ic[k] = 0;
-          }
-        } else {
-          const unsigned char* base = cells + (size_t)g * kGroupCells * 16;
-          double gv, hv;
-          if (kMode == 0) {
-            const double* d = reinterpret_cast<const double*>(base);
-            gv = d[k];
-            hv = d[kGroupCells + k];
-          } else {
-            const float* fl = reinterpret_cast<const float*>(base);
-            gv = (double)fl[k] + (double)fl[kGroupCells + k];
-            hv = (double)fl[2 * kGroupCells + k] + (double)fl[3 * kGroupCells + k];
-          }
-          if (gv != 0.0 || hv != 0.0) {
-            atomicAdd(outf + 2 * dst, gv);
-            atomicAdd(outf + 2 * dst + 1, hv);
-          }
-        }
+  // Adds cell i (over groups) of the CTAs `src` to the leaf histogram; cells
+  // outside the features' views are skipped.
+  auto emit = [&](int i, auto read_cell) {
+    const int g = i / kGroupCells, k = i % kGroupCells;
+    const int raw = k >> 5, fl = (g << 5) | (k & 31);
+    if (raw == 0 || raw > s_vlen[fl]) return;
+    const size_t dst = (size_t)s_vstart[fl] + raw - 1;
+    if constexpr (kMode == 2) {
+      int64_t gq, hq;
+      read_cell(i, gq, hq);
+      if (gq != 0 || hq != 0) atomicAdd(outi + dst, (unsigned long long)((uint64_t)(gq << 32) + (uint64_t)hq));
+    } else {
+      double gv, hv;
+      read_cell(i, gv, hv);
+      if (gv != 0.0 || hv != 0.0) {
+        atomicAdd(outf + 2 * dst, gv);
+        atomicAdd(outf + 2 * dst + 1, hv);
       }
+    }
+  };
+  // the (g, h) of cell i in the shared memory `base` of one CTA
+  auto cell_of = [&](const unsigned char* base, int i, auto& gv, auto& hv) {
+    const int g = i / kGroupCells, k = i % kGroupCells;
+    if constexpr (kMode == 2) {
+      const int32_t cell = reinterpret_cast<const int32_t*>(base)[i];
+      const int64_t h = (int64_t)(cell & 0xFFFF);
+      gv = (int64_t)((cell - (int32_t)h) >> 16);
+      hv = h;
+    } else if constexpr (kMode == 0) {
+      const double* d = reinterpret_cast<const double*>(base + (size_t)g * kGroupCells * 16);
+      gv = d[k];
+      hv = d[kGroupCells + k];
+    } else {
+      const float* fl = reinterpret_cast<const float*>(base + (size_t)g * kGroupCells * 16);
+      gv = (double)fl[k] + (double)fl[kGroupCells + k];
+      hv = (double)fl[2 * kGroupCells + k] + (double)fl[3 * kGroupCells + k];
     }
   };
   // registers of the next tile: this thread's row of it
@@ -331,7 +346,8 @@ __global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant_
   __syncthreads();
   for (int64_t t0 = r0; t0 < r1; t0 += kHistTileRows) {
     const int tile_rows = (int)min((int64_t)kHistTileRows, r1 - t0);
-    // stage this tile (the previous tile's accumulation has finished)
+    // stage this tile (the previous tile's accumulation has finished); rows
+    // past the range stage as zeros and add nothing
 #pragma unroll
     for (int k = 0; k < 2 * kNG; ++k) sbins[threadIdx.x * 2 * kNG + k] = nb[k];
     if (kMode == 2) sq[threadIdx.x] = nq;
@@ -339,67 +355,108 @@ __global__ void __launch_bounds__(kHistThreads, 2) k_hist(const __grid_constant_
     __syncthreads();
     // the next tile's gathers run while this one is accumulated
     if (t0 + kHistTileRows < r1) fetch(t0 + kHistTileRows + threadIdx.x);
-    const unsigned char* sb = reinterpret_cast<const unsigned char*>(sbins);
     const int rw0 = warp * kRowsPerWarp;
-    const int rw1 = min(rw0 + kRowsPerWarp, tile_rows);
-    for (int r = rw0; r < rw1; r += 4) {
-      uint32_t raw[4][kNG];
-      int32_t qv[4];
-      float gv[4], hv[4];
+    if (rw0 < tile_rows) {
+      const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + rw0 * kRowBytes + lane;
+      int32_t myq = 0;
+      float myg = 0.f, myh = 0.f;
+      if (kMode == 2) {
+        myq = sq[rw0 + lane];
+      } else {
+        const float2 v = sgh[rw0 + lane];
+        myg = v.x;
+        myh = v.y;
+      }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const bool ok = r + u < rw1;
+      for (int j = 0; j < kRowsPerWarp; ++j) {
+        int32_t q = 0;
+        float gv = 0.f, hv = 0.f;
         if (kMode == 2) {
-          qv[u] = ok ? sq[r + u] : 0;
+          q = __shfl_sync(0xffffffffu, myq, j);
         } else {
-          float2 v = ok ? sgh[r + u] : make_float2(0.f, 0.f);
-          gv[u] = v.x;
-          hv[u] = v.y;
+          gv = __shfl_sync(0xffffffffu, myg, j);
+          hv = __shfl_sync(0xffffffffu, myh, j);
         }
 #pragma unroll
-        for (int g = 0; g < kNG; ++g)
-          raw[u][g] = (ok && g < ngroups) ? (uint32_t)sb[(size_t)(r + u) * kRowBytes + 32 * g + lane] : 0u;
-      }
-      // A stored value indexes cells [0, 256) of the lane's own column, so no
-      // value can address outside the group; values past the feature's bins
-      // (lanes past the last feature read padding zeros) land in cells the
-      // flush ignores.
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-#pragma unroll
         for (int g = 0; g < kNG; ++g) {
-          if (raw[u][g] == 0u) continue;
-          const int k = (int)raw[u][g] * 32 + lane;
+          if (g >= ngroups) break;
+          const int raw = (int)rowp[j * kRowBytes + 32 * g];
+          // float cells take a compare-and-swap loop per add: skip value 0
+          if (kMode != 2 && raw == 0) continue;
+          const int k = raw * 32 + lane;
           if (kMode == 2) {
-            atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + k, qv[u]);
+            atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + k, q);
           } else if (kMode == 0) {
             double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
-            atomicAdd(d + k, (double)gv[u]);
-            atomicAdd(d + kGroupCells + k, (double)hv[u]);
+            atomicAdd(d + k, (double)gv);
+            atomicAdd(d + kGroupCells + k, (double)hv);
           } else {
             float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
-            float og = atomicAdd(fl + k, gv[u]);
-            float sg = __fadd_rn(og, gv[u]);
+            float og = atomicAdd(fl + k, gv);
+            float sg = __fadd_rn(og, gv);
             float bg = __fsub_rn(sg, og);
-            atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv[u], bg)));
-            float oh = atomicAdd(fl + 2 * kGroupCells + k, hv[u]);
-            float s2 = __fadd_rn(oh, hv[u]);
+            atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv, bg)));
+            float oh = atomicAdd(fl + 2 * kGroupCells + k, hv);
+            float s2 = __fadd_rn(oh, hv);
             float bh = __fsub_rn(s2, oh);
-            atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv[u], bh)));
+            atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv, bh)));
           }
         }
       }
     }
     since_flush += tile_rows;
     __syncthreads();
-    // int32 cells hold at most sub_rows rows before their 16-bit halves could wrap
-    if (kMode == 2 && t0 + kHistTileRows < r1 && since_flush + kHistTileRows > sub_rows) {
-      flush();
-      since_flush = 0;
-      __syncthreads();
+    // int32 cells hold at most sub_rows rows before their 16-bit halves could
+    // wrap: this CTA adds its own cells to the histogram and clears them
+    if constexpr (kMode == 2) {
+      if (t0 + kHistTileRows < r1 && since_flush + kHistTileRows > sub_rows) {
+        const int total = ngroups * kGroupCells;
+        for (int i = threadIdx.x; i < total; i += kHistThreads) {
+          emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
+          reinterpret_cast<int32_t*>(cells)[i] = 0;
+        }
+        since_flush = 0;
+        __syncthreads();
+      }
     }
   }
-  flush();
+  // cluster reduction: CTA rank r adds slice r of the cells, summed over the
+  // cluster's CTAs in rank order
+  cluster.sync();
+  {
+    const int total = ngroups * kGroupCells;
+    const int per = (total + kCl - 1) / kCl;
+    const int lo = (int)cluster.block_rank() * per, hi = min(total, lo + per);
+    for (int i = lo + (int)threadIdx.x; i < hi; i += kHistThreads) {
+      if constexpr (kMode == 2) {
+        emit(i, [&](int ii, int64_t& gv, int64_t& hv) {
+          gv = 0;
+          hv = 0;
+#pragma unroll
+          for (int r = 0; r < kCl; ++r) {
+            int64_t a, b;
+            cell_of(cluster.map_shared_rank(cells, r), ii, a, b);
+            gv += a;
+            hv += b;
+          }
+        });
+      } else {
+        emit(i, [&](int ii, double& gv, double& hv) {
+          gv = 0.0;
+          hv = 0.0;
+#pragma unroll
+          for (int r = 0; r < kCl; ++r) {
+            double a, b;
+            cell_of(cluster.map_shared_rank(cells, r), ii, a, b);
+            gv += a;
+            hv += b;
+          }
+        });
+      }
+    }
+  }
+  // no CTA leaves while another may still read its shared memory
+  cluster.sync();
 }
 
 #define LGBM_B200_HIST_INST(M, G) \
@@ -1005,13 +1062,20 @@ __device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R
   DSlotState* st = s.st;
   const DParams& p = c.p;
   const DTree& t = s.tree;
-  const DSplit& info = s.best[bl];
-  const DFeature& m = c.feats[info.inner];
-  int32_t node = R - 1;
-  bool numerical = m.bin_type == 0;
-  int32_t parent = t.leaf_parent[bl];
+  // every value read first (the stores below could alias them for the
+  // compiler), so their latencies overlap
+  const DSplit info = s.best[bl];
+  const int32_t parent = t.leaf_parent[bl];
+  const double old_value = t.leaf_value[bl];
+  const int32_t d = t.leaf_depth[bl] + 1;
+  const int32_t num_cat = st->num_cat;
+  const double cmin0 = p.use_monotone ? s.cmin[bl] : 0.0, cmax0 = p.use_monotone ? s.cmax[bl] : 0.0;
+  const DFeature m = c.feats[info.inner];
+  const int32_t parent_left = parent >= 0 ? t.left_child[parent] : 0;
+  const int32_t node = R - 1;
+  const bool numerical = m.bin_type == 0;
   if (parent >= 0) {
-    if (t.left_child[parent] == ~bl) t.left_child[parent] = node;
+    if (parent_left == ~bl) t.left_child[parent] = node;
     else t.right_child[parent] = node;
   }
   t.split_feature_inner[node] = info.inner;
@@ -1023,37 +1087,39 @@ __device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R
   t.leaf_parent[bl] = node;
   t.leaf_parent[R] = node;
   t.internal_weight[node] = info.left_sum_hessian + info.right_sum_hessian;
-  t.internal_value[node] = t.leaf_value[bl];
+  t.internal_value[node] = old_value;
   t.leaf_value[bl] = isnan(info.left_output) ? 0.0 : info.left_output;
   t.leaf_weight[bl] = info.left_sum_hessian;
   t.leaf_value[R] = isnan(info.right_output) ? 0.0 : info.right_output;
   t.leaf_weight[R] = info.right_sum_hessian;
-  int32_t d = t.leaf_depth[bl] + 1;
   t.leaf_depth[bl] = d;
   t.leaf_depth[R] = d;
   int8_t dt = 0;
-  bool default_left = numerical ? info.default_left != 0 : false;
+  const bool default_left = numerical ? info.default_left != 0 : false;
   if (default_left) dt |= 2;
   dt = (int8_t)((dt & 3) | (m.missing_type << 2));
   if (!numerical) dt |= 1;
   t.decision_type[node] = dt;
-  t.threshold_in_bin[node] = numerical ? info.threshold : (uint32_t)st->num_cat;
+  t.threshold_in_bin[node] = numerical ? info.threshold : (uint32_t)num_cat;
   for (int w = 0; w < kCatWords; ++w) t.cat_bits[node * kCatWords + w] = numerical ? 0u : info.cat_bits[w];
-  if (!numerical) st->num_cat += 1;
+  if (!numerical) st->num_cat = num_cat + 1;
   // basic monotone constraints (constraints.rs:467-480)
   if (p.use_monotone) {
-    s.cmin[R] = s.cmin[bl];
-    s.cmax[R] = s.cmax[bl];
+    double lmin = cmin0, lmax = cmax0, rmin = cmin0, rmax = cmax0;
     if (numerical) {
       double mid = (info.left_output + info.right_output) / 2.0;
       if (info.monotone_type < 0) {
-        s.cmin[bl] = mid < s.cmin[bl] ? s.cmin[bl] : mid;
-        s.cmax[R] = s.cmax[R] < mid ? s.cmax[R] : mid;
+        lmin = mid < lmin ? lmin : mid;
+        rmax = rmax < mid ? rmax : mid;
       } else if (info.monotone_type > 0) {
-        s.cmax[bl] = s.cmax[bl] < mid ? s.cmax[bl] : mid;
-        s.cmin[R] = mid < s.cmin[R] ? s.cmin[R] : mid;
+        lmax = lmax < mid ? lmax : mid;
+        rmin = mid < rmin ? rmin : mid;
       }
     }
+    s.cmin[bl] = lmin;
+    s.cmax[bl] = lmax;
+    s.cmin[R] = rmin;
+    s.cmax[R] = rmax;
   }
   st->num_leaves_cur = R + 1;
 }
@@ -1172,13 +1238,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
     lc.mc = p.use_monotone != 0;
     lc.cmin = s.cmin[ls.leaf];
     lc.cmax = s.cmax[ls.leaf];
-    DSplit& out = s.feat_res[side * nf + f];
+    // the result is built in shared memory and stored once
+    __shared__ DSplit out;
     bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
     if (tid == 0) {
       out.feature = m.real_index;
       out.inner = f;
       s.feat_ok[side * nf + f] = ok ? 1 : 0;
     }
+    __syncthreads();
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
+    for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
   }
 }
 template __global__ void k_scan<false>(const __grid_constant__ DCtx);
@@ -1204,46 +1275,60 @@ __device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsign
 
 __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left) {
   DSlotState* st = s.st;
-  int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
-  int32_t side = s.leaf_side[L];
-  int32_t nl = total_left, nr = cnt - total_left;
+  const DParams& p = c.p;
+  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
+  const int32_t side = s.leaf_side[L];
+  const int32_t buf_L = s.buf_of[L];
+  const int32_t depth = s.tree.leaf_depth[L];  // both children's depth, set by apply_split
+  const DSplit& info = s.best[L];
+  const DLeafSplits ls0{L, 0, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
+  const DLeafSplits rs0{R, 0, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
+  const int32_t status = st->status;
+  const int32_t nl = total_left, nr = cnt - total_left;
   s.leaf_count[L] = nl;
   s.leaf_begin[R] = begin + nl;
   s.leaf_count[R] = nr;
   s.leaf_side[L] = 1 - side;
   s.leaf_side[R] = 1 - side;
   const DTree& t = s.tree;
-  int32_t node = R - 1;
+  const int32_t node = R - 1;
   t.leaf_count[L] = nl;
   t.leaf_count[R] = nr;
   t.internal_count[node] = nl + nr;
-  const DSplit& info = s.best[L];
-  DLeafSplits ls{L, nl, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
-  DLeafSplits rs{R, nr, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
-  if (nl < nr) {
-    if (nl <= 0) st->status = kStatusEmptyChild;
-    st->smaller = ls;
-    st->larger = rs;
-  } else {
-    if (nr <= 0) st->status = kStatusEmptyChild;
-    st->smaller = rs;
-    st->larger = ls;
-  }
-  if (st->status != kStatusOk) {
+  DLeafSplits ls = ls0, rs = rs0;
+  ls.num_data = nl;
+  rs.num_data = nr;
+  int32_t new_status = status;
+  const bool left_smaller = nl < nr;
+  if ((left_smaller ? nl : nr) <= 0 && status == kStatusOk) new_status = kStatusEmptyChild;
+  st->smaller = left_smaller ? ls : rs;
+  st->larger = left_smaller ? rs : ls;
+  if (new_status != kStatusOk) {
+    st->status = new_status;
     st->done = 1;
     return;
   }
   // HistogramPool::Move: the parent's buffer goes to the larger leaf, the
   // fresh buffer R (zeroed by this kernel) to the smaller one.
-  if (st->larger.leaf == L) {
+  if (!left_smaller) {
     s.buf_of[R] = R;
   } else {
-    s.buf_of[R] = s.buf_of[L];
+    s.buf_of[R] = buf_L;
     s.buf_of[L] = R;
   }
   st->left_leaf = L;
   st->right_leaf = R;
-  st->need_find = before_find_best_split(c, s, L, R) ? 1 : 0;
+  // before_find_best_split (learner/mod.rs:712-731) on the values just written
+  bool need = true;
+  if (p.max_depth > 0 && depth >= p.max_depth) need = false;
+  else if (nr < p.min_data_in_leaf * 2 && nl < p.min_data_in_leaf * 2) need = false;
+  if (!need) {
+    s.best[L].gain = -INFINITY;
+    s.bgain[L] = -INFINITY;
+    s.best[R].gain = -INFINITY;
+    s.bgain[R] = -INFINITY;
+  }
+  st->need_find = need ? 1 : 0;
 }
 
 // Decision state a partition CTA derives from the scan results.
