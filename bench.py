@@ -29,7 +29,13 @@ sys.path.insert(0, os.path.join(ROOT, "lightgbm-rust_b200"))
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = "binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), max_bin 255, 255 leaves, lr 0.1, 500 rounds"
+WORKLOAD = ("binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), max_bin 255, 255 leaves, lr 0.1, "
+            "500 rounds; forms FP64, FP32-compensated, quantized (int8 g/h, 4 bins, stochastic rounding, FP64 leaf "
+            "renewal)")
+# DRAM bytes per histogrammed row of the quantized histogram kernel, from the
+# ncu capture of a 5M-row root launch (profiles/k_hist_k_scan_k_partition_binary5M_quantized.md);
+# traffic grows with the rows of a launch, so a launch's traffic is this times its rows
+HIST_DRAM_BYTES_PER_ROW = 40.8
 METRIC = "s per 500 rounds (quantized hist, equal AUC to FP64) + hist GB/s"
 ROUNDS = 500
 
@@ -129,6 +135,8 @@ def hist_bytes_per_row(nf, form):
 def run_form(lgb, data, ds, dv, form, args, device):
     params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8,
                   use_cuda_graph=True)
+    if form == "quantized":  # the workload's quantized form renews leaf outputs from FP64 gradients
+        params["quant_train_renew_leaf"] = True
     bst = lgb.Booster(params, ds, dv)
     L = bst.learner
     for _ in range(args.warmup):
@@ -187,6 +195,8 @@ def run_e2e(lgb, data, ds, form, args, device):
     from lgbm_b200.basic import objective_config, resolve_params
 
     params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8)
+    if form == "quantized":
+        params["quant_train_renew_leaf"] = True
     p = resolve_params(params)
     learner = lgb.Learner(ds, params)
     n = len(data["y"])
@@ -201,20 +211,29 @@ def run_e2e(lgb, data, ds, form, args, device):
     oc = objective_config(p)
     lr = float(p["learning_rate"])
 
+    parts = np.zeros(3)
+
     def step():
+        t0 = time.perf_counter()
         LL.check(LL.lib().lgbm_b200_gradients(C.byref(oc), label.ctypes.data, score.ctypes.data, n, None, 0,
                                               g.ctypes.data, h.ctypes.data, LL.HOST, device))
+        t1 = time.perf_counter()
         t = learner.train(g, h)[0]
+        t2 = time.perf_counter()
         lv = np.where(np.abs(t["leaf_value"] * lr) <= np.float32(1e-35), 0.0, t["leaf_value"] * lr)
         learner.add_leaf_outputs(0, lv, score)
+        parts[:] += (t1 - t0, t2 - t1, time.perf_counter() - t2)
 
     for _ in range(args.warmup):
         step()
+    parts[:] = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step()
     ms = 1000 * (time.perf_counter() - t0) / args.steps
     return {"value": ms * ROUNDS / 1000.0, "unit": "s/500 rounds", "ms_per_step": ms,
+            "ms_gradients": 1000 * parts[0] / args.steps, "ms_train": 1000 * parts[1] / args.steps,
+            "ms_add_leaf_outputs": 1000 * parts[2] / args.steps,
             # gradients: label + scores in, g/h out; train: g/h in; add_leaf_outputs: scores in and out
             "h2d_bytes_per_step": n * (4 + 8) + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
 
@@ -229,6 +248,8 @@ def run_cpu_baseline(lgb, form, sample_scale, iters):
     d = synthetic.make(2, scale=sample_scale)
     threads = os.cpu_count() or 8
     params = dict(d["params"], hist_precision=form, num_threads=threads)
+    if form == "quantized":
+        params["quant_train_renew_leaf"] = True
     p = lgb.resolve_params(params)
     ds = lgb.Dataset(d["X"], d["y"], params=params)
     b = ds.binned()
@@ -335,7 +356,10 @@ def main():
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
                       "hist_rows_per_tree": v["hist_rows_per_tree"]} for k, v in res.items()},
         "roofline": {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] / (int(data["params"]["num_leaves"]) - 1)
+                                 if head == "quantized" else None),
+                     "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
                      "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]},
         "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 5),

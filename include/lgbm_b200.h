@@ -221,7 +221,10 @@ int lgbm_b200_learner_quantized(LgbmB200Learner* h, int32_t slot, int64_t* packe
 /* ------------------------------------------------------------------------
  * Objective gradients: RowObjective::gradients (objective/mod.rs:52) for
  * binary (binary.rs:101), L2 (regression.rs:209), softmax (multiclass.rs:126)
- * and lambdarank (rank.rs:192). scores/grad/hess are class-major.
+ * and lambdarank (rank.rs:192). scores/grad/hess are class-major. Lambdarank
+ * takes query_boundaries in host memory ([num_queries + 1], from 0 to
+ * num_data; at most 10000 rows per query) and builds the objective's tables
+ * (rank.rs:119-176) on each call; other objectives ignore them.
  * ------------------------------------------------------------------------ */
 typedef struct {
   int32_t objective; /* LGBM_B200_OBJ_* */
@@ -253,8 +256,9 @@ typedef struct {
 } LgbmB200BoostConfig;
 
 /* `learner` stays owned by the caller and must outlive the booster. label: host
- * [num_data]; valid_bins: optional held-out bin matrix [num_valid x num_features]
- * scored every iteration like the reference's valid sets. */
+ * [num_data]; query_boundaries: host [num_queries + 1] for lambdarank (NULL
+ * otherwise); valid_bins: optional held-out bin matrix [num_valid x
+ * num_features] scored every iteration like the reference's valid sets. */
 int lgbm_b200_booster_create(LgbmB200Learner* learner, const LgbmB200BoostConfig* cfg, const float* label,
                              const int32_t* query_boundaries, int32_t num_queries, const uint8_t* valid_bins,
                              int64_t num_valid, LgbmB200Booster** out);

@@ -6,6 +6,7 @@
 #include <mutex>
 
 #include "learner_impl.h"
+#include "rank.h"
 
 using namespace lgbm_b200;
 
@@ -36,9 +37,12 @@ static double boost_from_score(const LgbmB200ObjectiveConfig& o, const std::vect
 }
 
 static Status launch_gradients(const LgbmB200ObjectiveConfig& o, const float* label, const double* score, int64_t n,
-                               float2* gh, float* g, float* h, int sms, cudaStream_t s) {
+                               float2* gh, float* g, float* h, int sms, cudaStream_t s, const DRank* rank = nullptr) {
   int blocks = std::max(1, (int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
   switch (o.objective) {
+    case LGBM_B200_OBJ_LAMBDARANK:
+      if (!rank) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "lambdarank needs query boundaries");
+      return launch_lambdarank(*rank, label, score, g, h, gh, sms, s);
     case LGBM_B200_OBJ_BINARY: k_grad_binary<<<blocks, 256, 0, s>>>(label, score, n, o.sigmoid, gh, g, h); break;
     case LGBM_B200_OBJ_REGRESSION: k_grad_l2<<<blocks, 256, 0, s>>>(label, score, n, gh, g, h); break;
     case LGBM_B200_OBJ_MULTICLASS:
@@ -112,13 +116,15 @@ struct LgbmB200Booster {
   int32_t used_cnt_bytree = 0;
   std::vector<HostTree> out_trees;
   double* lv_dev = nullptr;  // [K x L] shrunk leaf values
+  std::unique_ptr<RankTables> rank;  // lambdarank objective tables
   ~LgbmB200Booster() { arena.free_all(); }
 };
 
 namespace lgbm_b200 {
 
 static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB200BoostConfig* cfg,
-                             const float* label, const uint8_t* valid_bins, int64_t nv) {
+                             const float* label, const int32_t* query_boundaries, int32_t num_queries,
+                             const uint8_t* valid_bins, int64_t nv) {
   b->L = L;
   b->cfg = *cfg;
   b->K = L->K;
@@ -129,9 +135,15 @@ static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB
   int want_k = o.objective == LGBM_B200_OBJ_MULTICLASS ? o.num_class : 1;
   if (want_k != b->K)
     return Status(LGBM_B200_ERR_INVALID_PARAMETER, "learner num_tree_slots must equal the objective's tree count");
-  if (o.objective == LGBM_B200_OBJ_LAMBDARANK)
-    return Status(LGBM_B200_ERR_UNSUPPORTED, "lambdarank in the device-resident booster");
   const int64_t n = b->n;
+  if (o.objective == LGBM_B200_OBJ_LAMBDARANK) {  // rank.rs:119-176: tables built once
+    if (!query_boundaries || num_queries <= 0 || query_boundaries[0] != 0 || query_boundaries[num_queries] != n)
+      return Status(LGBM_B200_ERR_INVALID_DATA, "lambdarank needs query boundaries covering every row");
+    b->rank = std::make_unique<RankTables>();
+    Status rs = b->rank->build(label, query_boundaries, num_queries, o.sigmoid, o.lambdarank_truncation_level,
+                               o.lambdarank_norm != 0);
+    if (!rs.ok()) return rs;
+  }
   b->label_h.assign(label, label + n);
   DeviceArena& A = b->arena;
   Status s;
@@ -208,7 +220,8 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
     }
     b->init_scores = init;
   }
-  Status st = launch_gradients(b->cfg.objective, b->label_d, b->score, n, L->gh_all, nullptr, nullptr, sms, s);
+  Status st = launch_gradients(b->cfg.objective, b->label_d, b->score, n, L->gh_all, nullptr, nullptr, sms, s,
+                               b->rank ? &b->rank->d : nullptr);
   if (!st.ok()) return st;
   // bagging (sample_strategy.rs:280-320)
   if (b->bagging && ((b->bag_cnt < n && b->iter % b->cfg.bagging_freq == 0) || b->need_re_bagging)) {
@@ -252,7 +265,7 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
   CU(cudaMemcpyAsync(b->lv_dev, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice, s));
   {
     DCtx c = L->ctx;
-    k_add_leaf_outputs<<<dim3(std::max(1, sms * 4 / L->L + 1), L->L, K), 256, 0, s>>>(c, b->lv_dev, L->L, b->score, n);
+    k_add_leaf_outputs<<<dim3(sms * 4, 1, K), 256, 16 * (size_t)L->L, s>>>(c, b->lv_dev, L->L, b->score, n);
     CU_LAUNCH();
     if (b->bagging && b->oob_cnt > 0) {
       k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->oob_cnt + 255) / 256, sms * 8)), 1, K), 256, 0,
@@ -303,15 +316,33 @@ extern "C" {
 int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, const double* scores,
                         int64_t num_data, const int32_t* query_boundaries, int32_t num_queries, float* grad,
                         float* hess, int32_t location, int32_t device) {
-  (void)query_boundaries;
-  (void)num_queries;
   if (!cfg || !label || !scores || !grad || !hess || num_data <= 0)
     return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
   if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
   const int k = cfg->objective == LGBM_B200_OBJ_MULTICLASS ? cfg->num_class : 1;
   const size_t n = (size_t)num_data, nk = n * (size_t)k;
+  // lambdarank: the objective's tables from the labels and host query boundaries
+  std::unique_ptr<RankTables> rank;
+  if (cfg->objective == LGBM_B200_OBJ_LAMBDARANK) {
+    if (!query_boundaries || num_queries <= 0 || query_boundaries[0] != 0 ||
+        query_boundaries[num_queries] != num_data)
+      return fail(Status(LGBM_B200_ERR_INVALID_DATA, "lambdarank needs query boundaries covering every row"));
+    std::vector<float> lh;
+    const float* lp = label;
+    if (location == LGBM_B200_DEVICE) {
+      lh.resize(n);
+      if (cudaMemcpy(lh.data(), label, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(Status(LGBM_B200_ERR_CUDA, "label copy"));
+      lp = lh.data();
+    }
+    rank = std::make_unique<RankTables>();
+    Status rs = rank->build(lp, query_boundaries, num_queries, cfg->sigmoid, cfg->lambdarank_truncation_level,
+                            cfg->lambdarank_norm != 0);
+    if (!rs.ok()) return fail(rs);
+  }
+  const DRank* rk = rank ? &rank->d : nullptr;
   if (location == LGBM_B200_DEVICE) {
-    Status s = launch_gradients(*cfg, label, scores, num_data, nullptr, grad, hess, 148, 0);
+    Status s = launch_gradients(*cfg, label, scores, num_data, nullptr, grad, hess, 148, 0, rk);
     if (!s.ok()) return fail(s);
     cudaError_t e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
@@ -340,7 +371,7 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
   cudaStream_t s = w.stream;
   cudaMemcpyAsync(w.label, label, sizeof(float) * n, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(w.score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
-  Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, 148, s);
+  Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, 148, s, rk);
   if (!st.ok()) return fail(st);
   cudaMemcpyAsync(grad, w.g, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hess, w.h, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
@@ -352,11 +383,10 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
 int lgbm_b200_booster_create(LgbmB200Learner* learner, const LgbmB200BoostConfig* cfg, const float* label,
                              const int32_t* query_boundaries, int32_t num_queries, const uint8_t* valid_bins,
                              int64_t num_valid, LgbmB200Booster** out) {
-  (void)query_boundaries;
-  (void)num_queries;
   if (!learner || !cfg || !label || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
   auto b = std::make_unique<LgbmB200Booster>();
-  Status s = booster_create(b.get(), learner, cfg, label, valid_bins, valid_bins ? num_valid : 0);
+  Status s = booster_create(b.get(), learner, cfg, label, query_boundaries, num_queries, valid_bins,
+                            valid_bins ? num_valid : 0);
   if (!s.ok()) return fail(s);
   *out = b.release();
   return LGBM_B200_OK;
@@ -407,8 +437,14 @@ struct LgbmB200Forest {
   DeviceArena arena;
   DForest f{};
   int32_t ntpi = 1;
+  // staging of host rows and scores, grown on demand and kept: a pool
+  // allocation per call would be unmapped and mapped again around every
+  // synchronisation
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
   ~LgbmB200Forest() {
     arena.free_all();
+    if (stage) cudaFree(stage);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -512,9 +548,20 @@ int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t n
   double* otmp = nullptr;
   cudaError_t e = cudaSuccess;
   if (location == LGBM_B200_HOST) {
-    e = cudaMallocAsync(reinterpret_cast<void**>(&xtmp), sizeof(float) * nrow * ncol, s);
-    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&otmp), sizeof(double) * nrow * F->ntpi, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(xtmp, X, sizeof(float) * nrow * ncol, cudaMemcpyHostToDevice, s);
+    const size_t xb = (sizeof(float) * (size_t)nrow * ncol + 255) / 256 * 256;
+    const size_t need = xb + sizeof(double) * (size_t)nrow * F->ntpi;
+    if (F->stage_bytes < need) {
+      if (F->stage) cudaFree(F->stage);
+      F->stage = nullptr;
+      F->stage_bytes = 0;
+      e = cudaMalloc(&F->stage, need);
+      if (e == cudaSuccess) F->stage_bytes = need;
+    }
+    if (e == cudaSuccess) {
+      xtmp = static_cast<float*>(F->stage);
+      otmp = reinterpret_cast<double*>(static_cast<char*>(F->stage) + xb);
+      e = cudaMemcpyAsync(xtmp, X, sizeof(float) * nrow * ncol, cudaMemcpyHostToDevice, s);
+    }
     Xd = xtmp;
     od = otmp;
   }
@@ -524,8 +571,6 @@ int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t n
   }
   if (e == cudaSuccess && location == LGBM_B200_HOST)
     e = cudaMemcpyAsync(out, otmp, sizeof(double) * nrow * F->ntpi, cudaMemcpyDeviceToHost, s);
-  if (xtmp) cudaFreeAsync(xtmp, s);
-  if (otmp) cudaFreeAsync(otmp, s);
   cudaError_t e2 = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));

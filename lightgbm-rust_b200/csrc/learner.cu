@@ -27,8 +27,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   h->cfg = *cfg;
   if (n <= 0 || n > INT32_MAX) return Status(LGBM_B200_ERR_INVALID_DATA, "num_data must be in [1, 2^31-1]");
   if (nf <= 0) return Status(LGBM_B200_ERR_INVALID_DATA, "no features");
-  if (cfg->num_leaves < 2 && cfg->num_leaves != 0) {
-  }
+  if (cfg->num_leaves > 8192)
+    return Status(LGBM_B200_ERR_UNSUPPORTED, "num_leaves above 8192 on the device learner");
   h->device = cfg->device;
   CU(cudaSetDevice(h->device));
   cudaDeviceProp prop;
@@ -98,6 +98,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   const void* hk = hist_kernel(mode, h->hist_ng);
   CU(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
   h->scan_smem = sizeof(ScanSmem);
+  // the per-position leaf kernels hold a 16-byte table entry per leaf
+  CU(cudaFuncSetAttribute(k_leaf_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
+  CU(cudaFuncSetAttribute(k_add_leaf_outputs, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
   CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   {
@@ -306,7 +309,7 @@ static Status enqueue_tree(LgbmB200Learner* h) {
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
     CU(cudaMemsetAsync(h->leaf_sums, 0, sizeof(double) * K * L * 2, s));
-    k_leaf_sums<<<dim3(8, L, K), 256, 0, s>>>(c, h->leaf_sums);
+    k_leaf_sums<<<dim3(h->num_sms * 4, 1, K), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums);
     CU_LAUNCH();
     k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
     CU_LAUNCH();
@@ -650,20 +653,23 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
   double* sc = score;
   double* tmp = nullptr;
   if (e == cudaSuccess && location == LGBM_B200_HOST) {
-    e = cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(double) * n, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, score, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    // a staging buffer kept for the learner's lifetime: a pool allocation
+    // per call would be unmapped and mapped again around every synchronisation
+    if (!h->score_stage) {
+      Status st = h->arena.alloc_n(&h->score_stage, (size_t)n);
+      if (!st.ok()) return fail(st);
+    }
+    tmp = h->score_stage;
+    e = cudaMemcpyAsync(tmp, score, sizeof(double) * n, cudaMemcpyHostToDevice, s);
     sc = tmp;
   }
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   // launch only over this slot: grid.z = 1 with a context whose slots start at `slot`
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
-  k_add_leaf_outputs<<<dim3(std::max(1, h->num_sms * 4 / L + 1), L, 1), 256, 0, s>>>(c, lvd, 0, sc, 0);
+  k_add_leaf_outputs<<<dim3(h->num_sms * 4, 1, 1), 256, 16 * (size_t)L, s>>>(c, lvd, 0, sc, 0);
   e = cudaGetLastError();
-  if (e == cudaSuccess && tmp) {
-    e = cudaMemcpyAsync(score, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
-    cudaFreeAsync(tmp, s);
-  }
+  if (e == cudaSuccess && tmp) e = cudaMemcpyAsync(score, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   return LGBM_B200_OK;

@@ -214,7 +214,8 @@ struct LgbmB200Learner {
   // leaf renewal scratch [K][L][2]
   double* leaf_sums = nullptr;
   double* leaf_values_dev = nullptr;  // [K][L] for add_leaf_outputs
-  double* score_scratch = nullptr;
+  double* score_scratch = nullptr;  // host gradients staged for train (2 x num_data floats)
+  double* score_stage = nullptr;    // host scores staged for add_leaf_outputs (num_data doubles)
   // readback
   std::vector<DSlotState> st_h;
   std::vector<HostTree> trees;

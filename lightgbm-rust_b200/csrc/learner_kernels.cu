@@ -1688,25 +1688,98 @@ __global__ void __launch_bounds__(256) k_transpose_bins(const uint8_t* bins, int
 // score updates (partition.rs:306-319; tree.rs:605-711 binned routing)
 // =====================================================================================
 // Grid (G, num_leaves, slots): block (x, leaf) sums a chunk of the leaf's rows.
-__global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* sums /*[slots][leaves][2]*/) {
-  const DSlot& s = c.slots[blockIdx.z];
-  DSlotState* st = s.st;
-  int32_t leaf = blockIdx.y;
-  if (leaf >= st->num_leaves_cur) return;
-  int32_t begin = s.leaf_begin[leaf], cnt = s.leaf_count[leaf];
-  const uint32_t* idx = s.idx[s.leaf_side[leaf]] + begin;
-  double g = 0.0, h = 0.0;
-  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-    float2 v = s.gh[idx[i]];
-    g += (double)v.x;
-    h += (double)v.y;
+// Leaf of each row position: every CTA builds a table of the tree's
+// non-empty leaves in position order (a leaf is a contiguous range of the
+// partition) in shared memory, then walks positions grid-stride and finds
+// each position's leaf by binary search. Work is spread evenly over the
+// rows whatever the leaf sizes. Dynamic shared memory: 16 bytes per leaf.
+struct LeafTable {
+  int32_t* begin;  // sorted range starts
+  int32_t* leaf;
+  int32_t* side;
+  int32_t n;       // non-empty leaves
+  int32_t total;   // positions covered
+};
+
+__device__ LeafTable build_leaf_table(const DSlot& s, int32_t nl, int32_t* smem) {
+  int32_t* beg = smem;
+  int32_t* cnt = smem + nl;
+  LeafTable t;
+  t.begin = smem + 2 * nl;
+  t.leaf = smem + 3 * nl;
+  t.side = cnt;  // reused after ranking: side of the leaf at each rank
+  __shared__ int32_t s_n, s_total;
+  for (int32_t l = threadIdx.x; l < nl; l += blockDim.x) {
+    beg[l] = s.leaf_begin[l];
+    cnt[l] = s.leaf_count[l];
   }
-  g = warp_sum_d(g);
-  h = warp_sum_d(h);
-  if ((threadIdx.x & 31) == 0) {
-    double* o = sums + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
-    atomicAdd(o, g);
-    atomicAdd(o + 1, h);
+  if (threadIdx.x == 0) {
+    s_n = 0;
+    s_total = 0;
+  }
+  __syncthreads();
+  for (int32_t l = threadIdx.x; l < nl; l += blockDim.x) {
+    if (cnt[l] <= 0) continue;
+    const int32_t b = beg[l];
+    int32_t r = 0;  // non-empty leaves start at distinct positions
+    for (int32_t m = 0; m < nl; ++m) r += (cnt[m] > 0 && beg[m] < b) ? 1 : 0;
+    t.begin[r] = b;
+    t.leaf[r] = l;
+    atomicAdd(&s_n, 1);
+    atomicMax(&s_total, b + cnt[l]);
+  }
+  __syncthreads();
+  for (int32_t r = threadIdx.x; r < s_n; r += blockDim.x) t.side[r] = s.leaf_side[t.leaf[r]];
+  __syncthreads();
+  t.n = s_n;
+  t.total = s_total;
+  return t;
+}
+
+__device__ __forceinline__ int32_t leaf_rank_of(const LeafTable& t, int32_t p) {
+  int32_t lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi + 1) >> 1;
+    if (t.begin[mid] <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// FP64 (g, h) sums of each leaf's rows for the leaf renewal
+// (learner/mod.rs:736-747). Grid (G, 1, slots), 256 threads.
+__global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* sums /*[slots][leaves][2]*/) {
+  extern __shared__ int32_t lt_smem[];
+  const DSlot& s = c.slots[blockIdx.z];
+  const int32_t nl = s.st->num_leaves_cur;
+  const LeafTable t = build_leaf_table(s, nl, lt_smem);
+  const int lane = threadIdx.x & 31;
+  double* base = sums + (size_t)blockIdx.z * c.p.num_leaves * 2;
+  // whole warps step together so that a warp can reduce before its atomics
+  const int32_t stride = gridDim.x * blockDim.x;
+  for (int32_t p0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); p0 < t.total; p0 += stride) {
+    const int32_t p = p0 + lane;
+    int32_t leaf = -1;
+    double g = 0.0, h = 0.0;
+    if (p < t.total) {
+      const int32_t r = leaf_rank_of(t, p);
+      leaf = t.leaf[r];
+      const float2 v = s.gh[s.idx[t.side[r]][p]];
+      g = (double)v.x;
+      h = (double)v.y;
+    }
+    const int32_t first = __shfl_sync(0xffffffffu, leaf, 0);
+    if (__all_sync(0xffffffffu, leaf == first || leaf < 0)) {
+      g = warp_sum_d(g);
+      h = warp_sum_d(h);
+      if (lane == 0 && first >= 0) {
+        atomicAdd(base + 2 * first, g);
+        atomicAdd(base + 2 * first + 1, h);
+      }
+    } else if (leaf >= 0) {
+      atomicAdd(base + 2 * leaf, g);
+      atomicAdd(base + 2 * leaf + 1, h);
+    }
   }
 }
 
@@ -1719,19 +1792,20 @@ __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums)
   }
 }
 
-// score[row] += leaf_value[leaf] * scale over each leaf's rows.
-// Grid (G, num_leaves, slots).
+// score[row] += leaf_values[leaf of row] over the in-bag rows
+// (partition.rs:178-191). Grid (G, 1, slots), 256 threads.
 __global__ void __launch_bounds__(256) k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride,
                                                           double* score, int64_t score_stride) {
+  extern __shared__ int32_t lt_smem[];
   const DSlot& s = c.slots[blockIdx.z];
-  DSlotState* st = s.st;
-  int32_t leaf = blockIdx.y;
-  if (leaf >= st->num_leaves_cur) return;
-  double v = leaf_values[(size_t)blockIdx.z * lv_stride + leaf];
-  int32_t begin = s.leaf_begin[leaf], cnt = s.leaf_count[leaf];
-  const uint32_t* idx = s.idx[s.leaf_side[leaf]] + begin;
+  const int32_t nl = s.st->num_leaves_cur;
+  const LeafTable t = build_leaf_table(s, nl, lt_smem);
+  const double* lv = leaf_values + (size_t)blockIdx.z * lv_stride;
   double* sc = score + (size_t)blockIdx.z * score_stride;
-  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) sc[idx[i]] += v;
+  for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < t.total; p += gridDim.x * blockDim.x) {
+    const int32_t r = leaf_rank_of(t, p);
+    sc[s.idx[t.side[r]][p]] += lv[t.leaf[r]];
+  }
 }
 
 // Binned tree walk (tree.rs:588-633) for rows `rows` (or 0..n): score += leaf value.

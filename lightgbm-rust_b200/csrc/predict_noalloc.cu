@@ -1,8 +1,9 @@
 // Batched raw-score prediction from host buffers that allocates no device
 // memory: lgbm_b200_predict_noalloc.
 //
-// lgbm_b200_predict with host buffers takes two stream-ordered device
-// allocations per call (the feature rows and the scores). Some callers cannot
+// lgbm_b200_predict with host buffers allocates device staging for the
+// feature rows and the scores (on its first call, and again whenever a
+// larger batch arrives). Some callers cannot
 // allocate at prediction time: a serving process that gives all device memory
 // it does not hold to another allocator up front (a framework's caching
 // allocator, a fixed memory budget) gets out-of-memory there, and a

@@ -1,0 +1,229 @@
+// LambdarankNDCG gradients (crates/lgbm-core/src/objective/rank.rs:119-262,
+// RankingBase::gradients :63-111) on the device.
+//
+// Two launches per call:
+//   k_rank_sort    one CTA per query (grid-stride): the stable descending
+//                  order of the query's scores (dcg.rs:167-179) by rank
+//                  counting in shared memory
+//   k_lambdarank   one thread per query: the reference's pair loop in its
+//                  order, so every f32 lambda / hessian accumulation and the
+//                  FP64 sum of lambdas are formed exactly as on the CPU
+// The tables the reference builds in its constructor (label gains,
+// discounts, inverse max DCG per query, the 2^20-entry sigmoid table) are
+// built on the host by the same arithmetic and uploaded once.
+#include "rank.h"
+
+namespace lgbm_b200 {
+
+constexpr double kMinScoreD = -INFINITY;  // consts.rs kMinScore
+constexpr int kRankSortThreads = 128;
+constexpr int kRankSmemScores = 2048;  // queries up to this size sort from shared memory
+
+// Strict total order of the sort: larger score first, equal scores by
+// position (a stable sort); a NaN score orders after every number.
+__device__ __forceinline__ bool precedes(double sj, int j, double si, int i) {
+  const bool nj = isnan(sj), ni = isnan(si);
+  if (nj != ni) return ni;  // the number precedes the NaN
+  if (!nj && sj != si) return sj > si;
+  return j < i;
+}
+
+__global__ void __launch_bounds__(kRankSortThreads) k_rank_sort(DRank r, const double* score) {
+  __shared__ double s[kRankSmemScores];
+  for (int32_t q = blockIdx.x; q < r.nq; q += gridDim.x) {
+    const int32_t b0 = r.bnd[q], cnt = r.bnd[q + 1] - b0;
+    const double* sc = score + b0;
+    const bool in_smem = cnt <= kRankSmemScores;
+    __syncthreads();
+    if (in_smem)
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) s[i] = sc[i];
+    __syncthreads();
+    const double* src = in_smem ? s : sc;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const double si = src[i];
+      int32_t rank = 0;
+      for (int j = 0; j < cnt; ++j) rank += precedes(src[j], j, si, i) ? 1 : 0;
+      r.sorted[b0 + rank] = (uint32_t)i;
+    }
+  }
+}
+
+__device__ __forceinline__ double rank_sigmoid(const DRank& r, double score) {  // rank.rs:178-186
+  if (score <= r.min_in) return r.sigmoid_table[0];
+  if (score >= r.max_in) return r.sigmoid_table[kRankSigmoidBins - 1];
+  return r.sigmoid_table[(size_t)((score - r.min_in) * r.idx_factor)];
+}
+
+// LambdarankNDCG::one_query (rank.rs:192-262) for every query, one thread
+// each. Writes g/h (class-major float arrays) and/or the interleaved pairs.
+__global__ void __launch_bounds__(128) k_lambdarank(DRank r, const float* label, const double* score, float* g,
+                                                    float* h, float2* gh) {
+  for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < r.nq; q += gridDim.x * blockDim.x) {
+    const int32_t b0 = r.bnd[q], cnt = r.bnd[q + 1] - b0;
+    const float* lb = label + b0;
+    const double* sc = score + b0;
+    const uint32_t* sorted = r.sorted + b0;
+    float* lam = g ? g + b0 : nullptr;
+    float* hes = h ? h + b0 : nullptr;
+    float2* pair = gh ? gh + b0 : nullptr;
+    // the accumulators live in the output (g / h, else the interleaved pairs)
+    auto add = [&](int32_t i, float dl, float dh) {
+      if (lam) {
+        lam[i] += dl;
+        hes[i] += dh;
+      } else {
+        pair[i].x += dl;
+        pair[i].y += dh;
+      }
+    };
+    for (int32_t i = 0; i < cnt; ++i) {
+      if (lam) {
+        lam[i] = 0.0f;
+        hes[i] = 0.0f;
+      } else {
+        pair[i] = make_float2(0.0f, 0.0f);
+      }
+    }
+    if (cnt == 0) continue;
+    const double inverse_max_dcg = r.inv_max_dcg[q];
+    const double best_score = sc[sorted[0]];
+    int32_t worst_idx = cnt - 1;
+    if (worst_idx > 0 && sc[sorted[worst_idx]] == kMinScoreD) worst_idx -= 1;
+    const double worst_score = sc[sorted[worst_idx]];
+    double sum_lambdas = 0.0;
+    for (int32_t i = 0; i + 1 < cnt && i < r.truncation_level; ++i) {
+      const uint32_t si = sorted[i];
+      if (sc[si] == kMinScoreD) continue;
+      const float li = lb[si];
+      for (int32_t j = i + 1; j < cnt; ++j) {
+        const uint32_t sj = sorted[j];
+        if (sc[sj] == kMinScoreD) continue;
+        const float lj = lb[sj];
+        if (li == lj) continue;
+        int32_t high_rank = i, low_rank = j;
+        if (!(li > lj)) {
+          high_rank = j;
+          low_rank = i;
+        }
+        const uint32_t high = sorted[high_rank], low = sorted[low_rank];
+        const double high_score = sc[high], low_score = sc[low];
+        const double high_label_gain = r.label_gain[(int32_t)lb[high]];
+        const double low_label_gain = r.label_gain[(int32_t)lb[low]];
+        const double high_discount = r.discount[high_rank], low_discount = r.discount[low_rank];
+        const double delta_score = high_score - low_score;
+        const double dcg_gap = high_label_gain - low_label_gain;
+        const double paired_discount = fabs(high_discount - low_discount);
+        double delta_pair_ndcg = dcg_gap * paired_discount * inverse_max_dcg;
+        if (r.norm && best_score != worst_score) delta_pair_ndcg /= (double)0.01f + fabs(delta_score);
+        double p_lambda = rank_sigmoid(r, delta_score);
+        double p_hessian = p_lambda * (1.0 - p_lambda);
+        p_lambda *= -r.sigmoid * delta_pair_ndcg;
+        p_hessian *= r.sigmoid * r.sigmoid * delta_pair_ndcg;
+        add((int32_t)low, -(float)p_lambda, (float)p_hessian);
+        add((int32_t)high, (float)p_lambda, (float)p_hessian);
+        sum_lambdas -= 2.0 * p_lambda;
+      }
+    }
+    if (r.norm && sum_lambdas > 0.0) {
+      const double norm_factor = log2(1.0 + sum_lambdas) / sum_lambdas;
+      for (int32_t i = 0; i < cnt; ++i) {
+        if (lam) {
+          lam[i] = (float)((double)lam[i] * norm_factor);
+          hes[i] = (float)((double)hes[i] * norm_factor);
+        } else {
+          pair[i].x = (float)((double)pair[i].x * norm_factor);
+          pair[i].y = (float)((double)pair[i].y * norm_factor);
+        }
+      }
+    }
+  }
+}
+
+Status RankTables::build(const float* label_h, const int32_t* bnd_h, int32_t nq_, double sigmoid, int32_t trunc,
+                         bool norm) {
+  nq = nq_;
+  const int64_t n = bnd_h[nq];
+  for (int32_t q = 0; q < nq; ++q)
+    if (bnd_h[q + 1] < bnd_h[q]) return Status(LGBM_B200_ERR_INVALID_DATA, "query boundaries must not decrease");
+  // dcg.rs: label gains 2^i - 1 and discounts 1 / log2(2 + i)
+  std::vector<double> label_gain, discount;
+  label_gain.push_back(0.0);
+  for (int i = 1; i < 31; ++i) label_gain.push_back((double)((1 << i) - 1));
+  for (int i = 0; i < kRankMaxQuery; ++i) discount.push_back(1.0 / std::log2(2.0 + (double)i));
+  for (int64_t i = 0; i < n; ++i) {
+    const float l = label_h[i];
+    if (!(l >= 0.0f) || (int32_t)l >= (int32_t)label_gain.size())
+      return Status(LGBM_B200_ERR_INVALID_DATA, "lambdarank labels must be integers in [0, 30]");
+  }
+  // inverse max DCG at the truncation level per query (rank.rs:140-156)
+  std::vector<double> inv((size_t)nq);
+  const size_t k = (size_t)std::max(trunc, 0);
+  for (int32_t q = 0; q < nq; ++q) {
+    const size_t cnt_q = (size_t)(bnd_h[q + 1] - bnd_h[q]);
+    if (cnt_q > (size_t)kRankMaxQuery)
+      return Status(LGBM_B200_ERR_UNSUPPORTED, "a query holds more than 10000 rows");
+    std::vector<int32_t> cnt(label_gain.size(), 0);
+    for (size_t i = 0; i < cnt_q; ++i) cnt[(int32_t)label_h[bnd_h[q] + i]] += 1;
+    int32_t top = (int32_t)label_gain.size() - 1;
+    double v = 0.0;
+    for (size_t j = 0; j < std::min(k, cnt_q); ++j) {
+      while (top > 0 && cnt[top] <= 0) top -= 1;
+      if (top < 0) break;
+      v += discount[j] * label_gain[top];
+      cnt[top] -= 1;
+    }
+    inv[(size_t)q] = v > 0.0 ? 1.0 / v : v;
+  }
+  // the sigmoid table (rank.rs:162-176)
+  double min_in = -50.0 / sigmoid / 2.0;
+  double max_in = -min_in;
+  double idx_factor = (double)kRankSigmoidBins / (max_in - min_in);
+  std::vector<double> table((size_t)kRankSigmoidBins);
+  for (size_t i = 0; i < (size_t)kRankSigmoidBins; ++i) {
+    double score = (double)i / idx_factor + min_in;
+    table[i] = 1.0 / (1.0 + std::exp(score * sigmoid));
+  }
+  arena.free_all();
+  Status s;
+  int32_t* bnd_d;
+  double *inv_d, *table_d, *gain_d, *disc_d;
+  uint32_t* sorted_d;
+  if (!(s = arena.alloc_n(&bnd_d, (size_t)nq + 1)).ok() || !(s = arena.alloc_n(&inv_d, std::max<size_t>(1, nq))).ok() ||
+      !(s = arena.alloc_n(&table_d, table.size())).ok() || !(s = arena.alloc_n(&gain_d, label_gain.size())).ok() ||
+      !(s = arena.alloc_n(&disc_d, discount.size())).ok() ||
+      !(s = arena.alloc_n(&sorted_d, (size_t)std::max<int64_t>(1, n))).ok())
+    return s;
+  CU(cudaMemcpy(bnd_d, bnd_h, sizeof(int32_t) * ((size_t)nq + 1), cudaMemcpyHostToDevice));
+  if (nq > 0) CU(cudaMemcpy(inv_d, inv.data(), sizeof(double) * nq, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(table_d, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(gain_d, label_gain.data(), sizeof(double) * label_gain.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(disc_d, discount.data(), sizeof(double) * discount.size(), cudaMemcpyHostToDevice));
+  d.bnd = bnd_d;
+  d.nq = nq;
+  d.inv_max_dcg = inv_d;
+  d.sigmoid_table = table_d;
+  d.label_gain = gain_d;
+  d.discount = disc_d;
+  d.sorted = sorted_d;
+  d.sigmoid = sigmoid;
+  d.min_in = min_in;
+  d.max_in = max_in;
+  d.idx_factor = idx_factor;
+  d.truncation_level = trunc;
+  d.norm = norm ? 1 : 0;
+  return Status();
+}
+
+Status launch_lambdarank(const DRank& r, const float* label, const double* score, float* g, float* h, float2* gh,
+                         int sms, cudaStream_t s) {
+  if (r.nq == 0) return Status();
+  const int sort_grid = (int)std::min<int64_t>(r.nq, (int64_t)sms * 16);
+  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score);
+  CU_LAUNCH();
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((r.nq + 127) / 128, (int64_t)sms * 16));
+  k_lambdarank<<<grid, 128, 0, s>>>(r, label, score, g, h, gh);
+  CU_LAUNCH();
+  return Status();
+}
+
+}  // namespace lgbm_b200

@@ -359,9 +359,14 @@ class Booster:
                                float(p["bagging_fraction"]), int(p["bagging_freq"]), int(p["bagging_seed"]),
                                float(p["feature_fraction"]), int(p["feature_fraction_seed"]))
             label = np.ascontiguousarray(train_set.label, dtype=np.float32)
+            bnd = None
+            if train_set.group is not None:  # query boundaries (dataset.rs set_group)
+                bnd = np.concatenate([[0], np.cumsum(train_set.group)]).astype(np.int32)
+                self._bnd = bnd
             h = C.c_void_p()
             L.check(L.lib().lgbm_b200_booster_create(
-                self.learner.handle, C.byref(bc), _ptr(label, C.c_float), None, 0,
+                self.learner.handle, C.byref(bc), _ptr(label, C.c_float), _ptr(bnd, C.c_int32) if bnd is not None
+                else None, 0 if bnd is None else len(bnd) - 1,
                 _ptr(valid_bins, C.c_uint8) if valid_bins is not None else None, nv, C.byref(h)))
             self._b = h
             self.num_train = train_set.data.shape[0]

@@ -269,3 +269,36 @@ def test_predict_matches_oracle(lgb, orc):
     got = bst.predict(Xt, raw_score=True)
     want = om.predict_raw(Xt)[:, 0]
     assert np.array_equal(got, want)
+
+
+def _ranking_data(nq, f=16, seed=0):
+    rng = np.random.default_rng(seed)
+    group = np.clip(rng.geometric(1 / 20, nq), 1, 200).astype(np.int32)
+    n = int(group.sum())
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    X[rng.random(X.shape) < 0.2] = 0.0
+    s = X[:, 0] + 0.5 * X[:, 1] - 0.3 * X[:, 2] * X[:, 3] + 0.5 * rng.standard_normal(n)
+    y = np.digitize(s, np.quantile(s, [0.5, 0.75, 0.9, 0.97])).astype(np.float32)
+    return X, y, group
+
+
+def test_lambdarank_boosting_matches_oracle(lgb, orc):
+    X, y, group = _ranking_data(400, seed=30)
+    params = {"objective": "lambdarank", "num_leaves": 31, "min_data_in_leaf": 20, "learning_rate": 0.1}
+    rounds = 8
+    ds = lgb.Dataset(X, y, group=group, params=params)
+    bst = lgb.train(params, ds, rounds)
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, rounds, group=group)
+    assert bst.num_trees() == len(om.trees)
+    same = 0
+    for a, o in zip(bst.trees, om.trees):
+        if not (np.array_equal(a["split_feature"], o["split_feature"])
+                and np.array_equal(a["threshold_in_bin"], o["threshold_in_bin"])):
+            break
+        np.testing.assert_allclose(a["leaf_value"], o["leaf_value"], rtol=1e-6, atol=1e-12)
+        same += 1
+    assert same >= 4, same
+    ks = [1, 3, 5, 10]
+    got = orc.ndcg(y, bst.scores()[0], group, ks)
+    want = orc.ndcg(y, om.scores()[0], group, ks)
+    np.testing.assert_allclose(got, want, atol=1e-3)
