@@ -126,6 +126,9 @@ typedef struct {
   int32_t device;
   /* launch shape knobs; 0 picks the built-in defaults */
   int32_t hist_rows_per_block, hist_block_threads, use_cuda_graph;
+  /* 1: grow each tree in one persistent cooperative launch (grid barriers
+   * between the split phases); 0: one launch per kernel per split step */
+  int32_t persistent_grow;
 } LgbmB200LearnerConfig;
 
 typedef struct {

@@ -35,8 +35,9 @@ struct ScanSmem {
   double eg, eh;                          // the extra candidate t = -1
   int32_t ec, brk, ok;
   int64_t eq;
-  double wgain[kScanThreads / 32];        // per-warp best candidates
-  int32_t wt[kScanThreads / 32];
+  double wgain[32];                       // per-warp best candidates (up to 32 warps)
+  int32_t wt[32];
+  DSplit out;                             // the result, stored to global memory once
 };
 
 __global__ void k_tree_init(const __grid_constant__ DCtx c, const uint32_t* bag, const int32_t* n_used);
@@ -49,6 +50,19 @@ void launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, cons
                  int32_t sub_rows);
 template <bool kInt>
 __global__ void k_scan(const __grid_constant__ DCtx c);
+
+// Persistent tree growth (one cooperative launch per tree).
+constexpr int kGrowThreads = 512;
+struct GrowSync {
+  unsigned int count;  // CTAs arrived at the current barrier
+  unsigned int gen;    // barrier generation
+  int status;          // kStatusTimeout when a wait gave up
+  int pad;
+};
+const void* grow_kernel(int mode, int ng);
+size_t grow_smem_bytes(int mode, int ng);
+cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                        int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns);
 __global__ void k_partition(const __grid_constant__ DCtx c);
 __global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
 __global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* sums);

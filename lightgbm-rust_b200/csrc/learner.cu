@@ -117,6 +117,17 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
   }
   h->part_grid = h->num_sms * 4;
+  if (cfg->persistent_grow) {
+    // one resident CTA group per slot: the cooperative launch holds every CTA
+    const void* gk = grow_kernel(mode, h->hist_ng);
+    h->grow_smem = grow_smem_bytes(mode, h->hist_ng);
+    CU(cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->grow_smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, kGrowThreads, h->grow_smem));
+    const int k = std::max(1, cfg->num_tree_slots);
+    h->grow_grid = per_sm * h->num_sms / k * k;
+    if (h->grow_grid < k) return Status(LGBM_B200_ERR_UNSUPPORTED, "persistent growth does not fit on the device");
+  }
   int32_t rpb = cfg->hist_rows_per_block > 0 ? cfg->hist_rows_per_block : 512;
 
   // device buffers
@@ -207,6 +218,12 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   if (!(s = A.alloc_n(&h->leaf_sums, (size_t)K * L * 2)).ok()) return s;
   if (!(s = A.alloc_n(&h->leaf_values_dev, (size_t)K * L)).ok()) return s;
+  if (cfg->persistent_grow) {
+    if (!(s = A.alloc_n(&h->grow_sync, 1)).ok()) return s;
+    if (!(s = A.alloc_n(&h->phase_ns, 4)).ok()) return s;
+    CU(cudaMemset(h->grow_sync, 0, sizeof(GrowSync)));
+    CU(cudaMemset(h->phase_ns, 0, 4 * sizeof(long long)));
+  }
   if (mode == LGBM_B200_HIST_QUANT) {
     if (!(s = A.alloc_n(&h->maxbits, 2)).ok()) return s;
     if (!(s = A.alloc_n(&h->quant_counter, 1)).ok()) return s;
@@ -293,7 +310,13 @@ static Status enqueue_tree(LgbmB200Learner* h) {
   dim3 hist_grid(h->hist_grid, h->ntiles, K);
   dim3 scan_grid(h->nf, 2, K);
   dim3 part_grid(h->part_grid, 1, K);
-  for (int step = 0; step < L - 1; ++step) {
+  if (h->cfg.persistent_grow) {
+    CU(cudaMemsetAsync(h->grow_sync, 0, sizeof(GrowSync), s));
+    if (h->timing) CU(cudaMemsetAsync(h->phase_ns, 0, 4 * sizeof(long long), s));
+    CU(launch_grow(mode, h->hist_ng, h->grow_grid, h->grow_smem, s, c, h->tiles, h->sub_rows, h->ntiles,
+                   h->grow_sync, L - 1, h->timing ? h->phase_ns : nullptr));
+  }
+  for (int step = 0; step < (h->cfg.persistent_grow ? 0 : L - 1); ++step) {
     cudaEvent_t* ev = h->timing ? &h->ev[(size_t)4 * step] : nullptr;
     if (ev) CU(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal));
     launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows);
@@ -314,13 +337,15 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
     CU_LAUNCH();
   }
-  h->last_launches = 1 + 3 * (L - 1) + ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
+  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : 3 * (L - 1)) +
+                     ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
   return Status();
 }
 
 static Status run_tree(LgbmB200Learner* h) {
   cudaStream_t s = h->stream;
-  const bool graph = h->cfg.use_cuda_graph != 0;
+  // a cooperative launch is enqueued directly rather than captured
+  const bool graph = h->cfg.use_cuda_graph != 0 && !h->cfg.persistent_grow;
   const int key = (h->bagging ? 1 : 0) + 2 * h->ctx.bagging + 4 * (h->timing ? 1 : 0);
   if (!graph) return enqueue_tree(h);
   if (h->graph_exec == nullptr || h->graph_key != key) {
@@ -463,7 +488,16 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
   for (int k = 0; k < K; ++k)
     CU(cudaMemcpyAsync(&h->st_h[k], h->slots_h[k].st, sizeof(DSlotState), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
-  if (h->timing) {  // per-kernel-family device time of this tree
+  if (h->cfg.persistent_grow) {
+    GrowSync gsh;
+    long long ph[4] = {0, 0, 0, 0};
+    CU(cudaMemcpyAsync(&gsh, h->grow_sync, sizeof(gsh), cudaMemcpyDeviceToHost, s));
+    if (h->timing) CU(cudaMemcpyAsync(ph, h->phase_ns, sizeof(ph), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (gsh.status != 0) return Status(LGBM_B200_ERR_TIMEOUT, "device-side wait timed out (grid barrier)");
+    // phase times seen by the first CTA: histogram, scan, partition, bookkeeping
+    for (int i = 0; i < 4; ++i) h->last_ms[i] = (double)ph[i] / 1e6;
+  } else if (h->timing) {  // per-kernel-family device time of this tree
     for (int step = 0; step < h->L - 1; ++step) {
       cudaEvent_t* ev = &h->ev[(size_t)4 * step];
       float a, b, d;

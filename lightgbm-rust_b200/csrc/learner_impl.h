@@ -195,6 +195,10 @@ struct LgbmB200Learner {
   DTileTable tiles{};
   int ntiles = 1;
   int hist_ng = 1;  // 32-feature groups per histogram tile
+  int grow_grid = 0;       // CTAs of the persistent grow launch
+  size_t grow_smem = 0;
+  GrowSync* grow_sync = nullptr;
+  long long* phase_ns = nullptr;  // persistent growth: device ns per phase
   size_t hist_smem = 0, scan_smem = 0;
   int hist_grid = 148, part_grid = 592, root_grid = kRootBlocks;
   int32_t sub_rows = 8192;

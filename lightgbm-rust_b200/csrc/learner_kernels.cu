@@ -198,7 +198,8 @@ struct LeafRows {
 // the cluster's reduction (its row range may be empty); returns false for
 // CTAs of unused clusters and when no histogram is needed.
 template <int kCl>
-__device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, LeafRows& lr, int64_t& r0, int64_t& r1) {
+__device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int rank, int count, LeafRows& lr,
+                                           int64_t& r0, int64_t& r1) {
   DSlotState* st = s.st;
   if (st->done || !st->need_find) return false;
   int32_t leaf = st->smaller.leaf;
@@ -206,13 +207,12 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, LeafRo
   lr.begin = s.leaf_begin[leaf];
   lr.idx = s.idx[s.leaf_side[leaf]];
   int64_t per = c.rows_per_block;
-  int64_t active = min((int64_t)gridDim.x, (lr.count + per - 1) / per);
+  int64_t active = min((int64_t)count, (lr.count + per - 1) / per);
   active = (active + kCl - 1) / kCl * kCl;
-  if ((int64_t)blockIdx.x >= active) return false;
+  if ((int64_t)rank >= active) return false;
   int64_t chunk = (lr.count + active - 1) / active;
-  r0 = min(lr.count, (int64_t)blockIdx.x * chunk);
+  r0 = min(lr.count, (int64_t)rank * chunk);
   r1 = min(lr.count, r0 + chunk);
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) st->hist_rows += lr.count;
   return true;
 }
 
@@ -245,19 +245,12 @@ __device__ __forceinline__ void tile_of(const DTileTable& tt, int tile, int& f0,
 // (distributed shared memory) and adds it to the leaf histogram, so a
 // cluster issues one global atomic per cell instead of one per CTA. The
 // float forms (one 148 KB CTA per SM) flush each CTA's own cells.
-template <int kMode, int kNG>
-__global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kHistThreads, 2)
-    k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+template <int kMode, int kNG, int kCl>
+__device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, int tile, const LeafRows& lr,
+                          int64_t r0, int64_t r1, int32_t sub_rows, unsigned char* smem_raw) {
   namespace cg = cooperative_groups;
-  constexpr int kCl = hist_cluster(kMode);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const DSlot& s = c.slots[blockIdx.z];
-  LeafRows lr;
-  int64_t r0, r1;
-  if (!hist_setup<kCl>(c, s, lr, r0, r1)) return;
-  cg::cluster_group cluster = cg::this_cluster();
   int f0, f1, bin0, nbins;
-  tile_of(tt, blockIdx.y, f0, f1, bin0, nbins);
+  tile_of(tt, tile, f0, f1, bin0, nbins);
   (void)nbins;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kHistThreads / 32;
@@ -310,17 +303,18 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
   };
   // the (g, h) of cell i in the shared memory `base` of one CTA
   auto cell_of = [&](const unsigned char* base, int i, auto& gv, auto& hv) {
-    const int g = i / kGroupCells, k = i % kGroupCells;
     if constexpr (kMode == 2) {
       const int32_t cell = reinterpret_cast<const int32_t*>(base)[i];
       const int64_t h = (int64_t)(cell & 0xFFFF);
       gv = (int64_t)((cell - (int32_t)h) >> 16);
       hv = h;
     } else if constexpr (kMode == 0) {
+      const int g = i / kGroupCells, k = i % kGroupCells;
       const double* d = reinterpret_cast<const double*>(base + (size_t)g * kGroupCells * 16);
       gv = d[k];
       hv = d[kGroupCells + k];
     } else {
+      const int g = i / kGroupCells, k = i % kGroupCells;
       const float* fl = reinterpret_cast<const float*>(base + (size_t)g * kGroupCells * 16);
       gv = (double)fl[k] + (double)fl[kGroupCells + k];
       hv = (double)fl[2 * kGroupCells + k] + (double)fl[3 * kGroupCells + k];
@@ -333,7 +327,7 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
   uint4 nb[2 * kNG];
   auto fetch = [&](int64_t pos) {
     const bool live = pos < r1;
-    nrow = live ? __ldg(idx + pos) : 0u;
+    nrow = live ? __ldcg(idx + pos) : 0u;  // written by the partition: through L2
     if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
     else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
     const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
@@ -421,12 +415,15 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
     }
   }
   // cluster reduction: CTA rank r adds slice r of the cells, summed over the
-  // cluster's CTAs in rank order
-  cluster.sync();
+  // cluster's CTAs in rank order (a cluster of one adds its own cells)
+  if constexpr (kCl > 1) cg::this_cluster().sync();
+  else __syncthreads();
   {
     const int total = ngroups * kGroupCells;
     const int per = (total + kCl - 1) / kCl;
-    const int lo = (int)cluster.block_rank() * per, hi = min(total, lo + per);
+    int crank = 0;
+    if constexpr (kCl > 1) crank = (int)cg::this_cluster().block_rank();
+    const int lo = crank * per, hi = min(total, lo + per);
     for (int i = lo + (int)threadIdx.x; i < hi; i += kHistThreads) {
       if constexpr (kMode == 2) {
         emit(i, [&](int ii, int64_t& gv, int64_t& hv) {
@@ -435,7 +432,8 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
 #pragma unroll
           for (int r = 0; r < kCl; ++r) {
             int64_t a, b;
-            cell_of(cluster.map_shared_rank(cells, r), ii, a, b);
+            if constexpr (kCl > 1) cell_of(cg::this_cluster().map_shared_rank(cells, r), ii, a, b);
+            else cell_of(cells, ii, a, b);
             gv += a;
             hv += b;
           }
@@ -447,7 +445,8 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
 #pragma unroll
           for (int r = 0; r < kCl; ++r) {
             double a, b;
-            cell_of(cluster.map_shared_rank(cells, r), ii, a, b);
+            if constexpr (kCl > 1) cell_of(cg::this_cluster().map_shared_rank(cells, r), ii, a, b);
+            else cell_of(cells, ii, a, b);
             gv += a;
             hv += b;
           }
@@ -455,8 +454,21 @@ __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kH
       }
     }
   }
-  // no CTA leaves while another may still read its shared memory
-  cluster.sync();
+  // no CTA leaves (or reuses its cells) while another may still read them
+  if constexpr (kCl > 1) cg::this_cluster().sync();
+  else __syncthreads();
+}
+
+template <int kMode, int kNG>
+__global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kHistThreads, 2)
+    k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const DSlot& s = c.slots[blockIdx.z];
+  LeafRows lr;
+  int64_t r0, r1;
+  if (!hist_setup<hist_cluster(kMode)>(c, s, blockIdx.x, gridDim.x, lr, r0, r1)) return;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) s.st->hist_rows += lr.count;
+  hist_body<kMode, kNG, hist_cluster(kMode)>(c, s, tt, blockIdx.y, lr, r0, r1, sub_rows, smem_raw);
 }
 
 #define LGBM_B200_HIST_INST(M, G) \
@@ -942,7 +954,7 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
   if (tid == 0) {
     double bg = -INFINITY;
     int32_t bt = INT32_MIN;
-    for (int w = 0; w < kScanThreads / 32; ++w) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       double og = sm.wgain[w];
       int32_t ot = sm.wt[w];
       if (og > bg || (og == bg && ot != INT32_MIN && (bt == INT32_MIN || (reverse ? ot > bt : ot < bt)))) {
@@ -1124,20 +1136,14 @@ __device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R
   st->num_leaves_cur = R + 1;
 }
 
+// Threshold scan of feature f for one leaf side (0: smaller, 1: larger) of
+// slot s, by the whole CTA (at least kScanThreads threads): the leaf's view
+// is fixed (histogram.rs:42-56), the larger leaf's is formed as parent -
+// smaller (histogram.rs:59-63) and stored, and the best threshold is written
+// to feat_res / feat_ok.
 template <bool kInt>
-__global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ DCtx c) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ScanSmem& sm = *reinterpret_cast<ScanSmem*>(smem_raw);
-  const DSlot& s = c.slots[blockIdx.z];
+__device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSmem& sm) {
   DSlotState* st = s.st;
-  if (st->done) return;
-  // the partition that follows claims its row tiles from this counter
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-    st->part_ticket = 0;
-    st->part_done = 0;
-  }
-  const int f = blockIdx.x;
-  const int side = blockIdx.y;  // 0: the smaller leaf, 1: the larger leaf
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const DFeature m = c.feats[f];
   const DParams& p = c.p;
@@ -1146,19 +1152,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
   const bool need = st->need_find != 0;
   const int32_t L = st->left_leaf;
   const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
-  if (used && (side == 0 || have_larger)) {
+  if (!(used && (side == 0 || have_larger))) return;
+  {
     const DLeafSplits sl = st->smaller;
     const int len = m.view_len;
     const size_t sbase = (size_t)s.buf_of[sl.leaf] * c.total_bins + m.view_start;
     // the smaller leaf's view with its most frequent bin fixed (histogram.rs:42-56)
+    // histogram cells are written by other CTAs' atomics: loaded through L2
     if (kInt) {
-      const int64_t* hs = reinterpret_cast<const int64_t*>(s.hist) + sbase;
-      if (tid < len) sm.ig[tid] = hs[tid];
+      const long long* hs = reinterpret_cast<const long long*>(s.hist) + sbase;
+      if (tid < len) sm.ig[tid] = (int64_t)__ldcg(hs + tid);
     } else {
       const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
       if (tid < len) {
-        sm.g[tid] = hs[2 * tid];
-        sm.h[tid] = hs[2 * tid + 1];
+        sm.g[tid] = __ldcg(hs + 2 * tid);
+        sm.h[tid] = __ldcg(hs + 2 * tid + 1);
       }
     }
     __syncthreads();
@@ -1210,12 +1218,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
       if (tid < len) {
         if (kInt) {
           int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
-          int64_t v = (int64_t)((uint64_t)lh[tid] - (uint64_t)sm.ig[tid]);
+          int64_t v = (int64_t)((uint64_t)__ldcg(reinterpret_cast<const long long*>(lh) + tid) - (uint64_t)sm.ig[tid]);
           sm.ig[tid] = v;
           lh[tid] = v;
         } else {
           double* lh = reinterpret_cast<double*>(s.hist) + 2 * lbase;
-          double g = lh[2 * tid] - sm.g[tid], h = lh[2 * tid + 1] - sm.h[tid];
+          double g = __ldcg(lh + 2 * tid) - sm.g[tid], h = __ldcg(lh + 2 * tid + 1) - sm.h[tid];
           sm.g[tid] = g;
           sm.h[tid] = h;
           lh[2 * tid] = g;
@@ -1239,7 +1247,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
     lc.cmin = s.cmin[ls.leaf];
     lc.cmax = s.cmax[ls.leaf];
     // the result is built in shared memory and stored once
-    __shared__ DSplit out;
+    DSplit& out = sm.out;
     bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
     if (tid == 0) {
       out.feature = m.real_index;
@@ -1252,6 +1260,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
     for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
   }
 }
+
+template <bool kInt>
+__global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ DCtx c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  if (st->done) return;
+  // the partition that follows claims its row tiles from this counter
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    st->part_ticket = 0;
+    st->part_done = 0;
+  }
+  scan_item<kInt>(c, s, blockIdx.x, blockIdx.y, *reinterpret_cast<ScanSmem*>(smem_raw));
+}
 template __global__ void k_scan<false>(const __grid_constant__ DCtx);
 template __global__ void k_scan<true>(const __grid_constant__ DCtx);
 
@@ -1262,8 +1284,6 @@ template __global__ void k_scan<true>(const __grid_constant__ DCtx);
 // decoupled look-back on the running left count.
 // =====================================================================================
 constexpr int kPartThreads = 256;
-constexpr int kPartItems = 8;
-constexpr int kPartTile = kPartThreads * kPartItems;
 constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
 constexpr uint32_t kEpochMask = 0x7FFFFFFFu;
 constexpr unsigned long long kValueMask = (1ull << 31) - 1;
@@ -1336,8 +1356,8 @@ struct SplitDecision {
   double side_bg[2];     // best (penalized) gain of the smaller / larger new leaf
   int32_t side_feat[2];  // its real feature, -1 none
   int32_t side_bf[2];    // its inner feature, -1 none
-  double wbg[kPartThreads / 32];
-  int32_t wfeat[kPartThreads / 32], wleaf[kPartThreads / 32];
+  double wbg[32];
+  int32_t wfeat[32], wleaf[32];
   int32_t bl;            // the leaf to split, -1: the tree is finished
 };
 
@@ -1407,7 +1427,7 @@ __device__ void decide_split(const DCtx& c, const DSlot& s, SplitDecision& d) {
   } else {
     double bg = -INFINITY;
     int32_t bfeat = -1, bl = INT32_MAX;
-    for (int32_t l = tid - 64; l < NL; l += kPartThreads - 64) {
+    for (int32_t l = tid - 64; l < NL; l += (int32_t)blockDim.x - 64) {
       if (need && (l == S || l == G)) continue;
       double g = s.bgain[l];
       int32_t fe = s.bfeat[l];
@@ -1444,7 +1464,7 @@ __device__ void decide_split(const DCtx& c, const DSlot& s, SplitDecision& d) {
         bl = l;
       }
     };
-    for (int w = 2; w < kPartThreads / 32; ++w) offer(d.wbg[w], d.wfeat[w], d.wleaf[w]);
+    for (int w = 2; w < (int)(blockDim.x >> 5); ++w) offer(d.wbg[w], d.wfeat[w], d.wleaf[w]);
     if (need) {
       offer(d.side_bg[0], d.side_feat[0], S);
       if (have_larger) offer(d.side_bg[1], d.side_feat[1], G);
@@ -1507,76 +1527,74 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   }
 }
 
-// Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
-// step's split decision and the goes-left LUT, then claims row tiles.
-__global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
-  const DSlot& s = c.slots[blockIdx.z];
-  DSlotState* st = s.st;
-  if (st->done) return;
-  __shared__ uint8_t lut[kMaxBins];
-  __shared__ int32_t warp_tot[kPartThreads / 32];
-  __shared__ int32_t s_tile, s_prefix;
-  __shared__ SplitDecision dec;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int32_t R = st->num_leaves_cur;
-  const uint32_t epoch = st->part_epoch;
-  decide_split(c, s, dec);
-  const int32_t L = dec.bl;
-  if (L < 0) {
-    if (blockIdx.x == 0 && tid == 0) st->done = 1;
-    return;
-  }
+// Shared state of a partition CTA.
+struct PartShared {
+  uint8_t lut[kMaxBins];
+  int32_t warp_tot[32];
+  int32_t tile, prefix;
+  bool last;
+  SplitDecision dec;
+};
+
+constexpr int kPartTileRows = 2048;  // rows per partition tile (tile_status holds one word per tile)
+
+// Step prologue of a partition CTA: the split decision and, when a leaf is
+// split, its goes-left LUT in ps.lut. Returns the leaf to split (-1: the
+// tree is finished).
+__device__ int32_t partition_prologue(const DCtx& c, const DSlot& s, PartShared& ps) {
+  decide_split(c, s, ps.dec);
+  const int32_t L = ps.dec.bl;
+  if (L < 0) return -1;
+  const DSlotState* st = s.st;
   const int32_t nf = c.num_features;
-  const DSplit& info = (st->need_find && L == st->smaller.leaf)   ? s.feat_res[dec.side_bf[0]]
-                       : (st->need_find && L == st->larger.leaf) ? s.feat_res[nf + dec.side_bf[1]]
+  const DSplit& info = (st->need_find && L == st->smaller.leaf)   ? s.feat_res[ps.dec.side_bf[0]]
+                       : (st->need_find && L == st->larger.leaf) ? s.feat_res[nf + ps.dec.side_bf[1]]
                                                                   : s.best[L];
-  const int32_t inner = info.inner;
-  build_partition_lut(c, info, lut);
+  build_partition_lut(c, info, ps.lut);
+  return L;
+}
+
+// The inner feature the split of leaf L tests.
+__device__ __forceinline__ int32_t split_inner_of(const DCtx& c, const DSlot& s, const PartShared& ps, int32_t L) {
+  const DSlotState* st = s.st;
+  const int32_t nf = c.num_features;
+  if (st->need_find && L == st->smaller.leaf) return s.feat_res[ps.dec.side_bf[0]].inner;
+  if (st->need_find && L == st->larger.leaf) return s.feat_res[nf + ps.dec.side_bf[1]].inner;
+  return s.best[L].inner;
+}
+
+// Row tiles of the split leaf L claimed in order by the CTAs (kItems rows
+// per thread, blockDim.x * kItems == kPartTileRows), each chained to its
+// predecessors by a decoupled look-back on the left count. The CTA that
+// partitions the last tile posts the left count in st->part_left.
+template <int kItems>
+__device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, int32_t L, uint32_t epoch) {
+  DSlotState* st = s.st;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
   const int32_t side = s.leaf_side[L];
-  // zero the fresh histogram buffer R for the next smaller leaf
-  {
-    size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
-    double* h = reinterpret_cast<double*>(s.hist) + (size_t)R * cells;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h[i] = 0.0;
-  }
-  __syncthreads();
-  __shared__ bool s_last;
-  // the last CTA to exit ends the step
-  auto exit_step = [&]() {
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      s_last = atomicAdd(&st->part_done, 1) == (int)gridDim.x - 1;
-    }
-    __syncthreads();
-    if (s_last) {
-      __threadfence();
-      finish_step(c, s, dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
-    }
-  };
-  if (cnt == 0) {
-    exit_step();
-    return;
-  }
+  const int32_t inner = split_inner_of(c, s, ps, L);
+  if (cnt == 0) return;
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
-  const int32_t ntiles = (cnt + kPartTile - 1) / kPartTile;
+  const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
   const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
+  const uint8_t* lut = ps.lut;
   while (true) {
-    if (tid == 0) s_tile = atomicAdd(&st->part_ticket, 1);
     __syncthreads();
-    const int32_t tile = s_tile;
+    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+    __syncthreads();
+    const int32_t tile = ps.tile;
     if (tile >= ntiles) break;
-    const int32_t t0 = tile * kPartTile;
-    uint32_t rows[kPartItems];
+    const int32_t t0 = tile * kPartTileRows;
+    uint32_t rows[kItems];
     uint32_t flags = 0;
     int32_t nleft = 0;
 #pragma unroll
-    for (int k = 0; k < kPartItems; ++k) {
-      int32_t pos = t0 + tid * kPartItems + k;
+    for (int k = 0; k < kItems; ++k) {
+      int32_t pos = t0 + tid * kItems + k;
       if (pos < cnt) {
-        uint32_t r = in[pos];
+        uint32_t r = __ldcg(in + pos);
         rows[k] = r;
         uint32_t raw = col[r];
         if (lut[raw]) {
@@ -1591,12 +1609,12 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
       int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += v;
     }
-    if (lane == 31) warp_tot[warp] = incl;
+    if (lane == 31) ps.warp_tot[warp] = incl;
     __syncthreads();
     int32_t wbase = 0, tile_left = 0;
-    for (int w = 0; w < kPartThreads / 32; ++w) {
-      if (w < warp) wbase += warp_tot[w];
-      tile_left += warp_tot[w];
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      if (w < warp) wbase += ps.warp_tot[w];
+      tile_left += ps.warp_tot[w];
     }
     const int32_t excl = wbase + incl - nleft;
     // decoupled look-back on the left count: warp 0 reads 32 predecessors at a
@@ -1606,7 +1624,7 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
       if (tile == 0) {
         if (lane == 0) {
           atomicExch(&stat[0], pack_status(epoch, kFlagInc, (uint64_t)tile_left));
-          s_prefix = 0;
+          ps.prefix = 0;
         }
       } else {
         if (lane == 0) atomicExch(&stat[tile], pack_status(epoch, kFlagAgg, (uint64_t)tile_left));
@@ -1649,17 +1667,17 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
         }
         if (lane == 0) {
           atomicExch(&stat[tile], pack_status(epoch, kFlagInc, (uint64_t)(acc + tile_left)));
-          s_prefix = (int32_t)acc;
+          ps.prefix = (int32_t)acc;
         }
       }
     }
     __syncthreads();
-    const int32_t prefix = s_prefix;
+    const int32_t prefix = ps.prefix;
     // scatter: left rows ascending from begin, right rows descending from the end
     int32_t lrank = prefix + excl;
 #pragma unroll
-    for (int k = 0; k < kPartItems; ++k) {
-      int32_t pos = t0 + tid * kPartItems + k;
+    for (int k = 0; k < kItems; ++k) {
+      int32_t pos = t0 + tid * kItems + k;
       if (pos < cnt) {
         if (flags & (1u << k)) {
           out[lrank++] = rows[k];
@@ -1670,9 +1688,46 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
       }
     }
     if (tile == ntiles - 1 && tid == 0) st->part_left = prefix + tile_left;
-    __syncthreads();
   }
-  exit_step();
+}
+
+// Zeroes histogram buffer R (the next smaller leaf's), spread over `count`
+// CTAs of which this is `rank`.
+__device__ __forceinline__ void zero_hist_buffer(const DCtx& c, const DSlot& s, int32_t R, int rank, int count) {
+  size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+  double* h = reinterpret_cast<double*>(s.hist) + (size_t)R * cells;
+  for (size_t i = (size_t)rank * blockDim.x + threadIdx.x; i < cells; i += (size_t)count * blockDim.x) h[i] = 0.0;
+}
+
+// Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
+// step's split decision and the goes-left LUT, then claims row tiles; the
+// last CTA to exit ends the step.
+__global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  if (st->done) return;
+  __shared__ PartShared ps;
+  const int tid = threadIdx.x;
+  const int32_t R = st->num_leaves_cur;
+  const uint32_t epoch = st->part_epoch;
+  const int32_t L = partition_prologue(c, s, ps);
+  if (L < 0) {
+    if (blockIdx.x == 0 && tid == 0) st->done = 1;
+    return;
+  }
+  zero_hist_buffer(c, s, R, blockIdx.x, gridDim.x);
+  partition_rows<kPartTileRows / kPartThreads>(c, s, ps, L, epoch);
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    ps.last = atomicAdd(&st->part_done, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (ps.last) {
+    __threadfence();
+    const int32_t cnt = s.leaf_count[L];
+    finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+  }
 }
 
 // Column-major copy of the bin matrix (the partition reads one feature of the
@@ -1841,6 +1896,176 @@ __global__ void __launch_bounds__(256) k_add_tree_binned(const __grid_constant__
     }
     sc[r] += lv[node];
   }
+}
+
+// =====================================================================================
+// Persistent tree growth: one cooperative launch grows the whole tree (every
+// slot). Per split step the CTAs run the phases of the per-step kernels,
+// separated by grid barriers:
+//   H  histogram of each slot's smaller leaf (the slot's CTA group shares the rows)
+//   S  threshold scans, items (slot, feature, leaf side) over all CTAs
+//   P  split decision, LUT and row partition (each slot's CTA group)
+//   F  the step's bookkeeping by the first CTA of each group
+// The cooperative launch keeps every CTA resident, so a barrier never waits
+// on a CTA that has not started; every wait is still bounded and reports a
+// timeout instead of hanging.
+// =====================================================================================
+
+// Grid barrier over `nblocks` CTAs (sense reversal on a generation counter).
+// Returns false when a wait timed out here or anywhere in the grid.
+__device__ bool grid_barrier(GrowSync* gs, unsigned int nblocks) {
+  __shared__ int s_ok;
+  __threadfence();  // this thread's writes before the barrier are visible to the grid
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = &gs->gen;
+    const unsigned int g = *vgen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&gs->count, 1u) == nblocks - 1u) {
+      gs->count = 0;  // no CTA touches the count before the generation moves
+      __threadfence();
+      atomicAdd(&gs->gen, 1u);
+    } else {
+      int spins = 0;
+      while (*vgen == g) {
+        if (++spins > kSpinLimit) {
+          atomicExch(&gs->status, kStatusTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*reinterpret_cast<volatile int*>(&gs->status) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  __threadfence();  // later reads observe the other CTAs' writes
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ int64_t global_ns() {
+  int64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <int kMode, int kNG>
+__global__ void __launch_bounds__(kGrowThreads, 1)
+    k_grow(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows, int32_t ntiles, GrowSync* gs,
+           int32_t num_steps, long long* phase_ns) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PartShared ps;
+  __shared__ int s_any;
+  constexpr bool kInt = kMode == 2;
+  const unsigned int G = gridDim.x;
+  const int K = c.num_slots;
+  const int per = (int)G / K;  // CTAs per slot group (the host makes G a multiple of K)
+  const int slot = (int)blockIdx.x / per;
+  const int rank = (int)blockIdx.x - slot * per;
+  const DSlot& s = c.slots[slot];
+  DSlotState* st = s.st;
+  const int tid = threadIdx.x;
+  const int32_t nf = c.num_features;
+  const bool timer = blockIdx.x == 0 && tid == 0 && phase_ns != nullptr;
+  int64_t t_prev = timer ? global_ns() : 0;
+  auto mark = [&](int phase) {
+    if (timer) {
+      const int64_t t = global_ns();
+      phase_ns[phase] += t - t_prev;
+      t_prev = t;
+    }
+  };
+  for (int step = 0; step < num_steps; ++step) {
+    // every CTA reads the same flags after a barrier: the loop ends together
+    if (tid == 0) {
+      int any = 0;
+      for (int k = 0; k < K; ++k) any |= *reinterpret_cast<volatile int32_t*>(&c.slots[k].st->done) == 0;
+      s_any = any;
+    }
+    __syncthreads();
+    if (!s_any) break;
+    // H: histogram of the slot's smaller leaf
+    {
+      LeafRows lr;
+      int64_t r0, r1;
+      if (hist_setup<1>(c, s, rank, per, lr, r0, r1)) {
+        if (rank == 0 && tid == 0) st->hist_rows += lr.count;
+        for (int t = 0; t < ntiles; ++t) hist_body<kMode, kNG, 1>(c, s, tt, t, lr, r0, r1, sub_rows, smem_raw);
+      }
+    }
+    if (!grid_barrier(gs, G)) return;
+    mark(0);
+    // S: threshold scans
+    {
+      ScanSmem& sm = *reinterpret_cast<ScanSmem*>(smem_raw);
+      const int nitems = K * nf * 2;
+      for (int it = blockIdx.x; it < nitems; it += (int)G) {
+        const int k = it / (2 * nf), rem = it - k * 2 * nf;
+        const DSlot& sk = c.slots[k];
+        if (*reinterpret_cast<volatile int32_t*>(&sk.st->done)) continue;
+        scan_item<kInt>(c, sk, rem >> 1, rem & 1, sm);
+        __syncthreads();
+      }
+      if (blockIdx.x == 0 && tid < K) c.slots[tid].st->part_ticket = 0;
+    }
+    if (!grid_barrier(gs, G)) return;
+    mark(1);
+    // P: the split decision and the row partition of the slot
+    int32_t L = -1, R = 0;
+    if (!*reinterpret_cast<volatile int32_t*>(&st->done)) {
+      R = st->num_leaves_cur;
+      const uint32_t epoch = st->part_epoch;
+      L = partition_prologue(c, s, ps);
+      if (L < 0) {
+        if (rank == 0 && tid == 0) st->done = 1;
+      } else {
+        zero_hist_buffer(c, s, R, rank, per);
+        partition_rows<kPartTileRows / kGrowThreads>(c, s, ps, L, epoch);
+      }
+    }
+    if (!grid_barrier(gs, G)) return;
+    mark(2);
+    // F: bookkeeping of the step
+    if (L >= 0 && rank == 0) {
+      const int32_t cnt = s.leaf_count[L];
+      finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+    }
+    if (!grid_barrier(gs, G)) return;
+    mark(3);
+  }
+}
+
+#define LGBM_B200_GROW_INST(M, G)                                                                            \
+  template __global__ void k_grow<M, G>(const __grid_constant__ DCtx, DTileTable, int32_t, int32_t, GrowSync*, \
+                                        int32_t, long long*);
+LGBM_B200_GROW_INST(0, 1)
+LGBM_B200_GROW_INST(1, 1)
+LGBM_B200_GROW_INST(2, 1)
+LGBM_B200_GROW_INST(2, 2)
+LGBM_B200_GROW_INST(2, 3)
+LGBM_B200_GROW_INST(2, 4)
+#undef LGBM_B200_GROW_INST
+
+const void* grow_kernel(int mode, int ng) {
+  if (mode == 0) return reinterpret_cast<const void*>(&k_grow<0, 1>);
+  if (mode == 1) return reinterpret_cast<const void*>(&k_grow<1, 1>);
+  switch (ng) {
+    case 1: return reinterpret_cast<const void*>(&k_grow<2, 1>);
+    case 2: return reinterpret_cast<const void*>(&k_grow<2, 2>);
+    case 3: return reinterpret_cast<const void*>(&k_grow<2, 3>);
+    default: return reinterpret_cast<const void*>(&k_grow<2, 4>);
+  }
+}
+
+size_t grow_smem_bytes(int mode, int ng) { return std::max(hist_smem_bytes(mode, ng), sizeof(ScanSmem)); }
+
+cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                        int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns) {
+  void* args[] = {const_cast<DCtx*>(&c), const_cast<DTileTable*>(&tt), &sub_rows, &ntiles, &gs, &num_steps, &phase_ns};
+  return cudaLaunchCooperativeKernel(grow_kernel(mode, ng), dim3(grid), dim3(kGrowThreads), args, smem, st);
 }
 
 }  // namespace lgbm_b200

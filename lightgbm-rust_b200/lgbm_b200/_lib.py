@@ -55,7 +55,7 @@ class LearnerConfig(C.Structure):
                 ("num_grad_quant_bins", i32), ("stochastic_rounding", i32), ("quant_train_renew_leaf", i32),
                 ("seed", i32), ("quant_num_threads", i32), ("is_constant_hessian", i32),
                 ("num_tree_slots", i32), ("device", i32), ("hist_rows_per_block", i32),
-                ("hist_block_threads", i32), ("use_cuda_graph", i32)]
+                ("hist_block_threads", i32), ("use_cuda_graph", i32), ("persistent_grow", i32)]
 
 
 class FeatureMeta(C.Structure):

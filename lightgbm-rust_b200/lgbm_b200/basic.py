@@ -25,7 +25,7 @@ DEFAULTS = {
     "lambdarank_truncation_level": 30, "lambdarank_norm": True, "num_threads": 0, "monotone_constraints": None,
     "categorical_feature": None,
     # B200 path knobs
-    "hist_precision": "f64", "device": 0, "use_cuda_graph": True, "hist_rows_per_block": 0,
+    "hist_precision": "f64", "device": 0, "use_cuda_graph": True, "hist_rows_per_block": 0, "persistent_grow": False,
 }
 
 ALIASES = {
@@ -201,7 +201,7 @@ def learner_config(p, num_tree_slots=1):
         HIST[p["hist_precision"]], int(p["num_grad_quant_bins"]), int(bool(p["stochastic_rounding"])),
         int(bool(p["quant_train_renew_leaf"])), int(p["seed"]), int(p["num_threads"]) if p["num_threads"] else 1,
         int(obj == L.OBJ_REGRESSION), int(num_tree_slots), int(p["device"]), int(p["hist_rows_per_block"]), 0,
-        int(bool(p["use_cuda_graph"])))
+        int(bool(p["use_cuda_graph"])), int(bool(p["persistent_grow"])))
 
 
 class Learner:

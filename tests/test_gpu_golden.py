@@ -9,6 +9,17 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True, params=[False, True], ids=["per_step", "persistent"])
+def grow_mode(request, lgb):
+    """Every test runs with the per-step launches and with persistent growth."""
+    from lgbm_b200 import basic
+
+    old = basic.DEFAULTS["persistent_grow"]
+    basic.DEFAULTS["persistent_grow"] = request.param
+    yield request.param
+    basic.DEFAULTS["persistent_grow"] = old
+
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["binary_nan", "binary_quantized", "multiclass_categorical", "l2_bagging"]
 EXACT = ("split_feature", "threshold_in_bin", "decision_type", "left_child", "right_child", "leaf_count",

@@ -15,6 +15,17 @@ from conftest import binned_dataset
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True, params=[False, True], ids=["per_step", "persistent"])
+def grow_mode(request, lgb):
+    """Every test runs with the per-step launches and with persistent growth."""
+    from lgbm_b200 import basic
+
+    old = basic.DEFAULTS["persistent_grow"]
+    basic.DEFAULTS["persistent_grow"] = request.param
+    yield request.param
+    basic.DEFAULTS["persistent_grow"] = old
+
+
 def _binary_data(n, f=28, seed=0, nan_frac=0.0):
     rng = np.random.default_rng(seed)
     X = rng.standard_normal((n, f)).astype(np.float32)
