@@ -148,6 +148,14 @@ struct DCtx {
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
 };
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while its predecessor in the stream still runs.
+// pdl_wait blocks until the predecessor has finished and its writes are
+// visible (a no-op for an ordinary launch); pdl_trigger lets the next kernel
+// of the stream start launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- split arithmetic (learner/split.rs:124-231) -------------------------------------
 __device__ __forceinline__ double dsign(double x) { return (double)((x > 0.0) - (x < 0.0)); }
 __device__ __forceinline__ double threshold_l1(double s, double l1) {

@@ -1,6 +1,8 @@
 // Kernel declarations and launch-shape constants shared by the kernel
 // translation units and the host driver.
 #pragma once
+#include <utility>
+
 #include "device_common.cuh"
 
 namespace lgbm_b200 {
@@ -46,8 +48,27 @@ __global__ void k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t su
 // dynamic shared memory, kernel and launch of the histogram for a form and groups per tile
 size_t hist_smem_bytes(int mode, int ng);
 const void* hist_kernel(int mode, int ng);
-void launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
-                 int32_t sub_rows);
+cudaError_t launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                        int32_t sub_rows, bool pdl);
+
+// A kernel launch, optionally with programmatic stream serialisation (the
+// kernel may start launching while its predecessor in the stream runs; it
+// calls pdl_wait before reading anything the predecessor writes).
+template <typename... Params, typename... Args>
+inline cudaError_t launch_ex(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 template <bool kInt>
 __global__ void k_scan(const __grid_constant__ DCtx c);
 

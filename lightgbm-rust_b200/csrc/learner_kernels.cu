@@ -463,6 +463,8 @@ template <int kMode, int kNG>
 __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kHistThreads, 2)
     k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_wait();
+  pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
   LeafRows lr;
   int64_t r0, r1;
@@ -497,14 +499,14 @@ const void* hist_kernel(int mode, int ng) {
   }
 }
 
-void launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
-                 int32_t sub_rows) {
-  if (mode == 0) k_hist<0, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
-  else if (mode == 1) k_hist<1, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
-  else if (ng == 1) k_hist<2, 1><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
-  else if (ng == 2) k_hist<2, 2><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
-  else if (ng == 3) k_hist<2, 3><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
-  else k_hist<2, 4><<<grid, kHistThreads, smem, st>>>(c, tt, sub_rows);
+cudaError_t launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
+                        int32_t sub_rows, bool pdl) {
+  if (mode == 0) return launch_ex(k_hist<0, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+  if (mode == 1) return launch_ex(k_hist<1, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+  if (ng == 1) return launch_ex(k_hist<2, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+  if (ng == 2) return launch_ex(k_hist<2, 2>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+  if (ng == 3) return launch_ex(k_hist<2, 3>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+  return launch_ex(k_hist<2, 4>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
 }
 
 // =====================================================================================
@@ -1264,6 +1266,8 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
 template <bool kInt>
 __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ DCtx c) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_wait();
+  pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
@@ -1703,6 +1707,8 @@ __device__ __forceinline__ void zero_hist_buffer(const DCtx& c, const DSlot& s, 
 // step's split decision and the goes-left LUT, then claims row tiles; the
 // last CTA to exit ends the step.
 __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
+  pdl_wait();
+  pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   if (st->done) return;
