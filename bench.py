@@ -116,11 +116,13 @@ def _barrier():
 
 
 def _max_over_ranks(v):
+    """The largest of every rank's value (the job's time is its slowest rank's)."""
     import torch
     import torch.distributed as dist
 
     if dist.is_available() and dist.is_initialized():
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
     return v

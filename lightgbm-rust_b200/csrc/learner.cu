@@ -117,7 +117,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     if (clusters < 1) return Status(LGBM_B200_ERR_CUDA, "histogram cluster does not fit on the device");
     h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
   }
-  h->part_grid = h->num_sms * 4;
+  h->part_grid = h->num_sms * 2;  // 2 CTAs per SM measured best (4 and 8 per SM are slower)
+  // LGBM_B200_PART_GRID sets the partition's CTA count (launch-shape sweeps)
+  if (const char* e = std::getenv("LGBM_B200_PART_GRID")) h->part_grid = std::max(1, std::atoi(e));
   // LGBM_B200_PDL=1 chains the split steps by programmatic dependent launch
   // (off by default: on the 10M-row binary workload it measured 8% slower)
   if (const char* e = std::getenv("LGBM_B200_PDL")) h->use_pdl = std::atoi(e) != 0;

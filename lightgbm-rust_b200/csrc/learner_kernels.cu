@@ -1297,17 +1297,34 @@ __device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsign
   return flag | ((unsigned long long)(epoch & kEpochMask) << 31) | (v & kValueMask);
 }
 
-__device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left) {
+// What partition_finalize reads, loaded before apply_split runs so that the
+// two sets of loads overlap.
+struct FinalizeIn {
+  int32_t begin, cnt, side, buf_L, depth, status;
+  DLeafSplits ls0, rs0;
+};
+
+__device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L, int32_t R) {
+  FinalizeIn f;
+  f.begin = s.leaf_begin[L];
+  f.cnt = s.leaf_count[L];
+  f.side = s.leaf_side[L];
+  f.buf_L = s.buf_of[L];
+  f.depth = s.tree.leaf_depth[L] + 1;  // both children's depth after the split
+  f.status = s.st->status;
+  const DSplit& info = s.best[L];
+  f.ls0 = DLeafSplits{L, 0, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
+  f.rs0 = DLeafSplits{R, 0, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
+  return f;
+}
+
+__device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left,
+                                   const FinalizeIn& fin) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
-  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
-  const int32_t side = s.leaf_side[L];
-  const int32_t buf_L = s.buf_of[L];
-  const int32_t depth = s.tree.leaf_depth[L];  // both children's depth, set by apply_split
-  const DSplit& info = s.best[L];
-  const DLeafSplits ls0{L, 0, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
-  const DLeafSplits rs0{R, 0, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
-  const int32_t status = st->status;
+  const int32_t begin = fin.begin, cnt = fin.cnt, side = fin.side, buf_L = fin.buf_L, depth = fin.depth;
+  const DLeafSplits ls0 = fin.ls0, rs0 = fin.rs0;
+  const int32_t status = fin.status;
   const int32_t nl = total_left, nr = cnt - total_left;
   s.leaf_count[L] = nl;
   s.leaf_begin[R] = begin + nl;
@@ -1525,8 +1542,9 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   }
   __syncthreads();
   if (tid == 0) {
+    const FinalizeIn fin = finalize_inputs(s, bl, R);
     apply_split(c, s, bl, R);
-    partition_finalize(c, s, bl, R, total_left);
+    partition_finalize(c, s, bl, R, total_left, fin);
     st->part_epoch += 1;
   }
 }
