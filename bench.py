@@ -269,10 +269,91 @@ def run_cpu_baseline(lgb, form, sample_scale, iters):
                       f"{threads} threads), per-iteration time scaled by {scale:.0f}x rows and x{ROUNDS} rounds"}
 
 
+def _ndcg_at(y, s, group, k):
+    """Mean NDCG@k over queries (dcg.rs: gains 2^label - 1, discounts 1/log2(2 + rank),
+    stable descending order of the scores); queries without relevant rows count 1."""
+    q = np.repeat(np.arange(len(group)), group)
+    order = np.lexsort((np.arange(len(s)), -s, q))
+    start = np.r_[0, np.cumsum(group)[:-1]]
+    rank = np.arange(len(s)) - np.repeat(start, group)
+    gain = (2.0 ** y.astype(np.float64)) - 1.0
+    disc = 1.0 / np.log2(2.0 + rank)
+    top = rank < k
+    dcg = np.bincount(q, weights=np.where(top, gain[order] * disc, 0.0), minlength=len(group))
+    ideal_order = np.lexsort((-y, q))
+    idcg = np.bincount(q, weights=np.where(top, gain[ideal_order] * disc, 0.0), minlength=len(group))
+    return float(np.mean(np.where(idcg > 0, dcg / np.where(idcg > 0, idcg, 1.0), 1.0)))
+
+
+def run_workload(args):
+    """The other benchmark configurations: device time per boosting iteration
+    of each form on the seeded synthetic data, a quality figure after the
+    timed rounds, and (lambdarank) the batched prediction of the trained
+    model over every row. One JSON line, not the headline metric."""
+    import lgbm_b200 as lgb
+    from lgbm_b200 import synthetic
+
+    cfg = {"c1": 1, "c3": 3, "c4": 4}[args.workload]
+    d = synthetic.make(cfg, scale=args.scale)
+    forms = [f for f in args.forms.split(",") if f] if args.forms != "quantized,f32c,f64" else (
+        ["f64", "f32c"] if cfg == 1 else ["quantized", "f64"])
+    params = dict(d["params"])
+    params.pop("categorical_feature", None)
+    params.pop("eval_at", None)
+    for kv in args.param:
+        k, v = kv.split("=", 1)
+        try:
+            params[k] = json.loads(v)
+        except ValueError:
+            params[k] = v
+    t0 = time.perf_counter()
+    ds = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=params,
+                     categorical_feature=d.get("categorical")).construct(params)
+    build_s = time.perf_counter() - t0
+    out = {"workload": d["name"], "rows": int(len(d["y"])), "features": int(d["X"].shape[1]),
+           "rounds_in_config": d["num_rounds"], "dataset_build_s": build_s, "forms": {}}
+    for form in forms:
+        p = dict(params, hist_precision=form, num_threads=os.cpu_count() or 8)
+        if form == "quantized":
+            p["quant_train_renew_leaf"] = True
+        bst = lgb.Booster(p, ds)
+        L = bst.learner
+        for _ in range(args.warmup):
+            bst.update()
+        L.record(0)
+        for _ in range(args.steps):
+            bst.update()
+        L.record(1)
+        ms = L.elapsed(0, 1) / args.steps
+        sc = bst.scores()
+        rounds = args.warmup + args.steps
+        r = {"ms_per_iter": ms, "s_per_config_rounds": ms * d["num_rounds"] / 1000.0, "rounds_trained": rounds}
+        y = d["y"]
+        if cfg == 1:
+            r["train_rmse"] = float(np.sqrt(np.mean((sc[0] - y) ** 2)))
+        elif cfg == 3:
+            z = sc.T - sc.T.max(axis=1, keepdims=True)
+            lp = z - np.log(np.exp(z).sum(axis=1, keepdims=True))
+            r["train_multi_logloss"] = float(-np.mean(lp[np.arange(len(y)), y.astype(int)]))
+        else:
+            r["train_ndcg@10"] = _ndcg_at(y, sc[0], d["group"], 10)
+            # batched raw prediction of the trained model over every row
+            bst.predict(d["X"][:1000], raw_score=True)
+            t0 = time.perf_counter()
+            bst.predict(d["X"], raw_score=True)
+            pred_s = time.perf_counter() - t0
+            r["predict"] = {"rows": int(len(y)), "trees": bst.num_trees(), "s": pred_s,
+                            "rows_per_s": len(y) / pred_s, "tree_rows_per_s": len(y) * bst.num_trees() / pred_s,
+                            "note": "host f32 rows in, f64 scores out, copies included"}
+        out["forms"][form] = r
+        del bst
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--forms", default="quantized,f32c,f64")
@@ -281,7 +362,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rounds", type=int, default=ROUNDS, help="rounds trained per form (AUC after these)")
     ap.add_argument("--param", action="append", default=[], help="extra training parameter k=v (launch-shape sweeps)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4"],
+                    help="c2: the headline binary 10M workload; c1 / c3 / c4: the regression, multiclass and "
+                         "lambdarank configurations (a separate JSON line)")
     args = ap.parse_args()
+    if args.workload != "c2":
+        run_workload(args)
+        return
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
