@@ -156,15 +156,18 @@ def run_form(lgb, data, ds, dv, form, args, device):
     # histogram kernel timing over the same number of steps, events around every launch
     L.set_timing(True)
     hist_ms = scan_ms = part_ms = 0.0
-    rows = 0
+    rows = prows = 0
     launches = 0
+    fused = False
     for _ in range(args.steps):
         bst.update()
         t, r, nl = L.last_timing()
+        _, pr, fused = L.last_rows()
         hist_ms += t[0]
         scan_ms += t[1]
         part_ms += t[2]
         rows += r
+        prows += pr
         launches = nl
     L.set_timing(False)
     done = args.warmup + 2 * args.steps
@@ -173,13 +176,21 @@ def run_form(lgb, data, ds, dv, form, args, device):
             break
     auc = _auc(data["y_valid"], bst.scores(valid=True)[0])
     nf = ds.binned()["num_features"]
-    hist_launches = args.steps * (int(params["num_leaves"]) - 1)
+    steps_per_tree = int(params["num_leaves"]) - 1
+    hist_launches = args.steps * (1 if fused else steps_per_tree)
     hist_bytes = rows * hist_bytes_per_row(nf, form)
+    # fused form: the partition moves each row of the split leaf and adds it to
+    # its child's histogram: index in, bin row, packed gradient, index out
+    part_bytes = prows * (4 + nf + 4 + 4)
     return {
         "ms_per_step": ms, "wall_ms_per_step": 1000 * wall / args.steps, "s_per_500": ms * ROUNDS / 1000.0,
         "auc": auc, "hist_ms_per_launch": hist_ms / hist_launches, "hist_gbs": hist_bytes / (hist_ms / 1000) / 1e9,
         "hist_bytes_per_launch": hist_bytes / hist_launches, "hist_rows_per_tree": rows / args.steps,
         "scan_ms_per_step": scan_ms / args.steps, "partition_ms_per_step": part_ms / args.steps,
+        "fused": fused, "part_rows_per_tree": prows / args.steps,
+        "part_gbs": part_bytes / (part_ms / 1000) / 1e9 if part_ms > 0 else None,
+        "part_bytes_per_launch": part_bytes / (args.steps * steps_per_tree),
+        "part_ms_per_launch": part_ms / (args.steps * steps_per_tree),
         "hist_ms_per_step": hist_ms / args.steps, "kernel_launches_per_tree": launches, "clocks": clk,
         "num_trees": bst.num_trees(), "nf": nf,
     }
@@ -443,13 +454,19 @@ def main():
         "forms": {k: {"s_per_500_rounds": v["s_per_500"], "ms_per_step": v["ms_per_step"], "auc": v["auc"],
                       "hist_gbs": v["hist_gbs"], "hist_ms_per_step": v["hist_ms_per_step"],
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
-                      "hist_rows_per_tree": v["hist_rows_per_tree"]} for k, v in res.items()},
-        "roofline": {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] / (int(data["params"]["num_leaves"]) - 1)
-                                 if head == "quantized" else None),
-                     "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
-                     "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]},
+                      "hist_rows_per_tree": v["hist_rows_per_tree"], "fused": v["fused"], "part_gbs": v["part_gbs"],
+                      "part_rows_per_tree": v["part_rows_per_tree"]} for k, v in res.items()},
+        "roofline": ({"bound": "hbm", "kernel": "k_partition_fused (row partition + both children's histograms)",
+                      "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s", "frac": r["part_gbs"] / peak,
+                      "peak_kind": peak_kind, "traffic": None,
+                      "bytes_per_launch": r["part_bytes_per_launch"], "ms_per_launch": r["part_ms_per_launch"]}
+                     if r["fused"] else
+                     {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
+                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                      "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] /
+                                  (int(data["params"]["num_leaves"]) - 1) if head == "quantized" else None),
+                      "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
+                      "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]}),
         "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 5),
         "clocks": r["clocks"],

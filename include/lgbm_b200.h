@@ -208,6 +208,11 @@ int lgbm_b200_learner_elapsed(LgbmB200Learner* h, int32_t a, int32_t b, double* 
 /* Device time of the last train call summed per kernel family, ms:
  * [histogram, scan, partition, other]; rows histogrammed; kernels launched. */
 int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_rows, int32_t* launches);
+/* Rows of the last train call: histogrammed by the histogram kernel, and
+ * partitioned (in the fused quantized form, where *fused is 1, the partition
+ * also builds both children's histograms from the rows it moves). For the
+ * bench's bandwidth figures; no counterpart in the reference. */
+int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows, int32_t* fused);
 
 /* Diagnostics for the parity tests. lgbm_b200_learner_histogram runs the
  * learner's histogram kernel over `rows` (NULL: every row) of slot `slot`'s

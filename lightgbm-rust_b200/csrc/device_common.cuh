@@ -79,6 +79,7 @@ struct DSlotState {
   double grad_scale, hess_scale;  // quantized gradients
   DLeafSplits smaller, larger;
   int64_t hist_rows;       // rows histogrammed in this tree (statistics)
+  int64_t part_rows;       // rows partitioned in this tree (statistics)
 };
 
 // One node / leaf record of the tree grown on the device (tree.rs:120-160).
@@ -123,6 +124,7 @@ struct DSlot {
   const float2* gh;        // this slot's interleaved (gradient, hessian) [num_data]
   int32_t* packed;         // quantized gradients per row: (g << 16) + h
   uint8_t* bytree;         // by-tree feature mask [num_features]
+  long long* pair_hist;    // fused form: [2 pairs][2 children][total_bins] packed sums
   double* root_partials;   // [2 x kRootBlocks] (g, h) partial sums
   long long* root_ipartials;
   int32_t* root_counter;
@@ -146,6 +148,7 @@ struct DCtx {
   DSlot slots[kMaxSlots];  // by value: read from the constant bank
   int32_t num_slots;
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
+  int32_t fused;           // 1: the partition also builds both children's histograms (quantized, <= 32 features)
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

@@ -85,6 +85,8 @@ size_t grow_smem_bytes(int mode, int ng);
 cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
                         int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns);
 __global__ void k_partition(const __grid_constant__ DCtx c);
+__global__ void k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows);
+size_t fused_smem_bytes();
 __global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
 __global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* sums);
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums);

@@ -118,6 +118,25 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
   }
   h->part_grid = h->num_sms * 2;  // 2 CTAs per SM measured best (4 and 8 per SM are slower)
+  // LGBM_B200_FUSED=1: the quantized form with at most 32 features builds
+  // both children's histograms inside the partition. Off by default: on the
+  // 10M-row binary workload it measured slower (the first, largest splits
+  // move every row of the parent through one CTA per SM, where the separate
+  // histogram kernel reads only the smaller child's rows).
+  h->fused = false;
+  if (const char* e = std::getenv("LGBM_B200_FUSED"))
+    h->fused = std::atoi(e) != 0 && mode == LGBM_B200_HIST_QUANT && nf <= 32 && !cfg->persistent_grow;
+  if (h->fused) {
+    CU(cudaFuncSetAttribute(k_partition_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes()));
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(kHistCluster * 32, 1, 1);
+    lc.blockDim = dim3(512, 1, 1);
+    lc.dynamicSmemBytes = fused_smem_bytes();
+    int clusters = 0;
+    CU(cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_partition_fused, &lc));
+    if (clusters < 1) return Status(LGBM_B200_ERR_CUDA, "fused partition cluster does not fit on the device");
+    h->fused_grid = clusters * kHistCluster;
+  }
   // LGBM_B200_PART_GRID sets the partition's CTA count (launch-shape sweeps)
   if (const char* e = std::getenv("LGBM_B200_PART_GRID")) h->part_grid = std::max(1, std::atoi(e));
   // LGBM_B200_PDL=1 chains the split steps by programmatic dependent launch
@@ -188,6 +207,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     d.gh = nullptr;  // set below from the contiguous [K x n] buffer
     if (mode == LGBM_B200_HIST_QUANT) ALLOC(d.packed, n);
     ALLOC(d.bytree, nf);
+    if (h->fused) ALLOC(d.pair_hist, 4 * (size_t)h->total_bins);
     ALLOC(d.root_partials, 2 * kRootBlocks);
     ALLOC(d.root_ipartials, kRootBlocks);
     ALLOC(d.root_counter, 1);
@@ -290,6 +310,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   for (int k = 0; k < K; ++k) c.slots[k] = h->slots_h[k];
   c.num_slots = K;
   c.rows_per_block = rpb;
+  c.fused = h->fused ? 1 : 0;
   h->n_used = (int32_t)n;
   h->st_h.resize(K);
   h->trees.resize(K);
@@ -328,12 +349,16 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     // the three launches of a step chain by programmatic dependent launch
     // (not when events are recorded between them)
     const bool pdl = h->use_pdl && !h->timing;
-    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
+    // fused form: only the root needs a histogram launch
+    if (!h->fused || step == 0)
+      CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
     if (mode == LGBM_B200_HIST_QUANT) CU(launch_ex(k_scan<true>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl, c));
     else CU(launch_ex(k_scan<false>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
-    CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl, c));
+    if (h->fused)
+      CU(launch_ex(k_partition_fused, dim3(h->fused_grid, 1, K), dim3(512), fused_smem_bytes(), s, pdl, c, h->sub_rows));
+    else CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
@@ -343,7 +368,7 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
     CU_LAUNCH();
   }
-  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : 3 * (L - 1)) +
+  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : (h->fused ? 2 * (L - 1) + 1 : 3 * (L - 1))) +
                      ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
   return Status();
 }
@@ -516,9 +541,11 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
     }
   }
   h->last_hist_rows = 0;
+  h->last_part_rows = 0;
   for (int k = 0; k < K; ++k) {
     const DSlotState& ss = h->st_h[k];
     h->last_hist_rows += ss.hist_rows;
+    h->last_part_rows += ss.part_rows;
     if (ss.status == kStatusTimeout) return Status(LGBM_B200_ERR_TIMEOUT, "device-side wait timed out (partition)");
     if (ss.status == kStatusEmptyChild)
       return Status(LGBM_B200_ERR_INVALID_PARAMETER, "Check failed: (best_split_info.left_count) > (0)");
@@ -556,6 +583,7 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   // one slot only: a context whose slot array starts at `slot`
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
+  c.fused = 0;  // into the pool buffer 0
   dim3 grid(h->hist_grid, h->ntiles, 1);
   CU(launch_hist(mode, h->hist_ng, grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false));
   CU_LAUNCH();
@@ -743,6 +771,14 @@ int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_
     for (int i = 0; i < 4; ++i) ms[i] = h->last_ms[i];
   if (hist_rows) *hist_rows = h->last_hist_rows;
   if (launches) *launches = h->last_launches;
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows, int32_t* fused) {
+  if (!h) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null handle"));
+  if (hist_rows) *hist_rows = h->last_hist_rows;
+  if (partition_rows) *partition_rows = h->last_part_rows;
+  if (fused) *fused = h->fused ? 1 : 0;
   return LGBM_B200_OK;
 }
 

@@ -231,6 +231,9 @@ struct LgbmB200Learner {
   cudaEvent_t marks[16] = {};  // caller-placed timing marks on the learner's stream
   double last_ms[4] = {0, 0, 0, 0};
   int64_t last_hist_rows = 0;
+  int64_t last_part_rows = 0;
+  bool fused = false;  // partition builds both children's histograms
+  int fused_grid = 0;
   int32_t last_launches = 0;
   // captured tree growth
   cudaGraphExec_t graph_exec = nullptr;

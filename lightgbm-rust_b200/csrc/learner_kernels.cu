@@ -68,9 +68,10 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   // positions -> rows (identity, or the in-bag rows)
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + tid; i < n; i += (int64_t)gridDim.x * blockDim.x)
     s.idx[0][i] = bag ? bag[i] : (uint32_t)i;
-  // zero histogram buffer 0 (the root's)
+  // zero the root's histogram buffer (pool buffer 0; fused form: pair 1, child 0)
   size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
-  double* h0 = reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
+  double* h0 = c.fused ? reinterpret_cast<double*>(s.pair_hist + 2 * (size_t)c.total_bins)
+                       : reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
   for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h0[i] = 0.0;
 
   // deterministic partial sums over this block's contiguous chunk
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->part_ticket = 0;
   st->part_done = 0;
   st->hist_rows = 0;
+  st->part_rows = 0;
   st->smaller.leaf = 0;
   st->smaller.num_data = (int32_t)n;
   st->smaller.sum_gradients = a;
@@ -279,8 +281,10 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   const uint32_t* idx = lr.idx + lr.begin;
   const size_t stride = (size_t)c.stride;
   double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
-  unsigned long long* outi = reinterpret_cast<unsigned long long*>(s.hist) +
-                             (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
+  // fused form: only the root is histogrammed here, into pair 1, child 0
+  unsigned long long* outi = c.fused ? reinterpret_cast<unsigned long long*>(s.pair_hist + 2 * (size_t)c.total_bins)
+                                     : reinterpret_cast<unsigned long long*>(s.hist) +
+                                           (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
   // Adds cell i (over groups) of the CTAs `src` to the leaf histogram; cells
   // outside the features' views are skipped.
   auto emit = [&](int i, auto read_cell) {
@@ -1155,6 +1159,52 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
   const int32_t L = st->left_leaf;
   const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
   if (!(used && (side == 0 || have_larger))) return;
+  if (kInt && c.fused) {
+    // both leaves' histograms were built directly by the previous partition
+    // (the root's by the histogram kernel): each view is fixed from its own
+    // leaf's sum (histogram.rs:42-56); no subtraction
+    const DLeafSplits ls = side == 0 ? st->smaller : st->larger;
+    const int len = m.view_len;
+    const int k = st->num_leaves_cur - 1;
+    const int child = ls.leaf == st->left_leaf ? 0 : 1;
+    const long long* hs = s.pair_hist + ((size_t)(((k - 1) & 1) * 2 + child)) * c.total_bins + m.view_start;
+    if (tid < len) sm.ig[tid] = (int64_t)__ldcg(hs + tid);
+    __syncthreads();
+    if (m.most_freq_bin > 0 && warp == 0) {
+      int64_t part = 0;
+      for (int i = lane; i < m.num_bin; i += 32)
+        if (i != m.most_freq_bin) part = (int64_t)((uint64_t)part + (uint64_t)sm.ig[i]);
+      for (int o = 16; o > 0; o >>= 1)
+        part = (int64_t)((uint64_t)part + (uint64_t)__shfl_xor_sync(0xffffffffu, part, o));
+      __syncwarp();
+      if (lane == 0) sm.ig[m.most_freq_bin] = (int64_t)((uint64_t)ls.int_sum - (uint64_t)part);
+    }
+    __syncthreads();
+    LeafCtx lc;
+    lc.sum_g = ls.sum_gradients;
+    lc.sum_h = ls.sum_hessians;
+    lc.int_sum = ls.int_sum;
+    lc.gs = st->grad_scale;
+    lc.hs = st->hess_scale;
+    lc.num_data = ls.num_data;
+    lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
+                                                : ls.weight;
+    lc.mc = p.use_monotone != 0;
+    lc.cmin = s.cmin[ls.leaf];
+    lc.cmax = s.cmax[ls.leaf];
+    DSplit& out = sm.out;
+    bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
+    if (tid == 0) {
+      out.feature = m.real_index;
+      out.inner = f;
+      s.feat_ok[side * nf + f] = ok ? 1 : 0;
+    }
+    __syncthreads();
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
+    for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
+    return;
+  }
   {
     const DLeafSplits sl = st->smaller;
     const int len = m.view_len;
@@ -1275,6 +1325,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
     st->part_ticket = 0;
     st->part_done = 0;
+  }
+  if (kInt && c.fused) {  // the pair this step's partition fills (read by the scan before last)
+    const int k = st->num_leaves_cur - 1;
+    long long* z = s.pair_hist + (size_t)(k & 1) * 2 * c.total_bins;
+    const size_t n = 2 * (size_t)c.total_bins;
+    const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x, ctas = (size_t)gridDim.x * gridDim.y;
+    for (size_t i = cta * blockDim.x + threadIdx.x; i < n; i += ctas * blockDim.x) z[i] = 0;
   }
   scan_item<kInt>(c, s, blockIdx.x, blockIdx.y, *reinterpret_cast<ScanSmem*>(smem_raw));
 }
@@ -1585,46 +1642,16 @@ __device__ __forceinline__ int32_t split_inner_of(const DCtx& c, const DSlot& s,
   return s.best[L].inner;
 }
 
-// Row tiles of the split leaf L claimed in order by the CTAs (kItems rows
-// per thread, blockDim.x * kItems == kPartTileRows), each chained to its
-// predecessors by a decoupled look-back on the left count. The CTA that
-// partitions the last tile posts the left count in st->part_left.
+// One partition tile after its goes-left flags are known: a block scan of
+// the per-thread left counts, the decoupled look-back for the tile's prefix,
+// then the scatter (left rows ascending from the range start, right rows
+// descending from its end). The CTA of the last tile posts the left count.
 template <int kItems>
-__device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, int32_t L, uint32_t epoch) {
+__device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32_t ntiles, uint32_t epoch, int32_t t0,
+                             int32_t cnt, const uint32_t (&rows)[kItems], uint32_t flags, int32_t nleft,
+                             uint32_t* out) {
   DSlotState* st = s.st;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
-  const int32_t side = s.leaf_side[L];
-  const int32_t inner = split_inner_of(c, s, ps, L);
-  if (cnt == 0) return;
-  const uint32_t* in = s.idx[side] + begin;
-  uint32_t* out = s.idx[1 - side] + begin;
-  const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
-  const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
-  const uint8_t* lut = ps.lut;
-  while (true) {
-    __syncthreads();
-    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
-    __syncthreads();
-    const int32_t tile = ps.tile;
-    if (tile >= ntiles) break;
-    const int32_t t0 = tile * kPartTileRows;
-    uint32_t rows[kItems];
-    uint32_t flags = 0;
-    int32_t nleft = 0;
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-      int32_t pos = t0 + tid * kItems + k;
-      if (pos < cnt) {
-        uint32_t r = __ldcg(in + pos);
-        rows[k] = r;
-        uint32_t raw = col[r];
-        if (lut[raw]) {
-          flags |= 1u << k;
-          ++nleft;
-        }
-      }
-    }
     // block exclusive scan of per-thread left counts
     int32_t incl = nleft;
     for (int o = 1; o < 32; o <<= 1) {
@@ -1670,11 +1697,8 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, in
           const int first_inc = inc_mask ? __ffs(inc_mask) - 1 : 32;
           const unsigned need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
           if (bad_mask & need) {
-            if (++spins > kSpinLimit) {  // give up: the prefix 0 keeps every write in the leaf's range
-              if (lane == 0) {
-                st->status = kStatusTimeout;
-                st->done = 1;
-              }
+            if (++spins > kSpinLimit) {  // give up: the prefix 0 keeps every write in the leaf's range;
+              if (lane == 0) st->status = kStatusTimeout;  // the step's end then finishes the tree
               acc = 0;
               break;
             }
@@ -1710,6 +1734,49 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, in
       }
     }
     if (tile == ntiles - 1 && tid == 0) st->part_left = prefix + tile_left;
+}
+
+// Row tiles of the split leaf L claimed in order by the CTAs (kItems rows
+// per thread, blockDim.x * kItems == kPartTileRows), each chained to its
+// predecessors by a decoupled look-back on the left count. The CTA that
+// partitions the last tile posts the left count in st->part_left.
+template <int kItems>
+__device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, int32_t L, uint32_t epoch) {
+  DSlotState* st = s.st;
+  const int tid = threadIdx.x;
+  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
+  const int32_t side = s.leaf_side[L];
+  const int32_t inner = split_inner_of(c, s, ps, L);
+  if (cnt == 0) return;
+  const uint32_t* in = s.idx[side] + begin;
+  uint32_t* out = s.idx[1 - side] + begin;
+  const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
+  const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
+  const uint8_t* lut = ps.lut;
+  while (true) {
+    __syncthreads();
+    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+    __syncthreads();
+    const int32_t tile = ps.tile;
+    if (tile >= ntiles) break;
+    const int32_t t0 = tile * kPartTileRows;
+    uint32_t rows[kItems];
+    uint32_t flags = 0;
+    int32_t nleft = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int32_t pos = t0 + tid * kItems + k;
+      if (pos < cnt) {
+        uint32_t r = __ldcg(in + pos);
+        rows[k] = r;
+        uint32_t raw = col[r];
+        if (lut[raw]) {
+          flags |= 1u << k;
+          ++nleft;
+        }
+      }
+    }
+    tile_scatter<kItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out);
   }
 }
 
@@ -1740,6 +1807,7 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
     return;
   }
   zero_hist_buffer(c, s, R, blockIdx.x, gridDim.x);
+  if (blockIdx.x == 0 && tid == 0) st->part_rows += s.leaf_count[L];
   partition_rows<kPartTileRows / kPartThreads>(c, s, ps, L, epoch);
   __syncthreads();
   if (tid == 0) {
@@ -1750,6 +1818,190 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   if (ps.last) {
     __threadfence();
     const int32_t cnt = s.leaf_count[L];
+    finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+  }
+}
+
+// =====================================================================================
+// Fused partition and histograms (quantized form, at most 32 features): the
+// partition of the split leaf also accumulates the histograms of both
+// children, so no histogram launch follows and no larger = parent - smaller
+// subtraction is needed (integer sums: the direct sums equal the difference
+// exactly). Each row's 32-byte bin segment is read whole: it holds the split
+// feature's value (no column-major gather) and every feature's bin.
+// The children's packed sums go to pair (step & 1) of the slot's pair
+// buffers, child 0 the left child (the split leaf's index) and child 1 the
+// right one; the scan of the next step reads them and zeroes the other pair.
+// =====================================================================================
+constexpr int kFusedThreads = 512;
+constexpr int kFusedItems = kPartTileRows / kFusedThreads;
+constexpr int kFusedCells = kMaxBins * 32;  // one group of 32 features, per child
+
+size_t fused_smem_bytes() {
+  return (size_t)2 * kFusedCells * 4 + (size_t)kPartTileRows * 32 + (size_t)kPartTileRows * 4 + kPartTileRows;
+}
+
+__global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThreads, 1)
+    k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int32_t* cells = reinterpret_cast<int32_t*>(smem_raw);  // [child][raw][lane]
+  uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)2 * kFusedCells * 4);
+  int32_t* sq = reinterpret_cast<int32_t*>(sbins + 2 * kPartTileRows);
+  uint8_t* sf = reinterpret_cast<uint8_t*>(sq + kPartTileRows);
+  __shared__ PartShared ps;
+  __shared__ int32_t s_vlen[32], s_vstart[32];
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  // done changes during this launch only where every CTA returns here too
+  if (st->done) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t R = st->num_leaves_cur;
+  const int step = R - 1;
+  const uint32_t epoch = st->part_epoch;
+  const int32_t L = partition_prologue(c, s, ps);
+  if (L < 0) {
+    if (blockIdx.x == 0 && tid == 0) st->done = 1;
+    return;
+  }
+  const int32_t nf = c.num_features;
+  if (tid < 32) {
+    const bool ok = tid < nf;
+    s_vlen[tid] = ok ? c.feats[tid].view_len : 0;
+    s_vstart[tid] = ok ? c.feats[tid].view_start : 0;
+  }
+  {
+    uint4* z = reinterpret_cast<uint4*>(cells);
+    for (int i = tid; i < 2 * kFusedCells * 4 / 16; i += kFusedThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  __syncthreads();  // cells zeroed, feature facts and the LUT complete
+  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
+  const int32_t side = s.leaf_side[L];
+  const int32_t inner = split_inner_of(c, s, ps, L);
+  if (blockIdx.x == 0 && tid == 0) st->part_rows += cnt;
+  const uint32_t* in = s.idx[side] + begin;
+  uint32_t* out = s.idx[1 - side] + begin;
+  const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
+  const size_t stride = (size_t)c.stride;
+  const uint8_t* lut = ps.lut;
+  long long* pair = s.pair_hist + (size_t)(step & 1) * 2 * c.total_bins;
+  auto decode = [](int32_t cell, int64_t& g, int64_t& h) {
+    h = (int64_t)(cell & 0xFFFF);
+    g = (int64_t)((cell - (int32_t)h) >> 16);
+  };
+  // adds cell i ([child][raw][lane]) with sums (g, h) to the child's histogram
+  auto emit = [&](int i, int64_t g, int64_t h) {
+    const int child = i / kFusedCells, k = i - child * kFusedCells;
+    const int raw = k >> 5, fl = k & 31;
+    if (raw == 0 || raw > s_vlen[fl] || (g == 0 && h == 0)) return;
+    atomicAdd(reinterpret_cast<unsigned long long*>(pair + (size_t)child * c.total_bins + s_vstart[fl] + raw - 1),
+              (unsigned long long)((uint64_t)(g << 32) + (uint64_t)h));
+  };
+  int32_t since_flush = 0;
+  while (cnt > 0) {
+    __syncthreads();
+    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+    __syncthreads();
+    const int32_t tile = ps.tile;
+    if (tile >= ntiles) break;
+    const int32_t t0 = tile * kPartTileRows;
+    uint32_t rows[kFusedItems];
+    int32_t q[kFusedItems];
+    uint4 b0[kFusedItems], b1[kFusedItems];
+    uint32_t flags = 0;
+    int32_t nleft = 0;
+#pragma unroll
+    for (int k = 0; k < kFusedItems; ++k) {
+      const int32_t pos = t0 + tid * kFusedItems + k;
+      rows[k] = pos < cnt ? __ldcg(in + pos) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kFusedItems; ++k) {
+      const bool live = t0 + tid * kFusedItems + k < cnt;
+      const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)rows[k] * stride);
+      q[k] = live ? __ldg(s.packed + rows[k]) : 0;
+      b0[k] = live ? __ldg(src) : make_uint4(0u, 0u, 0u, 0u);
+      b1[k] = live ? __ldg(src + 1) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < kFusedItems; ++k) {
+      if (t0 + tid * kFusedItems + k >= cnt) continue;
+      const uint4 v = inner < 16 ? b0[k] : b1[k];
+      const int wsel = (inner >> 2) & 3;
+      const uint32_t w = wsel == 0 ? v.x : (wsel == 1 ? v.y : (wsel == 2 ? v.z : v.w));
+      if (lut[(w >> ((inner & 3) * 8)) & 0xFFu]) {
+        flags |= 1u << k;
+        ++nleft;
+      }
+    }
+    tile_scatter<kFusedItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out);
+    // the tile's rows into the children's cells (rows past the leaf stage as
+    // zeros: value 0 lands in cells no feature view contains)
+#pragma unroll
+    for (int k = 0; k < kFusedItems; ++k) {
+      const int r = tid * kFusedItems + k;
+      sbins[2 * r] = b0[k];
+      sbins[2 * r + 1] = b1[k];
+      sq[r] = q[k];
+      sf[r] = (uint8_t)((flags >> k) & 1u);
+    }
+    __syncthreads();
+    {
+      constexpr int kRowsPerWarp = kPartTileRows / (kFusedThreads / 32);
+      const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + lane;
+      for (int j0 = warp * kRowsPerWarp; j0 < (warp + 1) * kRowsPerWarp; j0 += 32) {
+        const int32_t myq = sq[j0 + lane];
+        const int32_t myc = sf[j0 + lane] ? 0 : kFusedCells;  // left child: cells 0, right: cells 1
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int32_t qq = __shfl_sync(0xffffffffu, myq, j);
+          const int32_t cb = __shfl_sync(0xffffffffu, myc, j);
+          const int raw = rowp[(j0 + j) * 32];
+          atomicAdd(cells + cb + raw * 32 + lane, qq);
+        }
+      }
+    }
+    since_flush += kPartTileRows;
+    __syncthreads();
+    // int32 cells hold at most sub_rows rows before their 16-bit halves could wrap
+    if (since_flush + kPartTileRows > sub_rows) {
+      for (int i = tid; i < 2 * kFusedCells; i += kFusedThreads) {
+        int64_t g, h;
+        decode(cells[i], g, h);
+        emit(i, g, h);
+        cells[i] = 0;
+      }
+      since_flush = 0;
+      __syncthreads();
+    }
+  }
+  // cluster reduction: CTA rank r adds slice r of both children's cells,
+  // summed over the cluster's CTAs in rank order
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster.sync();
+  {
+    const int per = 2 * kFusedCells / kHistCluster;
+    const int lo = (int)cluster.block_rank() * per;
+    for (int i = lo + tid; i < lo + per; i += kFusedThreads) {
+      int64_t g = 0, h = 0;
+#pragma unroll
+      for (int r = 0; r < kHistCluster; ++r) {
+        int64_t a, b;
+        decode(cluster.map_shared_rank(cells, r)[i], a, b);
+        g += a;
+        h += b;
+      }
+      emit(i, g, h);
+    }
+  }
+  cluster.sync();  // no CTA leaves while another may still read its cells
+  if (tid == 0) {
+    __threadfence();
+    ps.last = atomicAdd(&st->part_done, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (ps.last) {
+    __threadfence();
     finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
   }
 }

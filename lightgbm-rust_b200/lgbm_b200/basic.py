@@ -304,6 +304,12 @@ class Learner:
         L.check(L.lib().lgbm_b200_learner_last_timing(self.handle, ms, C.byref(rows), C.byref(launches)))
         return list(ms), int(rows.value), int(launches.value)
 
+    def last_rows(self):
+        """(rows histogrammed, rows partitioned, fused) of the last train call."""
+        h, pr, f = C.c_int64(), C.c_int64(), C.c_int32()
+        L.check(L.lib().lgbm_b200_learner_last_rows(self.handle, C.byref(h), C.byref(pr), C.byref(f)))
+        return int(h.value), int(pr.value), bool(f.value)
+
     def __del__(self):
         if getattr(self, "handle", None) is not None and L._lib is not None:
             L._lib.lgbm_b200_learner_destroy(self.handle)

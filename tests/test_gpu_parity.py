@@ -15,15 +15,16 @@ from conftest import binned_dataset
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(autouse=True, params=[False, True], ids=["per_step", "persistent"])
-def grow_mode(request, lgb):
-    """Every test runs with the per-step launches and with persistent growth."""
+@pytest.fixture(autouse=True, params=["per_step", "persistent", "fused"])
+def grow_mode(request, lgb, monkeypatch):
+    """Every test runs with each launch strategy: the per-step graph (the
+    default), persistent growth, and the fused partition + histograms (used
+    by the quantized form with at most 32 features)."""
     from lgbm_b200 import basic
 
-    old = basic.DEFAULTS["persistent_grow"]
-    basic.DEFAULTS["persistent_grow"] = request.param
+    monkeypatch.setitem(basic.DEFAULTS, "persistent_grow", request.param == "persistent")
+    monkeypatch.setenv("LGBM_B200_FUSED", "1" if request.param == "fused" else "0")
     yield request.param
-    basic.DEFAULTS["persistent_grow"] = old
 
 
 def _binary_data(n, f=28, seed=0, nan_frac=0.0):
