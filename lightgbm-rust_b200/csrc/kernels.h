@@ -37,6 +37,7 @@ struct ScanSmem {
   double eg, eh;                          // the extra candidate t = -1
   int32_t ec, brk, ok;
   int64_t eq;
+  int64_t wq[32], wa[32];                 // per-warp totals of the quantized cumulative scan
   double wgain[32];                       // per-warp best candidates (up to 32 warps)
   int32_t wt[32];
   DSplit out;                             // the result, stored to global memory once

@@ -782,8 +782,8 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
   const bool first_extra = !reverse && na_as_missing && offset == 1;
   const int32_t nstored = m.num_bin - offset;
   const int khi = len > 0 ? (len - 1) / kPer : -1;
-  if (warp == 0) {
-    if (!kInt) {
+  if (!kInt) {
+    if (warp == 0) {
       double a = 0.0, b = kEpsilon;
       int32_t c = 0;
       if (first_extra) {  // split.rs:787-800: the leaf sums minus every stored bin, ascending
@@ -815,49 +815,40 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
           sm.cc[t] = z;
         }
       });
-    } else {
-      // exact packed sums: lane-local part in scan order plus a warp scan of lane totals
-      int64_t loc = 0;
-      for (int jj = 0; jj < kPer; ++jj) {
-        int j = reverse ? kPer - 1 - jj : jj;
-        int t = lane * kPer + j;
-        if (visited(t)) {
-          loc = (int64_t)((uint64_t)loc + (uint64_t)sm.ig[t]);
-          sm.cq[t] = loc;
-        }
-      }
-      int64_t incl = loc;
-      for (int o = 1; o < 32; o <<= 1) {
-        int64_t other = reverse ? __shfl_down_sync(0xffffffffu, incl, o) : __shfl_up_sync(0xffffffffu, incl, o);
-        bool ok = reverse ? lane + o < 32 : lane >= o;
-        if (ok) incl = (int64_t)((uint64_t)incl + (uint64_t)other);
-      }
-      int64_t base = 0;
-      if (first_extra) {
-        int64_t all = 0;
-        for (int j = 0; j < kPer; ++j) {
-          int t = lane * kPer + j;
-          if (t < nstored && t < len) all = (int64_t)((uint64_t)all + (uint64_t)sm.ig[t]);
-        }
-        for (int o = 16; o > 0; o >>= 1)
-          all = (int64_t)((uint64_t)all + (uint64_t)__shfl_xor_sync(0xffffffffu, all, o));
-        base = (int64_t)((uint64_t)lc.int_sum - (uint64_t)all);
-        if (lane == 0) {
-          sm.eq = base;
-          sm.ec = round_int((double)int_hess(base) * cnt_factor);
-        }
-      }
-      const int64_t add = (int64_t)((uint64_t)base + (uint64_t)incl - (uint64_t)loc);
-      for (int j = 0; j < kPer; ++j) {
-        int t = lane * kPer + j;
-        if (visited(t)) {
-          int64_t v = (int64_t)((uint64_t)add + (uint64_t)sm.cq[t]);
-          sm.cq[t] = v;
-          sm.cc[t] = round_int((double)int_hess(v) * cnt_factor);
-        }
-      }
+      if (lane == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
     }
-    if (lane == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
+  } else {
+    // exact packed sums (any order): thread u holds scan position u, a block
+    // scan over the threads in scan order gives every cumulative sum
+    const int t = reverse ? len - 1 - tid : tid;
+    const bool vis = tid < len && visited(t);
+    const uint64_t v = vis ? (uint64_t)sm.ig[t] : 0ull;
+    const uint64_t a = (first_extra && tid < len && t < nstored) ? (uint64_t)sm.ig[t] : 0ull;  // every stored bin
+    uint64_t incl = v, asum = a;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t other = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += other;
+      asum += __shfl_xor_sync(0xffffffffu, asum, o);
+    }
+    if (lane == 31) sm.wq[warp] = (int64_t)incl;
+    if (lane == 0) sm.wa[warp] = (int64_t)asum;
+    if (tid == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
+    __syncthreads();
+    uint64_t pre = 0, all = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      if (w < warp) pre += (uint64_t)sm.wq[w];
+      all += (uint64_t)sm.wa[w];
+    }
+    const uint64_t base = first_extra ? (uint64_t)lc.int_sum - all : 0ull;
+    if (first_extra && tid == 0) {  // split.rs:1097-1103: the leaf sum minus every stored bin
+      sm.eq = (int64_t)base;
+      sm.ec = round_int((double)int_hess((int64_t)base) * cnt_factor);
+    }
+    if (vis) {
+      const int64_t cq = (int64_t)(base + pre + incl);
+      sm.cq[t] = cq;
+      sm.cc[t] = round_int((double)int_hess(cq) * cnt_factor);
+    }
   }
   __syncthreads();
   const int32_t min_data = p.min_data_in_leaf;
@@ -1451,14 +1442,18 @@ __device__ void new_leaf_best(const DCtx& c, const DSlot& s, int side, int32_t l
   bfeat = -1;
   bf = -1;
   for (int ff = lane; ff < nf; ff += 32) {
-    bool u = s.bytree[ff] && (!have_larger || s.splittable[Lft * nf + ff]);
-    if (!u) continue;
+    // every input read at once (none of these loads depends on another)
+    const uint8_t in_tree = s.bytree[ff];
+    const uint8_t split_ok = have_larger ? s.splittable[Lft * nf + ff] : (uint8_t)1;
     const DSplit& r = s.feat_res[side * nf + ff];
     double g = r.gain;
-    if (r.monotone_type != 0) g *= pen;
-    if (better_than(g, r.feature, bg, bfeat)) {
+    const int32_t fe = r.feature;
+    const int32_t mono = r.monotone_type;
+    if (!(in_tree && split_ok)) continue;
+    if (mono != 0) g *= pen;
+    if (better_than(g, fe, bg, bfeat)) {
       bg = g;
-      bfeat = r.feature;
+      bfeat = fe;
       bf = ff;
     }
   }
