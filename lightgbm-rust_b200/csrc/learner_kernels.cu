@@ -948,17 +948,15 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
     sm.wt[warp] = best_t;
   }
   const bool any = __syncthreads_or(splittable) != 0;
-  if (tid == 0) {
+  if (warp == 0) {
+    // the warps' winners reduced with the same rule (candidates are distinct t)
     double bg = -INFINITY;
     int32_t bt = INT32_MIN;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      double og = sm.wgain[w];
-      int32_t ot = sm.wt[w];
-      if (og > bg || (og == bg && ot != INT32_MIN && (bt == INT32_MIN || (reverse ? ot > bt : ot < bt)))) {
-        bg = og;
-        bt = ot;
-      }
+    if (lane < (int)(blockDim.x >> 5)) {
+      bg = sm.wgain[lane];
+      bt = sm.wt[lane];
     }
+    warp_pick(reverse, bg, bt);
     ScanBest r;
     r.splittable = any;
     r.gain = bg;

@@ -69,36 +69,31 @@ __device__ __forceinline__ void warp_pick(bool desc, double& gain, int32_t& t) {
   }
 }
 
-// The update of `out` after one direction (split.rs:864-889 / :1167-1188), lane 0.
+// The update of `out` after one direction (split.rs:864-889 / :1167-1188), by
+// one warp: lane 0 forms the left child's sums and output, lane 1 the right
+// child's (the same expressions, so the same values), and lane 0 writes.
 template <bool kInt>
 __device__ void apply_direction(const ScanBest& r, const DFeature& m, const DParams& p, double sum_g, double sum_h,
                                 int64_t int_sum, double gs, double hs, int32_t num_data, double parent_output, bool mc,
                                 double cmin, double cmax, double min_gain_shift, double cnt_factor, bool reverse,
                                 DSplit& out) {
+  const int lane = threadIdx.x & 31;
   // a basic constraint with min > max never accepts a threshold (split.rs:765-771)
   if (r.t == INT32_MIN || (mc && cmin > cmax)) return;
-  if (!(r.splittable && r.gain > out.gain + min_gain_shift)) return;
-  const int offset = m.offset;
-  out.threshold = (uint32_t)(reverse ? r.t - 1 + offset : r.t + offset);
+  const double cur = out.gain;
+  __syncwarp();
+  if (!(r.splittable && r.gain > cur + min_gain_shift)) return;
+  const bool right = (lane & 1) != 0;
+  double g, h, o;
+  int32_t cnt;
+  int64_t q = 0;
   if (kInt) {
-    int64_t left = reverse ? (int64_t)((uint64_t)int_sum - (uint64_t)r.acc_q) : r.acc_q;
-    int64_t right = (int64_t)((uint64_t)int_sum - (uint64_t)left);
-    double lg = (double)int_grad(left) * gs, lh = (double)int_hess(left) * hs;
-    double rg = (double)int_grad(right) * gs, rh = (double)int_hess(right) * hs;
-    int32_t lcnt = round_int((double)int_hess(left) * cnt_factor);
-    int32_t rcnt = round_int((double)int_hess(right) * cnt_factor);
-    double lo = leaf_output(lg, lh, p, lcnt, parent_output);
-    double ro = leaf_output(rg, rh, p, rcnt, parent_output);
-    out.left_output = mc ? clampc(lo, cmin, cmax) : lo;
-    out.right_output = mc ? clampc(ro, cmin, cmax) : ro;
-    out.left_count = lcnt;
-    out.right_count = rcnt;
-    out.left_sum_gradient = lg;
-    out.left_sum_hessian = lh;
-    out.right_sum_gradient = rg;
-    out.right_sum_hessian = rh;
-    out.left_sum_gh = left;
-    out.right_sum_gh = right;
+    const int64_t left = reverse ? (int64_t)((uint64_t)int_sum - (uint64_t)r.acc_q) : r.acc_q;
+    q = right ? (int64_t)((uint64_t)int_sum - (uint64_t)left) : left;
+    g = (double)int_grad(q) * gs;
+    h = (double)int_hess(q) * hs;
+    cnt = round_int((double)int_hess(q) * cnt_factor);
+    o = leaf_output(g, h, p, cnt, parent_output);
   } else {
     double slg, slh;
     int32_t left_count;
@@ -111,19 +106,36 @@ __device__ void apply_direction(const ScanBest& r, const DFeature& m, const DPar
       slh = r.acc_h;
       left_count = r.acc_c;
     }
-    double lo = leaf_output(slg, slh, p, left_count, parent_output);
-    double ro = leaf_output(sum_g - slg, sum_h - slh, p, num_data - left_count, parent_output);
-    out.left_output = mc ? clampc(lo, cmin, cmax) : lo;
-    out.right_output = mc ? clampc(ro, cmin, cmax) : ro;
-    out.left_count = left_count;
-    out.left_sum_gradient = slg;
-    out.left_sum_hessian = slh - kEpsilon;
-    out.right_count = num_data - left_count;
-    out.right_sum_gradient = sum_g - slg;
-    out.right_sum_hessian = sum_h - slh - kEpsilon;
+    g = right ? sum_g - slg : slg;
+    h = right ? sum_h - slh : slh;
+    cnt = right ? num_data - left_count : left_count;
+    o = leaf_output(g, h, p, cnt, parent_output);
+    h = right ? sum_h - slh - kEpsilon : slh - kEpsilon;  // the stored hessian sums
   }
-  out.gain = r.gain - min_gain_shift;
-  out.default_left = reverse ? 1 : 0;
+  if (mc) o = clampc(o, cmin, cmax);
+  const double rg = __shfl_sync(0xffffffffu, g, 1), rh = __shfl_sync(0xffffffffu, h, 1);
+  const double ro = __shfl_sync(0xffffffffu, o, 1);
+  const int32_t rc = __shfl_sync(0xffffffffu, cnt, 1);
+  const int64_t rq = __shfl_sync(0xffffffffu, q, 1);
+  if (lane == 0) {
+    const int offset = m.offset;
+    out.threshold = (uint32_t)(reverse ? r.t - 1 + offset : r.t + offset);
+    out.left_output = o;
+    out.right_output = ro;
+    out.left_count = cnt;
+    out.right_count = rc;
+    out.left_sum_gradient = g;
+    out.left_sum_hessian = h;
+    out.right_sum_gradient = rg;
+    out.right_sum_hessian = rh;
+    if (kInt) {
+      out.left_sum_gh = q;
+      out.right_sum_gh = rq;
+    }
+    out.gain = r.gain - min_gain_shift;
+    out.default_left = reverse ? 1 : 0;
+  }
+  __syncwarp();
 }
 
 }  // namespace lgbm_b200
