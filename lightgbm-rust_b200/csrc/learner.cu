@@ -576,6 +576,10 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   ss.done = 0;
   ss.need_find = 1;
   ss.smaller.leaf = 0;
+  ss.smaller.num_data = (int32_t)cnt;
+  ss.s_begin = 0;
+  ss.s_side = 0;
+  ss.s_buf = 0;
   CU(cudaMemcpyAsync(d.st, &ss, sizeof(ss), cudaMemcpyHostToDevice, s));
   const int mode = h->cfg.hist_precision;
   const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);

@@ -171,6 +171,10 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->part_rows = 0;
   st->smaller.leaf = 0;
   st->smaller.num_data = (int32_t)n;
+  st->s_begin = 0;
+  st->s_side = 0;
+  st->s_buf = 0;
+  st->l_buf = -1;
   st->smaller.sum_gradients = a;
   st->smaller.sum_hessians = b;
   st->smaller.int_sum = (int64_t)d;
@@ -205,9 +209,10 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int ra
   DSlotState* st = s.st;
   if (st->done || !st->need_find) return false;
   int32_t leaf = st->smaller.leaf;
-  lr.count = s.leaf_count[leaf];
-  lr.begin = s.leaf_begin[leaf];
-  lr.idx = s.idx[s.leaf_side[leaf]];
+  (void)leaf;
+  lr.count = st->smaller.num_data;
+  lr.begin = st->s_begin;
+  lr.idx = s.idx[st->s_side];
   int64_t per = c.rows_per_block;
   int64_t active = min((int64_t)count, (lr.count + per - 1) / per);
   active = (active + kCl - 1) / kCl * kCl;
@@ -280,11 +285,11 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   }
   const uint32_t* idx = lr.idx + lr.begin;
   const size_t stride = (size_t)c.stride;
-  double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins * 2;
+  double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.st->s_buf * c.total_bins * 2;
   // fused form: only the root is histogrammed here, into pair 1, child 0
   unsigned long long* outi = c.fused ? reinterpret_cast<unsigned long long*>(s.pair_hist + 2 * (size_t)c.total_bins)
                                      : reinterpret_cast<unsigned long long*>(s.hist) +
-                                           (size_t)s.buf_of[s.st->smaller.leaf] * c.total_bins;
+                                           (size_t)s.st->s_buf * c.total_bins;
   // Adds cell i (over groups) of the CTAs `src` to the leaf histogram; cells
   // outside the features' views are skipped.
   auto emit = [&](int i, auto read_cell) {
@@ -458,9 +463,14 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
       }
     }
   }
-  // no CTA leaves (or reuses its cells) while another may still read them
-  if constexpr (kCl > 1) cg::this_cluster().sync();
-  else __syncthreads();
+  // no CTA leaves (or reuses its cells) while another may still read them:
+  // the peers consumed what they read before arriving, so the arrive needs
+  // no release ordering (this CTA's global atomics need not be waited for)
+  if constexpr (kCl > 1) {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n\tbarrier.cluster.wait.aligned;" ::: "memory");
+  } else {
+    __syncthreads();
+  }
 }
 
 template <int kMode, int kNG>
@@ -1197,7 +1207,7 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
   {
     const DLeafSplits sl = st->smaller;
     const int len = m.view_len;
-    const size_t sbase = (size_t)s.buf_of[sl.leaf] * c.total_bins + m.view_start;
+    const size_t sbase = (size_t)st->s_buf * c.total_bins + m.view_start;
     // the smaller leaf's view with its most frequent bin fixed (histogram.rs:42-56)
     // histogram cells are written by other CTAs' atomics: loaded through L2
     if (kInt) {
@@ -1255,7 +1265,7 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
     }
     __syncthreads();
     if (side == 1) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
-      const size_t lbase = (size_t)s.buf_of[st->larger.leaf] * c.total_bins + m.view_start;
+      const size_t lbase = (size_t)st->l_buf * c.total_bins + m.view_start;
       if (tid < len) {
         if (kInt) {
           int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
@@ -1403,6 +1413,11 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int
     s.buf_of[R] = buf_L;
     s.buf_of[L] = R;
   }
+  // the next step's histogram and scan read these instead of the leaf arrays
+  st->s_begin = left_smaller ? begin : begin + nl;
+  st->s_side = 1 - side;
+  st->s_buf = R;
+  st->l_buf = buf_L;
   st->left_leaf = L;
   st->right_leaf = R;
   // before_find_best_split (learner/mod.rs:712-731) on the values just written
