@@ -1074,21 +1074,37 @@ __device__ void build_partition_lut(const DCtx& c, const DSplit& info, uint8_t* 
   }
 }
 
-// The selected split is applied to the tree (tree.rs:240-297); one thread.
-__device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R) {
+// What apply_split reads (loaded early, so that the loads overlap other work).
+struct ApplyIn {
+  DSplit info;
+  DFeature m;
+  int32_t parent, parent_left, depth, num_cat;
+  double old_value, cmin0, cmax0;
+};
+
+__device__ __forceinline__ ApplyIn apply_load(const DCtx& c, const DSlot& s, const DSplit& src, int32_t bl) {
+  ApplyIn a;
+  a.info = src;
+  a.parent = s.tree.leaf_parent[bl];
+  a.old_value = s.tree.leaf_value[bl];
+  a.depth = s.tree.leaf_depth[bl] + 1;
+  a.num_cat = s.st->num_cat;
+  a.cmin0 = c.p.use_monotone ? s.cmin[bl] : 0.0;
+  a.cmax0 = c.p.use_monotone ? s.cmax[bl] : 0.0;
+  a.m = c.feats[a.info.inner];
+  a.parent_left = a.parent >= 0 ? s.tree.left_child[a.parent] : 0;
+  return a;
+}
+
+// The selected split applied to the tree (tree.rs:240-297); one thread.
+__device__ void apply_split(const DCtx& c, const DSlot& s, int32_t bl, int32_t R, const ApplyIn& a) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
   const DTree& t = s.tree;
-  // every value read first (the stores below could alias them for the
-  // compiler), so their latencies overlap
-  const DSplit info = s.best[bl];
-  const int32_t parent = t.leaf_parent[bl];
-  const double old_value = t.leaf_value[bl];
-  const int32_t d = t.leaf_depth[bl] + 1;
-  const int32_t num_cat = st->num_cat;
-  const double cmin0 = p.use_monotone ? s.cmin[bl] : 0.0, cmax0 = p.use_monotone ? s.cmax[bl] : 0.0;
-  const DFeature m = c.feats[info.inner];
-  const int32_t parent_left = parent >= 0 ? t.left_child[parent] : 0;
+  const DSplit& info = a.info;
+  const DFeature& m = a.m;
+  const int32_t parent = a.parent, parent_left = a.parent_left, d = a.depth, num_cat = a.num_cat;
+  const double old_value = a.old_value, cmin0 = a.cmin0, cmax0 = a.cmax0;
   const int32_t node = R - 1;
   const bool numerical = m.bin_type == 0;
   if (parent >= 0) {
@@ -1360,7 +1376,7 @@ struct FinalizeIn {
   DLeafSplits ls0, rs0;
 };
 
-__device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L, int32_t R) {
+__device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L, int32_t R, const DSplit& info) {
   FinalizeIn f;
   f.begin = s.leaf_begin[L];
   f.cnt = s.leaf_count[L];
@@ -1368,7 +1384,6 @@ __device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L,
   f.buf_L = s.buf_of[L];
   f.depth = s.tree.leaf_depth[L] + 1;  // both children's depth after the split
   f.status = s.st->status;
-  const DSplit& info = s.best[L];
   f.ls0 = DLeafSplits{L, 0, info.left_sum_gradient, info.left_sum_hessian, info.left_sum_gh, info.left_output};
   f.rs0 = DLeafSplits{R, 0, info.right_sum_gradient, info.right_sum_hessian, info.right_sum_gh, info.right_output};
   return f;
@@ -1573,6 +1588,20 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   const bool need = st->need_find != 0;
   const int32_t S = st->smaller.leaf, G = st->larger.leaf, Lft = st->left_leaf;
   const bool have_larger = G >= 0;
+  // the split's record, where the decision found it (not modified below)
+  const DSplit& src = (need && bl == S)   ? s.feat_res[d.side_bf[0]]
+                      : (need && bl == G) ? s.feat_res[nf + d.side_bf[1]]
+                                          : s.best[bl];
+  // thread 0 starts the loads of the tree update before the stores below
+  ApplyIn ain;
+  FinalizeIn fin;
+  if (tid == 0) {
+    ain = apply_load(c, s, src, bl);
+    fin = finalize_inputs(s, bl, R, src);
+    // the persisted record carries the penalized gain
+    if (need && bl == S) ain.info.gain = d.side_bg[0];
+    else if (need && bl == G) ain.info.gain = d.side_bg[1];
+  }
   __syncthreads();
   if (need) {
     for (int ff = tid; ff < nf; ff += blockDim.x) {
@@ -1607,8 +1636,7 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   }
   __syncthreads();
   if (tid == 0) {
-    const FinalizeIn fin = finalize_inputs(s, bl, R);
-    apply_split(c, s, bl, R);
+    apply_split(c, s, bl, R, ain);
     partition_finalize(c, s, bl, R, total_left, fin);
     st->part_epoch += 1;
   }
