@@ -15,6 +15,8 @@
 //                (partition.rs:107-174, learner/mod.rs:1200-1208, :712-731)
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "device_common.cuh"
 #include "kernels.h"
 #include "scan_warp.cuh"
@@ -263,6 +265,7 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   constexpr int kWarps = kHistThreads / 32;
   constexpr int kRowsPerWarp = kHistTileRows / kWarps;
   static_assert(kRowsPerWarp == 32, "one staged row per lane of a warp");
+  static_assert(kNG >= 1 && kNG <= 4, "the row loop dispatches 1 to 4 lane groups");
   constexpr int kCellBytes = kMode == 2 ? 4 : 16;
   constexpr int kGroupCells = kMaxBins * 32;
   constexpr int kRowBytes = 32 * kNG;
@@ -334,9 +337,12 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   int32_t nq = 0;
   float2 ngh = make_float2(0.f, 0.f);
   uint4 nb[2 * kNG];
-  auto fetch = [&](int64_t pos) {
+  // row indices run one tile ahead of the gathers that use them
+  auto load_idx = [&](int64_t pos) { return pos < r1 ? __ldcg(idx + pos) : 0u; };  // written by the partition
+  uint32_t idx_ahead = 0;
+  auto fetch = [&](int64_t pos, uint32_t row) {
     const bool live = pos < r1;
-    nrow = live ? __ldcg(idx + pos) : 0u;  // written by the partition: through L2
+    nrow = row;
     if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
     else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
     const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
@@ -344,7 +350,11 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
     for (int k = 0; k < 2 * kNG; ++k)
       nb[k] = (live && (k >> 1) < ngroups) ? __ldg(src + k) : make_uint4(0u, 0u, 0u, 0u);
   };
-  fetch(r0 + threadIdx.x);
+  {
+    const uint32_t first = load_idx(r0 + threadIdx.x);
+    idx_ahead = load_idx(r0 + kHistTileRows + threadIdx.x);
+    fetch(r0 + threadIdx.x, first);
+  }
   int32_t since_flush = 0;
   __syncthreads();
   for (int64_t t0 = r0; t0 < r1; t0 += kHistTileRows) {
@@ -357,52 +367,92 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
     else sgh[threadIdx.x] = ngh;
     __syncthreads();
     // the next tile's gathers run while this one is accumulated
-    if (t0 + kHistTileRows < r1) fetch(t0 + kHistTileRows + threadIdx.x);
+    if (t0 + kHistTileRows < r1) {
+      fetch(t0 + kHistTileRows + threadIdx.x, idx_ahead);
+      idx_ahead = load_idx(t0 + 2 * kHistTileRows + threadIdx.x);
+    }
     const int rw0 = warp * kRowsPerWarp;
     if (rw0 < tile_rows) {
+      // this warp's 32 staged rows; lane l adds feature f0 + 32 g + l of
+      // each row. The gradients of two or four rows arrive in one broadcast
+      // load.
       const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + rw0 * kRowBytes + lane;
-      int32_t myq = 0;
-      float myg = 0.f, myh = 0.f;
-      if (kMode == 2) {
-        myq = sq[rw0 + lane];
-      } else {
-        const float2 v = sgh[rw0 + lane];
-        myg = v.x;
-        myh = v.y;
-      }
+      auto rows = [&](auto groups) {
+        constexpr int kG = decltype(groups)::value;
+        // rows per batch: every byte of a batch is loaded before its first
+        // atomic (the compiler cannot move loads past shared atomics that may
+        // alias them), so a batch waits for one shared-load latency
+        constexpr int kB = kG == 1 ? 8 : 4;
 #pragma unroll
-      for (int j = 0; j < kRowsPerWarp; ++j) {
-        int32_t q = 0;
-        float gv = 0.f, hv = 0.f;
-        if (kMode == 2) {
-          q = __shfl_sync(0xffffffffu, myq, j);
-        } else {
-          gv = __shfl_sync(0xffffffffu, myg, j);
-          hv = __shfl_sync(0xffffffffu, myh, j);
-        }
+        for (int jb = 0; jb < kRowsPerWarp / kB; ++jb) {
+          int raw[kB][kG];
 #pragma unroll
-        for (int g = 0; g < kNG; ++g) {
-          if (g >= ngroups) break;
-          const int raw = (int)rowp[j * kRowBytes + 32 * g];
-          // float cells take a compare-and-swap loop per add: skip value 0
-          if (kMode != 2 && raw == 0) continue;
-          const int k = raw * 32 + lane;
-          if (kMode == 2) {
-            atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + k, q);
-          } else if (kMode == 0) {
-            double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
-            atomicAdd(d + k, (double)gv);
-            atomicAdd(d + kGroupCells + k, (double)hv);
+          for (int u = 0; u < kB; ++u)
+#pragma unroll
+            for (int g = 0; g < kG; ++g) raw[u][g] = (int)rowp[(kB * jb + u) * kRowBytes + 32 * g];
+          if constexpr (kMode == 2) {
+            int32_t qs[kB];
+#pragma unroll
+            for (int v = 0; v < kB / 4; ++v) {
+              const int4 q4 = reinterpret_cast<const int4*>(sq + rw0 + kB * jb)[v];
+              qs[4 * v] = q4.x;
+              qs[4 * v + 1] = q4.y;
+              qs[4 * v + 2] = q4.z;
+              qs[4 * v + 3] = q4.w;
+            }
+#pragma unroll
+            for (int u = 0; u < kB; ++u)
+#pragma unroll
+              for (int g = 0; g < kG; ++g)
+                atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + raw[u][g] * 32 + lane, qs[u]);
           } else {
-            float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
-            float og = atomicAdd(fl + k, gv);
-            float sg = __fadd_rn(og, gv);
-            float bg = __fsub_rn(sg, og);
-            atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv, bg)));
-            float oh = atomicAdd(fl + 2 * kGroupCells + k, hv);
-            float s2 = __fadd_rn(oh, hv);
-            float bh = __fsub_rn(s2, oh);
-            atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv, bh)));
+            float gs[kB], hs[kB];
+#pragma unroll
+            for (int v = 0; v < kB / 2; ++v) {
+              const float4 t = reinterpret_cast<const float4*>(sgh + rw0 + kB * jb)[v];
+              gs[2 * v] = t.x;
+              hs[2 * v] = t.y;
+              gs[2 * v + 1] = t.z;
+              hs[2 * v + 1] = t.w;
+            }
+#pragma unroll
+            for (int u = 0; u < kB; ++u)
+#pragma unroll
+              for (int g = 0; g < kG; ++g) {
+                // float cells take a compare-and-swap loop per add: skip value 0
+                if (raw[u][g] == 0) continue;
+                const int k = raw[u][g] * 32 + lane;
+                const float gv = gs[u], hv = hs[u];
+                if constexpr (kMode == 0) {
+                  double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
+                  atomicAdd(d + k, (double)gv);
+                  atomicAdd(d + kGroupCells + k, (double)hv);
+                } else {
+                  float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
+                  float og = atomicAdd(fl + k, gv);
+                  float sg = __fadd_rn(og, gv);
+                  float bg = __fsub_rn(sg, og);
+                  atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv, bg)));
+                  float oh = atomicAdd(fl + 2 * kGroupCells + k, hv);
+                  float s2 = __fadd_rn(oh, hv);
+                  float bh = __fsub_rn(s2, oh);
+                  atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv, bh)));
+                }
+              }
+          }
+        }
+      };
+      // the group count is a compile-time constant inside the row loop
+      if (ngroups == kNG) {
+        rows(std::integral_constant<int, kNG>{});
+      } else {
+        if constexpr (kNG > 1) {
+          if (ngroups == 1) rows(std::integral_constant<int, 1>{});
+          else if constexpr (kNG > 2) {
+            if (ngroups == 2) rows(std::integral_constant<int, 2>{});
+            else if constexpr (kNG > 3) {
+              if (ngroups == 3) rows(std::integral_constant<int, 3>{});
+            }
           }
         }
       }
