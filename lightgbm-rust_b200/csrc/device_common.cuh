@@ -121,6 +121,8 @@ struct DSlot {
   double* cmax;
   void* hist;              // [num_leaves][total_bins] cells
   DSplit* feat_res;        // scan results [2][num_features]
+  uint8_t* lut_cand;       // goes-left flag per stored value of each scan result [2][num_features][kMaxBins]
+  uint8_t* leaf_lut;       // the same for each leaf's best split [num_leaves][kMaxBins]
   uint8_t* feat_ok;        // [2][num_features]
   unsigned long long* tile_status;  // partition look-back [max_tiles]
   const float2* gh;        // this slot's interleaved (gradient, hessian) [num_data]
@@ -215,6 +217,42 @@ __device__ __forceinline__ double split_gain(double lg, double lh, double rg, do
   if ((mono > 0 && left > right) || (mono < 0 && left < right)) return 0.0;
   return leaf_gain_given_output(lg, lh, p, left) + leaf_gain_given_output(rg, rh, p, right);
 }
+
+// The scan's hot code: with no L1, max_delta_step, path smoothing or
+// monotone bounds every formula above reduces to its plain form, evaluated
+// inline with the same operations; otherwise the full formula is called out
+// of line, which keeps the threshold scan's instruction footprint small.
+__device__ __forceinline__ bool plain_split(const DParams& p, bool mc) {
+  return !mc && !use_l1(p) && !use_max_output(p) && !use_smoothing(p);
+}
+static __device__ __noinline__ double split_gain_full(double lg, double lh, double rg, double rh, const DParams& p,
+                                                      int32_t lc, int32_t rc, double po, bool mc, double cmin,
+                                                      double cmax, int32_t mono) {
+  return split_gain(lg, lh, rg, rh, p, lc, rc, po, mc, cmin, cmax, mono);
+}
+static __device__ __noinline__ double leaf_output_full(double g, double h, const DParams& p, int32_t n, double po) {
+  return leaf_output(g, h, p, n, po);
+}
+static __device__ __noinline__ double leaf_gain_full(double g, double h, const DParams& p, int32_t n, double po) {
+  return leaf_gain(g, h, p, n, po);
+}
+__device__ __forceinline__ double split_gain_hot(bool plain, double lg, double lh, double rg, double rh,
+                                                 const DParams& p, int32_t lc, int32_t rc, double po, bool mc,
+                                                 double cmin, double cmax, int32_t mono) {
+  if (plain) return (lg * lg) / (lh + p.lambda_l2) + (rg * rg) / (rh + p.lambda_l2);
+  return split_gain_full(lg, lh, rg, rh, p, lc, rc, po, mc, cmin, cmax, mono);
+}
+__device__ __forceinline__ double leaf_output_hot(bool plain, double g, double h, const DParams& p, int32_t n,
+                                                  double po) {
+  if (plain) return -g / (h + p.lambda_l2);
+  return leaf_output_full(g, h, p, n, po);
+}
+__device__ __forceinline__ double leaf_gain_hot(bool plain, double g, double h, const DParams& p, int32_t n,
+                                                double po) {
+  if (plain) return (g * g) / (h + p.lambda_l2);
+  return leaf_gain_full(g, h, p, n, po);
+}
+
 __device__ __forceinline__ int32_t round_int(double x) { return (int32_t)(x + (double)0.5f); }
 
 // split.rs:114-121 SplitInfo::better_than

@@ -202,6 +202,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
       d.hist = hp;
     }
     ALLOC(d.feat_res, 2 * (size_t)nf);
+    ALLOC(d.lut_cand, 2 * (size_t)nf * kMaxBins);
+    ALLOC(d.leaf_lut, (size_t)L * kMaxBins);
     ALLOC(d.feat_ok, 4 * (size_t)nf);
     ALLOC(d.tile_status, max_tiles);
     d.gh = nullptr;  // set below from the contiguous [K x n] buffer

@@ -209,12 +209,13 @@ template <int kCl>
 __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int rank, int count, LeafRows& lr,
                                            int64_t& r0, int64_t& r1) {
   DSlotState* st = s.st;
-  if (st->done || !st->need_find) return false;
-  int32_t leaf = st->smaller.leaf;
-  (void)leaf;
-  lr.count = st->smaller.num_data;
-  lr.begin = st->s_begin;
-  lr.idx = s.idx[st->s_side];
+  // every field read at once
+  const int32_t done = st->done, need = st->need_find, count_s = st->smaller.num_data, begin_s = st->s_begin,
+                side_s = st->s_side;
+  if (done || !need) return false;
+  lr.count = count_s;
+  lr.begin = begin_s;
+  lr.idx = side_s == 0 ? s.idx[0] : s.idx[1];
   int64_t per = c.rows_per_block;
   int64_t active = min((int64_t)count, (lr.count + per - 1) / per);
   active = (active + kCl - 1) / kCl * kCl;
@@ -913,6 +914,7 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
   __syncthreads();
   const int32_t min_data = p.min_data_in_leaf;
   const double min_hess = p.min_sum_hessian_in_leaf;
+  const bool plain = plain_split(p, lc.mc);
   // accumulated side's values of candidate t (t = -1: the extra candidate)
   auto acc = [&](int t, double& ag, double& ah, int32_t& ac, int64_t& aq) {
     if (t < 0) {
@@ -991,10 +993,11 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
       gr = lc.sum_g - ag;
     }
     int32_t rc = lc.num_data - ac;
-    double gain = reverse ? split_gain(gr, hr, ga, ha, p, rc, ac, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
-                                       m.monotone_type)
-                          : split_gain(ga, ha, gr, hr, p, ac, rc, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
-                                       m.monotone_type);
+    // the left child is the rest when scanning in reverse
+    const double g1 = reverse ? gr : ga, h1 = reverse ? hr : ha, g2 = reverse ? ga : gr, h2 = reverse ? ha : hr;
+    const int32_t c1 = reverse ? rc : ac, c2 = reverse ? ac : rc;
+    double gain = split_gain_hot(plain, g1, h1, g2, h2, p, c1, c2, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
+                                 m.monotone_type);
     if (gain <= min_gain_shift) continue;
     splittable = true;
     if (gain > best_gain || (gain == best_gain && best_t != INT32_MIN && (reverse ? t > best_t : t < best_t))) {
@@ -1066,7 +1069,8 @@ __device__ bool find_best_threshold_block(ScanSmem& sm, const DFeature& m, const
     if (tid == 0) out.monotone_type = m.monotone_type;
     double sg = kInt ? (double)int_grad(lc.int_sum) * lc.gs : lc.sum_g;
     double sh = kInt ? (double)int_hess(lc.int_sum) * lc.hs : lc.sum_h;
-    double min_gain_shift = leaf_gain(sg, sh, p, lc.num_data, lc.parent_output) + p.min_gain_to_split;
+    double min_gain_shift = leaf_gain_hot(plain_split(p, lc.mc), sg, sh, p, lc.num_data, lc.parent_output) +
+                            p.min_gain_to_split;
     double cnt_factor =
         kInt ? (double)lc.num_data / (double)int_hess(lc.int_sum) : (double)lc.num_data / lc.sum_h;
     if (!kInt && tid < m.view_len) sm.ce[tid] = round_int(sm.h[tid] * cnt_factor);
@@ -1101,8 +1105,7 @@ __device__ __forceinline__ bool split_better(const DSplit& a, const DSplit& b) {
 // Partition LUT over stored group values (learner/mod.rs:1313-1329): one
 // goes-left flag per value a row of the split feature can hold; thread t
 // of the CTA writes value t.
-__device__ void build_partition_lut(const DCtx& c, const DSplit& info, uint8_t* lut) {
-  const DFeature& m = c.feats[info.inner];
+__device__ void build_partition_lut(const DFeature& m, const DSplit& info, uint8_t* lut) {
   const bool numerical = m.bin_type == 0;
   const bool default_left = numerical ? info.default_left != 0 : false;
   const int32_t ntb = m.view_len + 1;
@@ -1219,12 +1222,13 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
   const DFeature m = c.feats[f];
   const DParams& p = c.p;
   const int32_t nf = c.num_features;
-  const bool have_larger = st->larger.leaf >= 0;
-  const bool need = st->need_find != 0;
-  const int32_t L = st->left_leaf;
-  const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
-  if (!(used && (side == 0 || have_larger))) return;
   if (kInt && c.fused) {
+    if (st->done) return;
+    const bool have_larger = st->larger.leaf >= 0;
+    const bool need = st->need_find != 0;
+    const int32_t L = st->left_leaf;
+    const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
+    if (!(used && (side == 0 || have_larger))) return;
     // both leaves' histograms were built directly by the previous partition
     // (the root's by the histogram kernel): each view is fixed from its own
     // leaf's sum (histogram.rs:42-56); no subtraction
@@ -1268,22 +1272,57 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
     for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
+    // the partition's goes-left table for this candidate, ready if it wins
+    if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins);
     return;
   }
+  // The loads run in two waves so that their latencies overlap: the slot
+  // state, then everything that depends on it (the feature's flags, both
+  // histogram views, the leaf's output bounds).
+  const int32_t larger_leaf = st->larger.leaf, L = st->left_leaf, s_buf = st->s_buf, l_buf = st->l_buf;
+  const bool need = st->need_find != 0 && st->done == 0;
+  const int32_t nl_cur = st->num_leaves_cur;
+  const DLeafSplits sl = st->smaller;
+  const DLeafSplits ls = side == 0 ? sl : st->larger;
+  const double gsc = st->grad_scale, hsc = st->hess_scale;
+  const bool have_larger = larger_leaf >= 0;
+  // the buffers and the leaf are valid whenever this side has a leaf to search
+  const bool live = need && (side == 0 || have_larger);
+  const int len = m.view_len;
+  const size_t sbase = (size_t)s_buf * c.total_bins + m.view_start;
+  const size_t lbase = (size_t)l_buf * c.total_bins + m.view_start;
+  const bool in_view = live && tid < len;
+  const bool sub = side == 1 && in_view;
+  // histogram cells are written by other CTAs' atomics: loaded through L2
+  int64_t sq = 0, pq = 0;
+  double sgv = 0.0, shv = 0.0, pgv = 0.0, phv = 0.0;
+  if (kInt) {
+    const long long* hs = reinterpret_cast<const long long*>(s.hist);
+    if (in_view) sq = (int64_t)__ldcg(hs + sbase + tid);
+    if (sub) pq = (int64_t)__ldcg(hs + lbase + tid);
+  } else {
+    const double* hs = reinterpret_cast<const double*>(s.hist);
+    if (in_view) {
+      sgv = __ldcg(hs + 2 * (sbase + tid));
+      shv = __ldcg(hs + 2 * (sbase + tid) + 1);
+    }
+    if (sub) {
+      pgv = __ldcg(hs + 2 * (lbase + tid));
+      phv = __ldcg(hs + 2 * (lbase + tid) + 1);
+    }
+  }
+  const uint8_t in_tree = s.bytree[f];
+  const uint8_t split_ok = have_larger ? s.splittable[L * nf + f] : (uint8_t)1;
+  const double cmin = live ? s.cmin[ls.leaf] : 0.0, cmax = live ? s.cmax[ls.leaf] : 0.0;
+  if (!(live && in_tree && split_ok)) return;
   {
-    const DLeafSplits sl = st->smaller;
-    const int len = m.view_len;
-    const size_t sbase = (size_t)st->s_buf * c.total_bins + m.view_start;
     // the smaller leaf's view with its most frequent bin fixed (histogram.rs:42-56)
-    // histogram cells are written by other CTAs' atomics: loaded through L2
     if (kInt) {
-      const long long* hs = reinterpret_cast<const long long*>(s.hist) + sbase;
-      if (tid < len) sm.ig[tid] = (int64_t)__ldcg(hs + tid);
+      if (in_view) sm.ig[tid] = sq;
     } else {
-      const double* hs = reinterpret_cast<const double*>(s.hist) + 2 * sbase;
-      if (tid < len) {
-        sm.g[tid] = __ldcg(hs + 2 * tid);
-        sm.h[tid] = __ldcg(hs + 2 * tid + 1);
+      if (in_view) {
+        sm.g[tid] = sgv;
+        sm.h[tid] = shv;
       }
     }
     __syncthreads();
@@ -1331,16 +1370,15 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
     }
     __syncthreads();
     if (side == 1) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
-      const size_t lbase = (size_t)st->l_buf * c.total_bins + m.view_start;
-      if (tid < len) {
+      if (in_view) {
         if (kInt) {
           int64_t* lh = reinterpret_cast<int64_t*>(s.hist) + lbase;
-          int64_t v = (int64_t)((uint64_t)__ldcg(reinterpret_cast<const long long*>(lh) + tid) - (uint64_t)sm.ig[tid]);
+          int64_t v = (int64_t)((uint64_t)pq - (uint64_t)sm.ig[tid]);
           sm.ig[tid] = v;
           lh[tid] = v;
         } else {
           double* lh = reinterpret_cast<double*>(s.hist) + 2 * lbase;
-          double g = __ldcg(lh + 2 * tid) - sm.g[tid], h = __ldcg(lh + 2 * tid + 1) - sm.h[tid];
+          double g = pgv - sm.g[tid], h = phv - sm.h[tid];
           sm.g[tid] = g;
           sm.h[tid] = h;
           lh[2 * tid] = g;
@@ -1349,20 +1387,18 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
       }
       __syncthreads();
     }
-    const DLeafSplits ls = side == 0 ? st->smaller : st->larger;
     LeafCtx lc;
     lc.sum_g = ls.sum_gradients;
     lc.sum_h = ls.sum_hessians;
     lc.int_sum = ls.int_sum;
-    lc.gs = st->grad_scale;
-    lc.hs = st->hess_scale;
+    lc.gs = gsc;
+    lc.hs = hsc;
     lc.num_data = ls.num_data;
     // learner/mod.rs:1303-1309 parent output
-    lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
-                                                : ls.weight;
+    lc.parent_output = nl_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data) : ls.weight;
     lc.mc = p.use_monotone != 0;
-    lc.cmin = s.cmin[ls.leaf];
-    lc.cmax = s.cmax[ls.leaf];
+    lc.cmin = cmin;
+    lc.cmax = cmax;
     // the result is built in shared memory and stored once
     DSplit& out = sm.out;
     bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
@@ -1375,6 +1411,8 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
     for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
+    // the partition's goes-left table for this candidate, ready if it wins
+    if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins);
   }
 }
 
@@ -1385,13 +1423,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
   pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
-  if (st->done) return;
   // the partition that follows claims its row tiles from this counter
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && !st->done) {
     st->part_ticket = 0;
     st->part_done = 0;
   }
-  if (kInt && c.fused) {  // the pair this step's partition fills (read by the scan before last)
+  if (kInt && c.fused && !st->done) {  // the pair this step's partition fills (read by the scan before last)
     const int k = st->num_leaves_cur - 1;
     long long* z = s.pair_hist + (size_t)(k & 1) * 2 * c.total_bins;
     const size_t n = 2 * (size_t)c.total_bins;
@@ -1498,6 +1535,24 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int
   st->need_find = need ? 1 : 0;
 }
 
+// The slot-state fields a partition CTA reads first, loaded together.
+struct StepHead {
+  int32_t done, need, S, G, Lft, R;
+  uint32_t epoch;
+};
+
+__device__ __forceinline__ StepHead load_step_head(const DSlotState* st) {
+  StepHead h;
+  h.done = st->done;
+  h.need = st->need_find;
+  h.S = st->smaller.leaf;
+  h.G = st->larger.leaf;
+  h.Lft = st->left_leaf;
+  h.R = st->num_leaves_cur;
+  h.epoch = st->part_epoch;
+  return h;
+}
+
 // Decision state a partition CTA derives from the scan results.
 struct SplitDecision {
   double side_bg[2];     // best (penalized) gain of the smaller / larger new leaf
@@ -1559,11 +1614,10 @@ __device__ __forceinline__ bool leaf_takes(double og, int32_t ofe, int32_t ol, d
 // Split decision of this step, computed by every partition CTA: the best
 // split of the two new leaves (warps 0, 1), the best of the other leaves
 // (warps 2..), then the best leaf (thread 0).
-__device__ void decide_split(const DCtx& c, const DSlot& s, SplitDecision& d) {
+__device__ void decide_split(const DCtx& c, const DSlot& s, const StepHead& h, SplitDecision& d) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const DSlotState* st = s.st;
-  const bool need = st->need_find != 0;
-  const int32_t S = st->smaller.leaf, G = st->larger.leaf, Lft = st->left_leaf;
+  const bool need = h.need != 0;
+  const int32_t S = h.S, G = h.G, Lft = h.Lft;
   const bool have_larger = G >= 0;
   const int32_t NL = c.p.num_leaves;
   if (warp < 2) {
@@ -1669,6 +1723,9 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
         const uint32_t* src = reinterpret_cast<const uint32_t*>(&s.feat_res[warp * nf + bf]);
         uint32_t* w = reinterpret_cast<uint32_t*>(&dst);
         for (int i = lane; i < (int)(sizeof(DSplit) / 4); i += 32) w[i] = src[i];
+        if (lane < kMaxBins / 16)
+          reinterpret_cast<uint4*>(s.leaf_lut + (size_t)leaf * kMaxBins)[lane] =
+              reinterpret_cast<const uint4*>(s.lut_cand + ((size_t)warp * nf + bf) * kMaxBins)[lane];
         __syncwarp();
         if (lane == 0) {
           dst.gain = d.side_bg[warp];
@@ -1694,7 +1751,7 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
 
 // Shared state of a partition CTA.
 struct PartShared {
-  uint8_t lut[kMaxBins];
+  alignas(16) uint8_t lut[kMaxBins];
   int32_t warp_tot[32];
   int32_t tile, prefix;
   bool last;
@@ -1703,29 +1760,33 @@ struct PartShared {
 
 constexpr int kPartTileRows = 2048;  // rows per partition tile (tile_status holds one word per tile)
 
-// Step prologue of a partition CTA: the split decision and, when a leaf is
-// split, its goes-left LUT in ps.lut. Returns the leaf to split (-1: the
-// tree is finished).
-__device__ int32_t partition_prologue(const DCtx& c, const DSlot& s, PartShared& ps) {
-  decide_split(c, s, ps.dec);
-  const int32_t L = ps.dec.bl;
-  if (L < 0) return -1;
-  const DSlotState* st = s.st;
-  const int32_t nf = c.num_features;
-  const DSplit& info = (st->need_find && L == st->smaller.leaf)   ? s.feat_res[ps.dec.side_bf[0]]
-                       : (st->need_find && L == st->larger.leaf) ? s.feat_res[nf + ps.dec.side_bf[1]]
-                                                                  : s.best[L];
-  build_partition_lut(c, info, ps.lut);
-  return L;
-}
+// The leaf a step splits: its rows and the feature its split tests.
+struct SplitLeaf {
+  int32_t L, begin, cnt, side, inner;
+};
 
-// The inner feature the split of leaf L tests.
-__device__ __forceinline__ int32_t split_inner_of(const DCtx& c, const DSlot& s, const PartShared& ps, int32_t L) {
-  const DSlotState* st = s.st;
-  const int32_t nf = c.num_features;
-  if (st->need_find && L == st->smaller.leaf) return s.feat_res[ps.dec.side_bf[0]].inner;
-  if (st->need_find && L == st->larger.leaf) return s.feat_res[nf + ps.dec.side_bf[1]].inner;
-  return s.best[L].inner;
+// Step prologue of a partition CTA: the split decision and, when a leaf is
+// split, its goes-left LUT in ps.lut (built by the scan for each candidate
+// and kept per leaf when the candidates are stored). L < 0: the tree is
+// finished.
+__device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const StepHead& h, PartShared& ps) {
+  decide_split(c, s, h, ps.dec);
+  SplitLeaf sl;
+  sl.L = ps.dec.bl;
+  if (sl.L < 0) return sl;
+  const int32_t L = sl.L, nf = c.num_features;
+  const bool from_s = h.need && L == h.S, from_g = h.need && L == h.G;
+  const int32_t cand = from_s ? ps.dec.side_bf[0] : from_g ? nf + ps.dec.side_bf[1] : -1;
+  // every load of the leaf's facts and its table at once
+  const DSplit& info = cand >= 0 ? s.feat_res[cand] : s.best[L];
+  const uint8_t* lut = cand >= 0 ? s.lut_cand + (size_t)cand * kMaxBins : s.leaf_lut + (size_t)L * kMaxBins;
+  sl.begin = s.leaf_begin[L];
+  sl.cnt = s.leaf_count[L];
+  sl.side = s.leaf_side[L];
+  sl.inner = info.inner;
+  if (threadIdx.x < kMaxBins / 16)
+    reinterpret_cast<uint4*>(ps.lut)[threadIdx.x] = reinterpret_cast<const uint4*>(lut)[threadIdx.x];
+  return sl;
 }
 
 // One partition tile after its goes-left flags are known: a block scan of
@@ -1826,13 +1887,14 @@ __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32
 // per thread, blockDim.x * kItems == kPartTileRows), each chained to its
 // predecessors by a decoupled look-back on the left count. The CTA that
 // partitions the last tile posts the left count in st->part_left.
+// The leaf's row tiles, claimed in order from the ticket counter; with
+// `claimed` the CTA's first ticket is already in ps.tile.
 template <int kItems>
-__device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, int32_t L, uint32_t epoch) {
+__device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, const SplitLeaf& sl, uint32_t epoch,
+                               bool claimed) {
   DSlotState* st = s.st;
   const int tid = threadIdx.x;
-  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
-  const int32_t side = s.leaf_side[L];
-  const int32_t inner = split_inner_of(c, s, ps, L);
+  const int32_t begin = sl.begin, cnt = sl.cnt, side = sl.side, inner = sl.inner;
   if (cnt == 0) return;
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
@@ -1841,7 +1903,8 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, in
   const uint8_t* lut = ps.lut;
   while (true) {
     __syncthreads();
-    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+    if (tid == 0 && !claimed) ps.tile = atomicAdd(&st->part_ticket, 1);
+    claimed = false;
     __syncthreads();
     const int32_t tile = ps.tile;
     if (tile >= ntiles) break;
@@ -1882,19 +1945,24 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
-  if (st->done) return;
   __shared__ PartShared ps;
   const int tid = threadIdx.x;
-  const int32_t R = st->num_leaves_cur;
-  const uint32_t epoch = st->part_epoch;
-  const int32_t L = partition_prologue(c, s, ps);
+  // the step's fields and this CTA's first row tile, in one round trip (a
+  // finished tree's launch claims tickets nobody uses; the scan resets the
+  // counter before every partition of a live tree)
+  const StepHead h = load_step_head(st);
+  if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+  if (h.done) return;
+  const int32_t R = h.R;
+  const SplitLeaf sl = partition_prologue(c, s, h, ps);
+  const int32_t L = sl.L;
   if (L < 0) {
     if (blockIdx.x == 0 && tid == 0) st->done = 1;
     return;
   }
   zero_hist_buffer(c, s, R, blockIdx.x, gridDim.x);
-  if (blockIdx.x == 0 && tid == 0) st->part_rows += s.leaf_count[L];
-  partition_rows<kPartTileRows / kPartThreads>(c, s, ps, L, epoch);
+  if (blockIdx.x == 0 && tid == 0) st->part_rows += sl.cnt;
+  partition_rows<kPartTileRows / kPartThreads>(c, s, ps, sl, h.epoch, true);
   __syncthreads();
   if (tid == 0) {
     __threadfence();
@@ -1903,8 +1971,7 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   __syncthreads();
   if (ps.last) {
     __threadfence();
-    const int32_t cnt = s.leaf_count[L];
-    finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+    finish_step(c, s, ps.dec, L, R, sl.cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
   }
 }
 
@@ -1940,12 +2007,14 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   // done changes during this launch only where every CTA returns here too
-  if (st->done) return;
+  const StepHead hd = load_step_head(st);
+  if (hd.done) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int32_t R = st->num_leaves_cur;
+  const int32_t R = hd.R;
   const int step = R - 1;
-  const uint32_t epoch = st->part_epoch;
-  const int32_t L = partition_prologue(c, s, ps);
+  const uint32_t epoch = hd.epoch;
+  const SplitLeaf sl = partition_prologue(c, s, hd, ps);
+  const int32_t L = sl.L;
   if (L < 0) {
     if (blockIdx.x == 0 && tid == 0) st->done = 1;
     return;
@@ -1961,9 +2030,7 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
     for (int i = tid; i < 2 * kFusedCells * 4 / 16; i += kFusedThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
   }
   __syncthreads();  // cells zeroed, feature facts and the LUT complete
-  const int32_t begin = s.leaf_begin[L], cnt = s.leaf_count[L];
-  const int32_t side = s.leaf_side[L];
-  const int32_t inner = split_inner_of(c, s, ps, L);
+  const int32_t begin = sl.begin, cnt = sl.cnt, side = sl.side, inner = sl.inner;
   if (blockIdx.x == 0 && tid == 0) st->part_rows += cnt;
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
@@ -2376,25 +2443,25 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     if (!grid_barrier(gs, G)) return;
     mark(1);
     // P: the split decision and the row partition of the slot
-    int32_t L = -1, R = 0;
+    SplitLeaf sl;
+    sl.L = -1;
+    int32_t R = 0;
     if (!*reinterpret_cast<volatile int32_t*>(&st->done)) {
-      R = st->num_leaves_cur;
-      const uint32_t epoch = st->part_epoch;
-      L = partition_prologue(c, s, ps);
-      if (L < 0) {
+      const StepHead h = load_step_head(st);
+      R = h.R;
+      sl = partition_prologue(c, s, h, ps);
+      if (sl.L < 0) {
         if (rank == 0 && tid == 0) st->done = 1;
       } else {
         zero_hist_buffer(c, s, R, rank, per);
-        partition_rows<kPartTileRows / kGrowThreads>(c, s, ps, L, epoch);
+        partition_rows<kPartTileRows / kGrowThreads>(c, s, ps, sl, h.epoch, false);
       }
     }
     if (!grid_barrier(gs, G)) return;
     mark(2);
     // F: bookkeeping of the step
-    if (L >= 0 && rank == 0) {
-      const int32_t cnt = s.leaf_count[L];
-      finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
-    }
+    if (sl.L >= 0 && rank == 0)
+      finish_step(c, s, ps.dec, sl.L, R, sl.cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
     if (!grid_barrier(gs, G)) return;
     mark(3);
   }

@@ -93,7 +93,7 @@ __device__ void apply_direction(const ScanBest& r, const DFeature& m, const DPar
     g = (double)int_grad(q) * gs;
     h = (double)int_hess(q) * hs;
     cnt = round_int((double)int_hess(q) * cnt_factor);
-    o = leaf_output(g, h, p, cnt, parent_output);
+    o = leaf_output_hot(plain_split(p, mc), g, h, p, cnt, parent_output);
   } else {
     double slg, slh;
     int32_t left_count;
@@ -109,7 +109,7 @@ __device__ void apply_direction(const ScanBest& r, const DFeature& m, const DPar
     g = right ? sum_g - slg : slg;
     h = right ? sum_h - slh : slh;
     cnt = right ? num_data - left_count : left_count;
-    o = leaf_output(g, h, p, cnt, parent_output);
+    o = leaf_output_hot(plain_split(p, mc), g, h, p, cnt, parent_output);
     h = right ? sum_h - slh - kEpsilon : slh - kEpsilon;  // the stored hessian sums
   }
   if (mc) o = clampc(o, cmin, cmax);
