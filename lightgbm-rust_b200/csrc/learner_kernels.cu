@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
 struct LeafRows {
   const uint32_t* idx;  // position -> row
   int64_t begin, count;
+  int32_t buf;          // the leaf's histogram buffer
 };
 
 // Rows [r0, r1) of the smaller leaf for this CTA. CTAs are used in whole
@@ -211,8 +212,9 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int ra
   DSlotState* st = s.st;
   // every field read at once
   const int32_t done = st->done, need = st->need_find, count_s = st->smaller.num_data, begin_s = st->s_begin,
-                side_s = st->s_side;
+                side_s = st->s_side, buf_s = st->s_buf;
   if (done || !need) return false;
+  lr.buf = buf_s;
   lr.count = count_s;
   lr.begin = begin_s;
   lr.idx = side_s == 0 ? s.idx[0] : s.idx[1];
@@ -276,11 +278,15 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   int32_t* sq = reinterpret_cast<int32_t*>(sbins + kHistTileRows * 2 * kNG);
   float2* sgh = reinterpret_cast<float2*>(sq);
   __shared__ int32_t s_vlen[32 * kNG], s_vstart[32 * kNG];
-  for (int i = threadIdx.x; i < 32 * kNG; i += kHistThreads) {
-    const int f = f0 + i;
-    const bool ok = (i >> 5) < ngroups && f < f1;
-    s_vlen[i] = ok ? c.feats[f].view_len : 0;
-    s_vstart[i] = ok ? c.feats[f].view_start : 0;
+  static_assert(32 * kNG <= kHistThreads, "one feature view per thread");
+  // the views are stored to shared memory after the first gathers are issued
+  int32_t my_vlen = 0, my_vstart = 0;
+  if (threadIdx.x < 32 * kNG) {
+    const int f = f0 + (int)threadIdx.x;
+    if (((int)threadIdx.x >> 5) < ngroups && f < f1) {
+      my_vlen = c.feats[f].view_len;
+      my_vstart = c.feats[f].view_start;
+    }
   }
   {
     uint4* z = reinterpret_cast<uint4*>(cells);
@@ -289,11 +295,11 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   }
   const uint32_t* idx = lr.idx + lr.begin;
   const size_t stride = (size_t)c.stride;
-  double* outf = reinterpret_cast<double*>(s.hist) + (size_t)s.st->s_buf * c.total_bins * 2;
+  double* outf = reinterpret_cast<double*>(s.hist) + (size_t)lr.buf * c.total_bins * 2;
   // fused form: only the root is histogrammed here, into pair 1, child 0
   unsigned long long* outi = c.fused ? reinterpret_cast<unsigned long long*>(s.pair_hist + 2 * (size_t)c.total_bins)
                                      : reinterpret_cast<unsigned long long*>(s.hist) +
-                                           (size_t)s.st->s_buf * c.total_bins;
+                                           (size_t)lr.buf * c.total_bins;
   // Adds cell i (over groups) of the CTAs `src` to the leaf histogram; cells
   // outside the features' views are skipped.
   auto emit = [&](int i, auto read_cell) {
@@ -355,6 +361,10 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
     const uint32_t first = load_idx(r0 + threadIdx.x);
     idx_ahead = load_idx(r0 + kHistTileRows + threadIdx.x);
     fetch(r0 + threadIdx.x, first);
+  }
+  if (threadIdx.x < 32 * kNG) {
+    s_vlen[threadIdx.x] = my_vlen;
+    s_vstart[threadIdx.x] = my_vstart;
   }
   int32_t since_flush = 0;
   __syncthreads();
@@ -1696,15 +1706,18 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   const DSplit& src = (need && bl == S)   ? s.feat_res[d.side_bf[0]]
                       : (need && bl == G) ? s.feat_res[nf + d.side_bf[1]]
                                           : s.best[bl];
-  // thread 0 starts the loads of the tree update before the stores below
+  // the tree update (thread 0) and the leaf bookkeeping (thread 32) write
+  // disjoint fields and read only what they load here, before the stores
+  // below: they run side by side
   ApplyIn ain;
   FinalizeIn fin;
   if (tid == 0) {
     ain = apply_load(c, s, src, bl);
-    fin = finalize_inputs(s, bl, R, src);
     // the persisted record carries the penalized gain
     if (need && bl == S) ain.info.gain = d.side_bg[0];
     else if (need && bl == G) ain.info.gain = d.side_bg[1];
+  } else if (tid == 32) {
+    fin = finalize_inputs(s, bl, R, src);
   }
   __syncthreads();
   if (need) {
@@ -1744,6 +1757,7 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   __syncthreads();
   if (tid == 0) {
     apply_split(c, s, bl, R, ain);
+  } else if (tid == 32) {
     partition_finalize(c, s, bl, R, total_left, fin);
     st->part_epoch += 1;
   }
