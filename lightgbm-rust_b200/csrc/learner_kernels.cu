@@ -1915,13 +1915,15 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, co
   const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
   const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
   const uint8_t* lut = ps.lut;
+  int32_t next = -1;  // thread 0: the ticket after the current tile, claimed while the tile runs
   while (true) {
     __syncthreads();
-    if (tid == 0 && !claimed) ps.tile = atomicAdd(&st->part_ticket, 1);
+    if (tid == 0 && !claimed) ps.tile = next >= 0 ? next : atomicAdd(&st->part_ticket, 1);
     claimed = false;
     __syncthreads();
     const int32_t tile = ps.tile;
     if (tile >= ntiles) break;
+    if (tid == 0) next = atomicAdd(&st->part_ticket, 1);
     const int32_t t0 = tile * kPartTileRows;
     uint32_t rows[kItems];
     uint32_t flags = 0;
