@@ -141,7 +141,13 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   if (const char* e = std::getenv("LGBM_B200_PART_GRID")) h->part_grid = std::max(1, std::atoi(e));
   // LGBM_B200_PDL=1 chains the split steps by programmatic dependent launch
   // (off by default: on the 10M-row binary workload it measured 8% slower)
-  if (const char* e = std::getenv("LGBM_B200_PDL")) h->use_pdl = std::atoi(e) != 0;
+  // programmatic dependent launch per kernel edge: bit 0 histogram (after
+  // the partition), bit 1 scan (after the histogram), bit 2 partition (after
+  // the scan); 1 alone means every edge
+  if (const char* e = std::getenv("LGBM_B200_PDL")) {
+    const int v = std::atoi(e);
+    h->use_pdl = v == 1 ? 7 : v;
+  }
   if (cfg->persistent_grow) {
     // one resident CTA group per slot: the cooperative launch holds every CTA
     const void* gk = grow_kernel(mode, h->hist_ng);
@@ -350,17 +356,20 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     if (ev) CU(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal));
     // the three launches of a step chain by programmatic dependent launch
     // (not when events are recorded between them)
-    const bool pdl = h->use_pdl && !h->timing;
+    const int pdl_edges = h->timing ? 0 : h->use_pdl;
+    const bool pdl = (pdl_edges & 1) != 0, pdl_scan = (pdl_edges & 2) != 0, pdl_part = (pdl_edges & 4) != 0;
     // fused form: only the root needs a histogram launch
     if (!h->fused || step == 0)
       CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
-    if (mode == LGBM_B200_HIST_QUANT) CU(launch_ex(k_scan<true>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl, c));
-    else CU(launch_ex(k_scan<false>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl, c));
+    if (mode == LGBM_B200_HIST_QUANT)
+      CU(launch_ex(k_scan<true>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+    else CU(launch_ex(k_scan<false>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
     if (h->fused)
-      CU(launch_ex(k_partition_fused, dim3(h->fused_grid, 1, K), dim3(512), fused_smem_bytes(), s, pdl, c, h->sub_rows));
-    else CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl, c));
+      CU(launch_ex(k_partition_fused, dim3(h->fused_grid, 1, K), dim3(512), fused_smem_bytes(), s, pdl_part, c,
+                   h->sub_rows));
+    else CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl_part, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {

@@ -195,7 +195,7 @@ struct LgbmB200Learner {
   DTileTable tiles{};
   int ntiles = 1;
   int hist_ng = 1;  // 32-feature groups per histogram tile
-  bool use_pdl = false;    // chain the per-step launches by programmatic dependent launch (measured slower)
+  int use_pdl = 0;  // kernel edges chained by programmatic dependent launch (bits: histogram, scan, partition)
   int grow_grid = 0;       // CTAs of the persistent grow launch
   size_t grow_smem = 0;
   GrowSync* grow_sync = nullptr;

@@ -488,6 +488,46 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   // cluster's CTAs in rank order (a cluster of one adds its own cells)
   if constexpr (kCl > 1) cg::this_cluster().sync();
   else __syncthreads();
+  if constexpr (kCl > 1 && kMode == 2) {
+    // the slice's sums are read from the cluster's shared memories first;
+    // once they are in registers this CTA arrives at the final barrier (its
+    // reads of the peers are complete: every value has been consumed), then
+    // issues its global atomics while the peers arrive
+    constexpr int kSlice = (kNG * kGroupCells + kCl - 1) / kCl;
+    constexpr int kPerThread = (kSlice + kHistThreads - 1) / kHistThreads;
+    const int total = ngroups * kGroupCells;
+    const int per = (total + kCl - 1) / kCl;
+    const int crank = (int)cg::this_cluster().block_rank();
+    const int lo = crank * per, hi = min(total, lo + per);
+    int64_t sg[kPerThread], sh[kPerThread];
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j) {
+      const int i = lo + (int)threadIdx.x + j * kHistThreads;
+      sg[j] = 0;
+      sh[j] = 0;
+      if (i < hi) {
+#pragma unroll
+        for (int r = 0; r < kCl; ++r) {
+          int64_t a, b;
+          cell_of(cg::this_cluster().map_shared_rank(cells, r), i, a, b);
+          sg[j] += a;
+          sh[j] += b;
+        }
+      }
+    }
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j) {
+      const int i = lo + (int)threadIdx.x + j * kHistThreads;
+      if (i < hi) emit(i, [&](int, int64_t& gv, int64_t& hv) {
+          gv = sg[j];
+          hv = sh[j];
+        });
+    }
+    // no CTA leaves (or reuses its cells) while another may still read them
+    asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
+    return;
+  }
   {
     const int total = ngroups * kGroupCells;
     const int per = (total + kCl - 1) / kCl;
