@@ -68,7 +68,7 @@ struct DSlotState {
   int32_t status;
   int32_t need_find;       // before_find_best_split of (left_leaf, right_leaf)
   int32_t left_leaf, right_leaf;
-  int32_t scan_counter;
+  int32_t scan_done;       // CTAs of a scan + partition launch whose scans are stored
   int32_t part_ticket;     // next row tile of the running partition
   int32_t part_done;       // partition CTAs finished
   int32_t part_left;       // rows sent left (posted by the last tile)

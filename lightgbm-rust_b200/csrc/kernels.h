@@ -9,6 +9,7 @@ namespace lgbm_b200 {
 
 constexpr int kHistThreads = 512;
 constexpr int kHistTileRows = kHistThreads;  // rows staged per histogram tile: one per thread
+constexpr int kPartThreads = 256;             // threads of a partition CTA
 constexpr int kHistCluster = 8;              // CTAs per quantized histogram cluster (one reduction per cluster)
 // CTAs per histogram cluster of a form: the float forms' CTAs fill an SM each and flush alone
 __host__ __device__ constexpr int hist_cluster(int mode) { return mode == 2 ? kHistCluster : 1; }
@@ -72,6 +73,28 @@ inline cudaError_t launch_ex(void (*kernel)(Params...), dim3 grid, dim3 block, s
 }
 template <bool kInt>
 __global__ void k_scan(const __grid_constant__ DCtx c);
+// The threshold scans and the partition of one step in one cooperative
+// launch (the CTAs wait for each other's scans; co-residency is required).
+template <bool kInt>
+__global__ void k_scan_partition(const __grid_constant__ DCtx c);
+
+// A cooperative launch (every CTA of the grid resident at once), capturable
+// in a CUDA graph.
+template <typename... Params, typename... Args>
+inline cudaError_t launch_coop(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                               Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Persistent tree growth (one cooperative launch per tree).
 constexpr int kGrowThreads = 512;

@@ -139,8 +139,20 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   // LGBM_B200_PART_GRID sets the partition's CTA count (launch-shape sweeps)
   if (const char* e = std::getenv("LGBM_B200_PART_GRID")) h->part_grid = std::max(1, std::atoi(e));
-  // LGBM_B200_PDL=1 chains the split steps by programmatic dependent launch
-  // (off by default: on the 10M-row binary workload it measured 8% slower)
+  // LGBM_B200_SCANPART=1: the threshold scans and the partition of a step run
+  // as one cooperative launch (one kernel boundary less per split); the
+  // grid is what stays resident at once, shared by the tree slots
+  h->scan_part = false;
+  if (const char* e = std::getenv("LGBM_B200_SCANPART"))
+    h->scan_part = std::atoi(e) != 0 && !h->fused && !cfg->persistent_grow;
+  if (h->scan_part) {
+    const void* k = mode == LGBM_B200_HIST_QUANT ? (const void*)k_scan_partition<true> : (const void*)k_scan_partition<false>;
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPartThreads, h->scan_smem));
+    const int K = std::max(1, cfg->num_tree_slots);
+    h->scan_part_grid = std::min(h->part_grid, per_sm * h->num_sms / K);
+    if (h->scan_part_grid < 1) return Status(LGBM_B200_ERR_UNSUPPORTED, "scan + partition launch does not fit");
+  }
   // programmatic dependent launch per kernel edge: bit 0 histogram (after
   // the partition), bit 1 scan (after the histogram), bit 2 partition (after
   // the scan); 1 alone means every edge
@@ -362,6 +374,14 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     if (!h->fused || step == 0)
       CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
+    if (h->scan_part) {  // scans and partition in one launch: the scan interval records as empty
+      if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
+      const dim3 g(h->scan_part_grid, 1, K);
+      if (mode == LGBM_B200_HIST_QUANT) CU(launch_coop(k_scan_partition<true>, g, dim3(kPartThreads), h->scan_smem, s, c));
+      else CU(launch_coop(k_scan_partition<false>, g, dim3(kPartThreads), h->scan_smem, s, c));
+      if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
+      continue;
+    }
     if (mode == LGBM_B200_HIST_QUANT)
       CU(launch_ex(k_scan<true>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
     else CU(launch_ex(k_scan<false>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
@@ -379,7 +399,8 @@ static Status enqueue_tree(LgbmB200Learner* h) {
     k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
     CU_LAUNCH();
   }
-  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : (h->fused ? 2 * (L - 1) + 1 : 3 * (L - 1))) +
+  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : ((h->fused || h->scan_part) ? 2 * (L - 1) + (h->fused ? 1 : 0)
+                                                                                   : 3 * (L - 1))) +
                      ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
   return Status();
 }

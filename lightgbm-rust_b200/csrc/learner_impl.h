@@ -234,6 +234,8 @@ struct LgbmB200Learner {
   int64_t last_part_rows = 0;
   bool fused = false;  // partition builds both children's histograms
   int fused_grid = 0;
+  bool scan_part = false;  // scans and partition of a step in one cooperative launch
+  int scan_part_grid = 0;
   int32_t last_launches = 0;
   // captured tree growth
   cudaGraphExec_t graph_exec = nullptr;

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->done = 0;
   st->status = kStatusOk;
   st->num_cat = 0;
-  st->scan_counter = 0;
+  st->scan_done = 0;
   st->part_ticket = 0;
   st->part_done = 0;
   st->hist_rows = 0;
@@ -1496,7 +1496,6 @@ template __global__ void k_scan<true>(const __grid_constant__ DCtx);
 // from the end (reversed). Tiles are claimed in order and chained with a
 // decoupled look-back on the running left count.
 // =====================================================================================
-constexpr int kPartThreads = 256;
 constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
 constexpr uint32_t kEpochMask = 0x7FFFFFFFu;
 constexpr unsigned long long kValueMask = (1ull << 31) - 1;
@@ -1734,23 +1733,25 @@ __device__ void decide_split(const DCtx& c, const DSlot& s, const StepHead& h, S
 // to the tree (tree.rs:240-297) and the children's ranges, smaller / larger
 // choice and before_find_best_split are recorded. Every other CTA of the
 // launch has exited, so none of them reads the state changed here.
-__device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& d, int32_t bl, int32_t R,
-                            int32_t total_left) {
+__device__ void finish_step(const DCtx& c, const DSlot& s, const StepHead& h, const SplitDecision& d, int32_t bl,
+                            int32_t R, int32_t cnt) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   DSlotState* st = s.st;
   const int32_t nf = c.num_features;
-  const bool need = st->need_find != 0;
-  const int32_t S = st->smaller.leaf, G = st->larger.leaf, Lft = st->left_leaf;
+  const bool need = h.need != 0;
+  const int32_t S = h.S, G = h.G, Lft = h.Lft;
   const bool have_larger = G >= 0;
   // the split's record, where the decision found it (not modified below)
   const DSplit& src = (need && bl == S)   ? s.feat_res[d.side_bf[0]]
                       : (need && bl == G) ? s.feat_res[nf + d.side_bf[1]]
                                           : s.best[bl];
-  // the tree update (thread 0) and the leaf bookkeeping (thread 32) write
-  // disjoint fields and read only what they load here, before the stores
-  // below: they run side by side
+  // Every warp starts at once: the stored records of the new leaves (warps 2
+  // and 3) and their splittable flags (warps 4 and up) are nothing the tree
+  // update (thread 0) or the leaf bookkeeping (thread 32) reads, and the
+  // split's record is read from the scan results when it is a new leaf's.
   ApplyIn ain;
   FinalizeIn fin;
+  int32_t total_left = 0;
   if (tid == 0) {
     ain = apply_load(c, s, src, bl);
     // the persisted record carries the penalized gain
@@ -1758,31 +1759,34 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
     else if (need && bl == G) ain.info.gain = d.side_bg[1];
   } else if (tid == 32) {
     fin = finalize_inputs(s, bl, R, src);
+    total_left = cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0;
   }
-  __syncthreads();
   if (need) {
-    for (int ff = tid; ff < nf; ff += blockDim.x) {
+    // one thread per feature: its flag is read before it is overwritten (the
+    // smaller leaf can be the left leaf whose flags are read)
+    for (int ff = tid - 128; tid >= 128 && ff < nf; ff += (int)blockDim.x - 128) {
       bool u = s.bytree[ff] && (!have_larger || s.splittable[Lft * nf + ff]);
       uint8_t ns = u ? s.feat_ok[ff] : 0;
       uint8_t ng = u ? s.feat_ok[nf + ff] : 0;
       s.splittable[S * nf + ff] = ns;
       if (have_larger) s.splittable[G * nf + ff] = ng;
     }
-    if (warp < 2 && (warp == 0 || have_larger)) {
-      const int32_t leaf = warp == 0 ? S : G;
-      const int32_t bf = d.side_bf[warp];
+    const int side = warp - 2;
+    if ((side == 0 || (side == 1 && have_larger))) {
+      const int32_t leaf = side == 0 ? S : G;
+      const int32_t bf = d.side_bf[side];
       DSplit& dst = s.best[leaf];
       if (bf >= 0) {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&s.feat_res[warp * nf + bf]);
+        const uint32_t* from = reinterpret_cast<const uint32_t*>(&s.feat_res[side * nf + bf]);
         uint32_t* w = reinterpret_cast<uint32_t*>(&dst);
-        for (int i = lane; i < (int)(sizeof(DSplit) / 4); i += 32) w[i] = src[i];
+        for (int i = lane; i < (int)(sizeof(DSplit) / 4); i += 32) w[i] = from[i];
         if (lane < kMaxBins / 16)
           reinterpret_cast<uint4*>(s.leaf_lut + (size_t)leaf * kMaxBins)[lane] =
-              reinterpret_cast<const uint4*>(s.lut_cand + ((size_t)warp * nf + bf) * kMaxBins)[lane];
+              reinterpret_cast<const uint4*>(s.lut_cand + ((size_t)side * nf + bf) * kMaxBins)[lane];
         __syncwarp();
         if (lane == 0) {
-          dst.gain = d.side_bg[warp];
-          s.bgain[leaf] = d.side_bg[warp];
+          dst.gain = d.side_bg[side];
+          s.bgain[leaf] = d.side_bg[side];
           s.bfeat[leaf] = dst.feature;
         }
       } else if (lane == 0) {
@@ -1800,6 +1804,10 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const SplitDecision& 
   } else if (tid == 32) {
     partition_finalize(c, s, bl, R, total_left, fin);
     st->part_epoch += 1;
+    // every CTA of the launch has passed its last use of the step counters
+    st->part_ticket = 0;
+    st->part_done = 0;
+    st->scan_done = 0;
   }
 }
 
@@ -1993,22 +2001,11 @@ __device__ __forceinline__ void zero_hist_buffer(const DCtx& c, const DSlot& s, 
   for (size_t i = (size_t)rank * blockDim.x + threadIdx.x; i < cells; i += (size_t)count * blockDim.x) h[i] = 0.0;
 }
 
-// Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
-// step's split decision and the goes-left LUT, then claims row tiles; the
-// last CTA to exit ends the step.
-__global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
-  pdl_wait();
-  pdl_trigger();
-  const DSlot& s = c.slots[blockIdx.z];
+// The partition of a step after the step fields are loaded and the first
+// ticket is claimed (in ps.tile).
+__device__ __forceinline__ void partition_body(const DCtx& c, const DSlot& s, PartShared& ps, const StepHead& h) {
   DSlotState* st = s.st;
-  __shared__ PartShared ps;
   const int tid = threadIdx.x;
-  // the step's fields and this CTA's first row tile, in one round trip (a
-  // finished tree's launch claims tickets nobody uses; the scan resets the
-  // counter before every partition of a live tree)
-  const StepHead h = load_step_head(st);
-  if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
-  if (h.done) return;
   const int32_t R = h.R;
   const SplitLeaf sl = partition_prologue(c, s, h, ps);
   const int32_t L = sl.L;
@@ -2027,9 +2024,65 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   __syncthreads();
   if (ps.last) {
     __threadfence();
-    finish_step(c, s, ps.dec, L, R, sl.cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+    finish_step(c, s, h, ps.dec, L, R, sl.cnt);
   }
 }
+
+// Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
+// step's split decision and the goes-left LUT, then claims row tiles; the
+// last CTA to exit ends the step.
+__global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constant__ DCtx c) {
+  pdl_wait();
+  pdl_trigger();
+  const DSlot& s = c.slots[blockIdx.z];
+  __shared__ PartShared ps;
+  // the step's fields and this CTA's first row tile, in one round trip (a
+  // finished tree's launch claims tickets nobody uses; the counter is reset
+  // before every partition of a live tree)
+  const StepHead h = load_step_head(s.st);
+  if (threadIdx.x == 0) ps.tile = atomicAdd(&s.st->part_ticket, 1);
+  if (h.done) return;
+  partition_body(c, s, ps, h);
+}
+
+// Threshold scans, then the partition, of one step (one cooperative launch):
+// CTA b scans items b, b + grid, ... ((feature, side) pairs), publishes them
+// on the slot's scan counter and waits until every CTA of the slot has done
+// so. The wait is bounded: past kSpinLimit polls the CTA records
+// kStatusTimeout (the host reports it) and carries on.
+template <bool kInt>
+__global__ void __launch_bounds__(kPartThreads) k_scan_partition(const __grid_constant__ DCtx c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  __shared__ PartShared ps;
+  const StepHead h = load_step_head(st);
+  if (threadIdx.x == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
+  if (h.done) return;  // no CTA of this launch sets done before every CTA has passed the wait below
+  const int nitems = 2 * c.num_features;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    scan_item<kInt>(c, s, it >> 1, it & 1, *reinterpret_cast<ScanSmem*>(smem_raw));
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&st->scan_done, 1);
+    int spins = 0;
+    while (*reinterpret_cast<volatile int32_t*>(&st->scan_done) < (int)gridDim.x) {
+      if (++spins > kSpinLimit) {
+        st->status = kStatusTimeout;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  partition_body(c, s, ps, h);
+}
+template __global__ void k_scan_partition<false>(const __grid_constant__ DCtx);
+template __global__ void k_scan_partition<true>(const __grid_constant__ DCtx);
+
 
 // =====================================================================================
 // Fused partition and histograms (quantized form, at most 32 features): the
@@ -2211,7 +2264,7 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
   __syncthreads();
   if (ps.last) {
     __threadfence();
-    finish_step(c, s, ps.dec, L, R, cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+    finish_step(c, s, hd, ps.dec, L, R, cnt);
   }
 }
 
@@ -2502,8 +2555,9 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     SplitLeaf sl;
     sl.L = -1;
     int32_t R = 0;
+    StepHead h = {};
     if (!*reinterpret_cast<volatile int32_t*>(&st->done)) {
-      const StepHead h = load_step_head(st);
+      h = load_step_head(st);
       R = h.R;
       sl = partition_prologue(c, s, h, ps);
       if (sl.L < 0) {
@@ -2517,7 +2571,7 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     mark(2);
     // F: bookkeeping of the step
     if (sl.L >= 0 && rank == 0)
-      finish_step(c, s, ps.dec, sl.L, R, sl.cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0);
+      finish_step(c, s, h, ps.dec, sl.L, R, sl.cnt);
     if (!grid_barrier(gs, G)) return;
     mark(3);
   }
