@@ -10,6 +10,10 @@ namespace lgbm_b200 {
 constexpr int kHistThreads = 512;
 constexpr int kHistTileRows = kHistThreads;  // rows staged per histogram tile: one per thread
 constexpr int kPartThreads = 256;             // threads of a partition CTA
+#ifndef LGBM_B200_PART_TILE_ROWS
+#define LGBM_B200_PART_TILE_ROWS 1024
+#endif
+constexpr int kPartTileRows = LGBM_B200_PART_TILE_ROWS;  // rows per partition tile (one look-back word each)
 constexpr int kHistCluster = 8;              // CTAs per quantized histogram cluster (one reduction per cluster)
 // CTAs per histogram cluster of a form: the float forms' CTAs fill an SM each and flush alone
 __host__ __device__ constexpr int hist_cluster(int mode) { return mode == 2 ? kHistCluster : 1; }

@@ -194,7 +194,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   CU(cudaMemcpy(feats_d, h->feats.data(), sizeof(DFeature) * nf, cudaMemcpyHostToDevice));
   const int K = h->K, L = h->L;
   const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
-  const size_t max_tiles = ((size_t)n + 2047) / 2048 + 1;
+  const size_t max_tiles = ((size_t)n + kPartTileRows - 1) / kPartTileRows + 1;
   h->slots_h.resize(K);
   for (int k = 0; k < K; ++k) {
     DSlot& d = h->slots_h[k];

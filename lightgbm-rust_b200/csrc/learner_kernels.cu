@@ -1820,7 +1820,6 @@ struct PartShared {
   SplitDecision dec;
 };
 
-constexpr int kPartTileRows = 2048;  // rows per partition tile (tile_status holds one word per tile)
 
 // The leaf a step splits: its rows and the feature its split tests.
 struct SplitLeaf {
@@ -1949,11 +1948,12 @@ __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32
 // per thread, blockDim.x * kItems == kPartTileRows), each chained to its
 // predecessors by a decoupled look-back on the left count. The CTA that
 // partitions the last tile posts the left count in st->part_left.
-// The leaf's row tiles, claimed in order from the ticket counter; with
-// `claimed` the CTA's first ticket is already in ps.tile.
+// With `claimed` the CTA's first ticket is already in ps.tile; the next one
+// is claimed while a tile runs and used after it.
 template <int kItems>
 __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, const SplitLeaf& sl, uint32_t epoch,
                                bool claimed) {
+  static_assert(kItems <= 32, "one goes-left bit per item");
   DSlotState* st = s.st;
   const int tid = threadIdx.x;
   const int32_t begin = sl.begin, cnt = sl.cnt, side = sl.side, inner = sl.inner;
@@ -1963,7 +1963,7 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, co
   const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
   const uint8_t* col = c.colbins + (size_t)inner * (size_t)c.num_data;
   const uint8_t* lut = ps.lut;
-  int32_t next = -1;  // thread 0: the ticket after the current tile, claimed while the tile runs
+  int32_t next = -1;  // thread 0: the ticket after the current tile (the counter is contended: used a tile later)
   while (true) {
     __syncthreads();
     if (tid == 0 && !claimed) ps.tile = next >= 0 ? next : atomicAdd(&st->part_ticket, 1);

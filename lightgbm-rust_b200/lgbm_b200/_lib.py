@@ -7,7 +7,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblgbm_b200.so")
+# LGBM_B200_LIB names another build of the library (for example one compiled
+# with a different partition tile size)
+LIB_PATH = os.environ.get("LGBM_B200_LIB") or os.path.join(_HERE, "liblgbm_b200.so")
 
 OK = 0
 ERR_INVALID_PARAMETER = 1
