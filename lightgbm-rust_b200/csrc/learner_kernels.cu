@@ -1976,17 +1976,25 @@ __device__ void partition_rows(const DCtx& c, const DSlot& s, PartShared& ps, co
     uint32_t rows[kItems];
     uint32_t flags = 0;
     int32_t nleft = 0;
+    // every row index first, then every byte of the split feature: each
+    // group of loads is in flight together
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-      int32_t pos = t0 + tid * kItems + k;
-      if (pos < cnt) {
-        uint32_t r = __ldcg(in + pos);
-        rows[k] = r;
-        uint32_t raw = col[r];
-        if (lut[raw]) {
-          flags |= 1u << k;
-          ++nleft;
-        }
+      const int32_t pos = t0 + tid * kItems + k;
+      rows[k] = pos < cnt ? __ldcg(in + pos) : 0u;
+    }
+    uint32_t raws[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      const int32_t pos = t0 + tid * kItems + k;
+      raws[k] = pos < cnt ? (uint32_t)col[rows[k]] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      const int32_t pos = t0 + tid * kItems + k;
+      if (pos < cnt && lut[raws[k]]) {
+        flags |= 1u << k;
+        ++nleft;
       }
     }
     tile_scatter<kItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out);
@@ -2339,8 +2347,47 @@ __device__ __forceinline__ int32_t leaf_rank_of(const LeafTable& t, int32_t p) {
   return lo;
 }
 
+// Each warp takes a contiguous share of the positions [0, t.total), in steps
+// of 32 (lane = offset), and follows the leaf boundaries as it goes: its
+// first leaf is found once by binary search, later ones by stepping the
+// rank. visit(q, rank, same) is called for every position q of the share;
+// same is true when q lies in the warp's current leaf, which the warp
+// leaves through end_leaf(rank) (warp-uniform) before moving on.
+template <class Visit, class EndLeaf>
+__device__ __forceinline__ void walk_leaf_positions(const LeafTable& t, Visit visit, EndLeaf end_leaf) {
+  const int lane = threadIdx.x & 31;
+  const int32_t nwarps = (int32_t)(gridDim.x * (blockDim.x >> 5));
+  const int32_t gw = (int32_t)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+  const int32_t per = ((t.total + nwarps - 1) / nwarps + 31) & ~31;
+  const int32_t p0 = min(t.total, gw * per), p1 = min(t.total, p0 + per);
+  if (p0 >= p1 || t.n == 0) return;
+  int32_t r = leaf_rank_of(t, p0);
+  int32_t end = r + 1 < t.n ? t.begin[r + 1] : t.total;  // first position past leaf r
+  for (int32_t p = p0; p < p1; p += 32) {
+    const int32_t q = p + lane;
+    if (p + 32 <= end && p + 32 <= p1) {  // the whole step lies in leaf r
+      visit(q, r, true);
+      continue;
+    }
+    if (q < p1) {
+      int32_t rq = r;
+      while (rq + 1 < t.n && t.begin[rq + 1] <= q) ++rq;
+      visit(q, rq, rq == r);
+    }
+    if (p + 32 < p1) {  // leaf r ended inside this step; the share goes on
+      end_leaf(r);
+      while (r + 1 < t.n && t.begin[r + 1] <= p + 32) ++r;
+      end = r + 1 < t.n ? t.begin[r + 1] : t.total;
+    }
+  }
+  end_leaf(r);
+}
+
 // FP64 (g, h) sums of each leaf's rows for the leaf renewal
-// (learner/mod.rs:736-747). Grid (G, 1, slots), 256 threads.
+// (learner/mod.rs:736-747). Grid (G, 1, slots), 256 threads. A lane sums its
+// positions of the warp's current leaf in registers; the warp adds them to
+// the leaf's total when it leaves the leaf (positions of leaves shorter than
+// a step add theirs at once).
 __global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* sums /*[slots][leaves][2]*/) {
   extern __shared__ int32_t lt_smem[];
   const DSlot& s = c.slots[blockIdx.z];
@@ -2348,32 +2395,28 @@ __global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx 
   const LeafTable t = build_leaf_table(s, nl, lt_smem);
   const int lane = threadIdx.x & 31;
   double* base = sums + (size_t)blockIdx.z * c.p.num_leaves * 2;
-  // whole warps step together so that a warp can reduce before its atomics
-  const int32_t stride = gridDim.x * blockDim.x;
-  for (int32_t p0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); p0 < t.total; p0 += stride) {
-    const int32_t p = p0 + lane;
-    int32_t leaf = -1;
-    double g = 0.0, h = 0.0;
-    if (p < t.total) {
-      const int32_t r = leaf_rank_of(t, p);
-      leaf = t.leaf[r];
-      const float2 v = s.gh[s.idx[t.side[r]][p]];
-      g = (double)v.x;
-      h = (double)v.y;
-    }
-    const int32_t first = __shfl_sync(0xffffffffu, leaf, 0);
-    if (__all_sync(0xffffffffu, leaf == first || leaf < 0)) {
-      g = warp_sum_d(g);
-      h = warp_sum_d(h);
-      if (lane == 0 && first >= 0) {
-        atomicAdd(base + 2 * first, g);
-        atomicAdd(base + 2 * first + 1, h);
-      }
-    } else if (leaf >= 0) {
-      atomicAdd(base + 2 * leaf, g);
-      atomicAdd(base + 2 * leaf + 1, h);
-    }
-  }
+  double g = 0.0, h = 0.0;
+  walk_leaf_positions(
+      t,
+      [&](int32_t q, int32_t rank, bool same) {
+        const float2 v = s.gh[s.idx[t.side[rank]][q]];
+        if (same) {
+          g += (double)v.x;
+          h += (double)v.y;
+        } else {
+          atomicAdd(base + 2 * t.leaf[rank], (double)v.x);
+          atomicAdd(base + 2 * t.leaf[rank] + 1, (double)v.y);
+        }
+      },
+      [&](int32_t rank) {
+        const double sg = warp_sum_d(g), sh = warp_sum_d(h);
+        if (lane == 0) {
+          atomicAdd(base + 2 * t.leaf[rank], sg);
+          atomicAdd(base + 2 * t.leaf[rank] + 1, sh);
+        }
+        g = 0.0;
+        h = 0.0;
+      });
 }
 
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums) {
@@ -2395,10 +2438,8 @@ __global__ void __launch_bounds__(256) k_add_leaf_outputs(const __grid_constant_
   const LeafTable t = build_leaf_table(s, nl, lt_smem);
   const double* lv = leaf_values + (size_t)blockIdx.z * lv_stride;
   double* sc = score + (size_t)blockIdx.z * score_stride;
-  for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < t.total; p += gridDim.x * blockDim.x) {
-    const int32_t r = leaf_rank_of(t, p);
-    sc[s.idx[t.side[r]][p]] += lv[t.leaf[r]];
-  }
+  walk_leaf_positions(
+      t, [&](int32_t q, int32_t rank, bool) { sc[s.idx[t.side[rank]][q]] += lv[t.leaf[rank]]; }, [](int32_t) {});
 }
 
 // Binned tree walk (tree.rs:588-633) for rows `rows` (or 0..n): score += leaf value.
