@@ -76,12 +76,35 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
                        : reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
   for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h0[i] = 0.0;
 
-  // deterministic partial sums over this block's contiguous chunk
-  int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  int64_t b0 = (int64_t)blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  // deterministic partial sums over this block's contiguous chunk (a
+  // multiple of 8 rows, so that the in-order loops below load 16-byte
+  // aligned groups)
+  const int64_t chunk = ((n + gridDim.x - 1) / gridDim.x + 7) & ~(int64_t)7;
+  const int64_t b0 = min(n, (int64_t)blockIdx.x * chunk), b1 = min(n, b0 + chunk);
   double sg = 0.0, sh = 0.0;
   long long si = 0;
-  if (c.hist_mode == LGBM_B200_HIST_QUANT) {
+  if (c.hist_mode == LGBM_B200_HIST_QUANT && !bag) {
+    // rows in order: eight packed values per thread and iteration
+    const double gsc = s.st->grad_scale, hsc = s.st->hess_scale;
+    for (int64_t i = b0 + 8 * (int64_t)tid; i < b1; i += 8 * (int64_t)blockDim.x) {
+      int32_t w[8];
+      if (i + 8 <= b1) {
+        const int4 a = *reinterpret_cast<const int4*>(s.packed + i);
+        const int4 b = *reinterpret_cast<const int4*>(s.packed + i + 4);
+        w[0] = a.x, w[1] = a.y, w[2] = a.z, w[3] = a.w, w[4] = b.x, w[5] = b.y, w[6] = b.z, w[7] = b.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) w[j] = i + j < b1 ? s.packed[i + j] : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int64_t gq = (int64_t)(w[j] >> 16), hq = (int64_t)(w[j] & 0xFFFF);
+        si += (long long)((uint64_t)(gq << 32) + (uint64_t)hq);
+        sg += (double)(w[j] >> 16) * gsc;
+        sh += (double)(w[j] & 0xFFFF) * hsc;
+      }
+    }
+  } else if (c.hist_mode == LGBM_B200_HIST_QUANT) {
     for (int64_t i = b0 + tid; i < b1; i += blockDim.x) {
       // quant.rs:452-477: the bag variant sums packed values by position
       int64_t r = (c.bagging) ? i : (int64_t)(bag ? bag[i] : (uint32_t)i);
@@ -95,6 +118,26 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
       } else {
         sg += (double)(w >> 16) * s.st->grad_scale;
         sh += (double)(w & 0xFFFF) * s.st->hess_scale;
+      }
+    }
+  } else if (!bag && (reinterpret_cast<uintptr_t>(s.gh) & 15) == 0) {
+    // rows in order: four (g, h) pairs per thread and iteration (a slot's
+    // pairs start 16-byte aligned unless the row count is odd)
+    for (int64_t i = b0 + 4 * (int64_t)tid; i < b1; i += 4 * (int64_t)blockDim.x) {
+      float2 v[4];
+      if (i + 4 <= b1) {
+        const float4 a = *reinterpret_cast<const float4*>(s.gh + i);
+        const float4 b = *reinterpret_cast<const float4*>(s.gh + i + 2);
+        v[0] = make_float2(a.x, a.y), v[1] = make_float2(a.z, a.w), v[2] = make_float2(b.x, b.y),
+        v[3] = make_float2(b.z, b.w);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = i + j < b1 ? s.gh[i + j] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        sg += (double)v[j].x;
+        sh += (double)v[j].y;
       }
     }
   } else {

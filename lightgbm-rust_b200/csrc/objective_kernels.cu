@@ -122,7 +122,8 @@ __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n
     double g = (double)v.x;
     double rg = 0.5, rh = 0.5;
     if (stochastic) {
-      int64_t pos = (i + start) % n;
+      int64_t pos = i + start;  // (i + start) mod n, with i, start < n
+      if (pos >= n) pos -= n;
       rg = grv[pos];
       rh = hrv[pos];
     }
