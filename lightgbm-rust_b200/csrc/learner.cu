@@ -117,7 +117,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     if (clusters < 1) return Status(LGBM_B200_ERR_CUDA, "histogram cluster does not fit on the device");
     h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
   }
-  h->part_grid = h->num_sms * 2;  // 2 CTAs per SM measured best (4 and 8 per SM are slower)
+  h->part_grid = h->num_sms * 3;  // 3 CTAs per SM measured best with 1024-row tiles (2 and 2.5 per SM are slower)
   // LGBM_B200_FUSED=1: the quantized form with at most 32 features builds
   // both children's histograms inside the partition. Off by default: on the
   // 10M-row binary workload it measured slower (the first, largest splits
