@@ -14,7 +14,10 @@ constexpr int kPartThreads = 256;             // threads of a partition CTA
 #define LGBM_B200_PART_TILE_ROWS 1024
 #endif
 constexpr int kPartTileRows = LGBM_B200_PART_TILE_ROWS;  // rows per partition tile (one look-back word each)
-constexpr int kHistCluster = 8;              // CTAs per quantized histogram cluster (one reduction per cluster)
+#ifndef LGBM_B200_HIST_CLUSTER
+#define LGBM_B200_HIST_CLUSTER 8
+#endif
+constexpr int kHistCluster = LGBM_B200_HIST_CLUSTER;  // CTAs per quantized histogram cluster (one reduction each)
 // CTAs per histogram cluster of a form: the float forms' CTAs fill an SM each and flush alone
 __host__ __device__ constexpr int hist_cluster(int mode) { return mode == 2 ? kHistCluster : 1; }
 constexpr int kMaxTiles = 64;

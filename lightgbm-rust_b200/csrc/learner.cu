@@ -98,6 +98,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   // kernel attributes and grid sizes
   const void* hk = hist_kernel(mode, h->hist_ng);
   CU(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->hist_smem));
+  // clusters above 8 CTAs are a non-portable size the kernel must opt into
+  if (hist_cluster(mode) > 8) CU(cudaFuncSetAttribute(hk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   h->scan_smem = sizeof(ScanSmem);
   // the per-position leaf kernels hold a 16-byte table entry per leaf
   CU(cudaFuncSetAttribute(k_leaf_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
