@@ -300,6 +300,7 @@ struct GradWorkspace {
   std::mutex mu;
   int device = -1;
   cudaStream_t stream = nullptr;
+  ChunkStreams chunks;  // row chunks of the elementwise objectives
   DeviceArena arena;
   size_t cap = 0;
   float* label = nullptr;
@@ -354,7 +355,8 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
     w.arena.free_all();
     w.cap = 0;
     if (w.stream) cudaStreamDestroy(w.stream);
-    if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess)
+    w.chunks.release();
+    if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess || !w.chunks.init())
       return fail(Status(LGBM_B200_ERR_CUDA, "stream"));
     w.device = device;
   }
@@ -369,6 +371,33 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
     w.cap = nk;
   }
   cudaStream_t s = w.stream;
+  if (k == 1 && (cfg->objective == LGBM_B200_OBJ_BINARY || cfg->objective == LGBM_B200_OBJ_REGRESSION)) {
+    // one value per row: chunks of rows, each chunk's copies in, kernel and
+    // copies out on one of three streams, so that copies in and out of
+    // different chunks overlap
+    cudaError_t e = cudaSuccess;
+    for (int64_t r0 = 0, c = 0; r0 < num_data && e == cudaSuccess; r0 += ChunkStreams::kRows, ++c) {
+      const int64_t m = std::min<int64_t>(ChunkStreams::kRows, num_data - r0);
+      cudaStream_t cs = w.chunks.s[c % ChunkStreams::kN];
+      e = cudaMemcpyAsync(w.label + r0, label + r0, sizeof(float) * m, cudaMemcpyHostToDevice, cs);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(w.score + r0, scores + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
+      if (e == cudaSuccess) {
+        Status st = launch_gradients(*cfg, w.label + r0, w.score + r0, m, nullptr, w.g + r0, w.h + r0, 148, cs, rk);
+        if (!st.ok()) {
+          w.chunks.sync();
+          return fail(st);
+        }
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(grad + r0, w.g + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hess + r0, w.h + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+    }
+    cudaError_t e2 = w.chunks.sync();
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+    return LGBM_B200_OK;
+  }
   cudaMemcpyAsync(w.label, label, sizeof(float) * n, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(w.score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
   Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, 148, s, rk);

@@ -123,6 +123,8 @@ __global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* sums);
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums);
 __global__ void k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
                                    int64_t score_stride);
+__global__ void k_leaf_of_row(const __grid_constant__ DCtx c, int32_t* leaf_of_row);
+__global__ void k_add_by_row(const int32_t* leaf_of_row, const double* leaf_values, double* score, int64_t n);
 __global__ void k_add_tree_binned(const __grid_constant__ DCtx c, const uint8_t* bins, int32_t stride, const uint32_t* rows, int64_t n,
                                   const double* leaf_values, int32_t lv_stride, double* score, int64_t score_stride);
 

@@ -104,6 +104,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   // the per-position leaf kernels hold a 16-byte table entry per leaf
   CU(cudaFuncSetAttribute(k_leaf_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
   CU(cudaFuncSetAttribute(k_add_leaf_outputs, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
+  CU(cudaFuncSetAttribute(k_leaf_of_row, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
   CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
   {
@@ -756,26 +757,48 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
   for (int l = 0; l < std::min(num_leaves, L); ++l) lv[l] = leaf_values[l];
   double* lvd = h->leaf_values_dev + (size_t)slot * L;
   cudaError_t e = cudaMemcpyAsync(lvd, lv.data(), sizeof(double) * L, cudaMemcpyHostToDevice, s);
-  double* sc = score;
-  double* tmp = nullptr;
-  if (e == cudaSuccess && location == LGBM_B200_HOST) {
-    // a staging buffer kept for the learner's lifetime: a pool allocation
-    // per call would be unmapped and mapped again around every synchronisation
-    if (!h->score_stage) {
-      Status st = h->arena.alloc_n(&h->score_stage, (size_t)n);
-      if (!st.ok()) return fail(st);
-    }
-    tmp = h->score_stage;
-    e = cudaMemcpyAsync(tmp, score, sizeof(double) * n, cudaMemcpyHostToDevice, s);
-    sc = tmp;
-  }
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   // launch only over this slot: grid.z = 1 with a context whose slots start at `slot`
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
-  k_add_leaf_outputs<<<dim3(h->num_sms * 4, 1, 1), 256, 16 * (size_t)L, s>>>(c, lvd, 0, sc, 0);
+  if (location == LGBM_B200_HOST) {
+    // Host scores: the leaf of every row is found first (in row order), then
+    // the scores go through the device in chunks of rows, each chunk's copy
+    // in, update and copy out on one of three streams, so that copies in and
+    // out of different chunks overlap. The buffers are kept for the learner's
+    // lifetime (a pool allocation per call would be mapped again each time).
+    Status st;
+    if (!h->score_stage) st = h->arena.alloc_n(&h->score_stage, (size_t)n);
+    if (st.ok() && !h->leaf_of_row) st = h->arena.alloc_n(&h->leaf_of_row, (size_t)n);
+    if (!st.ok()) return fail(st);
+    if (!h->chunks.init()) return fail(Status(LGBM_B200_ERR_CUDA, "chunk streams"));
+    e = cudaMemsetAsync(h->leaf_of_row, 0xFF, sizeof(int32_t) * n, s);  // -1: out of the bag
+    if (e == cudaSuccess) {
+      k_leaf_of_row<<<h->num_sms * 4, 256, 16 * (size_t)L, s>>>(c, h->leaf_of_row);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->chunks.ready, s);
+    for (int64_t r0 = 0, k = 0; r0 < n && e == cudaSuccess; r0 += ChunkStreams::kRows, ++k) {
+      const int64_t m = std::min<int64_t>(ChunkStreams::kRows, n - r0);
+      cudaStream_t cs = h->chunks.s[k % ChunkStreams::kN];
+      e = cudaStreamWaitEvent(cs, h->chunks.ready, 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->score_stage + r0, score + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
+      if (e == cudaSuccess) {
+        const int blocks = (int)std::min<int64_t>((m + 255) / 256, (int64_t)h->num_sms * 8);
+        k_add_by_row<<<blocks, 256, 0, cs>>>(h->leaf_of_row + r0, lvd, h->score_stage + r0, m);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(score + r0, h->score_stage + r0, sizeof(double) * m, cudaMemcpyDeviceToHost, cs);
+    }
+    cudaError_t e2 = h->chunks.sync();
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+    return LGBM_B200_OK;
+  }
+  k_add_leaf_outputs<<<dim3(h->num_sms * 4, 1, 1), 256, 16 * (size_t)L, s>>>(c, lvd, 0, score, 0);
   e = cudaGetLastError();
-  if (e == cudaSuccess && tmp) e = cudaMemcpyAsync(score, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   return LGBM_B200_OK;

@@ -180,6 +180,37 @@ struct HostTree {  // the reference's Tree arrays for one trained tree
 
 using namespace lgbm_b200;
 
+// Streams over which a call with host buffers pipelines its row chunks: the
+// copy in, the kernel and the copy out of successive chunks overlap (the two
+// copy directions run on separate copy engines).
+struct ChunkStreams {
+  static constexpr int kN = 3;
+  static constexpr int64_t kRows = 1 << 20;  // rows per chunk
+  cudaStream_t s[kN] = {};
+  cudaEvent_t ready = nullptr;  // recorded on the caller's stream: the chunks start after it
+  bool init() {
+    if (ready) return true;
+    for (int i = 0; i < kN; ++i)
+      if (cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking) != cudaSuccess) return false;
+    return cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess;
+  }
+  cudaError_t sync() {
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < kN; ++i) {
+      cudaError_t ei = s[i] ? cudaStreamSynchronize(s[i]) : cudaSuccess;
+      if (e == cudaSuccess) e = ei;
+    }
+    return e;
+  }
+  void release() {
+    for (int i = 0; i < kN; ++i)
+      if (s[i]) cudaStreamDestroy(s[i]);
+    if (ready) cudaEventDestroy(ready);
+    for (int i = 0; i < kN; ++i) s[i] = nullptr;
+    ready = nullptr;
+  }
+};
+
 struct LgbmB200Learner {
   LgbmB200LearnerConfig cfg{};
   int device = 0;
@@ -221,6 +252,8 @@ struct LgbmB200Learner {
   double* leaf_values_dev = nullptr;  // [K][L] for add_leaf_outputs
   double* score_scratch = nullptr;  // host gradients staged for train (2 x num_data floats)
   double* score_stage = nullptr;    // host scores staged for add_leaf_outputs (num_data doubles)
+  int32_t* leaf_of_row = nullptr;   // leaf of each in-bag row (-1 out of bag), for add_leaf_outputs from host
+  ChunkStreams chunks;              // add_leaf_outputs from host buffers
   // readback
   std::vector<DSlotState> st_h;
   std::vector<HostTree> trees;
@@ -246,6 +279,7 @@ struct LgbmB200Learner {
     for (auto e : marks)
       if (e) cudaEventDestroy(e);
     arena.free_all();
+    chunks.release();
     if (stream) cudaStreamDestroy(stream);
   }
 };

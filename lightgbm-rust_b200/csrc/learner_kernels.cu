@@ -2485,6 +2485,28 @@ __global__ void __launch_bounds__(256) k_add_leaf_outputs(const __grid_constant_
       t, [&](int32_t q, int32_t rank, bool) { sc[s.idx[t.side[rank]][q]] += lv[t.leaf[rank]]; }, [](int32_t) {});
 }
 
+// The leaf of every in-bag row, in row order, for the score update from host
+// buffers (rows out of the bag keep -1). Grid (G, 1, 1), 256 threads, the
+// slot in c.slots[0].
+__global__ void __launch_bounds__(256) k_leaf_of_row(const __grid_constant__ DCtx c, int32_t* leaf_of_row) {
+  extern __shared__ int32_t lt_smem[];
+  const DSlot& s = c.slots[0];
+  const LeafTable t = build_leaf_table(s, s.st->num_leaves_cur, lt_smem);
+  walk_leaf_positions(
+      t, [&](int32_t q, int32_t rank, bool) { leaf_of_row[s.idx[t.side[rank]][q]] = t.leaf[rank]; },
+      [](int32_t) {});
+}
+
+// score[r] += leaf_values[leaf_of_row[r]] for rows [0, n) of a chunk
+// (partition.rs:178-191 in row order).
+__global__ void __launch_bounds__(256) k_add_by_row(const int32_t* leaf_of_row, const double* leaf_values,
+                                                    double* score, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t l = leaf_of_row[i];
+    if (l >= 0) score[i] += leaf_values[l];
+  }
+}
+
 // Binned tree walk (tree.rs:588-633) for rows `rows` (or 0..n): score += leaf value.
 __global__ void __launch_bounds__(256) k_add_tree_binned(const __grid_constant__ DCtx c, const uint8_t* bins, int32_t stride,
                                                          const uint32_t* rows, int64_t n, const double* leaf_values,

@@ -1,0 +1,55 @@
+"""The calls with host buffers that stream rows through the device in chunks
+of 1M rows (the gradients of objectives with one value per row, and the
+learner's score update), at sizes that take several chunks, one of them
+partial."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _ulps(a, b):
+    return np.abs(a.view(np.int32).astype(np.int64) - b.view(np.int32).astype(np.int64))
+
+
+def test_gradients_several_chunks(lgb, orc):
+    rng = np.random.default_rng(41)
+    n = 2_600_000
+    s = rng.standard_normal(n) * 3
+    yb = (rng.random(n) < 0.4).astype(np.float32)
+    for params, y in (({"objective": "binary"}, yb), ({"objective": "regression"}, rng.standard_normal(n))):
+        p = lgb.resolve_params(params)
+        for _ in range(2):  # the chunk streams are reused by the next call
+            g, h = lgb.gradients(params, y, s)
+            og, oh = orc.gradients(p, y, s)
+            # exp is not correctly rounded on either side: allow one f32 ulp
+            for a, o in ((g, og), (h, oh)):
+                u = _ulps(a, o)
+                assert u.max() <= 1, (params, u.max())
+                assert np.mean(u == 0) > 0.99
+
+
+@pytest.mark.parametrize("bagged", [False, True])
+def test_add_leaf_outputs_several_chunks(lgb, bagged):
+    rng = np.random.default_rng(42)
+    n = 2_300_000
+    X = rng.standard_normal((n, 6)).astype(np.float32)
+    y = (X[:, 0] + 0.5 * X[:, 1] > 0).astype(np.float32)
+    params = {"objective": "binary", "num_leaves": 31, "min_data_in_leaf": 20}
+    ds = lgb.Dataset(X, y, params=params).construct()
+    learner = lgb.Learner(ds, params)
+    if bagged:  # rows out of the bag keep their scores
+        learner.set_bagging(np.sort(rng.choice(n, int(0.7 * n), replace=False)).astype(np.uint32))
+    g, h = lgb.gradients(params, y, np.zeros(n))
+    tree = learner.train(g, h)[0]
+    nl = int(tree["num_leaves"])
+    beg, cnt, idx = learner.partition(0, nl)
+    score = rng.standard_normal(n)
+    for _ in range(2):
+        lv = rng.standard_normal(nl)
+        want = score.copy()
+        for leaf in range(nl):
+            rows = idx[beg[leaf]:beg[leaf] + cnt[leaf]]
+            want[rows] += lv[leaf]
+        learner.add_leaf_outputs(0, lv, score)
+        assert np.array_equal(score, want)  # one FP64 add per row: bit-exact
