@@ -321,8 +321,16 @@ def run_workload(args):
     ds = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=params,
                      categorical_feature=d.get("categorical")).construct(params)
     build_s = time.perf_counter() - t0
+    # the same dataset with its rows binned on the device (identical bytes)
+    t0 = time.perf_counter()
+    ds_dev = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=dict(params, device_binning=True),
+                         categorical_feature=d.get("categorical")).construct(dict(params, device_binning=True))
+    build_dev_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ds.binned()["bins"], ds_dev.binned()["bins"]))
+    del ds_dev
     out = {"workload": d["name"], "rows": int(len(d["y"])), "features": int(d["X"].shape[1]),
-           "rounds_in_config": d["num_rounds"], "dataset_build_s": build_s, "forms": {}}
+           "rounds_in_config": d["num_rounds"], "dataset_build_s": build_s,
+           "dataset_build_device_binning_s": build_dev_s, "device_binning_identical": same, "forms": {}}
     for form in forms:
         p = dict(params, hist_precision=form, num_threads=os.cpu_count() or 8)
         if form == "quantized":

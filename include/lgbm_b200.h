@@ -100,6 +100,17 @@ int lgbm_b200_dataset_create(const float* X, int64_t n, int32_t ncol, const Lgbm
 /* Dataset::from_dense_with_reference (dataset.rs:446): bins with `ref`'s mappers. */
 int lgbm_b200_dataset_create_valid(const float* X, int64_t n, int32_t ncol, const LgbmB200Dataset* ref,
                                    LgbmB200Dataset** out);
+/* The same two builds with the rows binned on CUDA device `device`
+ * (value_to_bin, binning.rs:637-667, and the group push,
+ * feature_group.rs:144-154, as a kernel over every row and used feature).
+ * The bin mappers are still found on the host from the row sample, and the
+ * resulting dataset is identical, byte for byte, to the host build's. Fails
+ * with LGBM_B200_ERR_UNSUPPORTED when a categorical feature holds a category
+ * value of 2^22 or more (the device keeps a dense table per feature). */
+int lgbm_b200_dataset_create_device(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams* params,
+                                    int32_t device, LgbmB200Dataset** out);
+int lgbm_b200_dataset_create_valid_device(const float* X, int64_t n, int32_t ncol, const LgbmB200Dataset* ref,
+                                          int32_t device, LgbmB200Dataset** out);
 /* The view points into the dataset; valid until lgbm_b200_dataset_free. */
 int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out);
 void lgbm_b200_dataset_free(LgbmB200Dataset* ds);

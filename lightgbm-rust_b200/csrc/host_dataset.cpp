@@ -378,7 +378,7 @@ static void push_bins(Dataset& d, const float* X, int64_t n, int32_t ncol) {
   }
 }
 
-Status build_dataset(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams& p, Dataset& d) {
+Status build_dataset(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams& p, Dataset& d, int device) {
   if (n <= 0 || ncol <= 0) return Status(LGBM_B200_ERR_INVALID_DATA, "empty matrix");
   if (n > INT32_MAX) return Status(LGBM_B200_ERR_INVALID_DATA, "more than 2^31-1 rows");
   std::vector<char> is_cat((size_t)ncol, 0);
@@ -448,17 +448,19 @@ Status build_dataset(const float* X, int64_t n, int32_t ncol, const LgbmB200BinP
     if (s[0] + s[1] <= total + max_conflict)
       return Status(LGBM_B200_ERR_UNSUPPORTED, "features could be bundled (exclusive feature bundling)");
   }
+  if (device >= 0) return push_bins_device(d, X, n, ncol, device);
   push_bins(d, X, n, ncol);
   return Status();
 }
 
-Status build_valid_dataset(const float* X, int64_t n, int32_t ncol, const Dataset& ref, Dataset& d) {
+Status build_valid_dataset(const float* X, int64_t n, int32_t ncol, const Dataset& ref, Dataset& d, int device) {
   if (ncol != ref.num_total_features)
     return Status(LGBM_B200_ERR_INVALID_DATA, "validation data has a different number of columns");
   d.num_data = n;
   d.num_total_features = ncol;
   d.used = ref.used;
   d.mappers = ref.mappers;
+  if (device >= 0) return push_bins_device(d, X, n, ncol, device);
   push_bins(d, X, n, ncol);
   return Status();
 }

@@ -667,6 +667,26 @@ int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out) {
   return LGBM_B200_OK;
 }
 
+int lgbm_b200_dataset_create_device(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams* params,
+                                    int32_t device, LgbmB200Dataset** out) {
+  if (!X || !params || !out || device < 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  auto d = std::make_unique<Dataset>();
+  Status s = build_dataset(X, n, ncol, *params, *d, device);
+  if (!s.ok()) return fail(s);
+  *out = reinterpret_cast<LgbmB200Dataset*>(d.release());
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_dataset_create_valid_device(const float* X, int64_t n, int32_t ncol, const LgbmB200Dataset* ref,
+                                          int32_t device, LgbmB200Dataset** out) {
+  if (!X || !ref || !out || device < 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  auto d = std::make_unique<Dataset>();
+  Status s = build_valid_dataset(X, n, ncol, *reinterpret_cast<const Dataset*>(ref), *d, device);
+  if (!s.ok()) return fail(s);
+  *out = reinterpret_cast<LgbmB200Dataset*>(d.release());
+  return LGBM_B200_OK;
+}
+
 void lgbm_b200_dataset_free(LgbmB200Dataset* ds) { delete reinterpret_cast<Dataset*>(ds); }
 
 int lgbm_b200_learner_create(const LgbmB200LearnerConfig* cfg, const uint8_t* bins, int64_t num_data,

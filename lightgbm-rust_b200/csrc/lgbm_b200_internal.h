@@ -49,7 +49,13 @@ struct Dataset {
   void fill_view(LgbmB200DatasetView* v);
 };
 
-Status build_dataset(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams& p, Dataset& d);
-Status build_valid_dataset(const float* X, int64_t n, int32_t ncol, const Dataset& ref, Dataset& d);
+// device < 0: the rows are binned on the host; else on that CUDA device
+// (the bin mappers come from the host's row sample either way)
+Status build_dataset(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams& p, Dataset& d,
+                     int device = -1);
+Status build_valid_dataset(const float* X, int64_t n, int32_t ncol, const Dataset& ref, Dataset& d,
+                           int device = -1);
+// The rows of X binned with d's mappers on `device` into d.bins (binning_kernels.cu).
+Status push_bins_device(Dataset& d, const float* X, int64_t n, int32_t ncol, int device);
 
 }  // namespace lgbm_b200

@@ -93,6 +93,8 @@ SIGNATURES = {
     "lgbm_b200_version": (C.c_char_p, []),
     "lgbm_b200_dataset_create": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, P(C.c_void_p)]),
+    "lgbm_b200_dataset_create_device": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), i32, P(C.c_void_p)]),
+    "lgbm_b200_dataset_create_valid_device": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_view": (C.c_int, [C.c_void_p, P(DatasetView)]),
     "lgbm_b200_dataset_free": (None, [C.c_void_p]),
     "lgbm_b200_learner_create": (C.c_int, [P(LearnerConfig), u8p, i64, i32, P(FeatureMeta), P(f64), P(i64),

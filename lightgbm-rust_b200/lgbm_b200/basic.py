@@ -26,6 +26,7 @@ DEFAULTS = {
     "categorical_feature": None,
     # B200 path knobs
     "hist_precision": "f64", "device": 0, "use_cuda_graph": True, "hist_rows_per_block": 0, "persistent_grow": False,
+    "device_binning": False,
 }
 
 ALIASES = {
@@ -99,10 +100,17 @@ class Dataset:
         lib = L.lib()
         n, ncol = self.data.shape
         h = C.c_void_p()
+        # device_binning: the rows are binned on the CUDA device `device` (the
+        # same dataset, byte for byte; the mappers still come from the host)
+        dev = int(p["device"]) if p.get("device_binning") else -1
         if self.reference is not None:
             self.reference.construct(params)
-            L.check(lib.lgbm_b200_dataset_create_valid(_ptr(self.data, C.c_float), n, ncol, self.reference._handle,
-                                                       C.byref(h)))
+            if dev >= 0:
+                L.check(lib.lgbm_b200_dataset_create_valid_device(_ptr(self.data, C.c_float), n, ncol,
+                                                                  self.reference._handle, dev, C.byref(h)))
+            else:
+                L.check(lib.lgbm_b200_dataset_create_valid(_ptr(self.data, C.c_float), n, ncol,
+                                                           self.reference._handle, C.byref(h)))
         else:
             cats = np.asarray(self.categorical_feature or p.get("categorical_feature") or [], dtype=np.int32)
             bp = L.BinParams(int(p["max_bin"]), int(p["min_data_in_bin"]), int(p["min_data_in_leaf"]),
@@ -110,7 +118,11 @@ class Dataset:
                              int(p["zero_as_missing"]), int(p["feature_pre_filter"]),
                              _ptr(cats, C.c_int32) if len(cats) else None, len(cats))
             self._cats = cats
-            L.check(lib.lgbm_b200_dataset_create(_ptr(self.data, C.c_float), n, ncol, C.byref(bp), C.byref(h)))
+            if dev >= 0:
+                L.check(lib.lgbm_b200_dataset_create_device(_ptr(self.data, C.c_float), n, ncol, C.byref(bp), dev,
+                                                            C.byref(h)))
+            else:
+                L.check(lib.lgbm_b200_dataset_create(_ptr(self.data, C.c_float), n, ncol, C.byref(bp), C.byref(h)))
         self._handle = h
         v = L.DatasetView()
         L.check(lib.lgbm_b200_dataset_view(h, C.byref(v)))
