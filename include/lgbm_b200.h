@@ -116,6 +116,36 @@ int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out);
 void lgbm_b200_dataset_free(LgbmB200Dataset* ds);
 
 /* ------------------------------------------------------------------------
+ * Evaluation metrics on the device (Metric::eval, metric.rs:520-770), so
+ * that validation scores kept on the device need not be copied back every
+ * iteration. Unweighted labels. AUC (metric.rs:701-731) is exact and equals
+ * the reference's value bit for bit; the loss metrics are FP64 means whose
+ * summation order differs from the reference's sequential loop.
+ * ------------------------------------------------------------------------ */
+enum {
+  LGBM_B200_METRIC_AUC = 0,
+  LGBM_B200_METRIC_BINARY_LOGLOSS = 1, /* on 1 / (1 + exp(-sigmoid * score)) (binary.rs:164-166) */
+  LGBM_B200_METRIC_BINARY_ERROR = 2,
+  LGBM_B200_METRIC_L2 = 3,
+  LGBM_B200_METRIC_RMSE = 4,
+  LGBM_B200_METRIC_MULTI_LOGLOSS = 5,  /* on the softmax of class-major scores [num_class x n] */
+  LGBM_B200_METRIC_MULTI_ERROR = 6
+};
+
+typedef struct {
+  int32_t metric;            /* LGBM_B200_METRIC_* */
+  int32_t num_class;         /* multiclass metrics */
+  double sigmoid;            /* binary metrics: the objective's sigmoid */
+  int32_t multi_error_top_k; /* multi_error: a row counts as an error when more than top_k classes score >= its label's */
+} LgbmB200MetricConfig;
+
+/* The metric of `score` against `label` (n rows; multiclass scores are
+ * class-major, n x num_class values) into *out. location: LGBM_B200_HOST
+ * or LGBM_B200_DEVICE for both buffers. */
+int lgbm_b200_metric_eval(const LgbmB200MetricConfig* cfg, const float* label, const double* score, int64_t n,
+                          int32_t location, int32_t device, double* out);
+
+/* ------------------------------------------------------------------------
  * Tree learner.
  * ------------------------------------------------------------------------ */
 typedef struct LgbmB200Learner LgbmB200Learner;

@@ -40,6 +40,14 @@ class BinParams(C.Structure):
                 ("num_categorical", i32)]
 
 
+class MetricConfig(C.Structure):
+    _fields_ = [("metric", i32), ("num_class", i32), ("sigmoid", f64), ("multi_error_top_k", i32)]
+
+
+METRICS = {"auc": 0, "binary_logloss": 1, "binary_error": 2, "l2": 3, "rmse": 4, "multi_logloss": 5,
+           "multi_error": 6}
+
+
 class DatasetView(C.Structure):
     _fields_ = [("num_data", i64), ("num_features", i32), ("num_total_features", i32), ("bins", u8p),
                 ("num_bin", P(i32)), ("missing_type", P(i32)), ("default_bin", P(i32)),
@@ -93,6 +101,7 @@ SIGNATURES = {
     "lgbm_b200_version": (C.c_char_p, []),
     "lgbm_b200_dataset_create": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, P(C.c_void_p)]),
+    "lgbm_b200_metric_eval": (C.c_int, [P(MetricConfig), P(C.c_float), P(f64), i64, i32, i32, P(f64)]),
     "lgbm_b200_dataset_create_device": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid_device": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_view": (C.c_int, [C.c_void_p, P(DatasetView)]),

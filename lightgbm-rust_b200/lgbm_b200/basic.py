@@ -334,6 +334,19 @@ def objective_config(p):
                              int(p["lambdarank_truncation_level"]), int(bool(p["lambdarank_norm"])))
 
 
+def metric(name, label, scores, num_class=1, sigmoid=1.0, multi_error_top_k=1, device=0):
+    """Metric::eval (metric.rs:520) of host scores on the device: auc,
+    binary_logloss, binary_error, l2, rmse, multi_logloss, multi_error
+    (unweighted; multiclass scores class-major)."""
+    label = np.ascontiguousarray(label, dtype=np.float32)
+    scores = np.ascontiguousarray(scores, dtype=np.float64)
+    cfg = L.MetricConfig(L.METRICS[name], int(num_class), float(sigmoid), int(multi_error_top_k))
+    out = C.c_double()
+    L.check(L.lib().lgbm_b200_metric_eval(C.byref(cfg), _ptr(label, C.c_float), _ptr(scores, C.c_double), len(label),
+                                          L.HOST, int(device), C.byref(out)))
+    return out.value
+
+
 def gradients(params, label, scores, group=None):
     """RowObjective::gradients on the GPU from host arrays."""
     p = resolve_params(params)
