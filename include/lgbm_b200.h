@@ -144,6 +144,13 @@ typedef struct {
  * or LGBM_B200_DEVICE for both buffers. */
 int lgbm_b200_metric_eval(const LgbmB200MetricConfig* cfg, const float* label, const double* score, int64_t n,
                           int32_t location, int32_t device, double* out);
+/* NDCG@eval_at[j] (metric.rs:546-598, dcg.rs; no query weights) into
+ * out[j]: per query the stable descending order of the scores and the best
+ * DCG from the label counts, the mean over queries. query_boundaries is host
+ * memory ([num_queries + 1], from 0); labels are integers in [0, 30]. */
+int lgbm_b200_metric_ndcg(const float* label, const double* score, const int32_t* query_boundaries,
+                          int32_t num_queries, const int32_t* eval_at, int32_t num_eval_at, int32_t location,
+                          int32_t device, double* out);
 
 /* ------------------------------------------------------------------------
  * Tree learner.

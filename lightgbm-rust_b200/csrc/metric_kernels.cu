@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "learner_impl.h"
+#include "rank.h"
 
 namespace lgbm_b200 {
 
@@ -333,4 +334,62 @@ extern "C" int lgbm_b200_metric_eval(const LgbmB200MetricConfig* cfg, const floa
   cudaFree(ld);
   cudaFree(sd);
   return st.ok() ? LGBM_B200_OK : fail(st);
+}
+
+extern "C" int lgbm_b200_metric_ndcg(const float* label, const double* score, const int32_t* query_boundaries,
+                                     int32_t num_queries, const int32_t* eval_at, int32_t num_eval_at,
+                                     int32_t location, int32_t device, double* out) {
+  if (!label || !score || !query_boundaries || num_queries <= 0 || !eval_at || num_eval_at <= 0 || !out ||
+      query_boundaries[0] != 0)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "ndcg: bad argument"));
+  for (int32_t j = 0; j < num_eval_at; ++j)
+    if (eval_at[j] <= 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "ndcg: eval_at must be positive"));
+  if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  const int64_t n = query_boundaries[num_queries];
+  // the label gains, discounts and query checks of the ranking objective's tables
+  std::vector<float> lh;
+  const float* lp = label;
+  if (location == LGBM_B200_DEVICE) {
+    lh.resize((size_t)n);
+    if (cudaMemcpy(lh.data(), label, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(Status(LGBM_B200_ERR_CUDA, "ndcg: label copy"));
+    lp = lh.data();
+  }
+  RankTables rt;
+  Status st = rt.build(lp, query_boundaries, num_queries, 1.0, 1, false);
+  if (!st.ok()) return fail(st);
+  float* ld = nullptr;
+  double* sd = nullptr;
+  int32_t* kd = nullptr;
+  double* od = nullptr;
+  const size_t nq = (size_t)num_queries, nk = (size_t)num_eval_at;
+  cudaError_t e = cudaSuccess;
+  if (location != LGBM_B200_DEVICE) {
+    if ((e = cudaMalloc(&ld, sizeof(float) * n)) == cudaSuccess) e = cudaMalloc(&sd, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMemcpy(ld, label, sizeof(float) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(sd, score, sizeof(double) * n, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&kd, sizeof(int32_t) * nk);
+  if (e == cudaSuccess) e = cudaMalloc(&od, sizeof(double) * nq * nk);
+  if (e == cudaSuccess) e = cudaMemcpy(kd, eval_at, sizeof(int32_t) * nk, cudaMemcpyHostToDevice);
+  std::vector<double> per(nq * nk);
+  if (e == cudaSuccess) {
+    const float* lbl = location == LGBM_B200_DEVICE ? label : ld;
+    const double* sc = location == LGBM_B200_DEVICE ? score : sd;
+    st = launch_ndcg(rt.d, lbl, sc, kd, num_eval_at, od, 148, 0);
+    if (st.ok()) e = cudaMemcpy(per.data(), od, sizeof(double) * nq * nk, cudaMemcpyDeviceToHost);
+  }
+  if (ld) cudaFree(ld);
+  if (sd) cudaFree(sd);
+  if (kd) cudaFree(kd);
+  if (od) cudaFree(od);
+  if (!st.ok()) return fail(st);
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, std::string("ndcg: ") + cudaGetErrorString(e)));
+  // the mean over queries, added in query order
+  for (size_t j = 0; j < nk; ++j) {
+    double acc = 0.0;
+    for (size_t q = 0; q < nq; ++q) acc += per[q * nk + j];
+    out[j] = acc / (double)num_queries;
+  }
+  return LGBM_B200_OK;
 }

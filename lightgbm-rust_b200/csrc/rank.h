@@ -33,5 +33,8 @@ struct RankTables {
 
 Status launch_lambdarank(const DRank& r, const float* label, const double* score, float* g, float* h, float2* gh,
                          int sms, cudaStream_t s);
+// NDCG@ks[j] of every query into out[q * nk + j] (device buffers).
+Status launch_ndcg(const DRank& r, const float* label, const double* score, const int32_t* ks, int32_t nk,
+                   double* out, int sms, cudaStream_t s);
 
 }  // namespace lgbm_b200

@@ -139,6 +139,61 @@ __global__ void __launch_bounds__(128) k_lambdarank(DRank r, const float* label,
   }
 }
 
+// NDCG@k of every query (metric.rs:546-598, no query weights), one thread
+// per query, with the additions in the reference's order: out[q * nk + j]
+// (1.0 for every k when the query's best DCG at ks[0] is 0). `r.sorted`
+// holds the stable descending order of the query's scores (k_rank_sort).
+__global__ void __launch_bounds__(128) k_ndcg(DRank r, const float* label, const int32_t* ks, int32_t nk,
+                                              double* out) {
+  for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < r.nq; q += gridDim.x * blockDim.x) {
+    const int32_t b0 = r.bnd[q], cnt = r.bnd[q + 1] - b0;
+    const float* lb = label + b0;
+    const uint32_t* sorted = r.sorted + b0;
+    double* o = out + (size_t)q * nk;
+    // dcg.rs max_dcg_at_k for each k, from the label counts
+    bool first_ok = true;
+    for (int32_t j = 0; j < nk; ++j) {
+      int32_t counts[31];
+      for (int v = 0; v < 31; ++v) counts[v] = 0;
+      for (int32_t i = 0; i < cnt; ++i) counts[(int32_t)lb[i]] += 1;
+      int32_t top = 30;
+      double v = 0.0;
+      const int32_t kk = min(ks[j], cnt);
+      for (int32_t i = 0; i < kk; ++i) {
+        while (top > 0 && counts[top] <= 0) top -= 1;
+        v += r.discount[i] * r.label_gain[top];
+        counts[top] -= 1;
+      }
+      o[j] = v > 0.0 ? 1.0 / v : -1.0;  // the inverse for now
+      if (j == 0) first_ok = o[0] > 0.0;
+    }
+    if (!first_ok) {
+      for (int32_t j = 0; j < nk; ++j) o[j] = 1.0;
+      continue;
+    }
+    double cur = 0.0;
+    int32_t left = 0;
+    for (int32_t j = 0; j < nk; ++j) {
+      const int32_t kk = min(ks[j], cnt);
+      for (int32_t i = left; i < kk; ++i) cur += r.label_gain[(int32_t)lb[sorted[i]]] * r.discount[i];
+      o[j] = cur * o[j];
+      left = kk;
+    }
+  }
+}
+
+Status launch_ndcg(const DRank& r, const float* label, const double* score, const int32_t* ks, int32_t nk,
+                   double* out, int sms, cudaStream_t s) {
+  if (r.nq == 0) return Status();
+  const int sort_grid = (int)std::min<int64_t>(r.nq, (int64_t)sms * 16);
+  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score);
+  CU_LAUNCH();
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((r.nq + 127) / 128, (int64_t)sms * 16));
+  k_ndcg<<<grid, 128, 0, s>>>(r, label, ks, nk, out);
+  CU_LAUNCH();
+  return Status();
+}
+
 Status RankTables::build(const float* label_h, const int32_t* bnd_h, int32_t nq_, double sigmoid, int32_t trunc,
                          bool norm) {
   nq = nq_;

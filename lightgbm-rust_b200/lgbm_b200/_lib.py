@@ -102,6 +102,7 @@ SIGNATURES = {
     "lgbm_b200_dataset_create": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, P(C.c_void_p)]),
     "lgbm_b200_metric_eval": (C.c_int, [P(MetricConfig), P(C.c_float), P(f64), i64, i32, i32, P(f64)]),
+    "lgbm_b200_metric_ndcg": (C.c_int, [P(C.c_float), P(f64), P(i32), i32, P(i32), i32, i32, i32, P(f64)]),
     "lgbm_b200_dataset_create_device": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid_device": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_view": (C.c_int, [C.c_void_p, P(DatasetView)]),

@@ -347,6 +347,20 @@ def metric(name, label, scores, num_class=1, sigmoid=1.0, multi_error_top_k=1, d
     return out.value
 
 
+def ndcg(label, scores, group, eval_at, device=0):
+    """NDCG@k for each k of eval_at on the device (metric.rs:546-598);
+    `group` holds the query sizes."""
+    label = np.ascontiguousarray(label, dtype=np.float32)
+    scores = np.ascontiguousarray(scores, dtype=np.float64)
+    bnd = np.concatenate([[0], np.cumsum(group)]).astype(np.int32)
+    ks = np.ascontiguousarray(eval_at, dtype=np.int32)
+    out = np.zeros(len(ks), np.float64)
+    L.check(L.lib().lgbm_b200_metric_ndcg(_ptr(label, C.c_float), _ptr(scores, C.c_double), _ptr(bnd, C.c_int32),
+                                          len(bnd) - 1, _ptr(ks, C.c_int32), len(ks), L.HOST, int(device),
+                                          _ptr(out, C.c_double)))
+    return out
+
+
 def gradients(params, label, scores, group=None):
     """RowObjective::gradients on the GPU from host arrays."""
     p = resolve_params(params)

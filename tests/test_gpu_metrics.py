@@ -66,3 +66,16 @@ def test_multiclass_metrics(lgb):
     for top_k in (1, 2):
         err = float(np.mean((p >= pl).sum(axis=0) > top_k))
         assert lgb.metric("multi_error", y, sc.ravel(), num_class=k, multi_error_top_k=top_k) == err
+
+
+def test_ndcg_matches_oracle(lgb, orc):
+    rng = np.random.default_rng(9)
+    group = np.clip(rng.geometric(1.0 / 30.0, 3000), 1, 400).astype(np.int32)
+    n = int(group.sum())
+    label = rng.integers(0, 5, n).astype(np.float32)
+    label[:group[0]] = 0  # a query whose best DCG is 0
+    score = np.round(rng.standard_normal(n), 1)  # ties inside queries: the stable order decides
+    for ks in ([1, 3, 5, 10], [10, 5, 1], [1000]):
+        got = lgb.ndcg(label, score, group, ks)
+        want = orc.ndcg(label, score, group, ks)
+        assert np.array_equal(got, want), (ks, got, want)
