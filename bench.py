@@ -174,7 +174,15 @@ def run_form(lgb, data, ds, dv, form, args, device):
     for _ in range(max(0, args.rounds - done)):
         if bst.update():
             break
-    auc = _auc(data["y_valid"], bst.scores(valid=True)[0])
+    sv = bst.scores(valid=True)[0]
+    t0 = time.perf_counter()
+    auc = _auc(data["y_valid"], sv)
+    auc_numpy_ms = 1000 * (time.perf_counter() - t0)
+    # the same AUC on the device (lgbm_b200_metric_eval: host scores in, copies included)
+    lgb.metric("auc", data["y_valid"][:1000], sv[:1000], device=device)
+    t0 = time.perf_counter()
+    auc_device = lgb.metric("auc", data["y_valid"], sv, device=device)
+    auc_device_ms = 1000 * (time.perf_counter() - t0)
     nf = ds.binned()["num_features"]
     steps_per_tree = int(params["num_leaves"]) - 1
     hist_launches = args.steps * (1 if fused else steps_per_tree)
@@ -184,7 +192,8 @@ def run_form(lgb, data, ds, dv, form, args, device):
     part_bytes = prows * (4 + nf + 4 + 4)
     return {
         "ms_per_step": ms, "wall_ms_per_step": 1000 * wall / args.steps, "s_per_500": ms * ROUNDS / 1000.0,
-        "auc": auc, "hist_ms_per_launch": hist_ms / hist_launches, "hist_gbs": hist_bytes / (hist_ms / 1000) / 1e9,
+        "auc": auc, "auc_device": auc_device, "auc_device_ms": auc_device_ms, "auc_numpy_ms": auc_numpy_ms,
+        "hist_ms_per_launch": hist_ms / hist_launches, "hist_gbs": hist_bytes / (hist_ms / 1000) / 1e9,
         "hist_bytes_per_launch": hist_bytes / hist_launches, "hist_rows_per_tree": rows / args.steps,
         "scan_ms_per_step": scan_ms / args.steps, "partition_ms_per_step": part_ms / args.steps,
         "fused": fused, "part_rows_per_tree": prows / args.steps,
@@ -355,7 +364,12 @@ def run_workload(args):
             lp = z - np.log(np.exp(z).sum(axis=1, keepdims=True))
             r["train_multi_logloss"] = float(-np.mean(lp[np.arange(len(y)), y.astype(int)]))
         else:
+            t0 = time.perf_counter()
             r["train_ndcg@10"] = _ndcg_at(y, sc[0], d["group"], 10)
+            r["ndcg_numpy_s"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            r["train_ndcg@10_device"] = float(lgb.ndcg(y, sc[0], d["group"], [10])[0])
+            r["ndcg_device_s"] = time.perf_counter() - t0
             # batched raw prediction of the trained model over every row
             bst.predict(d["X"][:1000], raw_score=True)
             t0 = time.perf_counter()
@@ -460,6 +474,8 @@ def main():
                    "l2": "inputs larger than L2 (bin matrix 320 MB, gradients 80 MB)", "rows": len(data["y"]),
                    "held_out_rows": len(data["y_valid"])},
         "forms": {k: {"s_per_500_rounds": v["s_per_500"], "ms_per_step": v["ms_per_step"], "auc": v["auc"],
+                      "auc_device": v["auc_device"], "auc_device_ms": v["auc_device_ms"],
+                      "auc_numpy_ms": v["auc_numpy_ms"],
                       "hist_gbs": v["hist_gbs"], "hist_ms_per_step": v["hist_ms_per_step"],
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
                       "hist_rows_per_tree": v["hist_rows_per_tree"], "fused": v["fused"], "part_gbs": v["part_gbs"],
