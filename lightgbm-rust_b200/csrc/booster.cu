@@ -117,7 +117,14 @@ struct LgbmB200Booster {
   std::vector<HostTree> out_trees;
   double* lv_dev = nullptr;  // [K x L] shrunk leaf values
   std::unique_ptr<RankTables> rank;  // lambdarank objective tables
-  ~LgbmB200Booster() { arena.free_all(); }
+  // by-tree feature masks: the last one sent per class, and pinned staging
+  // (a mask is sent without a synchronisation, and only when it changes)
+  std::vector<std::vector<uint8_t>> sent_mask;
+  uint8_t* mask_h = nullptr;
+  ~LgbmB200Booster() {
+    arena.free_all();
+    if (mask_h) cudaFreeHost(mask_h);
+  }
 };
 
 namespace lgbm_b200 {
@@ -196,6 +203,16 @@ static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB
   return Status();
 }
 
+// The shrunk leaf values of each slot's new tree (tree.rs shrinkage:
+// round_to_zero(value * rate)), 0 for a tree of one leaf (no update).
+// Grid (1, 1, slots).
+__global__ void k_shrink_leaves(const __grid_constant__ DCtx c, double rate, double* lv, int32_t L) {
+  const DSlot& s = c.slots[blockIdx.z];
+  const int32_t nl = s.st->num_leaves_cur;
+  for (int32_t l = threadIdx.x; l < L; l += blockDim.x)
+    lv[(size_t)blockIdx.z * L + l] = (nl > 1 && l < nl) ? maybe_round_to_zero(s.tree.leaf_value[l] * rate) : 0.0;
+}
+
 static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
   LgbmB200Learner* L = b->L;
   CU(cudaSetDevice(L->device));
@@ -239,32 +256,31 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
     int rc = lgbm_b200_learner_set_bagging(L, b->bag, b->bag_cnt, LGBM_B200_DEVICE);
     if (rc != LGBM_B200_OK) return Status(rc, lgbm_b200_last_error());
   }
-  // by-tree column samples, one per class tree (col_sampler.rs:88-96)
+  // by-tree column samples, one per class tree (col_sampler.rs:88-96); the
+  // staging is pinned and rewritten only after the iteration's final
+  // synchronisation, so no copy waits
+  if (!b->mask_h) CU(cudaHostAlloc(reinterpret_cast<void**>(&b->mask_h), (size_t)K * L->nf, cudaHostAllocDefault));
+  b->sent_mask.resize((size_t)K);
   for (int k = 0; k < K; ++k) {
     std::vector<uint8_t> used((size_t)L->nf, 1);
     if (b->cfg.feature_fraction < 1.0) {
       std::fill(used.begin(), used.end(), 0);
       for (int32_t i : b->col_rand->sample(L->nf, b->used_cnt_bytree)) used[(size_t)i] = 1;
     }
-    CU(cudaMemcpyAsync(L->slots_h[k].bytree, used.data(), used.size(), cudaMemcpyHostToDevice, s));
-    CU(cudaStreamSynchronize(s));
-  }
-  if (!(st = train(L, nullptr, nullptr, LGBM_B200_DEVICE)).ok()) return st;
-  // score updates (boosting.rs:1381-1408) with the shrunk leaf values
-  bool should_continue = false;
-  std::vector<double> lv((size_t)K * L->L, 0.0);
-  for (int k = 0; k < K; ++k) {
-    HostTree& t = b->out_trees[k];
-    t = L->trees[k];
-    if (t.num_leaves > 1) {
-      should_continue = true;
-      shrink(t, b->cfg.learning_rate);
-      for (int l = 0; l < t.num_leaves; ++l) lv[(size_t)k * L->L + l] = t.leaf_value[l];
+    if (used != b->sent_mask[(size_t)k]) {
+      uint8_t* h = b->mask_h + (size_t)k * L->nf;
+      std::copy(used.begin(), used.end(), h);
+      CU(cudaMemcpyAsync(L->slots_h[k].bytree, h, used.size(), cudaMemcpyHostToDevice, s));
+      b->sent_mask[(size_t)k] = used;
     }
   }
-  CU(cudaMemcpyAsync(b->lv_dev, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice, s));
+  if (!(st = train_enqueue(L, nullptr, nullptr, LGBM_B200_DEVICE)).ok()) return st;
+  // score updates (boosting.rs:1381-1408) with the leaf values shrunk on the
+  // device, enqueued before the trees are read back
   {
     DCtx c = L->ctx;
+    k_shrink_leaves<<<dim3(1, 1, K), 256, 0, s>>>(c, b->cfg.learning_rate, b->lv_dev, L->L);
+    CU_LAUNCH();
     k_add_leaf_outputs<<<dim3(sms * 4, 1, K), 256, 16 * (size_t)L->L, s>>>(c, b->lv_dev, L->L, b->score, n);
     CU_LAUNCH();
     if (b->bagging && b->oob_cnt > 0) {
@@ -278,7 +294,16 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
       CU_LAUNCH();
     }
   }
-  CU(cudaStreamSynchronize(s));
+  if (!(st = train_collect(L)).ok()) return st;  // synchronises
+  bool should_continue = false;
+  for (int k = 0; k < K; ++k) {
+    HostTree& t = b->out_trees[k];
+    t = L->trees[k];
+    if (t.num_leaves > 1) {
+      should_continue = true;
+      shrink(t, b->cfg.learning_rate);
+    }
+  }
   for (int k = 0; k < K; ++k) {
     HostTree& t = b->out_trees[k];
     if (t.num_leaves > 1) {

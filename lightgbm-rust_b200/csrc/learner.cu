@@ -509,6 +509,12 @@ static Status read_tree(LgbmB200Learner* h, int k) {
 }
 
 Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location) {
+  Status st = train_enqueue(h, grad, hess, location);
+  return st.ok() ? train_collect(h) : st;
+}
+
+// Everything of one tree up to its growth, enqueued on the learner's stream.
+Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location) {
   CU(cudaSetDevice(h->device));
   const int K = h->K;
   const int64_t n = h->n;
@@ -549,8 +555,16 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
     }
   }
   h->last_ms[0] = h->last_ms[1] = h->last_ms[2] = h->last_ms[3] = 0;
-  Status st = run_tree(h);
-  if (!st.ok()) return st;
+  return run_tree(h);
+}
+
+// The trees of the last train_enqueue, read back once the stream has run
+// (with every status check).
+Status train_collect(LgbmB200Learner* h) {
+  CU(cudaSetDevice(h->device));
+  const int K = h->K;
+  cudaStream_t s = h->stream;
+  Status st;
   for (int k = 0; k < K; ++k)
     CU(cudaMemcpyAsync(&h->st_h[k], h->slots_h[k].st, sizeof(DSlotState), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));

@@ -289,6 +289,9 @@ namespace lgbm_b200 {
 // One tree per slot from the given gradients (class-major [K x n]); NULL
 // gradients reuse the slots' interleaved buffers filled by the caller.
 Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
+// train in two halves: enqueue the tree's work; read the trees back (synchronises)
+Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
+Status train_collect(LgbmB200Learner* h);
 Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int64_t nrows, void* out);
 }  // namespace lgbm_b200
 
