@@ -209,12 +209,10 @@ def run_e2e(lgb, data, ds, form, args, device):
     """The drop-in call sequence with host buffers: RowObjective::gradients,
     SerialTreeLearner::train and add_leaf_outputs through the C ABI, with
     pinned host memory and every host<->device copy inside the timed region."""
-    import ctypes as C
 
     import torch
 
-    from lgbm_b200 import _lib as LL
-    from lgbm_b200.basic import objective_config, resolve_params
+    from lgbm_b200.basic import resolve_params
 
     params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8)
     if form == "quantized":
@@ -230,15 +228,17 @@ def run_e2e(lgb, data, ds, form, args, device):
     score[:] = np.log(pavg / (1 - pavg))
     g = pin(n, torch.float32)
     h = pin(n, torch.float32)
-    oc = objective_config(p)
     lr = float(p["learning_rate"])
 
     parts = np.zeros(3)
 
+    # the objective holds the labels on the device (RowObjective::init);
+    # every step moves the scores in and the gradients out
+    obj = lgb.Objective(dict(params), label)
+
     def step():
         t0 = time.perf_counter()
-        LL.check(LL.lib().lgbm_b200_gradients(C.byref(oc), label.ctypes.data, score.ctypes.data, n, None, 0,
-                                              g.ctypes.data, h.ctypes.data, LL.HOST, device))
+        obj.gradients(score, g, h)
         t1 = time.perf_counter()
         t = learner.train(g, h)[0]
         t2 = time.perf_counter()
@@ -256,8 +256,8 @@ def run_e2e(lgb, data, ds, form, args, device):
     return {"value": ms * ROUNDS / 1000.0, "unit": "s/500 rounds", "ms_per_step": ms,
             "ms_gradients": 1000 * parts[0] / args.steps, "ms_train": 1000 * parts[1] / args.steps,
             "ms_add_leaf_outputs": 1000 * parts[2] / args.steps,
-            # gradients: label + scores in, g/h out; train: g/h in; add_leaf_outputs: scores in and out
-            "h2d_bytes_per_step": n * (4 + 8) + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
+            # gradients: scores in, g/h out; train: g/h in; add_leaf_outputs: scores in and out
+            "h2d_bytes_per_step": n * 8 + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
 
 
 def run_cpu_baseline(lgb, form, sample_scale, iters):

@@ -293,6 +293,20 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
                         int64_t num_data, const int32_t* query_boundaries, int32_t num_queries, float* grad,
                         float* hess, int32_t location, int32_t device);
 
+/* An objective bound to its labels once (RowObjective::init,
+ * objective/mod.rs:50): the labels (and the lambdarank tables) stay on the
+ * device, and each RowObjective::gradients call (objective/mod.rs:52) moves
+ * only the scores in and the gradients out. label and query_boundaries are
+ * host memory. */
+typedef struct LgbmB200Objective LgbmB200Objective;
+int lgbm_b200_objective_create(const LgbmB200ObjectiveConfig* cfg, const float* label, int64_t num_data,
+                               const int32_t* query_boundaries, int32_t num_queries, int32_t device,
+                               LgbmB200Objective** out);
+/* scores [k x num_data] in, grad / hess [k x num_data] out, all at `location`. */
+int lgbm_b200_objective_gradients(LgbmB200Objective* obj, const double* scores, float* grad, float* hess,
+                                  int32_t location);
+void lgbm_b200_objective_free(LgbmB200Objective* obj);
+
 /* ------------------------------------------------------------------------
  * Device-resident boosting: Gbdt::train_one_iter (boosting.rs:957) with the
  * gradients, bagging draw (sample_strategy.rs:280-320), tree learner and

@@ -337,6 +337,27 @@ static GradWorkspace g_ws;
 
 }  // namespace lgbm_b200
 
+// ---- an objective bound to its labels (RowObjective::init, objective/mod.rs:50) -------------
+struct LgbmB200Objective {
+  LgbmB200ObjectiveConfig cfg{};
+  int device = 0;
+  int64_t n = 0;
+  int k = 1;
+  lgbm_b200::DeviceArena arena;
+  float* label = nullptr;  // on the device for the objective's lifetime
+  double* score = nullptr;  // staging of host scores [k x n]
+  float* g = nullptr;
+  float* h = nullptr;
+  std::unique_ptr<lgbm_b200::RankTables> rank;
+  cudaStream_t stream = nullptr;
+  ChunkStreams chunks;
+  ~LgbmB200Objective() {
+    chunks.release();
+    arena.free_all();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
 extern "C" {
 
 int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, const double* scores,
@@ -432,6 +453,93 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   return LGBM_B200_OK;
+}
+
+int lgbm_b200_objective_create(const LgbmB200ObjectiveConfig* cfg, const float* label, int64_t num_data,
+                               const int32_t* query_boundaries, int32_t num_queries, int32_t device,
+                               LgbmB200Objective** out) {
+  if (!cfg || !label || !out || num_data <= 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  auto o = std::make_unique<LgbmB200Objective>();
+  o->cfg = *cfg;
+  o->device = device;
+  o->n = num_data;
+  o->k = cfg->objective == LGBM_B200_OBJ_MULTICLASS ? std::max(1, cfg->num_class) : 1;
+  if (cfg->objective == LGBM_B200_OBJ_LAMBDARANK) {
+    if (!query_boundaries || num_queries <= 0 || query_boundaries[0] != 0 ||
+        query_boundaries[num_queries] != num_data)
+      return fail(Status(LGBM_B200_ERR_INVALID_DATA, "lambdarank needs query boundaries covering every row"));
+    o->rank = std::make_unique<RankTables>();
+    Status rs = o->rank->build(label, query_boundaries, num_queries, cfg->sigmoid, cfg->lambdarank_truncation_level,
+                               cfg->lambdarank_norm != 0);
+    if (!rs.ok()) return fail(rs);
+  }
+  const size_t n = (size_t)num_data, nk = n * (size_t)o->k;
+  Status st;
+  if (!(st = o->arena.alloc_n(&o->label, n)).ok() || !(st = o->arena.alloc_n(&o->score, nk)).ok() ||
+      !(st = o->arena.alloc_n(&o->g, nk)).ok() || !(st = o->arena.alloc_n(&o->h, nk)).ok())
+    return fail(st);
+  if (cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking) != cudaSuccess || !o->chunks.init())
+    return fail(Status(LGBM_B200_ERR_CUDA, "stream"));
+  if (cudaMemcpy(o->label, label, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(Status(LGBM_B200_ERR_CUDA, "label copy"));
+  *out = o.release();
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_objective_gradients(LgbmB200Objective* o, const double* scores, float* grad, float* hess,
+                                  int32_t location) {
+  if (!o || !scores || !grad || !hess) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
+  if (cudaSetDevice(o->device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  const DRank* rk = o->rank ? &o->rank->d : nullptr;
+  const int64_t n = o->n;
+  const size_t nk = (size_t)n * (size_t)o->k;
+  cudaError_t e = cudaSuccess;
+  if (location == LGBM_B200_DEVICE) {
+    Status st = launch_gradients(o->cfg, o->label, scores, n, nullptr, grad, hess, 148, o->stream, rk);
+    if (!st.ok()) return fail(st);
+    e = cudaStreamSynchronize(o->stream);
+  } else if (o->k == 1 && (o->cfg.objective == LGBM_B200_OBJ_BINARY || o->cfg.objective == LGBM_B200_OBJ_REGRESSION)) {
+    // one value per row: scores in and g/h out stream in chunks over three
+    // streams, so that copies in and out of different chunks overlap
+    for (int64_t r0 = 0, c = 0; r0 < n && e == cudaSuccess; r0 += ChunkStreams::kRows, ++c) {
+      const int64_t m = std::min<int64_t>(ChunkStreams::kRows, n - r0);
+      cudaStream_t cs = o->chunks.s[c % ChunkStreams::kN];
+      e = cudaMemcpyAsync(o->score + r0, scores + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
+      if (e == cudaSuccess) {
+        Status st = launch_gradients(o->cfg, o->label + r0, o->score + r0, m, nullptr, o->g + r0, o->h + r0, 148, cs, rk);
+        if (!st.ok()) {
+          o->chunks.sync();
+          return fail(st);
+        }
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(grad + r0, o->g + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hess + r0, o->h + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+    }
+    cudaError_t e2 = o->chunks.sync();
+    if (e == cudaSuccess) e = e2;
+  } else {
+    cudaStream_t s = o->stream;
+    e = cudaMemcpyAsync(o->score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+      Status st = launch_gradients(o->cfg, o->label, o->score, n, nullptr, o->g, o->h, 148, s, rk);
+      if (!st.ok()) return fail(st);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grad, o->g, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hess, o->h, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+  return LGBM_B200_OK;
+}
+
+void lgbm_b200_objective_free(LgbmB200Objective* o) {
+  if (o) {
+    cudaSetDevice(o->device);
+    delete o;
+  }
 }
 
 int lgbm_b200_booster_create(LgbmB200Learner* learner, const LgbmB200BoostConfig* cfg, const float* label,

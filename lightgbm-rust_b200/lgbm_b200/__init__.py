@@ -5,6 +5,6 @@ this package is the host-side harness that mirrors lightgbm-rust's Python
 API for the path: Dataset, Booster, train.
 """
 from ._lib import LightGBMError, lib  # noqa: F401
-from .basic import Booster, Dataset, Learner, gradients, metric, ndcg, resolve_params, train  # noqa: F401
+from .basic import Booster, Dataset, Learner, Objective, gradients, metric, ndcg, resolve_params, train  # noqa: F401
 
-__all__ = ["Booster", "Dataset", "Learner", "LightGBMError", "gradients", "lib", "metric", "ndcg", "resolve_params", "train"]
+__all__ = ["Booster", "Dataset", "Learner", "LightGBMError", "Objective", "gradients", "lib", "metric", "ndcg", "resolve_params", "train"]

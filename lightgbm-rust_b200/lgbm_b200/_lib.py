@@ -122,6 +122,10 @@ SIGNATURES = {
     "lgbm_b200_learner_elapsed": (C.c_int, [C.c_void_p, i32, i32, P(f64)]),
     "lgbm_b200_learner_histogram": (C.c_int, [C.c_void_p, i32, P(C.c_uint32), i64, C.c_void_p]),
     "lgbm_b200_learner_quantized": (C.c_int, [C.c_void_p, i32, P(i64), P(f64)]),
+    "lgbm_b200_objective_create": (C.c_int, [P(ObjectiveConfig), C.c_void_p, i64, P(i32), i32, i32,
+                                             P(C.c_void_p)]),
+    "lgbm_b200_objective_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, i32]),
+    "lgbm_b200_objective_free": (None, [C.c_void_p]),
     "lgbm_b200_gradients": (C.c_int, [P(ObjectiveConfig), C.c_void_p, C.c_void_p, i64, P(i32), i32, C.c_void_p,
                                       C.c_void_p, i32, i32]),
     "lgbm_b200_booster_create": (C.c_int, [C.c_void_p, P(BoostConfig), P(C.c_float), P(i32), i32, u8p, i64,

@@ -334,6 +334,40 @@ def objective_config(p):
                              int(p["lambdarank_truncation_level"]), int(bool(p["lambdarank_norm"])))
 
 
+class Objective:
+    """An objective bound to its labels once (RowObjective::init): the labels
+    stay on the device and gradients() moves only the scores in and g / h out."""
+
+    def __init__(self, params, label, group=None):
+        p = resolve_params(params)
+        self.label = np.ascontiguousarray(label, dtype=np.float32)
+        self.k = int(p["num_class"]) if p["objective"] in ("multiclass", "softmax") else 1
+        self.cfg = objective_config(p)
+        bnd = None if group is None else np.concatenate([[0], np.cumsum(group)]).astype(np.int32)
+        self._bnd = bnd
+        h = C.c_void_p()
+        L.check(L.lib().lgbm_b200_objective_create(C.byref(self.cfg), self.label.ctypes.data, len(self.label),
+                                                   _ptr(bnd, C.c_int32) if bnd is not None else None,
+                                                   len(bnd) - 1 if bnd is not None else 0, int(p["device"]),
+                                                   C.byref(h)))
+        self.handle = h
+
+    def gradients(self, scores, grad=None, hess=None):
+        """g, h (float32 [k * n]) of scores (float64 [k * n], class-major)."""
+        n = len(self.label) * self.k
+        sc = np.ascontiguousarray(scores, dtype=np.float64)
+        g = np.empty(n, np.float32) if grad is None else grad
+        h = np.empty(n, np.float32) if hess is None else hess
+        L.check(L.lib().lgbm_b200_objective_gradients(self.handle, sc.ctypes.data, g.ctypes.data, h.ctypes.data,
+                                                      L.HOST))
+        return g, h
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            L.lib().lgbm_b200_objective_free(self.handle)
+            self.handle = None
+
+
 def metric(name, label, scores, num_class=1, sigmoid=1.0, multi_error_top_k=1, device=0):
     """Metric::eval (metric.rs:520) of host scores on the device: auc,
     binary_logloss, binary_error, l2, rmse, multi_logloss, multi_error

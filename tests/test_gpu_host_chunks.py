@@ -53,3 +53,24 @@ def test_add_leaf_outputs_several_chunks(lgb, bagged):
             want[rows] += lv[leaf]
         learner.add_leaf_outputs(0, lv, score)
         assert np.array_equal(score, want)  # one FP64 add per row: bit-exact
+
+
+def test_objective_handle_matches_stateless_gradients(lgb):
+    """lgbm_b200_objective_* (labels bound once) gives exactly the gradients
+    of lgbm_b200_gradients (labels passed every call): the same kernels."""
+    rng = np.random.default_rng(43)
+    n = 2_200_000
+    cases = [({"objective": "binary"}, (rng.random(n) < 0.4).astype(np.float32), rng.standard_normal(n) * 3, None),
+             ({"objective": "regression"}, rng.standard_normal(n).astype(np.float32), rng.standard_normal(n), None),
+             ({"objective": "multiclass", "num_class": 3}, rng.integers(0, 3, 50000).astype(np.float32),
+              rng.standard_normal(3 * 50000), None)]
+    group = np.clip(rng.geometric(1.0 / 20.0, 2000), 1, 200).astype(np.int32)
+    m = int(group.sum())
+    cases.append(({"objective": "lambdarank"}, rng.integers(0, 5, m).astype(np.float32), rng.standard_normal(m),
+                  group))
+    for params, y, s, grp in cases:
+        obj = lgb.Objective(params, y, group=grp)
+        for _ in range(2):
+            g, h = obj.gradients(s)
+            g0, h0 = lgb.gradients(params, y, s, group=grp)
+            assert np.array_equal(g, g0) and np.array_equal(h, h0), params["objective"]
