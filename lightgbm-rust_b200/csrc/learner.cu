@@ -156,13 +156,10 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     h->scan_part_grid = std::min(h->part_grid, per_sm * h->num_sms / K);
     if (h->scan_part_grid < 1) return Status(LGBM_B200_ERR_UNSUPPORTED, "scan + partition launch does not fit");
   }
-  // programmatic dependent launch per kernel edge: bit 0 histogram (after
-  // the partition), bit 1 scan (after the histogram), bit 2 partition (after
-  // the scan); 1 alone means every edge
-  if (const char* e = std::getenv("LGBM_B200_PDL")) {
-    const int v = std::atoi(e);
-    h->use_pdl = v == 1 ? 7 : v;
-  }
+  // programmatic dependent launch per kernel edge, a bit mask: 1 the
+  // histogram (after the partition), 2 the scan (after the histogram), 4 the
+  // partition (after the scan)
+  if (const char* e = std::getenv("LGBM_B200_PDL")) h->use_pdl = std::atoi(e) & 7;
   if (cfg->persistent_grow) {
     // one resident CTA group per slot: the cooperative launch holds every CTA
     const void* gk = grow_kernel(mode, h->hist_ng);
