@@ -150,7 +150,7 @@ Status push_bins_device(Dataset& d, const float* X, int64_t n, int32_t ncol, int
     // a buffer is reused by the chunk three later, on the same stream: in order
     BIN_CU(cudaMemcpyAsync(x_d[i], X + r0 * ncol, sizeof(float) * (size_t)m * (size_t)ncol, cudaMemcpyHostToDevice, s));
     const int64_t items = m * (int64_t)nf;
-    const int blocks = (int)std::min<int64_t>((items + 255) / 256, 148 * 16);
+    const int blocks = (int)std::min<int64_t>((items + 255) / 256, current_device_sms() * 16);
     k_bin_rows<<<blocks, 256, 0, s>>>(x_d[i], m, ncol, nf, metas_d, ub_d, cat_d, b_d[i]);
     BIN_CU(cudaGetLastError());
     BIN_CU(cudaMemcpyAsync(d.bins.data() + (size_t)r0 * (size_t)nf, b_d[i], (size_t)m * (size_t)nf,

@@ -389,7 +389,7 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
   }
   const DRank* rk = rank ? &rank->d : nullptr;
   if (location == LGBM_B200_DEVICE) {
-    Status s = launch_gradients(*cfg, label, scores, num_data, nullptr, grad, hess, 148, 0, rk);
+    Status s = launch_gradients(*cfg, label, scores, num_data, nullptr, grad, hess, current_device_sms(), 0, rk);
     if (!s.ok()) return fail(s);
     cudaError_t e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
@@ -429,7 +429,7 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(w.score + r0, scores + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
       if (e == cudaSuccess) {
-        Status st = launch_gradients(*cfg, w.label + r0, w.score + r0, m, nullptr, w.g + r0, w.h + r0, 148, cs, rk);
+        Status st = launch_gradients(*cfg, w.label + r0, w.score + r0, m, nullptr, w.g + r0, w.h + r0, current_device_sms(), cs, rk);
         if (!st.ok()) {
           w.chunks.sync();
           return fail(st);
@@ -446,7 +446,7 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
   }
   cudaMemcpyAsync(w.label, label, sizeof(float) * n, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(w.score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
-  Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, 148, s, rk);
+  Status st = launch_gradients(*cfg, w.label, w.score, num_data, nullptr, w.g, w.h, current_device_sms(), s, rk);
   if (!st.ok()) return fail(st);
   cudaMemcpyAsync(grad, w.g, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hess, w.h, sizeof(float) * nk, cudaMemcpyDeviceToHost, s);
@@ -496,7 +496,7 @@ int lgbm_b200_objective_gradients(LgbmB200Objective* o, const double* scores, fl
   const size_t nk = (size_t)n * (size_t)o->k;
   cudaError_t e = cudaSuccess;
   if (location == LGBM_B200_DEVICE) {
-    Status st = launch_gradients(o->cfg, o->label, scores, n, nullptr, grad, hess, 148, o->stream, rk);
+    Status st = launch_gradients(o->cfg, o->label, scores, n, nullptr, grad, hess, current_device_sms(), o->stream, rk);
     if (!st.ok()) return fail(st);
     e = cudaStreamSynchronize(o->stream);
   } else if (o->k == 1 && (o->cfg.objective == LGBM_B200_OBJ_BINARY || o->cfg.objective == LGBM_B200_OBJ_REGRESSION)) {
@@ -507,7 +507,7 @@ int lgbm_b200_objective_gradients(LgbmB200Objective* o, const double* scores, fl
       cudaStream_t cs = o->chunks.s[c % ChunkStreams::kN];
       e = cudaMemcpyAsync(o->score + r0, scores + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
       if (e == cudaSuccess) {
-        Status st = launch_gradients(o->cfg, o->label + r0, o->score + r0, m, nullptr, o->g + r0, o->h + r0, 148, cs, rk);
+        Status st = launch_gradients(o->cfg, o->label + r0, o->score + r0, m, nullptr, o->g + r0, o->h + r0, current_device_sms(), cs, rk);
         if (!st.ok()) {
           o->chunks.sync();
           return fail(st);
@@ -523,7 +523,7 @@ int lgbm_b200_objective_gradients(LgbmB200Objective* o, const double* scores, fl
     cudaStream_t s = o->stream;
     e = cudaMemcpyAsync(o->score, scores, sizeof(double) * nk, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-      Status st = launch_gradients(o->cfg, o->label, o->score, n, nullptr, o->g, o->h, 148, s, rk);
+      Status st = launch_gradients(o->cfg, o->label, o->score, n, nullptr, o->g, o->h, current_device_sms(), s, rk);
       if (!st.ok()) return fail(st);
       e = cudaGetLastError();
     }

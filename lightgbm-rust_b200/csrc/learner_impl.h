@@ -180,6 +180,18 @@ struct HostTree {  // the reference's Tree arrays for one trained tree
 
 using namespace lgbm_b200;
 
+// Multiprocessors of the current device (queried once per device).
+inline int current_device_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cached[dev] == 0) {
+    int v = 0;
+    cached[dev] = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0 ? v : 148;
+  }
+  return cached[dev];
+}
+
 // Streams over which a call with host buffers pipelines its row chunks: the
 // copy in, the kernel and the copy out of successive chunks overlap (the two
 // copy directions run on separate copy engines).

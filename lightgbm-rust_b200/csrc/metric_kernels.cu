@@ -239,7 +239,7 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
       free_all();
       return Status(LGBM_B200_ERR_CUDA, std::string("metric: ") + cudaGetErrorString(e));
     }
-    const int grid = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
+    const int grid = (int)std::min<int64_t>((m + 255) / 256, current_device_sms() * 16);
     k_auc_keys<<<grid, 256, 0, s>>>(label, score, n, m, key, cls);
     // bitonic sort: stages up to kSortBlock in shared memory, then each larger
     // stage's steps of span >= kSortBlock in global memory and its tail in shared
@@ -248,7 +248,7 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
       for (int64_t j = k >> 1; j >= kSortBlock; j >>= 1) k_bitonic_global<<<grid, 256, 0, s>>>(key, cls, m, k, j);
       k_bitonic_shared<<<(unsigned)nb, kSortBlock / 2, 0, s>>>(key, cls, k, k);
     }
-    k_auc_block_pos<<<(unsigned)std::min<int64_t>(nb, 148 * 8), 256, 0, s>>>(cls, nb, block_pos);
+    k_auc_block_pos<<<(unsigned)std::min<int64_t>(nb, current_device_sms() * 8), 256, 0, s>>>(cls, nb, block_pos);
     std::vector<int32_t> bp((size_t)nb);
     std::vector<int64_t> bf((size_t)nb);
     e = cudaMemcpyAsync(bp.data(), block_pos, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s);
@@ -279,7 +279,7 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
   a.top_k = cfg.multi_error_top_k;
   a.sigmoid = cfg.sigmoid;
   a.neg_log_eps = -(double)std::log(1e-15f);  // consts.rs neg_log_epsilon: the f32 log, promoted
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, current_device_sms() * 8));
   double* partial = nullptr;
   if ((e = dalloc((void**)&partial, sizeof(double) * grid)) != cudaSuccess) {
     free_all();
@@ -376,7 +376,7 @@ extern "C" int lgbm_b200_metric_ndcg(const float* label, const double* score, co
   if (e == cudaSuccess) {
     const float* lbl = location == LGBM_B200_DEVICE ? label : ld;
     const double* sc = location == LGBM_B200_DEVICE ? score : sd;
-    st = launch_ndcg(rt.d, lbl, sc, kd, num_eval_at, od, 148, 0);
+    st = launch_ndcg(rt.d, lbl, sc, kd, num_eval_at, od, current_device_sms(), 0);
     if (st.ok()) e = cudaMemcpy(per.data(), od, sizeof(double) * nq * nk, cudaMemcpyDeviceToHost);
   }
   if (ld) cudaFree(ld);
