@@ -260,10 +260,11 @@ def run_e2e(lgb, data, ds, form, args, device):
             "h2d_bytes_per_step": n * 8 + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
 
 
-def run_cpu_baseline(lgb, form, sample_scale, iters):
+def run_cpu_baseline(lgb, form, sample_scale, iters, warmup=3):
     """The oracle (the reference's CPU learner restated) on the host cores, on
     a bounded sample of the workload; seconds per 500 rounds scaled to the
-    full row count."""
+    full row count. The iterations after `warmup` ones are timed: a run of
+    warmup + iters rounds minus a run of warmup rounds (both seeded alike)."""
     from lgbm_b200 import synthetic
     from oracle import oracle as orc
 
@@ -276,17 +277,18 @@ def run_cpu_baseline(lgb, form, sample_scale, iters):
     ds = lgb.Dataset(d["X"], d["y"], params=params)
     b = ds.binned()
     t0 = time.perf_counter()
-    orc.train(p, b, d["y"], 1)
+    orc.train(p, b, d["y"], warmup)
     t1 = time.perf_counter()
-    orc.train(p, b, d["y"], 1 + iters)
+    orc.train(p, b, d["y"], warmup + iters)
     t2 = time.perf_counter()
     per_iter = ((t2 - t1) - (t1 - t0)) / iters
-    per_iter = max(per_iter, (t2 - t1) / (1 + iters))
+    per_iter = max(per_iter, (t2 - t1) / (warmup + iters))
     rows = len(d["y"])
     scale = 10_000_000 / rows
     return {"value": per_iter * scale * ROUNDS, "unit": "s/500 rounds", "cores": threads, "kind": "port",
-            "sample": f"{rows} rows of the same generator, {iters} timed iterations ({form} form, "
-                      f"{threads} threads), per-iteration time scaled by {scale:.0f}x rows and x{ROUNDS} rounds"}
+            "sample": f"{rows} rows of the same generator, {iters} timed iterations after {warmup} warm-up ones "
+                      f"({form} form, {threads} threads), per-iteration time scaled by {scale:.0f}x rows and "
+                      f"x{ROUNDS} rounds", "warmup": warmup}
 
 
 def _ndcg_at(y, s, group, k):
@@ -414,10 +416,11 @@ def main():
 
         sample = 0.1 * args.scale
         iters = max(1, min(args.steps, 3))
+        warm = min(args.warmup, 5)  # at least 3 (above); bounded so the CPU run stays within minutes
         t0 = time.perf_counter()
-        cb = run_cpu_baseline(lgb, "quantized", sample, iters)
+        cb = run_cpu_baseline(lgb, "quantized", sample, iters, warm)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s/500 rounds",
-                "n_gpus": args.gpus, "steps": iters, "warmup": 1, "ms_per_step": cb["value"] / ROUNDS * 1000,
+                "n_gpus": args.gpus, "steps": iters, "warmup": warm, "ms_per_step": cb["value"] / ROUNDS * 1000,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
                 "data": "synthetic", "config": {"workload": WORKLOAD, "form": "quantized",
                                                 "sample_rows": int(10_000_000 * sample)},
