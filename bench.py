@@ -134,6 +134,39 @@ def hist_bytes_per_row(nf, form):
     return nf * 1 + (4 if form == "quantized" else 8) + 4
 
 
+def _shape_key(args, form):
+    """Key of a workload's tuned launch shape: workload, scale, histogram form."""
+    return f"{args.workload}{'' if args.scale == 1.0 else '@' + format(args.scale, 'g')}/{form}"
+
+
+def launch_shape_before(L, key, use_record, device):
+    """The learner's launch shape before warm-up: the recorded tuned shape of
+    this workload when `use_record` and there is one for this device."""
+    import torch
+
+    from lgbm_b200 import autotune
+
+    if use_record:
+        shape = autotune.lookup(key, torch.cuda.get_device_properties(device).multi_processor_count)
+        if shape is not None:
+            L.launch_shape = shape
+            return L.launch_shape, "tuned (lgbm_b200/launch_shapes.json)"
+    return L.launch_shape, "built-in defaults"
+
+
+def launch_shape_tune(L, key, device):
+    """--autotune: search the shapes on the warmed-up learner and record the choice."""
+    import torch
+
+    from lgbm_b200 import autotune
+
+    props = torch.cuda.get_device_properties(device)
+    default = L.launch_shape
+    best, best_ms, default_ms, trials = autotune.tune(L, reps=3)
+    autotune.record(key, best, best_ms, default, default_ms, trials, props.name, props.multi_processor_count)
+    return L.launch_shape, "autotuned in this run"
+
+
 def run_form(lgb, data, ds, dv, form, args, device):
     params = dict(data["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8,
                   use_cuda_graph=True)
@@ -141,8 +174,15 @@ def run_form(lgb, data, ds, dv, form, args, device):
         params["quant_train_renew_leaf"] = True
     bst = lgb.Booster(params, ds, dv)
     L = bst.learner
+    key = _shape_key(args, form)
+    shape, shape_src = launch_shape_before(L, key, not args.autotune, device)
     for _ in range(args.warmup):
         bst.update()
+    extra = 0
+    if args.autotune:
+        shape, shape_src = launch_shape_tune(L, key, device)
+        bst.update()  # captures the tuned launches before the timed steps
+        extra = 1
     _barrier()
     L.record(0)
     clocks = Clocks(device)
@@ -170,7 +210,7 @@ def run_form(lgb, data, ds, dv, form, args, device):
         prows += pr
         launches = nl
     L.set_timing(False)
-    done = args.warmup + 2 * args.steps
+    done = args.warmup + extra + 2 * args.steps
     for _ in range(max(0, args.rounds - done)):
         if bst.update():
             break
@@ -201,7 +241,7 @@ def run_form(lgb, data, ds, dv, form, args, device):
         "part_bytes_per_launch": part_bytes / (args.steps * steps_per_tree),
         "part_ms_per_launch": part_ms / (args.steps * steps_per_tree),
         "hist_ms_per_step": hist_ms / args.steps, "kernel_launches_per_tree": launches, "clocks": clk,
-        "num_trees": bst.num_trees(), "nf": nf,
+        "num_trees": bst.num_trees(), "nf": nf, "launch_shape": shape, "launch_shape_source": shape_src,
     }
 
 
@@ -219,6 +259,7 @@ def run_e2e(lgb, data, ds, form, args, device):
         params["quant_train_renew_leaf"] = True
     p = resolve_params(params)
     learner = lgb.Learner(ds, params)
+    launch_shape_before(learner, _shape_key(args, form), True, device)  # recorded by run_form when --autotune
     n = len(data["y"])
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
     label = pin(n, torch.float32)
@@ -348,16 +389,24 @@ def run_workload(args):
             p["quant_train_renew_leaf"] = True
         bst = lgb.Booster(p, ds)
         L = bst.learner
+        key = _shape_key(args, form)
+        shape, shape_src = launch_shape_before(L, key, not args.autotune, 0)
         for _ in range(args.warmup):
             bst.update()
+        extra = 0
+        if args.autotune:
+            shape, shape_src = launch_shape_tune(L, key, 0)
+            bst.update()  # captures the tuned launches before the timed steps
+            extra = 1
         L.record(0)
         for _ in range(args.steps):
             bst.update()
         L.record(1)
         ms = L.elapsed(0, 1) / args.steps
         sc = bst.scores()
-        rounds = args.warmup + args.steps
-        r = {"ms_per_iter": ms, "s_per_config_rounds": ms * d["num_rounds"] / 1000.0, "rounds_trained": rounds}
+        rounds = args.warmup + extra + args.steps
+        r = {"ms_per_iter": ms, "s_per_config_rounds": ms * d["num_rounds"] / 1000.0, "rounds_trained": rounds,
+             "launch_shape": shape, "launch_shape_source": shape_src}
         y = d["y"]
         if cfg == 1:
             r["train_rmse"] = float(np.sqrt(np.mean((sc[0] - y) ** 2)))
@@ -396,11 +445,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rounds", type=int, default=ROUNDS, help="rounds trained per form (AUC after these)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="search the per-step launch shape after warm-up and record it for the workload")
     ap.add_argument("--param", action="append", default=[], help="extra training parameter k=v (launch-shape sweeps)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4"],
                     help="c2: the headline binary 10M workload; c1 / c3 / c4: the regression, multiclass and "
                          "lambdarank configurations (a separate JSON line)")
     args = ap.parse_args()
+    if args.autotune and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        ap.error("--autotune records one device's choice: run it with one process")
     if args.workload != "c2":
         run_workload(args)
         return
@@ -475,14 +528,16 @@ def main():
         "data": "synthetic (seeded generator with the workload's shapes and distributions)",
         "config": {"workload": WORKLOAD, "form": head, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (bin matrix 320 MB, gradients 80 MB)", "rows": len(data["y"]),
-                   "held_out_rows": len(data["y_valid"])},
+                   "held_out_rows": len(data["y_valid"]), "launch_shape": r["launch_shape"],
+                   "launch_shape_source": r["launch_shape_source"]},
         "forms": {k: {"s_per_500_rounds": v["s_per_500"], "ms_per_step": v["ms_per_step"], "auc": v["auc"],
                       "auc_device": v["auc_device"], "auc_device_ms": v["auc_device_ms"],
                       "auc_numpy_ms": v["auc_numpy_ms"],
                       "hist_gbs": v["hist_gbs"], "hist_ms_per_step": v["hist_ms_per_step"],
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
                       "hist_rows_per_tree": v["hist_rows_per_tree"], "fused": v["fused"], "part_gbs": v["part_gbs"],
-                      "part_rows_per_tree": v["part_rows_per_tree"]} for k, v in res.items()},
+                      "part_rows_per_tree": v["part_rows_per_tree"], "launch_shape": v["launch_shape"],
+                      "launch_shape_source": v["launch_shape_source"]} for k, v in res.items()},
         "roofline": ({"bound": "hbm", "kernel": "k_partition_fused (row partition + both children's histograms)",
                       "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s", "frac": r["part_gbs"] / peak,
                       "peak_kind": peak_kind, "traffic": None,

@@ -246,6 +246,29 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
 int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* leaf_begin, int32_t* leaf_count,
                                     uint32_t* indices);
 
+/* Launch shape of the per-split-step kernels (the default launch strategy;
+ * the persistent one has none). No field changes a result: the shapes differ
+ * only in speed. No counterpart in the reference, whose CPU learner has a
+ * thread count instead. */
+typedef struct {
+  int32_t partition_ctas;      /* CTAs of the row partition per tree slot, in [1, 65535] */
+  int32_t hist_ctas;           /* histogram CTAs per tree slot and feature tile, in [1, 65535];
+                                  rounded up to a multiple of the histogram cluster size */
+  int32_t hist_rows_per_block; /* least rows a histogram CTA takes, in [32, 1 << 24] */
+} LgbmB200LaunchShape;
+
+int lgbm_b200_learner_get_launch_shape(LgbmB200Learner* h, LgbmB200LaunchShape* out);
+int lgbm_b200_learner_set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape* shape);
+
+/* The autotuner's measurement: regrows the trees of the last train call
+ * (the same gradients and quantization offsets, so the same trees) under each
+ * candidate shape, `reps` timed times after one untimed replay, writes each
+ * candidate's median device ms per tree to ms_per_tree[i], and keeps the
+ * fastest (its index in *chosen). The random streams of later train calls
+ * are untouched. Requires a train call before it; not with persistent_grow. */
+int lgbm_b200_learner_autotune(LgbmB200Learner* h, const LgbmB200LaunchShape* candidates, int32_t num_candidates,
+                               int32_t reps, int32_t* chosen, double* ms_per_tree);
+
 /* Per-kernel timing: when enabled, every split step of the next train calls
  * is bracketed by CUDA events on the learner's stream (no extra syncs). */
 int lgbm_b200_learner_set_timing(LgbmB200Learner* h, int32_t enabled);

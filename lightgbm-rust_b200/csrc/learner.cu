@@ -153,7 +153,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPartThreads, h->scan_smem));
     const int K = std::max(1, cfg->num_tree_slots);
-    h->scan_part_grid = std::min(h->part_grid, per_sm * h->num_sms / K);
+    h->scan_part_max = per_sm * h->num_sms / K;
+    h->scan_part_grid = std::min(h->part_grid, h->scan_part_max);
     if (h->scan_part_grid < 1) return Status(LGBM_B200_ERR_UNSUPPORTED, "scan + partition launch does not fit");
   }
   // programmatic dependent launch per kernel edge, a bit mask: 1 the
@@ -510,9 +511,10 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
   return st.ok() ? train_collect(h) : st;
 }
 
-// Everything of one tree up to its growth, enqueued on the learner's stream.
-Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location) {
-  CU(cudaSetDevice(h->device));
+// The gradients and their quantization for one tree, enqueued on the
+// learner's stream. `replay` quantizes with the last call's offsets instead
+// of drawing new ones (the autotuner's replays of the same tree).
+static Status prepare_tree(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location, bool replay) {
   const int K = h->K;
   const int64_t n = h->n;
   cudaStream_t s = h->stream;
@@ -544,13 +546,24 @@ Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, i
       k_quant_absmax<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->maxbits, h->quant_counter, h->slots_h[k].st,
                                             h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks);
       CU_LAUNCH();
-      int64_t start = h->start_eng->uniform_int(0, (int32_t)n);
+      if (h->last_start.size() < (size_t)K) h->last_start.resize((size_t)K, 0);
+      const int64_t start = replay ? h->last_start[k] : h->start_eng->uniform_int(0, (int32_t)n);
+      h->last_start[k] = start;
       k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, start, h->slots_h[k].st,
                                            h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
                                            h->slots_h[k].packed);
       CU_LAUNCH();
     }
   }
+  return Status();
+}
+
+// Everything of one tree up to its growth, enqueued on the learner's stream.
+Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location) {
+  CU(cudaSetDevice(h->device));
+  Status st = prepare_tree(h, grad, hess, location, false);
+  if (!st.ok()) return st;
+  h->trained = true;
   h->last_ms[0] = h->last_ms[1] = h->last_ms[2] = h->last_ms[3] = 0;
   return run_tree(h);
 }
@@ -598,6 +611,93 @@ Status train_collect(LgbmB200Learner* h) {
     if (!(st = read_tree(h, k)).ok()) return st;
   }
   return Status();
+}
+
+Status get_launch_shape(const LgbmB200Learner* h, LgbmB200LaunchShape* out) {
+  out->partition_ctas = h->part_grid;
+  out->hist_ctas = h->hist_grid;
+  out->hist_rows_per_block = h->ctx.rows_per_block;
+  return Status();
+}
+
+static Status check_launch_shape(const LgbmB200LaunchShape& in) {
+  if (in.partition_ctas < 1 || in.partition_ctas > 65535 || in.hist_ctas < 1 || in.hist_ctas > 65535 ||
+      in.hist_rows_per_block < 32 || in.hist_rows_per_block > (1 << 24))
+    return Status(LGBM_B200_ERR_INVALID_PARAMETER, "launch shape out of range");
+  return Status();
+}
+
+// No kernel sizes a buffer or a wait by these grids: the partition's tiles
+// are claimed by ticket and its last CTA is found by an exit counter, the
+// histogram CTAs split the leaf's rows among themselves. The cooperative
+// scan + partition launch stays within what is resident at once.
+Status set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape& in) {
+  Status st = check_launch_shape(in);
+  if (!st.ok()) return st;
+  const int cl = hist_cluster(h->cfg.hist_precision);
+  h->part_grid = in.partition_ctas;
+  h->hist_grid = (in.hist_ctas + cl - 1) / cl * cl;
+  h->ctx.rows_per_block = in.hist_rows_per_block;
+  if (h->scan_part) h->scan_part_grid = std::max(1, std::min(h->part_grid, h->scan_part_max));
+  if (h->graph_exec) {  // the captured launches carry the old grids
+    CU(cudaGraphExecDestroy(h->graph_exec));
+    h->graph_exec = nullptr;
+  }
+  return Status();
+}
+
+Status autotune(LgbmB200Learner* h, const LgbmB200LaunchShape* cand, int32_t num, int32_t reps, int32_t* chosen,
+                double* ms) {
+  if (h->cfg.persistent_grow)
+    return Status(LGBM_B200_ERR_UNSUPPORTED, "the persistent launch has no per-step launch shape");
+  if (!h->trained) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "autotune replays the last train call: train first");
+  if (num < 1 || reps < 1 || reps > 1000) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "candidates or reps");
+  for (int32_t i = 0; i < num; ++i) {
+    Status st = check_launch_shape(cand[i]);
+    if (!st.ok()) return st;
+  }
+  CU(cudaSetDevice(h->device));
+  cudaStream_t s = h->stream;
+  // events and the per-step timing flag are restored on every exit
+  struct Guard {
+    LgbmB200Learner* h;
+    bool timing;
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Guard() {
+      for (auto x : e)
+        if (x) cudaEventDestroy(x);
+      h->timing = timing;
+    }
+  } g{h, h->timing};
+  h->timing = false;
+  CU(cudaEventCreate(&g.e[0]));
+  CU(cudaEventCreate(&g.e[1]));
+  Status st = prepare_tree(h, nullptr, nullptr, LGBM_B200_DEVICE, true);
+  if (!st.ok()) return st;
+  std::vector<DSlotState> ss((size_t)h->K);
+  std::vector<float> t((size_t)reps);
+  int32_t best = -1;
+  for (int32_t i = 0; i < num; ++i) {
+    if (!(st = set_launch_shape(h, cand[i])).ok()) return st;
+    if (!(st = run_tree(h)).ok()) return st;  // captures the graph
+    for (int32_t r = 0; r < reps; ++r) {
+      CU(cudaEventRecord(g.e[0], s));
+      if (!(st = run_tree(h)).ok()) return st;
+      CU(cudaEventRecord(g.e[1], s));
+      CU(cudaEventSynchronize(g.e[1]));
+      CU(cudaEventElapsedTime(&t[(size_t)r], g.e[0], g.e[1]));
+    }
+    for (int k = 0; k < h->K; ++k)
+      CU(cudaMemcpyAsync(&ss[(size_t)k], h->slots_h[k].st, sizeof(DSlotState), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    for (const DSlotState& x : ss)
+      if (x.status == kStatusTimeout) return Status(LGBM_B200_ERR_TIMEOUT, "device-side wait timed out (partition)");
+    std::sort(t.begin(), t.end());
+    ms[i] = (double)t[(size_t)reps / 2];
+    if (best < 0 || ms[i] < ms[best]) best = i;
+  }
+  *chosen = best;
+  return set_launch_shape(h, cand[best]);
 }
 
 // The learner's histogram kernel over an arbitrary row subset of the
@@ -921,6 +1021,27 @@ int lgbm_b200_learner_elapsed(LgbmB200Learner* h, int32_t a, int32_t b, double* 
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   *ms = t;
   return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_get_launch_shape(LgbmB200Learner* h, LgbmB200LaunchShape* out) {
+  if (!h || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  Status st = lgbm_b200::get_launch_shape(h, out);
+  return st.ok() ? LGBM_B200_OK : fail(st);
+}
+
+int lgbm_b200_learner_set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape* shape) {
+  if (!h || !shape) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  if (cudaSetDevice(h->device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  Status st = lgbm_b200::set_launch_shape(h, *shape);
+  return st.ok() ? LGBM_B200_OK : fail(st);
+}
+
+int lgbm_b200_learner_autotune(LgbmB200Learner* h, const LgbmB200LaunchShape* candidates, int32_t num_candidates,
+                               int32_t reps, int32_t* chosen, double* ms_per_tree) {
+  if (!h || !candidates || !chosen || !ms_per_tree)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  Status st = lgbm_b200::autotune(h, candidates, num_candidates, reps, chosen, ms_per_tree);
+  return st.ok() ? LGBM_B200_OK : fail(st);
 }
 
 int lgbm_b200_learner_set_timing(LgbmB200Learner* h, int32_t enabled) {

@@ -281,6 +281,10 @@ struct LgbmB200Learner {
   int fused_grid = 0;
   bool scan_part = false;  // scans and partition of a step in one cooperative launch
   int scan_part_grid = 0;
+  int scan_part_max = 0;  // CTAs of that launch resident at once, shared by the slots
+  // the last train call: whether one ran, and each slot's quantization offset
+  bool trained = false;
+  std::vector<int64_t> last_start;
   int32_t last_launches = 0;
   // captured tree growth
   cudaGraphExec_t graph_exec = nullptr;
@@ -304,6 +308,10 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
 // train in two halves: enqueue the tree's work; read the trees back (synchronises)
 Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
 Status train_collect(LgbmB200Learner* h);
+Status get_launch_shape(const LgbmB200Learner* h, LgbmB200LaunchShape* out);
+Status set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape& in);
+Status autotune(LgbmB200Learner* h, const LgbmB200LaunchShape* cand, int32_t num, int32_t reps, int32_t* chosen,
+                double* ms);
 Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int64_t nrows, void* out);
 }  // namespace lgbm_b200
 

@@ -95,6 +95,10 @@ class BoostConfig(C.Structure):
                 ("feature_fraction", f64), ("feature_fraction_seed", i32)]
 
 
+class LaunchShape(C.Structure):
+    _fields_ = [("partition_ctas", i32), ("hist_ctas", i32), ("hist_rows_per_block", i32)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "lgbm_b200_last_error": (C.c_char_p, []),
@@ -115,6 +119,9 @@ SIGNATURES = {
     "lgbm_b200_learner_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, i32, P(TreeView)]),
     "lgbm_b200_learner_add_leaf_outputs": (C.c_int, [C.c_void_p, i32, P(f64), i32, C.c_void_p, i32]),
     "lgbm_b200_learner_get_partition": (C.c_int, [C.c_void_p, i32, P(i32), P(i32), P(C.c_uint32)]),
+    "lgbm_b200_learner_get_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),
+    "lgbm_b200_learner_set_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),
+    "lgbm_b200_learner_autotune": (C.c_int, [C.c_void_p, P(LaunchShape), i32, i32, P(i32), P(f64)]),
     "lgbm_b200_learner_set_timing": (C.c_int, [C.c_void_p, i32]),
     "lgbm_b200_learner_last_timing": (C.c_int, [C.c_void_p, P(f64), P(i64), P(i32)]),
     "lgbm_b200_learner_last_rows": (C.c_int, [C.c_void_p, P(i64), P(i64), P(i32)]),

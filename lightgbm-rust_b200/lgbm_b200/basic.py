@@ -306,6 +306,30 @@ class Learner:
         L.check(L.lib().lgbm_b200_learner_elapsed(self.handle, int(a), int(b), C.byref(ms)))
         return ms.value
 
+    @property
+    def launch_shape(self):
+        """The per-step kernels' launch shape: partition_ctas, hist_ctas and
+        hist_rows_per_block (dict)."""
+        s = L.LaunchShape()
+        L.check(L.lib().lgbm_b200_learner_get_launch_shape(self.handle, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in L.LaunchShape._fields_}
+
+    @launch_shape.setter
+    def launch_shape(self, shape):
+        s = L.LaunchShape(*(int(shape[k]) for k, _ in L.LaunchShape._fields_))
+        L.check(L.lib().lgbm_b200_learner_set_launch_shape(self.handle, C.byref(s)))
+
+    def time_shapes(self, shapes, reps=3):
+        """Regrow the last train call's trees under each shape (the same
+        trees), keep the fastest; returns (index chosen, median ms per tree
+        of each shape)."""
+        arr = (L.LaunchShape * len(shapes))(*(L.LaunchShape(*(int(sh[k]) for k, _ in L.LaunchShape._fields_))
+                                              for sh in shapes))
+        ms = (C.c_double * len(shapes))()
+        chosen = C.c_int32()
+        L.check(L.lib().lgbm_b200_learner_autotune(self.handle, arr, len(shapes), int(reps), C.byref(chosen), ms))
+        return int(chosen.value), list(ms)
+
     def set_timing(self, on):
         L.check(L.lib().lgbm_b200_learner_set_timing(self.handle, int(bool(on))))
 
