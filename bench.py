@@ -227,9 +227,10 @@ def run_form(lgb, data, ds, dv, form, args, device):
     steps_per_tree = int(params["num_leaves"]) - 1
     hist_launches = args.steps * (1 if fused else steps_per_tree)
     hist_bytes = rows * hist_bytes_per_row(nf, form)
-    # fused form: the partition moves each row of the split leaf and adds it to
+    # the partition moves each row of the split leaf: index in, its byte of the
+    # split feature (column copy), index out; the fused form also adds the row to
     # its child's histogram: index in, bin row, packed gradient, index out
-    part_bytes = prows * (4 + nf + 4 + 4)
+    part_bytes = prows * ((4 + nf + 4 + 4) if fused else (4 + 1 + 4))
     return {
         "ms_per_step": ms, "wall_ms_per_step": 1000 * wall / args.steps, "s_per_500": ms * ROUNDS / 1000.0,
         "auc": auc, "auc_device": auc_device, "auc_device_ms": auc_device_ms, "auc_numpy_ms": auc_numpy_ms,
@@ -551,8 +552,20 @@ def main():
                       "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]}),
         "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 5),
+        # device-time shares of the three split-step kernels (events around every launch)
+        "kernel_share": {k: r[f"{k}_ms_per_step"] / (r["hist_ms_per_step"] + r["scan_ms_per_step"] +
+                                                     r["partition_ms_per_step"])
+                         for k in ("hist", "scan", "partition")},
         "clocks": r["clocks"],
     }
+    if not r["fused"]:
+        # the row partition, the largest share of device time (its launches are
+        # latency-bound: most leaves are small)
+        line["roofline_partition"] = {
+            "bound": "hbm", "kernel": "k_partition", "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": r["part_gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
+            "bytes_per_row": 9, "bytes_per_launch": r["part_bytes_per_launch"],
+            "ms_per_launch": r["part_ms_per_launch"]}
     if "f64" in res and head in res:
         line["speedup_vs_f64"] = res["f64"]["ms_per_step"] / res[head]["ms_per_step"]
         line["auc_delta_vs_f64"] = res[head]["auc"] - res["f64"]["auc"]

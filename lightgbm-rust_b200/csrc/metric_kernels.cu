@@ -14,6 +14,7 @@
 // The losses are FP64 sums of per-row terms; their order differs from the
 // reference's sequential loop (within a few ulps of the mean).
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "learner_impl.h"
@@ -210,17 +211,47 @@ __global__ void __launch_bounds__(kSortBlock) k_auc_groups(const uint64_t* key, 
 
 namespace {
 
-Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const double* score, int64_t n,
-                     cudaStream_t s, double* out) {
-  std::vector<void*> bufs;
-  auto dalloc = [&](void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
-    if (e == cudaSuccess) bufs.push_back(*p);
-    return e;
-  };
-  auto free_all = [&]() {
-    for (void* p : bufs) cudaFree(p);
-  };
+// Device memory of metric_eval, one set per device: allocated on first use
+// and reallocated only when a call needs more (never shrunk), so a call
+// allocates and frees nothing (cudaFree synchronises the whole device).
+// Calls on one device are serialised by the mutex. The buffers live until
+// the process ends.
+enum WsSlot { kWsKey, kWsCls, kWsBlockPos, kWsBefore, kWsAcc, kWsPartial, kWsLabel, kWsScore, kWsSlots };
+constexpr int kMaxMetricDevices = 64;
+
+struct MetricWorkspace {
+  std::mutex mu;
+  void* buf[kWsSlots] = {};
+  size_t cap[kWsSlots] = {};
+  cudaError_t get(WsSlot slot, size_t bytes, void** p) {
+    bytes = std::max<size_t>(bytes, 256);
+    if (cap[slot] < bytes) {
+      if (buf[slot]) {
+        cudaError_t e = cudaFree(buf[slot]);
+        buf[slot] = nullptr;
+        cap[slot] = 0;
+        if (e != cudaSuccess) return e;
+      }
+      cudaError_t e = cudaMalloc(&buf[slot], bytes);
+      if (e != cudaSuccess) {
+        buf[slot] = nullptr;
+        return e;
+      }
+      cap[slot] = bytes;
+    }
+    *p = buf[slot];
+    return cudaSuccess;
+  }
+};
+
+MetricWorkspace& metric_workspace(int device) {
+  static MetricWorkspace ws[kMaxMetricDevices];
+  return ws[device];
+}
+
+Status metric_device(MetricWorkspace& ws, const LgbmB200MetricConfig& cfg, const float* label, const double* score,
+                     int64_t n, cudaStream_t s, double* out) {
+  auto dalloc = [&](WsSlot slot, void** p, size_t bytes) { return ws.get(slot, bytes, p); };
   cudaError_t e = cudaSuccess;
   if (cfg.metric == LGBM_B200_METRIC_AUC) {
     int64_t m = kSortBlock;
@@ -231,14 +262,12 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
     int32_t* block_pos = nullptr;
     int64_t* before = nullptr;
     double* acc = nullptr;
-    if ((e = dalloc((void**)&key, sizeof(uint64_t) * m)) != cudaSuccess ||
-        (e = dalloc((void**)&cls, (size_t)m)) != cudaSuccess ||
-        (e = dalloc((void**)&block_pos, sizeof(int32_t) * nb)) != cudaSuccess ||
-        (e = dalloc((void**)&before, sizeof(int64_t) * nb)) != cudaSuccess ||
-        (e = dalloc((void**)&acc, sizeof(double))) != cudaSuccess) {
-      free_all();
+    if ((e = dalloc(kWsKey, (void**)&key, sizeof(uint64_t) * m)) != cudaSuccess ||
+        (e = dalloc(kWsCls, (void**)&cls, (size_t)m)) != cudaSuccess ||
+        (e = dalloc(kWsBlockPos, (void**)&block_pos, sizeof(int32_t) * nb)) != cudaSuccess ||
+        (e = dalloc(kWsBefore, (void**)&before, sizeof(int64_t) * nb)) != cudaSuccess ||
+        (e = dalloc(kWsAcc, (void**)&acc, sizeof(double))) != cudaSuccess)
       return Status(LGBM_B200_ERR_CUDA, std::string("metric: ") + cudaGetErrorString(e));
-    }
     const int grid = (int)std::min<int64_t>((m + 255) / 256, current_device_sms() * 16);
     k_auc_keys<<<grid, 256, 0, s>>>(label, score, n, m, key, cls);
     // bitonic sort: stages up to kSortBlock in shared memory, then each larger
@@ -267,7 +296,6 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(&accum, acc, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    free_all();
     if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("metric: ") + cudaGetErrorString(e));
     const double sp = (double)sum_pos, sw = (double)n;
     *out = (sp > 0.0 && sp != sw) ? accum / (sp * (sw - sp)) : 1.0;  // metric.rs:724-730
@@ -281,16 +309,13 @@ Status metric_device(const LgbmB200MetricConfig& cfg, const float* label, const 
   a.neg_log_eps = -(double)std::log(1e-15f);  // consts.rs neg_log_epsilon: the f32 log, promoted
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, current_device_sms() * 8));
   double* partial = nullptr;
-  if ((e = dalloc((void**)&partial, sizeof(double) * grid)) != cudaSuccess) {
-    free_all();
+  if ((e = dalloc(kWsPartial, (void**)&partial, sizeof(double) * grid)) != cudaSuccess)
     return Status(LGBM_B200_ERR_CUDA, std::string("metric: ") + cudaGetErrorString(e));
-  }
   k_metric_sum<<<grid, 256, 0, s>>>(a, label, score, n, partial);
   std::vector<double> ph((size_t)grid);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(ph.data(), partial, sizeof(double) * grid, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  free_all();
   if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("metric: ") + cudaGetErrorString(e));
   double sum = 0.0;
   for (double v : ph) sum += v;
@@ -313,26 +338,27 @@ extern "C" int lgbm_b200_metric_eval(const LgbmB200MetricConfig* cfg, const floa
     return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "metric: unknown metric"));
   const bool multi = cfg->metric == LGBM_B200_METRIC_MULTI_LOGLOSS || cfg->metric == LGBM_B200_METRIC_MULTI_ERROR;
   if (multi && cfg->num_class < 2) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "metric: num_class < 2"));
+  if (device < 0 || device >= kMaxMetricDevices) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "metric: device"));
   if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
   const int64_t ns = n * (multi ? cfg->num_class : 1);
+  MetricWorkspace& ws = metric_workspace(device);
+  std::lock_guard<std::mutex> lock(ws.mu);
+  // the legacy default stream: device inputs written by work on it are ordered before the metric
   if (location == LGBM_B200_DEVICE) {
-    Status st = metric_device(*cfg, label, score, n, 0, out);
+    Status st = metric_device(ws, *cfg, label, score, n, 0, out);
     return st.ok() ? LGBM_B200_OK : fail(st);
   }
   float* ld = nullptr;
   double* sd = nullptr;
-  if (cudaMalloc(&ld, sizeof(float) * n) != cudaSuccess || cudaMalloc(&sd, sizeof(double) * ns) != cudaSuccess) {
-    if (ld) cudaFree(ld);
+  if (ws.get(kWsLabel, sizeof(float) * n, (void**)&ld) != cudaSuccess ||
+      ws.get(kWsScore, sizeof(double) * ns, (void**)&sd) != cudaSuccess)
     return fail(Status(LGBM_B200_ERR_CUDA, "metric: cudaMalloc"));
-  }
   Status st;
   if (cudaMemcpy(ld, label, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(sd, score, sizeof(double) * ns, cudaMemcpyHostToDevice) != cudaSuccess)
     st = Status(LGBM_B200_ERR_CUDA, "metric: copy");
   else
-    st = metric_device(*cfg, ld, sd, n, 0, out);
-  cudaFree(ld);
-  cudaFree(sd);
+    st = metric_device(ws, *cfg, ld, sd, n, 0, out);
   return st.ok() ? LGBM_B200_OK : fail(st);
 }
 
