@@ -36,6 +36,10 @@ WORKLOAD = ("binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), m
 # ncu capture of a 5M-row root launch (profiles/k_hist_k_scan_k_partition_binary5M_quantized.md);
 # traffic grows with the rows of a launch, so a launch's traffic is this times its rows
 HIST_DRAM_BYTES_PER_ROW = 40.8
+# DRAM bytes per moved row of the partition kernel, from the ncu capture of its
+# first launch in a 5M-row run (the root split: every row; profiles/k_partition_root_binary5M_quantized.md).
+# The index writes stay in L2 during the launch, so this is below the 9 algorithmic bytes.
+PART_DRAM_BYTES_PER_ROW = 5.02
 METRIC = "s per 500 rounds (quantized hist, equal AUC to FP64) + hist GB/s"
 ROUNDS = 500
 
@@ -563,7 +567,9 @@ def main():
         # latency-bound: most leaves are small)
         line["roofline_partition"] = {
             "bound": "hbm", "kernel": "k_partition", "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s",
-            "frac": r["part_gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
+            "frac": r["part_gbs"] / peak, "peak_kind": peak_kind,
+            "traffic": PART_DRAM_BYTES_PER_ROW * r["part_rows_per_tree"] / (int(data["params"]["num_leaves"]) - 1),
+            "traffic_note": "ncu DRAM bytes per row of the 5M-row root split x rows per launch (average)",
             "bytes_per_row": 9, "bytes_per_launch": r["part_bytes_per_launch"],
             "ms_per_launch": r["part_ms_per_launch"]}
     if "f64" in res and head in res:
