@@ -2,6 +2,7 @@
 // the stand-alone objective gradients (RowObjective::gradients) and the
 // batched predictor (predict.rs:231), behind the C ABI of include/lgbm_b200.h.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -121,7 +122,13 @@ struct LgbmB200Booster {
   // (a mask is sent without a synchronisation, and only when it changes)
   std::vector<std::vector<uint8_t>> sent_mask;
   uint8_t* mask_h = nullptr;
+  // one captured graph per iteration (gradients, quantization, the tree, the
+  // score updates), recaptured when the learner's launch settings change
+  bool iter_graph = true;
+  cudaGraphExec_t iter_exec = nullptr;
+  int iter_key = -1;
   ~LgbmB200Booster() {
+    if (iter_exec) cudaGraphExecDestroy(iter_exec);
     arena.free_all();
     if (mask_h) cudaFreeHost(mask_h);
   }
@@ -194,6 +201,9 @@ static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB
     if (!(s = A.alloc_n(&b->counts, 2)).ok()) return s;
     b->bag_cnt = (int32_t)n;
   }
+  // LGBM_B200_ITER_GRAPH=0: every iteration runs launch by launch (each tree
+  // still replays its own graph)
+  if (const char* e = std::getenv("LGBM_B200_ITER_GRAPH")) b->iter_graph = std::atoi(e) != 0;
   b->col_rand = std::make_unique<Lcg>(cfg->feature_fraction_seed);
   int32_t total = L->nf;
   b->used_cnt_bytree = cfg->feature_fraction < 1.0
@@ -211,6 +221,46 @@ __global__ void k_shrink_leaves(const __grid_constant__ DCtx c, double rate, dou
   const int32_t nl = s.st->num_leaves_cur;
   for (int32_t l = threadIdx.x; l < L; l += blockDim.x)
     lv[(size_t)blockIdx.z * L + l] = (nl > 1 && l < nl) ? maybe_round_to_zero(s.tree.leaf_value[l] * rate) : 0.0;
+}
+
+// Score updates (boosting.rs:1381-1408) with the leaf values shrunk on the
+// device, enqueued before the trees are read back.
+static Status enqueue_score_updates(LgbmB200Booster* b) {
+  LgbmB200Learner* L = b->L;
+  cudaStream_t s = L->stream;
+  const int K = b->K;
+  const int64_t n = b->n;
+  const int sms = L->num_sms;
+  DCtx c = L->ctx;
+  k_shrink_leaves<<<dim3(1, 1, K), 256, 0, s>>>(c, b->cfg.learning_rate, b->lv_dev, L->L);
+  CU_LAUNCH();
+  k_add_leaf_outputs<<<dim3(sms * 4, 1, K), 256, 16 * (size_t)L->L, s>>>(c, b->lv_dev, L->L, b->score, n);
+  CU_LAUNCH();
+  if (b->bagging && b->oob_cnt > 0) {
+    k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->oob_cnt + 255) / 256, sms * 8)), 1, K), 256, 0,
+                        s>>>(c, c.bins, c.stride, b->oob, b->oob_cnt, b->lv_dev, L->L, b->score, n);
+    CU_LAUNCH();
+  }
+  if (b->nv > 0) {
+    k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->nv + 255) / 256, sms * 8)), 1, K), 256, 0, s>>>(
+        c, b->valid_bins, b->valid_stride, nullptr, b->nv, b->lv_dev, L->L, b->valid_score, b->nv);
+    CU_LAUNCH();
+  }
+  return Status();
+}
+
+// One iteration's device work after the masks and the quantization offsets
+// are staged: gradients, quantization, the tree's launches and the score
+// updates. No launch carries a value that changes between iterations, so the
+// sequence is captured once and replayed.
+static Status enqueue_iteration(LgbmB200Booster* b) {
+  LgbmB200Learner* L = b->L;
+  Status st = launch_gradients(b->cfg.objective, b->label_d, b->score, b->n, L->gh_all, nullptr, nullptr, L->num_sms,
+                               L->stream, b->rank ? &b->rank->d : nullptr);
+  if (!st.ok()) return st;
+  if (L->cfg.hist_precision == LGBM_B200_HIST_QUANT && !(st = enqueue_quant(L)).ok()) return st;
+  if (!(st = enqueue_tree(L)).ok()) return st;
+  return enqueue_score_updates(b);
 }
 
 static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
@@ -237,9 +287,17 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
     }
     b->init_scores = init;
   }
-  Status st = launch_gradients(b->cfg.objective, b->label_d, b->score, n, L->gh_all, nullptr, nullptr, sms, s,
-                               b->rank ? &b->rank->d : nullptr);
-  if (!st.ok()) return st;
+  // the first iteration (boost from average, constant trees) and bagged ones
+  // (the bag size is read back mid-iteration) run launch by launch; the others
+  // replay one captured graph
+  const bool graphed = b->iter_graph && !b->first && !b->bagging && L->cfg.use_cuda_graph &&
+                       !L->cfg.persistent_grow && !L->timing;
+  Status st;
+  if (!graphed) {
+    st = launch_gradients(b->cfg.objective, b->label_d, b->score, n, L->gh_all, nullptr, nullptr, sms, s,
+                          b->rank ? &b->rank->d : nullptr);
+    if (!st.ok()) return st;
+  }
   // bagging (sample_strategy.rs:280-320)
   if (b->bagging && ((b->bag_cnt < n && b->iter % b->cfg.bagging_freq == 0) || b->need_re_bagging)) {
     b->need_re_bagging = false;
@@ -274,25 +332,31 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
       b->sent_mask[(size_t)k] = used;
     }
   }
-  if (!(st = train_enqueue(L, nullptr, nullptr, LGBM_B200_DEVICE)).ok()) return st;
-  // score updates (boosting.rs:1381-1408) with the leaf values shrunk on the
-  // device, enqueued before the trees are read back
-  {
-    DCtx c = L->ctx;
-    k_shrink_leaves<<<dim3(1, 1, K), 256, 0, s>>>(c, b->cfg.learning_rate, b->lv_dev, L->L);
-    CU_LAUNCH();
-    k_add_leaf_outputs<<<dim3(sms * 4, 1, K), 256, 16 * (size_t)L->L, s>>>(c, b->lv_dev, L->L, b->score, n);
-    CU_LAUNCH();
-    if (b->bagging && b->oob_cnt > 0) {
-      k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->oob_cnt + 255) / 256, sms * 8)), 1, K), 256, 0,
-                          s>>>(c, c.bins, c.stride, b->oob, b->oob_cnt, b->lv_dev, L->L, b->score, n);
-      CU_LAUNCH();
+  if (graphed) {
+    // the offsets are drawn on the host and staged; the graph's copy reads them
+    if (L->cfg.hist_precision == LGBM_B200_HIST_QUANT) draw_quant_starts(L, false);
+    if (b->iter_exec == nullptr || b->iter_key != L->config_epoch) {
+      if (b->iter_exec) {
+        cudaGraphExecDestroy(b->iter_exec);
+        b->iter_exec = nullptr;
+      }
+      cudaGraph_t g;
+      CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      st = enqueue_iteration(b);
+      cudaError_t e = cudaStreamEndCapture(s, &g);
+      if (!st.ok()) return st;
+      if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&b->iter_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+      b->iter_key = L->config_epoch;
     }
-    if (b->nv > 0) {
-      k_add_tree_binned<<<dim3(std::max(1, (int)std::min<int64_t>((b->nv + 255) / 256, sms * 8)), 1, K), 256, 0, s>>>(
-          c, b->valid_bins, b->valid_stride, nullptr, b->nv, b->lv_dev, L->L, b->valid_score, b->nv);
-      CU_LAUNCH();
-    }
+    CU(cudaGraphLaunch(b->iter_exec, s));
+    L->trained = true;
+    L->last_ms[0] = L->last_ms[1] = L->last_ms[2] = L->last_ms[3] = 0;
+  } else {
+    if (!(st = train_enqueue(L, nullptr, nullptr, LGBM_B200_DEVICE)).ok()) return st;
+    if (!(st = enqueue_score_updates(b)).ok()) return st;
   }
   if (!(st = train_collect(L)).ok()) return st;  // synchronises
   bool should_continue = false;

@@ -137,8 +137,9 @@ __global__ void k_grad_softmax(const float* label, const double* score, int64_t 
 __global__ void k_interleave(const float* g, const float* h, int64_t n, float2* gh);
 __global__ void k_quant_absmax(const float2* gh, int64_t n, unsigned long long* maxbits, int32_t* counter,
                                DSlotState* st, int32_t bins, int32_t const_hess, int32_t num_blocks);
-__global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv, int64_t start,
-                              const DSlotState* st, int32_t const_hess, int32_t stochastic, int32_t* packed);
+__global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv,
+                              const int64_t* start_dev, const DSlotState* st, int32_t const_hess, int32_t stochastic,
+                              int32_t* packed);
 __global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag);
 __global__ void k_compact_bag(const uint8_t* in_bag, int64_t n, uint32_t* bag, uint32_t* oob, int32_t* counts,
                               int32_t* block_counts, int32_t num_blocks);

@@ -299,6 +299,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
       CU(cudaMemcpy(h->hrv, hh.data(), n * sizeof(double), cudaMemcpyHostToDevice));
     }
     h->start_eng = std::make_unique<Mt19937>((uint32_t)cfg->seed);
+    if (!(s = A.alloc_n(&h->start_dev, (size_t)K)).ok()) return s;
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&h->start_h), sizeof(int64_t) * K, cudaHostAllocDefault));
   }
   // context
   DCtx& c = h->ctx;
@@ -347,7 +349,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
 
 // Enqueue one whole tree (every slot) on the stream: init, the split steps
 // and leaf renewal. Nothing here reads device memory back.
-static Status enqueue_tree(LgbmB200Learner* h) {
+Status enqueue_tree(LgbmB200Learner* h) {
   const DCtx& c = h->ctx;
   const int K = h->K, L = h->L;
   const int mode = h->cfg.hist_precision;
@@ -511,6 +513,42 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
   return st.ok() ? train_collect(h) : st;
 }
 
+// The quantization offsets of the next tree, one per slot in slot order:
+// drawn from the tree-start engine (learner/quant.rs:114), or the last
+// tree's again (`replay`). They go to pinned staging, which is written only
+// after the stream's last synchronisation (every train and booster iteration
+// ends with one), and which the copy in enqueue_quant reads when it runs.
+void draw_quant_starts(LgbmB200Learner* h, bool replay) {
+  const int K = h->K;
+  if (h->last_start.size() < (size_t)K) h->last_start.resize((size_t)K, 0);
+  for (int k = 0; k < K; ++k) {
+    const int64_t start = replay ? h->last_start[k] : h->start_eng->uniform_int(0, (int32_t)h->n);
+    h->last_start[k] = start;
+    h->start_h[k] = start;
+  }
+}
+
+// The quantization of every slot's gradients (learner/quant.rs:92-158),
+// enqueued: the offsets staged by draw_quant_starts, then each slot's max-abs
+// and packing. Nothing here depends on host values that change per tree, so
+// it can be captured once and replayed.
+Status enqueue_quant(LgbmB200Learner* h) {
+  cudaStream_t s = h->stream;
+  const int64_t n = h->n;
+  CU(cudaMemcpyAsync(h->start_dev, h->start_h, sizeof(int64_t) * h->K, cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < h->K; ++k) {
+    int blocks = h->num_sms * 4;
+    k_quant_absmax<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->maxbits, h->quant_counter, h->slots_h[k].st,
+                                          h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks);
+    CU_LAUNCH();
+    k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, h->start_dev + k, h->slots_h[k].st,
+                                         h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
+                                         h->slots_h[k].packed);
+    CU_LAUNCH();
+  }
+  return Status();
+}
+
 // The gradients and their quantization for one tree, enqueued on the
 // learner's stream. `replay` quantizes with the last call's offsets instead
 // of drawing new ones (the autotuner's replays of the same tree).
@@ -541,19 +579,8 @@ static Status prepare_tree(LgbmB200Learner* h, const float* grad, const float* h
     }
   }
   if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT) {
-    for (int k = 0; k < K; ++k) {
-      int blocks = h->num_sms * 4;
-      k_quant_absmax<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->maxbits, h->quant_counter, h->slots_h[k].st,
-                                            h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks);
-      CU_LAUNCH();
-      if (h->last_start.size() < (size_t)K) h->last_start.resize((size_t)K, 0);
-      const int64_t start = replay ? h->last_start[k] : h->start_eng->uniform_int(0, (int32_t)n);
-      h->last_start[k] = start;
-      k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, start, h->slots_h[k].st,
-                                           h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
-                                           h->slots_h[k].packed);
-      CU_LAUNCH();
-    }
+    draw_quant_starts(h, replay);
+    return enqueue_quant(h);
   }
   return Status();
 }
@@ -639,6 +666,7 @@ Status set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape& in) {
   h->hist_grid = (in.hist_ctas + cl - 1) / cl * cl;
   h->ctx.rows_per_block = in.hist_rows_per_block;
   if (h->scan_part) h->scan_part_grid = std::max(1, std::min(h->part_grid, h->scan_part_max));
+  h->config_epoch += 1;
   if (h->graph_exec) {  // the captured launches carry the old grids
     CU(cudaGraphExecDestroy(h->graph_exec));
     h->graph_exec = nullptr;
@@ -837,6 +865,7 @@ int lgbm_b200_learner_set_bagging(LgbmB200Learner* h, const uint32_t* used, int6
     cudaError_t e0 = cudaMemcpyAsync(h->n_used_dev, &nn, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
     if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(h->stream);
     if (e0 != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e0)));
+    h->config_epoch += 1;
     return LGBM_B200_OK;
   }
   if (num_used < 0 || num_used > h->n) return fail(Status(LGBM_B200_ERR_INVALID_DATA, "bag size"));
@@ -851,6 +880,7 @@ int lgbm_b200_learner_set_bagging(LgbmB200Learner* h, const uint32_t* used, int6
   h->bagging = true;
   h->n_used = (int32_t)num_used;
   h->ctx.bagging = num_used < h->n ? 1 : 0;
+  h->config_epoch += 1;
   return LGBM_B200_OK;
 }
 

@@ -252,6 +252,8 @@ struct LgbmB200Learner {
   double* grv = nullptr;
   double* hrv = nullptr;
   std::unique_ptr<Mt19937> start_eng;
+  int64_t* start_dev = nullptr;  // [K] each slot's offset into the rounding tables, read by k_quant_apply
+  int64_t* start_h = nullptr;    // [K] pinned staging of those offsets
   unsigned long long* maxbits = nullptr;
   int32_t* quant_counter = nullptr;
   // bagging
@@ -285,6 +287,9 @@ struct LgbmB200Learner {
   // the last train call: whether one ran, and each slot's quantization offset
   bool trained = false;
   std::vector<int64_t> last_start;
+  // bumped whenever a host-side setting that enqueue_tree's launches carry
+  // changes (launch shape, bagging): graphs captured before it are stale
+  int config_epoch = 0;
   int32_t last_launches = 0;
   // captured tree growth
   cudaGraphExec_t graph_exec = nullptr;
@@ -296,6 +301,7 @@ struct LgbmB200Learner {
       if (e) cudaEventDestroy(e);
     arena.free_all();
     chunks.release();
+    if (start_h) cudaFreeHost(start_h);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -308,6 +314,12 @@ Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t l
 // train in two halves: enqueue the tree's work; read the trees back (synchronises)
 Status train_enqueue(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);
 Status train_collect(LgbmB200Learner* h);
+// the pieces of train_enqueue a captured booster iteration uses: the host
+// draw of the quantization offsets, then (capturable) their copy and the
+// quantization, and the launches of one tree
+void draw_quant_starts(LgbmB200Learner* h, bool replay);
+Status enqueue_quant(LgbmB200Learner* h);
+Status enqueue_tree(LgbmB200Learner* h);
 Status get_launch_shape(const LgbmB200Learner* h, LgbmB200LaunchShape* out);
 Status set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape& in);
 Status autotune(LgbmB200Learner* h, const LgbmB200LaunchShape* cand, int32_t num, int32_t reps, int32_t* chosen,

@@ -111,10 +111,14 @@ __device__ __forceinline__ int32_t to_i8(double x) {
   return (int32_t)(int8_t)t;
 }
 
-// quant.rs:434-447; packed[i] = (g << 16) + (h as u8).
+// quant.rs:434-447; packed[i] = (g << 16) + (h as u8). The tree's start
+// offset into the rounding tables is read from device memory, so a captured
+// launch takes each tree's new offset.
 __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n, const double* grv,
-                                                     const double* hrv, int64_t start, const DSlotState* st,
-                                                     int32_t const_hess, int32_t stochastic, int32_t* packed) {
+                                                     const double* hrv, const int64_t* start_dev,
+                                                     const DSlotState* st, int32_t const_hess, int32_t stochastic,
+                                                     int32_t* packed) {
+  const int64_t start = *start_dev;
   const double inv_g = 1.0 / st->grad_scale;
   const double inv_h = 1.0 / st->hess_scale;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
