@@ -340,11 +340,14 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
         cudaGraphExecDestroy(b->iter_exec);
         b->iter_exec = nullptr;
       }
-      cudaGraph_t g;
+      cudaGraph_t g = nullptr;
       CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       st = enqueue_iteration(b);
       cudaError_t e = cudaStreamEndCapture(s, &g);
-      if (!st.ok()) return st;
+      if (!st.ok()) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+      }
       if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
       e = cudaGraphInstantiate(&b->iter_exec, g, 0);
       cudaGraphDestroy(g);

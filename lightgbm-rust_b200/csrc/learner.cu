@@ -419,11 +419,14 @@ static Status run_tree(LgbmB200Learner* h) {
       cudaGraphExecDestroy(h->graph_exec);
       h->graph_exec = nullptr;
     }
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     Status st = enqueue_tree(h);
     cudaError_t e = cudaStreamEndCapture(s, &g);
-    if (!st.ok()) return st;
+    if (!st.ok()) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
     if (e != cudaSuccess) return Status(LGBM_B200_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
     CU(cudaGraphInstantiate(&h->graph_exec, g, 0));
     cudaGraphDestroy(g);
