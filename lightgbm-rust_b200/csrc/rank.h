@@ -17,6 +17,8 @@ struct DRank {
   const double* label_gain;    // [31]
   const double* discount;      // [kRankMaxQuery]
   uint32_t* sorted;            // [n] per query: positions in descending score order
+  double* sorted_score;        // [n] the query's scores in that order
+  float* sorted_label;         // [n] the query's labels in that order
   double sigmoid, min_in, max_in, idx_factor;
   int32_t truncation_level;
   int32_t norm;

@@ -4,10 +4,20 @@
 // Two launches per call:
 //   k_rank_sort    one CTA per query (grid-stride): the stable descending
 //                  order of the query's scores (dcg.rs:167-179) by rank
-//                  counting in shared memory
-//   k_lambdarank   one thread per query: the reference's pair loop in its
-//                  order, so every f32 lambda / hessian accumulation and the
-//                  FP64 sum of lambdas are formed exactly as on the CPU
+//                  counting in shared memory, with the scores and labels
+//                  written out in that order
+//   k_lambdarank   one warp per query. The reference's pair loop (outer
+//                  position i below the truncation level, inner j > i) adds
+//                  to the row at position p first the pairs (i, p) for
+//                  i < p in order of i, then, when p itself is an outer
+//                  position, the pairs (p, j) in order of j. Lane l takes
+//                  the positions l, l + 32, ... and adds exactly those pairs
+//                  in that order in registers, so every f32 lambda and
+//                  hessian is formed as on the CPU. The FP64 sum of the
+//                  lambdas (for the normalisation) is one sequential chain
+//                  in the loop's order: the lanes compute 32 consecutive
+//                  pair values at a time and lane 0 subtracts them in order
+//                  (a skipped pair adds +0.0, which changes no sum).
 // The tables the reference builds in its constructor (label gains,
 // discounts, inverse max DCG per query, the 2^20-entry sigmoid table) are
 // built on the host by the same arithmetic and uploaded once.
@@ -28,7 +38,7 @@ __device__ __forceinline__ bool precedes(double sj, int j, double si, int i) {
   return j < i;
 }
 
-__global__ void __launch_bounds__(kRankSortThreads) k_rank_sort(DRank r, const double* score) {
+__global__ void __launch_bounds__(kRankSortThreads) k_rank_sort(DRank r, const double* score, const float* label) {
   __shared__ double s[kRankSmemScores];
   for (int32_t q = blockIdx.x; q < r.nq; q += gridDim.x) {
     const int32_t b0 = r.bnd[q], cnt = r.bnd[q + 1] - b0;
@@ -44,6 +54,8 @@ __global__ void __launch_bounds__(kRankSortThreads) k_rank_sort(DRank r, const d
       int32_t rank = 0;
       for (int j = 0; j < cnt; ++j) rank += precedes(src[j], j, si, i) ? 1 : 0;
       r.sorted[b0 + rank] = (uint32_t)i;
+      r.sorted_score[b0 + rank] = si;
+      r.sorted_label[b0 + rank] = label[b0 + i];
     }
   }
 }
@@ -54,85 +66,138 @@ __device__ __forceinline__ double rank_sigmoid(const DRank& r, double score) {  
   return r.sigmoid_table[(size_t)((score - r.min_in) * r.idx_factor)];
 }
 
-// LambdarankNDCG::one_query (rank.rs:192-262) for every query, one thread
+// One query's sorted scores and labels and the values its pairs share.
+struct QueryView {
+  const double* ssc;
+  const float* slb;
+  double inverse_max_dcg;
+  bool scale_by_score;  // norm and best_score != worst_score (rank.rs:231-233)
+};
+
+__device__ __forceinline__ QueryView query_view(const DRank& r, int32_t q, int32_t b0, int32_t cnt) {
+  QueryView v;
+  v.ssc = r.sorted_score + b0;
+  v.slb = r.sorted_label + b0;
+  v.inverse_max_dcg = r.inv_max_dcg[q];
+  const double best_score = v.ssc[0];
+  int32_t worst_idx = cnt - 1;
+  if (worst_idx > 0 && v.ssc[worst_idx] == kMinScoreD) worst_idx -= 1;
+  v.scale_by_score = r.norm && best_score != v.ssc[worst_idx];
+  return v;
+}
+
+// The pair of sorted positions a < b (labels la != lb, neither score the
+// minimum): its lambda and hessian by the reference's FP64 operations
+// (rank.rs:217-252), and whether a is the higher-labelled of the two. Both
+// rows of a pair evaluate the same operations, so they get the same values.
+__device__ __forceinline__ void pair_value(const DRank& r, const QueryView& v, int32_t a, int32_t b, float la,
+                                           float lb, double& p_lambda, double& p_hessian, bool& a_high) {
+  a_high = la > lb;
+  const int32_t high_rank = a_high ? a : b, low_rank = a_high ? b : a;
+  const double high_score = v.ssc[high_rank], low_score = v.ssc[low_rank];
+  const double high_label_gain = r.label_gain[(int32_t)(a_high ? la : lb)];
+  const double low_label_gain = r.label_gain[(int32_t)(a_high ? lb : la)];
+  const double high_discount = r.discount[high_rank], low_discount = r.discount[low_rank];
+  const double delta_score = high_score - low_score;
+  const double dcg_gap = high_label_gain - low_label_gain;
+  const double paired_discount = fabs(high_discount - low_discount);
+  double delta_pair_ndcg = dcg_gap * paired_discount * v.inverse_max_dcg;
+  if (v.scale_by_score) delta_pair_ndcg /= (double)0.01f + fabs(delta_score);
+  double pl = rank_sigmoid(r, delta_score);
+  double ph = pl * (1.0 - pl);
+  pl *= -r.sigmoid * delta_pair_ndcg;
+  ph *= r.sigmoid * r.sigmoid * delta_pair_ndcg;
+  p_lambda = pl;
+  p_hessian = ph;
+}
+
+constexpr int kRankWarps = 8;  // queries per CTA (one warp each)
+
+// LambdarankNDCG::one_query (rank.rs:192-262) for every query, one warp
 // each. Writes g/h (class-major float arrays) and/or the interleaved pairs.
-__global__ void __launch_bounds__(128) k_lambdarank(DRank r, const float* label, const double* score, float* g,
-                                                    float* h, float2* gh) {
-  for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < r.nq; q += gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kRankWarps * 32) k_lambdarank(DRank r, float* g, float* h, float2* gh) {
+  __shared__ double chain[kRankWarps][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int32_t T = r.truncation_level;
+  for (int64_t q = (int64_t)blockIdx.x * kRankWarps + wib; q < r.nq; q += (int64_t)gridDim.x * kRankWarps) {
     const int32_t b0 = r.bnd[q], cnt = r.bnd[q + 1] - b0;
-    const float* lb = label + b0;
-    const double* sc = score + b0;
-    const uint32_t* sorted = r.sorted + b0;
-    float* lam = g ? g + b0 : nullptr;
-    float* hes = h ? h + b0 : nullptr;
-    float2* pair = gh ? gh + b0 : nullptr;
-    // the accumulators live in the output (g / h, else the interleaved pairs)
-    auto add = [&](int32_t i, float dl, float dh) {
-      if (lam) {
-        lam[i] += dl;
-        hes[i] += dh;
-      } else {
-        pair[i].x += dl;
-        pair[i].y += dh;
-      }
-    };
-    for (int32_t i = 0; i < cnt; ++i) {
-      if (lam) {
-        lam[i] = 0.0f;
-        hes[i] = 0.0f;
-      } else {
-        pair[i] = make_float2(0.0f, 0.0f);
-      }
-    }
     if (cnt == 0) continue;
-    const double inverse_max_dcg = r.inv_max_dcg[q];
-    const double best_score = sc[sorted[0]];
-    int32_t worst_idx = cnt - 1;
-    if (worst_idx > 0 && sc[sorted[worst_idx]] == kMinScoreD) worst_idx -= 1;
-    const double worst_score = sc[sorted[worst_idx]];
-    double sum_lambdas = 0.0;
-    for (int32_t i = 0; i + 1 < cnt && i < r.truncation_level; ++i) {
-      const uint32_t si = sorted[i];
-      if (sc[si] == kMinScoreD) continue;
-      const float li = lb[si];
-      for (int32_t j = i + 1; j < cnt; ++j) {
-        const uint32_t sj = sorted[j];
-        if (sc[sj] == kMinScoreD) continue;
-        const float lj = lb[sj];
-        if (li == lj) continue;
-        int32_t high_rank = i, low_rank = j;
-        if (!(li > lj)) {
-          high_rank = j;
-          low_rank = i;
+    const QueryView v = query_view(r, (int32_t)q, b0, cnt);
+    // every row's lambda and hessian, the pairs added in the reference's order
+    for (int32_t p = lane; p < cnt; p += 32) {
+      float acc_l = 0.0f, acc_h = 0.0f;
+      const double sp = v.ssc[p];
+      const float lp = v.slb[p];
+      if (sp != kMinScoreD) {
+        // as the inner position: the outer positions i < p (all i + 1 < cnt)
+        const int32_t imax = min(p, T);
+        for (int32_t i = 0; i < imax; ++i) {
+          if (v.ssc[i] == kMinScoreD) continue;
+          const float li = v.slb[i];
+          if (li == lp) continue;
+          double pl, ph;
+          bool i_high;
+          pair_value(r, v, i, p, li, lp, pl, ph, i_high);
+          acc_l += i_high ? -(float)pl : (float)pl;  // the lower-labelled row takes -lambda
+          acc_h += (float)ph;
         }
-        const uint32_t high = sorted[high_rank], low = sorted[low_rank];
-        const double high_score = sc[high], low_score = sc[low];
-        const double high_label_gain = r.label_gain[(int32_t)lb[high]];
-        const double low_label_gain = r.label_gain[(int32_t)lb[low]];
-        const double high_discount = r.discount[high_rank], low_discount = r.discount[low_rank];
-        const double delta_score = high_score - low_score;
-        const double dcg_gap = high_label_gain - low_label_gain;
-        const double paired_discount = fabs(high_discount - low_discount);
-        double delta_pair_ndcg = dcg_gap * paired_discount * inverse_max_dcg;
-        if (r.norm && best_score != worst_score) delta_pair_ndcg /= (double)0.01f + fabs(delta_score);
-        double p_lambda = rank_sigmoid(r, delta_score);
-        double p_hessian = p_lambda * (1.0 - p_lambda);
-        p_lambda *= -r.sigmoid * delta_pair_ndcg;
-        p_hessian *= r.sigmoid * r.sigmoid * delta_pair_ndcg;
-        add((int32_t)low, -(float)p_lambda, (float)p_hessian);
-        add((int32_t)high, (float)p_lambda, (float)p_hessian);
-        sum_lambdas -= 2.0 * p_lambda;
+        // as the outer position
+        if (p < T && p + 1 < cnt) {
+          for (int32_t j = p + 1; j < cnt; ++j) {
+            if (v.ssc[j] == kMinScoreD) continue;
+            const float lj = v.slb[j];
+            if (lj == lp) continue;
+            double pl, ph;
+            bool p_high;
+            pair_value(r, v, p, j, lp, lj, pl, ph, p_high);
+            acc_l += p_high ? (float)pl : -(float)pl;
+            acc_h += (float)ph;
+          }
+        }
+      }
+      const uint32_t row = r.sorted[b0 + p];
+      if (g) {
+        g[b0 + row] = acc_l;
+        h[b0 + row] = acc_h;
+      } else {
+        gh[b0 + row] = make_float2(acc_l, acc_h);
       }
     }
-    if (r.norm && sum_lambdas > 0.0) {
+    if (!r.norm) continue;
+    // sum_lambdas -= 2 p_lambda over the pairs in the loop's order (lane 0's chain)
+    double sum_lambdas = 0.0;
+    for (int32_t i = 0; i + 1 < cnt && i < T; ++i) {
+      if (v.ssc[i] == kMinScoreD) continue;  // uniform over the warp
+      const float li = v.slb[i];
+      for (int32_t jb = i + 1; jb < cnt; jb += 32) {
+        const int32_t j = jb + lane;
+        double val = 0.0;
+        if (j < cnt && v.ssc[j] != kMinScoreD && v.slb[j] != li) {
+          double pl, ph;
+          bool i_high;
+          pair_value(r, v, i, j, li, v.slb[j], pl, ph, i_high);
+          val = 2.0 * pl;
+        }
+        chain[wib][lane] = val;
+        __syncwarp();
+        if (lane == 0) {
+          const int32_t m = min(32, cnt - jb);
+          for (int32_t k = 0; k < m; ++k) sum_lambdas -= chain[wib][k];
+        }
+        __syncwarp();
+      }
+    }
+    sum_lambdas = __shfl_sync(0xffffffffu, sum_lambdas, 0);
+    if (sum_lambdas > 0.0) {  // every lane's rows are written (the warp's stores are ordered by __syncwarp)
+      __syncwarp();
       const double norm_factor = log2(1.0 + sum_lambdas) / sum_lambdas;
-      for (int32_t i = 0; i < cnt; ++i) {
-        if (lam) {
-          lam[i] = (float)((double)lam[i] * norm_factor);
-          hes[i] = (float)((double)hes[i] * norm_factor);
+      for (int32_t x = lane; x < cnt; x += 32) {
+        if (g) {
+          g[b0 + x] = (float)((double)g[b0 + x] * norm_factor);
+          h[b0 + x] = (float)((double)h[b0 + x] * norm_factor);
         } else {
-          pair[i].x = (float)((double)pair[i].x * norm_factor);
-          pair[i].y = (float)((double)pair[i].y * norm_factor);
+          gh[b0 + x].x = (float)((double)gh[b0 + x].x * norm_factor);
+          gh[b0 + x].y = (float)((double)gh[b0 + x].y * norm_factor);
         }
       }
     }
@@ -186,7 +251,7 @@ Status launch_ndcg(const DRank& r, const float* label, const double* score, cons
                    double* out, int sms, cudaStream_t s) {
   if (r.nq == 0) return Status();
   const int sort_grid = (int)std::min<int64_t>(r.nq, (int64_t)sms * 16);
-  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score);
+  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score, label);
   CU_LAUNCH();
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((r.nq + 127) / 128, (int64_t)sms * 16));
   k_ndcg<<<grid, 128, 0, s>>>(r, label, ks, nk, out);
@@ -243,10 +308,13 @@ Status RankTables::build(const float* label_h, const int32_t* bnd_h, int32_t nq_
   int32_t* bnd_d;
   double *inv_d, *table_d, *gain_d, *disc_d;
   uint32_t* sorted_d;
+  double* sorted_score_d;
+  float* sorted_label_d;
+  const size_t n1 = (size_t)std::max<int64_t>(1, n);
   if (!(s = arena.alloc_n(&bnd_d, (size_t)nq + 1)).ok() || !(s = arena.alloc_n(&inv_d, std::max<size_t>(1, nq))).ok() ||
       !(s = arena.alloc_n(&table_d, table.size())).ok() || !(s = arena.alloc_n(&gain_d, label_gain.size())).ok() ||
-      !(s = arena.alloc_n(&disc_d, discount.size())).ok() ||
-      !(s = arena.alloc_n(&sorted_d, (size_t)std::max<int64_t>(1, n))).ok())
+      !(s = arena.alloc_n(&disc_d, discount.size())).ok() || !(s = arena.alloc_n(&sorted_d, n1)).ok() ||
+      !(s = arena.alloc_n(&sorted_score_d, n1)).ok() || !(s = arena.alloc_n(&sorted_label_d, n1)).ok())
     return s;
   CU(cudaMemcpy(bnd_d, bnd_h, sizeof(int32_t) * ((size_t)nq + 1), cudaMemcpyHostToDevice));
   if (nq > 0) CU(cudaMemcpy(inv_d, inv.data(), sizeof(double) * nq, cudaMemcpyHostToDevice));
@@ -260,6 +328,8 @@ Status RankTables::build(const float* label_h, const int32_t* bnd_h, int32_t nq_
   d.label_gain = gain_d;
   d.discount = disc_d;
   d.sorted = sorted_d;
+  d.sorted_score = sorted_score_d;
+  d.sorted_label = sorted_label_d;
   d.sigmoid = sigmoid;
   d.min_in = min_in;
   d.max_in = max_in;
@@ -273,10 +343,10 @@ Status launch_lambdarank(const DRank& r, const float* label, const double* score
                          int sms, cudaStream_t s) {
   if (r.nq == 0) return Status();
   const int sort_grid = (int)std::min<int64_t>(r.nq, (int64_t)sms * 16);
-  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score);
+  k_rank_sort<<<sort_grid, kRankSortThreads, 0, s>>>(r, score, label);
   CU_LAUNCH();
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((r.nq + 127) / 128, (int64_t)sms * 16));
-  k_lambdarank<<<grid, 128, 0, s>>>(r, label, score, g, h, gh);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((r.nq + kRankWarps - 1) / kRankWarps, (int64_t)sms * 32));
+  k_lambdarank<<<grid, kRankWarps * 32, 0, s>>>(r, g, h, gh);
   CU_LAUNCH();
   return Status();
 }
