@@ -110,6 +110,8 @@ struct LgbmB200Booster {
   uint32_t* bag = nullptr;
   uint32_t* oob = nullptr;
   int32_t* counts = nullptr;
+  int32_t* block_in = nullptr;    // in-bag rows per 1024-row block
+  int32_t* block_base = nullptr;  // in-bag rows of the blocks before each
   int32_t bag_cnt = 0, oob_cnt = 0;
   bool need_re_bagging = true;
   // column sampler (col_sampler.rs)
@@ -199,6 +201,8 @@ static Status booster_create(LgbmB200Booster* b, LgbmB200Learner* L, const LgbmB
     if (!(s = A.alloc_n(&b->bag, (size_t)n)).ok()) return s;
     if (!(s = A.alloc_n(&b->oob, (size_t)n)).ok()) return s;
     if (!(s = A.alloc_n(&b->counts, 2)).ok()) return s;
+    if (!(s = A.alloc_n(&b->block_in, (size_t)nb)).ok()) return s;
+    if (!(s = A.alloc_n(&b->block_base, (size_t)nb)).ok()) return s;
     b->bag_cnt = (int32_t)n;
   }
   // LGBM_B200_ITER_GRAPH=0: every iteration runs launch by launch (each tree
@@ -302,9 +306,12 @@ static Status booster_iter(LgbmB200Booster* b, int32_t* stop) {
   if (b->bagging && ((b->bag_cnt < n && b->iter % b->cfg.bagging_freq == 0) || b->need_re_bagging)) {
     b->need_re_bagging = false;
     int64_t nb = (n + 1023) / 1024;
-    k_bagging<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b->rng, n, b->cfg.bagging_fraction, b->in_bag);
+    k_bagging<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b->rng, n, b->cfg.bagging_fraction, b->in_bag,
+                                                           b->block_in);
     CU_LAUNCH();
-    k_compact_bag<<<1, 1024, 0, s>>>(b->in_bag, n, b->bag, b->oob, b->counts, nullptr, 0);
+    k_bag_scan<<<1, 1024, 0, s>>>(b->block_in, (int32_t)nb, n, b->block_base, b->counts);
+    CU_LAUNCH();
+    k_bag_scatter<<<(unsigned)nb, 1024, 0, s>>>(b->in_bag, n, b->block_base, b->bag, b->oob);
     CU_LAUNCH();
     int32_t cnt[2];
     CU(cudaMemcpyAsync(cnt, b->counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));

@@ -140,9 +140,10 @@ __global__ void k_quant_absmax(const float2* gh, int64_t n, unsigned long long* 
 __global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv,
                               const int64_t* start_dev, const DSlotState* st, int32_t const_hess, int32_t stochastic,
                               int32_t* packed);
-__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag);
-__global__ void k_compact_bag(const uint8_t* in_bag, int64_t n, uint32_t* bag, uint32_t* oob, int32_t* counts,
-                              int32_t* block_counts, int32_t num_blocks);
+__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag, int32_t* block_in);
+__global__ void k_bag_scan(const int32_t* block_in, int32_t nb, int64_t n, int32_t* block_base, int32_t* counts);
+__global__ void k_bag_scatter(const uint8_t* in_bag, int64_t n, const int32_t* block_base, uint32_t* bag,
+                              uint32_t* oob);
 __global__ void k_add_const(double* score, int64_t n, double v);
 
 }  // namespace lgbm_b200

@@ -139,67 +139,86 @@ __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n
 
 // sample_strategy.rs:280-320: rows of block b draw from the LCG `state[b]`
 // (Random(bagging_seed + b)) in row order; r < fraction keeps the row.
-// One thread per 1024-row block; block_counts receives each block's in-bag count.
-__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag) {
+// One thread per 1024-row block; block_in[b] receives the block's in-bag count.
+__global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag, int32_t* block_in) {
   int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t r0 = b * 1024;
   if (r0 >= n) return;
   int64_t r1 = min(n, r0 + 1024);
   uint32_t x = rng_state[b];
+  int32_t cnt = 0;
   for (int64_t r = r0; r < r1; ++r) {
     x = x * 214013u + 2531011u;
     float f = (float)((x >> 16) & 0x7FFF) / 32768.0f;
-    in_bag[r] = (double)f < fraction ? 1 : 0;
+    const bool keep = (double)f < fraction;
+    in_bag[r] = keep ? 1 : 0;
+    cnt += keep ? 1 : 0;
   }
   rng_state[b] = x;
+  block_in[b] = cnt;
 }
 
-// Ascending in-bag rows and the out-of-bag rows. A single CTA walks the
-// 1024-row blocks in order: each warp ballots 32 rows at a time.
-__global__ void __launch_bounds__(1024) k_compact_bag(const uint8_t* in_bag, int64_t n, uint32_t* bag, uint32_t* oob,
-                                                      int32_t* counts, int32_t* block_counts, int32_t num_blocks) {
-  __shared__ int32_t warp_in[32], warp_out[32];
-  __shared__ int32_t base_in, base_out;
+// Exclusive prefix of the blocks' in-bag counts (one CTA of 1024 threads,
+// each over a contiguous run of blocks); counts[0] / counts[1] receive the
+// in-bag and out-of-bag totals.
+__global__ void __launch_bounds__(1024) k_bag_scan(const int32_t* block_in, int32_t nb, int64_t n, int32_t* block_base,
+                                                   int32_t* counts) {
+  __shared__ int32_t warp_sum[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t per = (nb + (int32_t)blockDim.x - 1) / (int32_t)blockDim.x;
+  const int32_t b0 = min(nb, tid * per), b1 = min(nb, b0 + per);
+  int32_t local = 0;
+  for (int32_t b = b0; b < b1; ++b) local += block_in[b];
+  int32_t incl = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  int32_t base = 0, total = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    if (w < warp) base += warp_sum[w];
+    total += warp_sum[w];
+  }
+  int32_t run = base + incl - local;
+  for (int32_t b = b0; b < b1; ++b) {
+    block_base[b] = run;
+    run += block_in[b];
+  }
   if (tid == 0) {
-    base_in = 0;
-    base_out = 0;
+    counts[0] = total;
+    counts[1] = (int32_t)(n - total);
+  }
+}
+
+// Ascending in-bag rows and the out-of-bag rows: CTA b places the rows of
+// 1024-row block b after the block_base[b] in-bag (b * 1024 - block_base[b]
+// out-of-bag) rows of the blocks before it.
+__global__ void __launch_bounds__(1024) k_bag_scatter(const uint8_t* in_bag, int64_t n, const int32_t* block_base,
+                                                      uint32_t* bag, uint32_t* oob) {
+  __shared__ int32_t warp_in[32], warp_out[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t r = (int64_t)blockIdx.x * 1024 + tid;
+  const bool valid = r < n;
+  const bool in = valid && in_bag[r];
+  const unsigned bi = __ballot_sync(0xffffffffu, in);
+  const unsigned bo = __ballot_sync(0xffffffffu, valid && !in);
+  if (lane == 0) {
+    warp_in[warp] = __popc(bi);
+    warp_out[warp] = __popc(bo);
   }
   __syncthreads();
-  for (int64_t r0 = 0; r0 < n; r0 += blockDim.x) {
-    int64_t r = r0 + tid;
-    bool valid = r < n;
-    bool in = valid && in_bag[r];
-    unsigned bi = __ballot_sync(0xffffffffu, in);
-    unsigned bo = __ballot_sync(0xffffffffu, valid && !in);
-    if (lane == 0) {
-      warp_in[warp] = __popc(bi);
-      warp_out[warp] = __popc(bo);
-    }
-    __syncthreads();
-    int32_t pi = 0, po = 0, ti = 0, to = 0;
-    for (int w = 0; w < 32; ++w) {
-      if (w < warp) {
-        pi += warp_in[w];
-        po += warp_out[w];
-      }
-      ti += warp_in[w];
-      to += warp_out[w];
-    }
-    unsigned below = (1u << lane) - 1u;
-    if (in) bag[base_in + pi + __popc(bi & below)] = (uint32_t)r;
-    else if (valid) oob[base_out + po + __popc(bo & below)] = (uint32_t)r;
-    __syncthreads();
-    if (tid == 0) {
-      base_in += ti;
-      base_out += to;
-    }
-    __syncthreads();
+  int32_t pi = 0, po = 0;
+  for (int w = 0; w < warp; ++w) {
+    pi += warp_in[w];
+    po += warp_out[w];
   }
-  if (tid == 0) {
-    counts[0] = base_in;
-    counts[1] = base_out;
-  }
+  const int32_t base_in = block_base[blockIdx.x];
+  const int32_t base_out = (int32_t)((int64_t)blockIdx.x * 1024 - base_in);
+  const unsigned below = (1u << lane) - 1u;
+  if (in) bag[base_in + pi + __popc(bi & below)] = (uint32_t)r;
+  else if (valid) oob[base_out + po + __popc(bo & below)] = (uint32_t)r;
 }
 
 __global__ void __launch_bounds__(256) k_add_const(double* score, int64_t n, double v) {
