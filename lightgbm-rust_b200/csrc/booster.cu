@@ -678,9 +678,17 @@ struct LgbmB200Forest {
   // synchronisation
   void* stage = nullptr;
   size_t stage_bytes = 0;
+  // pinned staging of two row chunks and their scores (host rows), and the
+  // event marking when each chunk's buffers are free again
+  void* pin = nullptr;
+  size_t pin_bytes = 0;
+  cudaEvent_t chunk_done[2] = {nullptr, nullptr};
   ~LgbmB200Forest() {
     arena.free_all();
     if (stage) cudaFree(stage);
+    if (pin) cudaFreeHost(pin);
+    for (auto e : chunk_done)
+      if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -772,43 +780,111 @@ void lgbm_b200_forest_destroy(LgbmB200Forest* f) {
   }
 }
 
+namespace {
+
+// dst[0, bytes) = src[0, bytes), split over the host's OpenMP threads in 4 MB pieces.
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPiece = (size_t)4 << 20;
+  const int64_t pieces = (int64_t)((bytes + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < pieces; ++i) {
+    const size_t o = (size_t)i * kPiece;
+    std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(kPiece, bytes - o));
+  }
+}
+
+cudaError_t grow_device(void** p, size_t* have, size_t need) {
+  if (*have >= need) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e == cudaSuccess) *have = need;
+  return e;
+}
+
+cudaError_t grow_pinned(void** p, size_t* have, size_t need) {
+  if (*have >= need) return cudaSuccess;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaHostAlloc(p, need, cudaHostAllocDefault);
+  if (e == cudaSuccess) *have = need;
+  return e;
+}
+
+// Prediction of host rows: they stream through the device in chunks of
+// about 256 MB. The host's threads copy chunk c into one of two pinned
+// buffers while the copy engine moves chunk c - 1 and the kernel predicts
+// it; each chunk's scores come back through pinned memory and are copied out
+// two chunks later, when that buffer is needed again. (One copy from
+// pageable memory goes through the driver's own staging, a single thread's
+// memcpy wide.)
+cudaError_t predict_host(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t ncol, double* out) {
+  cudaStream_t s = F->stream;
+  const int64_t row_bytes = (int64_t)sizeof(float) * ncol;
+  int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(nrow, ((int64_t)256 << 20) / row_bytes));
+  // LGBM_B200_PREDICT_CHUNK_ROWS: a smaller chunk (tests of the chunk pipeline)
+  if (const char* v = std::getenv("LGBM_B200_PREDICT_CHUNK_ROWS"))
+    chunk = std::max<int64_t>(1, std::min<int64_t>(chunk, std::atoll(v)));
+  const size_t xb = ((size_t)(chunk * row_bytes) + 255) / 256 * 256;
+  const size_t ob = (sizeof(double) * (size_t)chunk * F->ntpi + 255) / 256 * 256;
+  cudaError_t e = grow_device(&F->stage, &F->stage_bytes, 2 * (xb + ob));
+  if (e == cudaSuccess) e = grow_pinned(&F->pin, &F->pin_bytes, 2 * (xb + ob));
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b)
+    if (!F->chunk_done[b]) e = cudaEventCreateWithFlags(&F->chunk_done[b], cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  char* dbase = static_cast<char*>(F->stage);
+  char* hbase = static_cast<char*>(F->pin);
+  const int64_t nchunks = (nrow + chunk - 1) / chunk;
+  // scores of chunk c (in pinned buffer c % 2) to the caller's array
+  auto copy_out = [&](int64_t c) {
+    const int64_t r0 = c * chunk, m = std::min(chunk, nrow - r0);
+    parallel_copy(out + (size_t)r0 * F->ntpi, hbase + (c & 1) * (xb + ob) + xb, sizeof(double) * (size_t)m * F->ntpi);
+  };
+  for (int64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
+    const int b = (int)(c & 1);
+    const int64_t r0 = c * chunk, m = std::min(chunk, nrow - r0);
+    float* hx = reinterpret_cast<float*>(hbase + b * (xb + ob));
+    double* ho = reinterpret_cast<double*>(hbase + b * (xb + ob) + xb);
+    float* dx = reinterpret_cast<float*>(dbase + b * (xb + ob));
+    double* dout = reinterpret_cast<double*>(dbase + b * (xb + ob) + xb);
+    if (c >= 2) {  // buffer b last served chunk c - 2: its copies have run, its scores go out
+      if ((e = cudaEventSynchronize(F->chunk_done[b])) != cudaSuccess) break;
+      copy_out(c - 2);
+    }
+    parallel_copy(hx, X + (size_t)r0 * ncol, (size_t)(m * row_bytes));
+    e = cudaMemcpyAsync(dx, hx, (size_t)(m * row_bytes), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+      launch_predict(F->f, dx, m, ncol, dout, s);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ho, dout, sizeof(double) * (size_t)m * F->ntpi, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(F->chunk_done[b], s);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return e;
+  for (int64_t c = std::max<int64_t>(0, nchunks - 2); c < nchunks; ++c) copy_out(c);
+  return cudaSuccess;
+}
+
+}  // namespace
+
 int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t ncol, double* out,
                       int32_t location) {
   if (!F || !X || !out || nrow < 0 || ncol <= 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
   if (nrow == 0) return LGBM_B200_OK;
   cudaSetDevice(F->device);
-  cudaStream_t s = F->stream;
-  const float* Xd = X;
-  double* od = out;
-  float* xtmp = nullptr;
-  double* otmp = nullptr;
-  cudaError_t e = cudaSuccess;
+  cudaError_t e;
   if (location == LGBM_B200_HOST) {
-    const size_t xb = (sizeof(float) * (size_t)nrow * ncol + 255) / 256 * 256;
-    const size_t need = xb + sizeof(double) * (size_t)nrow * F->ntpi;
-    if (F->stage_bytes < need) {
-      if (F->stage) cudaFree(F->stage);
-      F->stage = nullptr;
-      F->stage_bytes = 0;
-      e = cudaMalloc(&F->stage, need);
-      if (e == cudaSuccess) F->stage_bytes = need;
-    }
-    if (e == cudaSuccess) {
-      xtmp = static_cast<float*>(F->stage);
-      otmp = reinterpret_cast<double*>(static_cast<char*>(F->stage) + xb);
-      e = cudaMemcpyAsync(xtmp, X, sizeof(float) * nrow * ncol, cudaMemcpyHostToDevice, s);
-    }
-    Xd = xtmp;
-    od = otmp;
-  }
-  if (e == cudaSuccess) {
-    launch_predict(F->f, Xd, nrow, ncol, od, s);
+    e = predict_host(F, X, nrow, ncol, out);
+  } else {
+    launch_predict(F->f, X, nrow, ncol, out, F->stream);
     e = cudaGetLastError();
+    cudaError_t e2 = cudaStreamSynchronize(F->stream);
+    if (e == cudaSuccess) e = e2;
   }
-  if (e == cudaSuccess && location == LGBM_B200_HOST)
-    e = cudaMemcpyAsync(out, otmp, sizeof(double) * nrow * F->ntpi, cudaMemcpyDeviceToHost, s);
-  cudaError_t e2 = cudaStreamSynchronize(s);
-  if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
   return LGBM_B200_OK;
 }
