@@ -408,10 +408,20 @@ def run_workload(args):
             bst.update()
         L.record(1)
         ms = L.elapsed(0, 1) / args.steps
+        # device time per kernel family over a few more iterations (events around every launch)
+        L.set_timing(True)
+        fam = np.zeros(3)
+        timed = 3
+        for _ in range(timed):
+            bst.update()
+            t, _, _ = L.last_timing()
+            fam += np.asarray(t[:3])
+        L.set_timing(False)
         sc = bst.scores()
-        rounds = args.warmup + extra + args.steps
+        rounds = args.warmup + extra + args.steps + timed
         r = {"ms_per_iter": ms, "s_per_config_rounds": ms * d["num_rounds"] / 1000.0, "rounds_trained": rounds,
-             "launch_shape": shape, "launch_shape_source": shape_src}
+             "launch_shape": shape, "launch_shape_source": shape_src,
+             "kernel_ms_per_iter": {"hist": fam[0] / timed, "scan": fam[1] / timed, "partition": fam[2] / timed}}
         y = d["y"]
         if cfg == 1:
             r["train_rmse"] = float(np.sqrt(np.mean((sc[0] - y) ** 2)))

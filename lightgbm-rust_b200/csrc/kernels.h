@@ -78,7 +78,8 @@ inline cudaError_t launch_ex(void (*kernel)(Params...), dim3 grid, dim3 block, s
   cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
-template <bool kInt>
+constexpr int kScanWideBlocks = 4;  // scan CTAs per SM when a step's scans span several waves
+template <bool kInt, int kMinBlocks>
 __global__ void k_scan(const __grid_constant__ DCtx c);
 // The threshold scans and the partition of one step in one cooperative
 // launch (the CTAs wait for each other's scans; co-residency is required).

@@ -105,8 +105,17 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   CU(cudaFuncSetAttribute(k_leaf_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
   CU(cudaFuncSetAttribute(k_add_leaf_outputs, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
   CU(cudaFuncSetAttribute(k_leaf_of_row, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * h->L));
-  CU(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
-  CU(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
+  CU(cudaFuncSetAttribute(k_scan<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
+  CU(cudaFuncSetAttribute(k_scan<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->scan_smem));
+  CU(cudaFuncSetAttribute(k_scan<false, kScanWideBlocks>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)h->scan_smem));
+  CU(cudaFuncSetAttribute(k_scan<true, kScanWideBlocks>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)h->scan_smem));
+  // a step's scans are (feature, side, slot) CTAs: beyond two CTAs per SM they
+  // run in waves, and the register-capped variant keeps more of them resident
+  // (LGBM_B200_SCAN_WIDE=0/1 forces either)
+  h->scan_wide = (int64_t)nf * 2 * std::max(1, cfg->num_tree_slots) > 2 * (int64_t)h->num_sms;
+  if (const char* e = std::getenv("LGBM_B200_SCAN_WIDE")) h->scan_wide = std::atoi(e) != 0;
   {
     // the histogram runs in clusters (of hist_cluster(mode) CTAs): as many
     // clusters as fit on the device at once, shared among the feature tiles
@@ -385,9 +394,15 @@ Status enqueue_tree(LgbmB200Learner* h) {
       if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
       continue;
     }
-    if (mode == LGBM_B200_HIST_QUANT)
-      CU(launch_ex(k_scan<true>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
-    else CU(launch_ex(k_scan<false>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+    if (mode == LGBM_B200_HIST_QUANT) {
+      if (h->scan_wide)
+        CU(launch_ex(k_scan<true, kScanWideBlocks>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+      else CU(launch_ex(k_scan<true, 1>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+    } else if (h->scan_wide) {
+      CU(launch_ex(k_scan<false, kScanWideBlocks>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+    } else {
+      CU(launch_ex(k_scan<false, 1>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
+    }
     if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
     if (h->fused)
       CU(launch_ex(k_partition_fused, dim3(h->fused_grid, 1, K), dim3(512), fused_smem_bytes(), s, pdl_part, c,

@@ -281,6 +281,7 @@ struct LgbmB200Learner {
   int64_t last_part_rows = 0;
   bool fused = false;  // partition builds both children's histograms
   int fused_grid = 0;
+  bool scan_wide = false;  // the register-capped scan variant (many CTAs per step)
   bool scan_part = false;  // scans and partition of a step in one cooperative launch
   int scan_part_grid = 0;
   int scan_part_max = 0;  // CTAs of that launch resident at once, shared by the slots

@@ -1509,8 +1509,13 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
   }
 }
 
-template <bool kInt>
-__global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ DCtx c) {
+// kMinBlocks: CTAs the compiler keeps resident per SM (registers capped to
+// fit). 1 for a step of few features, where each CTA's latency is what counts;
+// kScanWideBlocks when a step's (feature, side, slot) CTAs span several waves
+// (many features or tree slots), where residency counts more than the few
+// registers that then spill.
+template <bool kInt, int kMinBlocks>
+__global__ void __launch_bounds__(kScanThreads, kMinBlocks) k_scan(const __grid_constant__ DCtx c) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_wait();
   pdl_trigger();
@@ -1530,8 +1535,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const __grid_constant__ D
   }
   scan_item<kInt>(c, s, blockIdx.x, blockIdx.y, *reinterpret_cast<ScanSmem*>(smem_raw));
 }
-template __global__ void k_scan<false>(const __grid_constant__ DCtx);
-template __global__ void k_scan<true>(const __grid_constant__ DCtx);
+template __global__ void k_scan<false, 1>(const __grid_constant__ DCtx);
+template __global__ void k_scan<true, 1>(const __grid_constant__ DCtx);
+template __global__ void k_scan<false, kScanWideBlocks>(const __grid_constant__ DCtx);
+template __global__ void k_scan<true, kScanWideBlocks>(const __grid_constant__ DCtx);
 
 // =====================================================================================
 // partition (partition.rs:107-174): out-of-place split of the leaf's rows into

@@ -146,3 +146,29 @@ def test_launch_shape_errors(lgb):
     persistent.train(g, h)
     with pytest.raises(lgb.LightGBMError, match="persistent"):
         persistent.time_shapes([before])
+
+
+@pytest.mark.parametrize("form", ["quantized", "f64"])
+def test_wide_scan_grows_the_same_trees(lgb, monkeypatch, form):
+    """The register-capped scan (LGBM_B200_SCAN_WIDE, chosen when a step's
+    scans span several waves) against the default one, numerical and
+    categorical features."""
+    X, y = _data(60_000, seed=5)
+    rng = np.random.default_rng(6)
+    X[:, 18] = rng.integers(0, 12, len(y))
+    X[:, 19] = rng.integers(0, 40, len(y))
+    y = np.where(np.isin(X[:, 19], [3, 7, 11, 20]), 1.0 - y, y).astype(np.float32)
+    params = dict(_params(form), max_cat_to_onehot=4)
+    ds = binned_dataset(lgb, X, y, params, categorical=[18, 19])
+    monkeypatch.setenv("LGBM_B200_SCAN_WIDE", "0")
+    base = lgb.Learner(ds, params)
+    monkeypatch.setenv("LGBM_B200_SCAN_WIDE", "1")
+    wide = lgb.Learner(ds, params)
+    categorical = False
+    for it in range(2):
+        g, h = _grads(lgb, params, y, 1, 300 + it)
+        a = base.train(g, h)[0]
+        b = wide.train(g, h)[0]
+        _same(a, b, exact=form == "quantized")
+        categorical |= bool(np.any(np.asarray(a["decision_type"]) & 1))
+    assert categorical  # the categorical scan ran in both variants
