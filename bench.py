@@ -565,7 +565,10 @@ def main():
                       "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
                       "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]}),
         "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 5),
+        # per iteration: the tree's launches (init, 3 per split, leaf renewal), then the
+        # gradients, the quantization (max-abs, packing), the leaf shrinkage, the training
+        # rows' score update and the held-out rows' scoring
+        "gpu_launches": args.steps * (r["kernel_launches_per_tree"] + 1 + (2 if head == "quantized" else 0) + 3),
         # device-time shares of the three split-step kernels (events around every launch)
         "kernel_share": {k: r[f"{k}_ms_per_step"] / (r["hist_ms_per_step"] + r["scan_ms_per_step"] +
                                                      r["partition_ms_per_step"])
