@@ -1,6 +1,6 @@
 """Parity of the CUDA tree-learning path with the CPU oracle, through the C ABI.
 
-Tolerances (from the north-star contract):
+Tolerances:
   - bins, per-bin integer sums, leaf row sets, tree structure: exact;
   - FP64 histogram sums: 1e-12 relative to the oracle's single-threaded
     row-order sums (atomics reorder the additions);
