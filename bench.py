@@ -33,11 +33,11 @@ WORKLOAD = ("binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), m
             "500 rounds; forms FP64, FP32-compensated, quantized (int8 g/h, 4 bins, stochastic rounding, FP64 leaf "
             "renewal)")
 # DRAM bytes per histogrammed row of the quantized histogram kernel, from the
-# ncu capture of a 5M-row root launch (profiles/k_hist_k_scan_k_partition_binary5M_quantized.md);
+# ncu capture of a 5M-row root launch (summarised under profiles/);
 # traffic grows with the rows of a launch, so a launch's traffic is this times its rows
 HIST_DRAM_BYTES_PER_ROW = 40.8
 # DRAM bytes per moved row of the partition kernel, from the ncu capture of its
-# first launch in a 5M-row run (the root split: every row; profiles/k_partition_root_binary5M_quantized.md).
+# first launch in a 5M-row run (the root split: every row; summarised under profiles/).
 # The index writes stay in L2 during the launch, so this is below the 9 algorithmic bytes.
 PART_DRAM_BYTES_PER_ROW = 5.02
 METRIC = "s per 500 rounds (quantized hist, equal AUC to FP64) + hist GB/s"
