@@ -36,15 +36,15 @@ def candidates(base, knob):
     allow resident at once; the candidates go down to one CTA per 16 SMs
     (tree slots batched in one launch share the SMs: K = 10 class trees
     measured fastest at the lowest candidates). The histogram's default is
-    every cluster resident at once; the candidates are a quarter, a half and
-    all of it."""
+    every cluster resident at once; the candidates are an eighth, a quarter,
+    a half and all of it."""
     if knob not in KNOBS:
         raise ValueError(f"unknown launch-shape knob {knob!r}")
     d = int(base[knob])
     if knob == "partition_ctas":
         vals = {max(1, d * f // 48) for f in (1, 2, 4, 8, 16, 32, 48)}
     elif knob == "hist_ctas":
-        vals = {max(1, d // 4), max(1, d // 2), d}
+        vals = {max(1, d // 8), max(1, d // 4), max(1, d // 2), d}
     else:
         vals = {128, 256, 512, 1024, 2048, d}
     return sorted(vals)

@@ -12,7 +12,7 @@ BASE = {"partition_ctas": 444, "hist_ctas": 264, "hist_rows_per_block": 512}
 
 def test_candidates_around_the_built_in_shape():
     assert autotune.candidates(BASE, "partition_ctas") == [9, 18, 37, 74, 148, 296, 444]
-    assert autotune.candidates(BASE, "hist_ctas") == [66, 132, 264]
+    assert autotune.candidates(BASE, "hist_ctas") == [33, 66, 132, 264]
     assert autotune.candidates(BASE, "hist_rows_per_block") == [128, 256, 512, 1024, 2048]
     assert autotune.candidates(dict(BASE, hist_rows_per_block=100), "hist_rows_per_block") == [100, 128, 256, 512,
                                                                                                  1024, 2048]
@@ -56,7 +56,7 @@ def test_tune_is_a_coordinate_search():
     assert best == {"partition_ctas": 148, "hist_ctas": 132, "hist_rows_per_block": 1024}
     assert fl.shape == {"partition_ctas": 148, "hist_ctas": 136, "hist_rows_per_block": 1024}  # rounded
     assert default_ms == pytest.approx(cost(BASE)) and best_ms == pytest.approx(cost(best))
-    assert len(fl.calls) == 4 and len(trials) == 7 + 3 + 5 + 2
+    assert len(fl.calls) == 4 and len(trials) == 7 + 4 + 5 + 2
     assert fl.calls[3] == [BASE, best]  # the winner confirmed against the start
     # each pass varies one knob from the best so far
     assert all(s["hist_ctas"] == 264 and s["hist_rows_per_block"] == 512 for s in fl.calls[0])
