@@ -306,35 +306,42 @@ def run_e2e(lgb, data, ds, form, args, device):
             "h2d_bytes_per_step": n * 8 + n * 8 + n * 8, "d2h_bytes_per_step": n * 8 + n * 8}
 
 
-def run_cpu_baseline(lgb, form, sample_scale, iters, warmup=3):
-    """The oracle (the reference's CPU learner restated) on the host cores, on
-    a bounded sample of the workload; seconds per 500 rounds scaled to the
-    full row count. The iterations after `warmup` ones are timed: a run of
-    warmup + iters rounds minus a run of warmup rounds (both seeded alike)."""
+def _oracle_sample(lgb, form, sample_scale, threads):
+    """The oracle's booster on a bounded sample of the workload, binned by the
+    oracle's own restatement of the reference's binning (no product code)."""
     from lgbm_b200 import synthetic
     from oracle import oracle as orc
 
     d = synthetic.make(2, scale=sample_scale)
-    threads = os.cpu_count() or 8
     params = dict(d["params"], hist_precision=form, num_threads=threads)
     if form == "quantized":
         params["quant_train_renew_leaf"] = True
     p = lgb.resolve_params(params)
-    ds = lgb.Dataset(d["X"], d["y"], params=params)
-    b = ds.binned()
-    t0 = time.perf_counter()
-    orc.train(p, b, d["y"], warmup)
-    t1 = time.perf_counter()
-    orc.train(p, b, d["y"], warmup + iters)
-    t2 = time.perf_counter()
-    per_iter = ((t2 - t1) - (t1 - t0)) / iters
-    per_iter = max(per_iter, (t2 - t1) / (warmup + iters))
-    rows = len(d["y"])
+    od = orc.Dataset(d["X"], p)
+    return orc.train(p, od.binned(), d["y"], 0), len(d["y"])
+
+
+def run_cpu_baseline(lgb, form, sample_scale, iters, warmup=3, threads=None):
+    """The oracle (the reference's CPU learner restated) on the host cores, on
+    a bounded sample of the workload: `warmup` boosting iterations, then
+    `iters` iterations timed one by one; seconds per 500 rounds scaled to the
+    full row count."""
+    threads = threads or os.cpu_count() or 8
+    m, rows = _oracle_sample(lgb, form, sample_scale, threads)
+    for _ in range(warmup):
+        m.update()
+    per = []
+    for _ in range(iters):
+        t0 = time.perf_counter()
+        m.update()
+        per.append(time.perf_counter() - t0)
+    per_iter = float(np.mean(per))
     scale = 10_000_000 / rows
     return {"value": per_iter * scale * ROUNDS, "unit": "s/500 rounds", "cores": threads, "kind": "port",
-            "sample": f"{rows} rows of the same generator, {iters} timed iterations after {warmup} warm-up ones "
-                      f"({form} form, {threads} threads), per-iteration time scaled by {scale:.0f}x rows and "
-                      f"x{ROUNDS} rounds", "warmup": warmup}
+            "sample": f"{rows} rows of the same generator (binned by the oracle), {iters} boosting iterations timed "
+                      f"one by one after {warmup} warm-up ones ({form} form, {threads} threads); the mean "
+                      f"iteration time scaled by {scale:.0f}x rows and x{ROUNDS} rounds", "warmup": warmup,
+            "ms_per_iter_sample": 1000 * per_iter}
 
 
 def _ndcg_at(y, s, group, k):
@@ -353,15 +360,15 @@ def _ndcg_at(y, s, group, k):
     return float(np.mean(np.where(idcg > 0, dcg / np.where(idcg > 0, idcg, 1.0), 1.0)))
 
 
-def run_workload(args):
+def run_workload(args, workload=None, predict_trees=None, compare_binning=True):
     """The other benchmark configurations: device time per boosting iteration
     of each form on the seeded synthetic data, a quality figure after the
-    timed rounds, and (lambdarank) the batched prediction of the trained
-    model over every row. One JSON line, not the headline metric."""
+    timed rounds, and (lambdarank) the batched prediction of a trained model
+    over every row. Returns one dict (not the headline metric)."""
     import lgbm_b200 as lgb
     from lgbm_b200 import synthetic
 
-    cfg = {"c1": 1, "c3": 3, "c4": 4}[args.workload]
+    cfg = {"c1": 1, "c3": 3, "c4": 4}[workload or args.workload]
     d = synthetic.make(cfg, scale=args.scale)
     forms = [f for f in args.forms.split(",") if f] if args.forms != "quantized,f32c,f64" else (
         ["f64", "f32c"] if cfg == 1 else ["quantized", "f64"])
@@ -374,17 +381,22 @@ def run_workload(args):
             params[k] = json.loads(v)
         except ValueError:
             params[k] = v
-    t0 = time.perf_counter()
-    ds = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=params,
-                     categorical_feature=d.get("categorical")).construct(params)
-    build_s = time.perf_counter() - t0
+    build_s = same = None
+    if compare_binning:
+        t0 = time.perf_counter()
+        ds = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=params,
+                         categorical_feature=d.get("categorical")).construct(params)
+        build_s = time.perf_counter() - t0
     # the same dataset with its rows binned on the device (identical bytes)
     t0 = time.perf_counter()
     ds_dev = lgb.Dataset(d["X"], d["y"], group=d.get("group"), params=dict(params, device_binning=True),
                          categorical_feature=d.get("categorical")).construct(dict(params, device_binning=True))
     build_dev_s = time.perf_counter() - t0
-    same = bool(np.array_equal(ds.binned()["bins"], ds_dev.binned()["bins"]))
-    del ds_dev
+    if compare_binning:
+        same = bool(np.array_equal(ds.binned()["bins"], ds_dev.binned()["bins"]))
+        del ds_dev
+    else:
+        ds = ds_dev
     out = {"workload": d["name"], "rows": int(len(d["y"])), "features": int(d["X"].shape[1]),
            "rounds_in_config": d["num_rounds"], "dataset_build_s": build_s,
            "dataset_build_device_binning_s": build_dev_s, "device_binning_identical": same, "forms": {}}
@@ -436,17 +448,250 @@ def run_workload(args):
             t0 = time.perf_counter()
             r["train_ndcg@10_device"] = float(lgb.ndcg(y, sc[0], d["group"], [10])[0])
             r["ndcg_device_s"] = time.perf_counter() - t0
-            # batched raw prediction of the trained model over every row
-            bst.predict(d["X"][:1000], raw_score=True)
-            t0 = time.perf_counter()
-            bst.predict(d["X"], raw_score=True)
-            pred_s = time.perf_counter() - t0
-            r["predict"] = {"rows": int(len(y)), "trees": bst.num_trees(), "s": pred_s,
-                            "rows_per_s": len(y) / pred_s, "tree_rows_per_s": len(y) * bst.num_trees() / pred_s,
-                            "note": "host f32 rows in, f64 scores out, copies included"}
+            if form == forms[0]:
+                # batched raw prediction of the model over every row, after
+                # training it to `predict_trees` trees (the config's 300)
+                want = predict_trees or bst.num_trees()
+                while bst.num_trees() < want:
+                    if bst.update():
+                        break
+                r["predict"] = predict_bench(lgb, bst, d["X"])
         out["forms"][form] = r
         del bst
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def predict_bench(lgb, bst, X):
+    """Batched prediction (lgbm_b200_predict) of a booster's trees over the
+    rows X: kernel-only (rows already in device memory) and from host rows
+    (copies included). Node visits are counted from the trees' leaf depths and
+    training counts, exact when X holds the training rows (no bagging)."""
+    import ctypes as C
+
+    import torch
+
+    L = lgb._lib
+    n, ncol = X.shape
+    k = bst.num_class
+    visits = sum(int(np.sum(t["leaf_count"].astype(np.int64) * t["leaf_depth"])) for t in bst.trees)
+    fh = bst._forest_handle()
+    xd = torch.from_numpy(X).cuda()
+    od = torch.empty(n * k, dtype=torch.float64, device="cuda")
+    L.check(L.lib().lgbm_b200_predict(fh, C.c_void_p(xd.data_ptr()), n, ncol, C.c_void_p(od.data_ptr()), L.DEVICE))
+    torch.cuda.synchronize()
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):  # each call synchronises the forest's stream
+        L.check(L.lib().lgbm_b200_predict(fh, C.c_void_p(xd.data_ptr()), n, ncol, C.c_void_p(od.data_ptr()),
+                                          L.DEVICE))
+    dev_s = (time.perf_counter() - t0) / reps
+    del xd
+    bst.predict(X[:1000], raw_score=True)
+    t0 = time.perf_counter()
+    host_out = bst.predict(X, raw_score=True)
+    host_s = time.perf_counter() - t0
+    same = bool(np.array_equal(np.asarray(host_out).reshape(-1), od.cpu().numpy()))
+    first_touch = n * ncol * 4 + 8 * n * k
+    return {"rows": int(n), "trees": bst.num_trees(), "kernel_s": dev_s, "rows_per_s": n / dev_s,
+            "node_visits": visits, "node_visits_per_s": visits / dev_s, "first_touch_gbs": first_touch / dev_s / 1e9,
+            "host_rows_s": host_s, "host_rows_per_s": n / host_s, "device_equals_host": same,
+            "note": "kernel_s: rows already on the device (one launch per call); host_rows_s: f32 rows from host "
+                    "memory, f64 scores back, copies included"}
+
+
+def _logloss(y, score):
+    """Mean binary logloss of raw scores (sigmoid 1)."""
+    pr = 1.0 / (1.0 + np.exp(-score))
+    pr = np.clip(pr, 1e-15, 1 - 1e-15)
+    return float(-np.mean(y * np.log(pr) + (1 - y) * np.log(1 - pr)))
+
+
+def run_auc_seeds(lgb, args, device, res, seeds=(3, 4, 5, 6)):
+    """Held-out AUC after the workload's 500 rounds, quantized and FP64, on the
+    headline seed (from the main run) and four more seeds of the same
+    generator at full size: is the quantized form's AUC gap seed noise?"""
+    from lgbm_b200 import synthetic
+
+    out = [{"seed": 2, "auc_quantized": res["quantized"]["auc"], "auc_f64": res["f64"]["auc"]}]
+    for seed in seeds:
+        d = synthetic.make(2, scale=args.scale, seed=seed)
+        ds = lgb.Dataset(d["X"], d["y"], params=d["params"]).construct()
+        dv = lgb.Dataset(d["X_valid"], d["y_valid"], params=d["params"], reference=ds).construct()
+        row = {"seed": seed}
+        for form in ("quantized", "f64"):
+            params = dict(d["params"], hist_precision=form, device=device, num_threads=os.cpu_count() or 8)
+            if form == "quantized":
+                params["quant_train_renew_leaf"] = True
+            bst = lgb.Booster(params, ds, dv)
+            for _ in range(args.rounds):
+                if bst.update():
+                    break
+            row[f"auc_{form}"] = _auc(d["y_valid"], bst.scores(valid=True)[0])
+            del bst
+        out.append(row)
+        del ds, dv, d
+    deltas = np.array([r["auc_quantized"] - r["auc_f64"] for r in out])
+    return {"rounds": args.rounds, "per_seed": out, "delta_mean": float(deltas.mean()),
+            "delta_std": float(deltas.std(ddof=1)), "delta_max_abs": float(np.abs(deltas).max()),
+            "note": "held-out AUC of the quantized form minus the FP64 form's, same data and rounds"}
+
+
+def run_precision(lgb, device, scale=0.02, rounds=50, checkpoints=(0, 10, 25)):
+    """Error of the FP32-compensated and quantized forms against the FP64
+    oracle on the 10M-row workload's generator at `scale` (200k + 20k rows):
+    histogram relative error (all rows, the gradients of each checkpoint),
+    split agreement and leaf-value error of one tree grown on the same
+    gradients, and the held-out AUC / logloss after `rounds` rounds."""
+    from lgbm_b200 import synthetic
+    from oracle import oracle as orc
+
+    d = synthetic.make(2, scale=scale)
+    base = dict(d["params"], device=device, num_threads=16)
+    p64 = lgb.resolve_params(dict(base, hist_precision="f64"))
+    ds = lgb.Dataset(d["X"], d["y"], params=base).construct()
+    dv = lgb.Dataset(d["X_valid"], d["y_valid"], params=base, reference=ds).construct()
+    b = ds.binned()
+    om = orc.train(p64, b, d["y"], 0, valid_binned=dv.binned())
+    grads = {}
+    for it in range(rounds):
+        if it in checkpoints:
+            grads[it] = orc.gradients(p64, d["y"], om.scores()[0])
+        om.update()
+    auc64 = orc.auc(d["y_valid"], om.scores(valid=True)[0])
+    ll64 = _logloss(d["y_valid"], om.scores(valid=True)[0])
+    out = {"rows": int(len(d["y"])), "held_out_rows": int(len(d["y_valid"])), "rounds": rounds,
+           "checkpoints": list(checkpoints), "oracle_f64": {"auc": auc64, "logloss": ll64}, "forms": {}}
+    for form in ("f64", "f32c", "quantized"):
+        params = dict(base, hist_precision=form)
+        if form == "quantized":
+            params.update(quant_train_renew_leaf=True)
+        pf = lgb.resolve_params(params)
+        learner = lgb.Learner(ds, params)
+        herr_max, herr_mean, agree, nodes, ident, lv_err = [], [], 0, 0, 0, []
+        for it, (g, h) in grads.items():
+            t = learner.train(g, h)[0]
+            want = orc.hist(b, None, g, h).reshape(-1, 2)
+            got = learner.histogram(None)
+            if form == "quantized":
+                _, scales = learner.quantized()
+                hi = got & 0xFFFFFFFF
+                gi = (got - hi) >> 32
+                got = np.stack([gi * scales[0], hi * scales[1]], axis=1)
+            else:
+                got = got.reshape(-1, 2)
+            den = np.maximum(np.abs(want), 1e-12 * np.abs(want).max(axis=0))
+            rel = np.abs(got - want) / den
+            herr_max.append(float(rel.max()))
+            herr_mean.append(float(rel.mean()))
+            ot = orc.train_trees(p64, b, g, h).trees[0]
+            nn = min(t["num_leaves"], ot["num_leaves"]) - 1
+            same = (t["split_feature"][:nn] == ot["split_feature"][:nn]) & \
+                   (t["threshold_in_bin"][:nn] == ot["threshold_in_bin"][:nn])
+            agree += int(np.sum(same))
+            nodes += ot["num_leaves"] - 1
+            if t["num_leaves"] == ot["num_leaves"] and bool(np.all(same)):
+                ident += 1
+                lv_err.append(np.abs(t["leaf_value"] - ot["leaf_value"]) /
+                              np.maximum(np.abs(ot["leaf_value"]), 1e-300))
+        lv = np.concatenate(lv_err) if lv_err else np.zeros(0)
+        bst = lgb.Booster(params, ds, dv)
+        for _ in range(rounds):
+            if bst.update():
+                break
+        sv = bst.scores(valid=True)[0]
+        auc = orc.auc(d["y_valid"], sv)
+        out["forms"][form] = {
+            "hist_rel_err_max": max(herr_max), "hist_rel_err_mean": float(np.mean(herr_mean)),
+            "split_agreement": agree / max(nodes, 1), "identical_trees": ident, "trees_compared": len(grads),
+            "leaf_rel_err_max": float(lv.max()) if lv.size else None,
+            "leaf_rel_err_mean": float(lv.mean()) if lv.size else None,
+            "auc": auc, "auc_delta_vs_oracle_f64": auc - auc64,
+            "logloss_delta_vs_oracle_f64": _logloss(d["y_valid"], sv) - ll64}
+        del bst, learner
+    out["note"] = ("one tree per checkpoint grown by each form and by the FP64 oracle on the same gradients (the "
+                   "FP64 oracle run's at that iteration); split agreement = splits equal in node order / oracle "
+                   "splits; leaf error over the trees whose structure is identical")
+    return out
+
+
+def run_config0(lgb, device):
+    """The CPU-runnable binary workload end to end at its exact settings
+    (20k + 5k rows x 28, 31 leaves, min_data_in_leaf 20, lr 0.1, 100 rounds,
+    FP64 histograms) on the GPU and in the oracle: identical trees, held-out
+    AUC / logloss, and the model text of both."""
+    from lgbm_b200 import synthetic
+    from oracle import oracle as orc
+
+    d = synthetic.config0()
+    params = dict(d["params"], device=device)
+    p = lgb.resolve_params(params)
+    ds = lgb.Dataset(d["X"], d["y"], params=params)
+    dv = lgb.Dataset(d["X_valid"], d["y_valid"], params=params, reference=ds)
+    ds.construct()
+    dv.construct()
+    t0 = time.perf_counter()
+    bst = lgb.train(params, ds, d["num_rounds"], valid_sets=[dv])
+    gpu_s = time.perf_counter() - t0
+    od = orc.Dataset(d["X"], p)
+    odv = orc.Dataset(d["X_valid"], p, reference=od)
+    bins_equal = bool(np.array_equal(ds.binned()["bins"], od.binned()["bins"]) and
+                      np.array_equal(dv.binned()["bins"], odv.binned()["bins"]))
+    t0 = time.perf_counter()
+    om = orc.train(p, od.binned(), d["y"], d["num_rounds"], valid_binned=odv.binned())
+    orc_s = time.perf_counter() - t0
+    same = 0
+    for a, o in zip(bst.trees, om.trees):
+        if not (a["num_leaves"] == o["num_leaves"] and np.array_equal(a["split_feature"], o["split_feature"]) and
+                np.array_equal(a["threshold_in_bin"], o["threshold_in_bin"])):
+            break
+        same += 1
+    lv = [np.max(np.abs(a["leaf_value"] - o["leaf_value"]) / np.maximum(np.abs(o["leaf_value"]), 1e-300))
+          for a, o in zip(bst.trees[:same], om.trees[:same])]
+    sg, so = bst.scores(valid=True)[0], om.scores(valid=True)[0]
+    tg = bst.model_to_string()
+    to = om.model_to_string(d["X"].shape[1], od.feature_infos)
+    lg, lo = tg.split("\n"), to.split("\n")
+    return {"rows": len(d["y"]), "held_out_rows": len(d["y_valid"]), "rounds": d["num_rounds"],
+            "bins_equal_oracle_binning": bins_equal, "trees": len(bst.trees), "identical_trees": same,
+            "leaf_rel_err_max": float(max(lv)) if lv else None,
+            "auc_gpu": orc.auc(d["y_valid"], sg), "auc_oracle": orc.auc(d["y_valid"], so),
+            "logloss_gpu": _logloss(d["y_valid"], sg), "logloss_oracle": _logloss(d["y_valid"], so),
+            "model_text_identical": tg == to, "model_text_bytes": len(tg),
+            "model_text_lines_differing": int(sum(a != b for a, b in zip(lg, lo)) + abs(len(lg) - len(lo))),
+            "gpu_s": gpu_s, "oracle_1t_s": orc_s}
+
+
+def config_dict(head, world, rows, held_out):
+    """The workload's config, the same in both arms."""
+    return {"workload": WORKLOAD, "form": head, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (bin matrix 320 MB, gradients 80 MB)", "rows": rows,
+            "held_out_rows": held_out}
+
+
+def run_reference_arm(args, world):
+    """--impl reference: the reference's CPU learner (restated by the oracle:
+    the reference is Rust and no Rust toolchain is available) on the host's
+    cores, binned by the oracle's own binning, so no product code runs. A step
+    is one boosting iteration of a 1M-row sample of the workload (the same
+    generator); W warm-up iterations, then exactly K timed ones. The value is
+    the mean iteration time scaled to the 10M-row workload and 500 rounds.
+    A single-threaded run of the same restatement on a smaller sample
+    (cpu_ref_1t) is reported beside it."""
+    import lgbm_b200 as lgb  # the Python package only: the product library is never loaded here
+
+    t0 = time.perf_counter()
+    threads = os.cpu_count() or 8
+    cb = run_cpu_baseline(lgb, "quantized", 0.1 * args.scale, args.steps, args.warmup, threads)
+    one = run_cpu_baseline(lgb, "quantized", 0.01, 2, 1, 1)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s/500 rounds",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["value"] / ROUNDS * 1000, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8", "data": "synthetic (seeded generator with the workload's shapes and "
+            "distributions)", "config": config_dict("quantized", world, 10_000_000, 1_000_000),
+            "cpu_baseline": cb, "cpu_ref_1t": one,
+            "e2e": {"value": cb["value"], "unit": "s/500 rounds", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -459,6 +704,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the AUC seeds, precision report, the 20k-row workload and the other workloads")
     ap.add_argument("--rounds", type=int, default=ROUNDS, help="rounds trained per form (AUC after these)")
     ap.add_argument("--autotune", action="store_true",
                     help="search the per-step launch shape after warm-up and record it for the workload")
@@ -470,7 +717,7 @@ def main():
     if args.autotune and int(os.environ.get("WORLD_SIZE", "1")) > 1:
         ap.error("--autotune records one device's choice: run it with one process")
     if args.workload != "c2":
-        run_workload(args)
+        print(json.dumps(run_workload(args)), flush=True)
         return
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -480,22 +727,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        import lgbm_b200 as lgb
-
-        sample = 0.1 * args.scale
-        iters = max(1, min(args.steps, 3))
-        warm = min(args.warmup, 5)  # at least 3 (above); bounded so the CPU run stays within minutes
-        t0 = time.perf_counter()
-        cb = run_cpu_baseline(lgb, "quantized", sample, iters, warm)
-        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s/500 rounds",
-                "n_gpus": args.gpus, "steps": iters, "warmup": warm, "ms_per_step": cb["value"] / ROUNDS * 1000,
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
-                "data": "synthetic", "config": {"workload": WORKLOAD, "form": "quantized",
-                                                "sample_rows": int(10_000_000 * sample)},
-                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "s/500 rounds", "h2d_bytes_per_step": 0,
-                                             "d2h_bytes_per_step": 0},
-                "wall_s": time.perf_counter() - t0}
-        print(json.dumps(line), flush=True)
+        run_reference_arm(args, world)
         return
 
     if world > 1:
@@ -527,7 +759,7 @@ def main():
     ms = _max_over_ranks(r["ms_per_step"])
     value = ms * ROUNDS / 1000.0 / world
     e2e = None if args.no_e2e else run_e2e(lgb, data, ds, head, args, local_rank)
-    cpu = None if (args.no_cpu or rank != 0) else run_cpu_baseline(lgb, head, 0.1 * args.scale, 3)
+    cpu = None if (args.no_cpu or rank != 0 or world > 1) else run_cpu_baseline(lgb, head, 0.1 * args.scale, 3)
     peak, peak_kind = _peaks()
     achieved = r["hist_gbs"]
     if world > 1:
@@ -541,10 +773,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8" if head == "quantized" else ("f32" if head == "f32c" else "f64"),
         "data": "synthetic (seeded generator with the workload's shapes and distributions)",
-        "config": {"workload": WORKLOAD, "form": head, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (bin matrix 320 MB, gradients 80 MB)", "rows": len(data["y"]),
-                   "held_out_rows": len(data["y_valid"]), "launch_shape": r["launch_shape"],
-                   "launch_shape_source": r["launch_shape_source"]},
+        "config": config_dict(head, world, len(data["y"]), len(data["y_valid"])),
+        "launch_shape": r["launch_shape"], "launch_shape_source": r["launch_shape_source"],
         "forms": {k: {"s_per_500_rounds": v["s_per_500"], "ms_per_step": v["ms_per_step"], "auc": v["auc"],
                       "auc_device": v["auc_device"], "auc_device_ms": v["auc_device_ms"],
                       "auc_numpy_ms": v["auc_numpy_ms"],
@@ -588,6 +818,20 @@ def main():
     if "f64" in res and head in res:
         line["speedup_vs_f64"] = res["f64"]["ms_per_step"] / res[head]["ms_per_step"]
         line["auc_delta_vs_f64"] = res[head]["auc"] - res["f64"]["auc"]
+    if world == 1 and not args.no_extras:
+        # beside the headline (not part of its timed region): the AUC gap over
+        # more seeds, the precision forms' errors against the FP64 oracle, and
+        # the other workloads
+        t0 = time.perf_counter()
+        if "f64" in res and "quantized" in res:
+            line["auc_seeds"] = run_auc_seeds(lgb, args, local_rank, res)
+        line["precision"] = run_precision(lgb, local_rank)
+        line["config0"] = run_config0(lgb, local_rank)
+        wargs = argparse.Namespace(**vars(args))
+        wargs.forms, wargs.scale, wargs.steps, wargs.warmup, wargs.autotune = "quantized,f32c,f64", 1.0, 5, 3, False
+        line["workloads"] = {w: run_workload(wargs, w, predict_trees=300 if w == "c4" else None,
+                                             compare_binning=False) for w in ("c1", "c3", "c4")}
+        line["extras_s"] = time.perf_counter() - t0
     print(json.dumps(line), flush=True)
 
 

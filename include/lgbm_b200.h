@@ -113,6 +113,12 @@ int lgbm_b200_dataset_create_valid_device(const float* X, int64_t n, int32_t nco
                                           int32_t device, LgbmB200Dataset** out);
 /* The view points into the dataset; valid until lgbm_b200_dataset_free. */
 int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out);
+/* Dataset::feature_infos (dataset.rs:770-776) as the model text's
+ * feature_infos line holds it: one entry per input column, space-separated
+ * ("[min:max]" for a numerical feature, its categories joined by ':' for a
+ * categorical one, "none" for an unused column). *out stays valid until
+ * lgbm_b200_dataset_free. */
+int lgbm_b200_dataset_feature_infos(LgbmB200Dataset* ds, const char** out);
 void lgbm_b200_dataset_free(LgbmB200Dataset* ds);
 
 /* ------------------------------------------------------------------------
@@ -209,6 +215,10 @@ typedef struct {
   const uint32_t* cat_threshold;       /* category bitsets */
   const int32_t* cat_boundaries_inner; /* num_cat + 1 */
   const uint32_t* cat_threshold_inner; /* bin bitsets */
+  /* the FP64 gain of each split before split_gain rounds it to f32 (the
+   * reference keeps only the f32; for parity checks). May be NULL in views a
+   * caller passes in. */
+  const double* split_gain_f64;
 } LgbmB200TreeView;
 
 /* SerialTreeLearner::new (learner/mod.rs:220): uploads the bin matrix
@@ -229,10 +239,13 @@ int lgbm_b200_learner_set_bagging(LgbmB200Learner* h, const uint32_t* used, int6
  * for tree slot `slot`; NULL uses every feature. */
 int lgbm_b200_learner_set_feature_mask(LgbmB200Learner* h, int32_t slot, const uint8_t* is_used);
 
-/* train(grad, hess) (learner/mod.rs:572) for every tree slot: grad/hess are
- * class-major [num_tree_slots x num_data]. `out` receives num_tree_slots views. */
-int lgbm_b200_learner_train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location,
-                            LgbmB200TreeView* out);
+/* train(grad, hess, is_first_tree) (learner/mod.rs:572) for every tree
+ * slot: grad/hess are class-major [num_tree_slots x num_data]. `out`
+ * receives num_tree_slots views. is_first_tree is accepted as the reference
+ * takes it; there it only keeps linear-tree leaves constant, and linear
+ * trees are not on this path. */
+int lgbm_b200_learner_train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t is_first_tree,
+                            int32_t location, LgbmB200TreeView* out);
 
 /* add_leaf_outputs(leaf_values, score) (learner/mod.rs:537) for slot
  * `slot`: score[row] += leaf_values[leaf of row] over the in-bag rows. */
@@ -240,9 +253,9 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
                                        int32_t num_leaves, double* score, int32_t location);
 
 /* partition() (learner/mod.rs:312): the rows of each leaf of the last tree
- * of `slot`. leaf_begin/leaf_count: [num_leaves]; indices: [num_used]. The
- * order of rows inside a leaf is unspecified (the reference keeps them
- * ascending); the sets are exact. */
+ * of `slot`. leaf_begin/leaf_count: [num_leaves]; indices: [num_used]. Each
+ * leaf's rows are in ascending order, as the reference's stable partition
+ * keeps them (partition.rs:107-174). */
 int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* leaf_begin, int32_t* leaf_count,
                                     uint32_t* indices);
 
@@ -391,7 +404,8 @@ int lgbm_b200_predict(LgbmB200Forest* f, const float* X, int64_t nrow, int32_t n
  * device: calls that overlap in time on one device race on it and must be
  * serialised by the caller. The first call on a device resolves the array's
  * address (cudaGetSymbolAddress); make it before capturing any stream on
- * that device. Results equal lgbm_b200_predict's. */
+ * that device. The calling thread's current device is left as it was.
+ * Results equal lgbm_b200_predict's. */
 int lgbm_b200_predict_noalloc(LgbmB200Forest* f, const float* X, int64_t nrow, int32_t ncol, double* out);
 
 #ifdef __cplusplus

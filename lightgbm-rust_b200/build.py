@@ -1,4 +1,5 @@
-"""Builds liblgbm_b200.so (CUDA kernels for sm_100a + host C++) in-tree.
+"""Builds liblgbm_b200.so and liblgbm_b200.a (CUDA kernels for sm_100a +
+host C++) in-tree.
 
 Usage: python lightgbm-rust_b200/build.py [--clean]
 """
@@ -12,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "lgbm_b200", "liblgbm_b200.so")
+STATIC = os.path.join(HERE, "lgbm_b200", "liblgbm_b200.a")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: every a*b+c stays a rounded multiply and a rounded add, as on
@@ -71,6 +73,16 @@ def build(verbose=False, extra_nvcc=()):
         if r.returncode != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    if jobs or not os.path.exists(STATIC):
+        # the same objects as a static archive, for a Rust build.rs that links
+        # `static=lgbm_b200` with `static=cudart_static` (every .cu file is
+        # compiled whole, so no device-link step is needed)
+        if os.path.exists(STATIC):
+            os.remove(STATIC)
+        r = subprocess.run(["ar", "rcs", STATIC] + objs, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("archive failed")
     return OUT
 
 

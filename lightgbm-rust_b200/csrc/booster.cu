@@ -698,17 +698,27 @@ static Status forest_create(LgbmB200Forest* F, const LgbmB200TreeView* trees, in
                             int32_t device) {
   F->device = device;
   F->ntpi = std::max(1, ntpi);
-  CU(cudaSetDevice(device));
-  CU(cudaStreamCreateWithFlags(&F->stream, cudaStreamNonBlocking));
-  std::vector<int32_t> node_off, leaf_off, num_leaves, feature, left, right, cat_idx, cat_bnd{0};
-  std::vector<double> threshold, leaf_value;
-  std::vector<int8_t> dtype;
-  std::vector<uint32_t> cat_words;
+  bool wide = false;
   for (int32_t t = 0; t < nt; ++t) {
     const LgbmB200TreeView& v = trees[t];
-    node_off.push_back((int32_t)feature.size());
-    leaf_off.push_back((int32_t)leaf_value.size());
-    num_leaves.push_back(v.num_leaves);
+    if (v.num_leaves < 1) return Status(LGBM_B200_ERR_INVALID_PARAMETER, "forest_create: a tree has no leaves");
+    if (v.num_leaves > 32768) wide = true;
+    for (int32_t nd = 0; nd < v.num_leaves - 1; ++nd)
+      if (v.split_feature[nd] < 0 || v.split_feature[nd] >= (1 << kNodeFeatureBits))
+        return Status(LGBM_B200_ERR_UNSUPPORTED, "forest_create: split feature index outside [0, 2^24)");
+  }
+  CU(cudaSetDevice(device));
+  CU(cudaStreamCreateWithFlags(&F->stream, cudaStreamNonBlocking));
+  std::vector<int4> tree;
+  std::vector<DNode> nodes;
+  std::vector<DNodeWide> wnodes;
+  std::vector<int32_t> cat_bnd{0};
+  std::vector<double> leaf_value;
+  std::vector<uint32_t> cat_words;
+  int32_t node_count = 0;
+  for (int32_t t = 0; t < nt; ++t) {
+    const LgbmB200TreeView& v = trees[t];
+    tree.push_back(make_int4(node_count, (int32_t)leaf_value.size(), v.num_leaves, 0));
     int32_t cat_base = (int32_t)cat_bnd.size() - 1;
     for (int32_t c = 0; c < v.num_cat; ++c) {
       int32_t b0 = v.cat_boundaries[c], b1 = v.cat_boundaries[c + 1];
@@ -716,12 +726,20 @@ static Status forest_create(LgbmB200Forest* F, const LgbmB200TreeView* trees, in
       cat_bnd.push_back((int32_t)cat_words.size());
     }
     for (int32_t nd = 0; nd < v.num_leaves - 1; ++nd) {
-      feature.push_back(v.split_feature[nd]);
-      threshold.push_back(v.threshold[nd]);
-      dtype.push_back(v.decision_type[nd]);
-      left.push_back(v.left_child[nd]);
-      right.push_back(v.right_child[nd]);
-      cat_idx.push_back((v.decision_type[nd] & 1) ? cat_base + (int32_t)v.threshold[nd] : -1);
+      double thr = v.threshold[nd];
+      if (v.decision_type[nd] & 1) {  // categorical: the bitset's index in the threshold's bits
+        const int64_t ci = cat_base + (int64_t)v.threshold[nd];
+        std::memcpy(&thr, &ci, sizeof(thr));
+      }
+      const int32_t fd = v.split_feature[nd] | ((int32_t)(uint8_t)v.decision_type[nd] << kNodeFeatureBits);
+      if (wide) {
+        DNodeWide n{thr, fd, 0, v.left_child[nd], v.right_child[nd]};
+        wnodes.push_back(n);
+      } else {
+        DNode n{thr, fd, (int16_t)v.left_child[nd], (int16_t)v.right_child[nd]};
+        nodes.push_back(n);
+      }
+      ++node_count;
     }
     for (int32_t l = 0; l < v.num_leaves; ++l) leaf_value.push_back(v.leaf_value[l]);
   }
@@ -735,28 +753,23 @@ static Status forest_create(LgbmB200Forest* F, const LgbmB200TreeView* trees, in
   DForest& f = F->f;
   f.num_trees = nt;
   f.ntpi = F->ntpi;
+  f.wide = wide;
   Status s;
-  int32_t *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8;
-  double *d1, *d2;
-  int8_t* i8;
-  uint32_t* u1;
-  if (!(s = up(node_off, &a1)).ok() || !(s = up(leaf_off, &a2)).ok() || !(s = up(num_leaves, &a3)).ok() ||
-      !(s = up(feature, &a4)).ok() || !(s = up(left, &a5)).ok() || !(s = up(right, &a6)).ok() ||
-      !(s = up(cat_idx, &a7)).ok() || !(s = up(cat_bnd, &a8)).ok() || !(s = up(threshold, &d1)).ok() ||
-      !(s = up(leaf_value, &d2)).ok() || !(s = up(dtype, &i8)).ok() || !(s = up(cat_words, &u1)).ok())
+  int4* tt;
+  DNode* dn = nullptr;
+  DNodeWide* dw = nullptr;
+  int32_t* cb;
+  double* lv;
+  uint32_t* cw;
+  if (!(s = up(tree, &tt)).ok() || !(s = up(cat_bnd, &cb)).ok() || !(s = up(leaf_value, &lv)).ok() ||
+      !(s = up(cat_words, &cw)).ok())
     return s;
-  f.node_off = a1;
-  f.leaf_off = a2;
-  f.num_leaves = a3;
-  f.feature = a4;
-  f.left = a5;
-  f.right = a6;
-  f.cat_idx = a7;
-  f.cat_bnd = a8;
-  f.threshold = d1;
-  f.leaf_value = d2;
-  f.dtype = i8;
-  f.cat_words = u1;
+  if (!(s = wide ? up(wnodes, &dw) : up(nodes, &dn)).ok()) return s;
+  f.tree = tt;
+  f.nodes = wide ? static_cast<const void*>(dw) : static_cast<const void*>(dn);
+  f.cat_bnd = cb;
+  f.leaf_value = lv;
+  f.cat_words = cw;
   return Status();
 }
 }  // namespace lgbm_b200
@@ -856,8 +869,7 @@ cudaError_t predict_host(LgbmB200Forest* F, const float* X, int64_t nrow, int32_
     parallel_copy(hx, X + (size_t)r0 * ncol, (size_t)(m * row_bytes));
     e = cudaMemcpyAsync(dx, hx, (size_t)(m * row_bytes), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-      launch_predict(F->f, dx, m, ncol, dout, s);
-      e = cudaGetLastError();
+      e = launch_predict(F->f, dx, m, ncol, dout, s);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(ho, dout, sizeof(double) * (size_t)m * F->ntpi, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaEventRecord(F->chunk_done[b], s);
@@ -880,8 +892,7 @@ int lgbm_b200_predict(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t n
   if (location == LGBM_B200_HOST) {
     e = predict_host(F, X, nrow, ncol, out);
   } else {
-    launch_predict(F->f, X, nrow, ncol, out, F->stream);
-    e = cudaGetLastError();
+    e = launch_predict(F->f, X, nrow, ncol, out, F->stream);
     cudaError_t e2 = cudaStreamSynchronize(F->stream);
     if (e == cudaSuccess) e = e2;
   }

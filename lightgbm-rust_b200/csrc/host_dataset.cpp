@@ -12,6 +12,7 @@
 // with LGBM_B200_ERR_UNSUPPORTED.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -463,6 +464,39 @@ Status build_valid_dataset(const float* X, int64_t n, int32_t ncol, const Datase
   if (device >= 0) return push_bins_device(d, X, n, ncol, device);
   push_bins(d, X, n, ncol);
   return Status();
+}
+
+// dataset.rs:770-776 with BinMapper::bin_info_string (binning.rs:680-686):
+// "[min:max]" (%.17g, the reference's fmt_g17) for a numerical feature, the
+// category of every bin joined by ':' for a categorical one, "none" for a
+// column left out as trivial.
+const std::string& Dataset::infos() {
+  if (!feature_infos.empty() || num_total_features == 0) return feature_infos;
+  std::vector<int32_t> inner((size_t)num_total_features, -1);
+  for (size_t k = 0; k < used.size(); ++k) inner[(size_t)used[k]] = (int32_t)k;
+  std::string s;
+  char buf[64];
+  for (int32_t c = 0; c < num_total_features; ++c) {
+    if (c) s += ' ';
+    if (inner[(size_t)c] < 0) {
+      s += "none";
+      continue;
+    }
+    const BinMapper& m = mappers[(size_t)inner[(size_t)c]];
+    if (m.bin_type == 1) {
+      for (size_t i = 0; i < m.bin_2_categorical.size(); ++i) {
+        if (i) s += ':';
+        s += std::to_string(m.bin_2_categorical[i]);
+      }
+    } else {
+      std::snprintf(buf, sizeof(buf), "[%.17g:", m.min_val);
+      s += buf;
+      std::snprintf(buf, sizeof(buf), "%.17g]", m.max_val);
+      s += buf;
+    }
+  }
+  feature_infos = s;
+  return feature_infos;
 }
 
 void Dataset::fill_view(LgbmB200DatasetView* v) {

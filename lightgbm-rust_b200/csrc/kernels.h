@@ -120,8 +120,9 @@ __global__ void k_partition(const __grid_constant__ DCtx c);
 __global__ void k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows);
 size_t fused_smem_bytes();
 __global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
-__global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* sums);
-__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums);
+__global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* partial, int32_t* rank);
+__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* partial, const int32_t* rank,
+                             int32_t nwarps);
 __global__ void k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
                                    int64_t score_stride);
 __global__ void k_leaf_of_row(const __grid_constant__ DCtx c, int32_t* leaf_of_row);

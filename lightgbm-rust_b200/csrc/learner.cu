@@ -8,6 +8,7 @@
 // arrays back and rebuilds the reference's Tree layout on the host.
 #include <cstdlib>
 #include <algorithm>
+#include <functional>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -272,7 +273,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     int32_t nn = (int32_t)n;
     CU(cudaMemcpy(h->n_used_dev, &nn, sizeof(int32_t), cudaMemcpyHostToDevice));
   }
-  if (!(s = A.alloc_n(&h->leaf_sums, (size_t)K * L * 2)).ok()) return s;
+  // leaf renewal: a sum pair per (warp share, leaf) segment and each leaf's rank
+  if (!(s = A.alloc_n(&h->leaf_sums, (size_t)K * (leaf_sum_warps(h) + L) * 2)).ok()) return s;
+  if (!(s = A.alloc_n(&h->leaf_rank, (size_t)K * (L + 1))).ok()) return s;
   if (!(s = A.alloc_n(&h->leaf_values_dev, (size_t)K * L)).ok()) return s;
   if (cfg->persistent_grow) {
     if (!(s = A.alloc_n(&h->grow_sync, 1)).ok()) return s;
@@ -411,10 +414,9 @@ Status enqueue_tree(LgbmB200Learner* h) {
     if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
-    CU(cudaMemsetAsync(h->leaf_sums, 0, sizeof(double) * K * L * 2, s));
-    k_leaf_sums<<<dim3(h->num_sms * 4, 1, K), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums);
+    k_leaf_sums<<<dim3(leaf_sum_warps(h) / 8, 1, K), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums, h->leaf_rank);
     CU_LAUNCH();
-    k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums);
+    k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums, h->leaf_rank, leaf_sum_warps(h));
     CU_LAUNCH();
   }
   h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : ((h->fused || h->scan_part) ? 2 * (L - 1) + (h->fused ? 1 : 0)
@@ -824,6 +826,12 @@ int lgbm_b200_dataset_view(LgbmB200Dataset* ds, LgbmB200DatasetView* out) {
   return LGBM_B200_OK;
 }
 
+int lgbm_b200_dataset_feature_infos(LgbmB200Dataset* ds, const char** out) {
+  if (!ds || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  *out = reinterpret_cast<Dataset*>(ds)->infos().c_str();
+  return LGBM_B200_OK;
+}
+
 int lgbm_b200_dataset_create_device(const float* X, int64_t n, int32_t ncol, const LgbmB200BinParams* params,
                                     int32_t device, LgbmB200Dataset** out) {
   if (!X || !params || !out || device < 0) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "bad argument"));
@@ -914,9 +922,12 @@ int lgbm_b200_learner_set_feature_mask(LgbmB200Learner* h, int32_t slot, const u
   return LGBM_B200_OK;
 }
 
-int lgbm_b200_learner_train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location,
-                            LgbmB200TreeView* out) {
+int lgbm_b200_learner_train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t is_first_tree,
+                            int32_t location, LgbmB200TreeView* out) {
   if (!h || !grad || !hess) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  // is_first_tree only keeps the leaves of linear trees constant
+  // (learner/mod.rs:571-572, :685); linear trees are not on this path
+  (void)is_first_tree;
   Status s = lgbm_b200::train(h, grad, hess, location);
   if (!s.ok()) return fail(s);
   if (out)
@@ -1002,6 +1013,20 @@ int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* l
       cudaMemcpyAsync(indices + beg[l], d.idx[side[l]] + beg[l], sizeof(uint32_t) * cnt[l], cudaMemcpyDeviceToHost, s);
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "readback"));
+  // The device keeps a split's left rows in their order and writes its right
+  // rows reversed, so each leaf's rows are in ascending or descending order.
+  // partition() hands them out ascending, as the reference's stable
+  // partition does (partition.rs:107-174).
+  if (indices) {
+    for (int l = 0; l < nl; ++l) {
+      if (cnt[l] < 2) continue;
+      uint32_t* a = indices + beg[l];
+      uint32_t* e = a + cnt[l];
+      if (std::is_sorted(a, e)) continue;
+      if (std::is_sorted(a, e, std::greater<uint32_t>())) std::reverse(a, e);
+      else std::sort(a, e);
+    }
+  }
   return LGBM_B200_OK;
 }
 

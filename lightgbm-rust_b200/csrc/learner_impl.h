@@ -173,6 +173,7 @@ struct HostTree {  // the reference's Tree arrays for one trained tree
     v->cat_threshold = cat_threshold.data();
     v->cat_boundaries_inner = cat_boundaries_inner.data();
     v->cat_threshold_inner = cat_threshold_inner.data();
+    v->split_gain_f64 = node_gain.data();
   }
 };
 
@@ -261,8 +262,9 @@ struct LgbmB200Learner {
   int32_t* n_used_dev = nullptr;  // in-bag row count read by k_tree_init
   int32_t n_used = 0;
   bool bagging = false;
-  // leaf renewal scratch [K][L][2]
+  // leaf renewal scratch: [K][leaf_sum_warps + L][2] segment sums, [K][L + 1] leaf ranks
   double* leaf_sums = nullptr;
+  int32_t* leaf_rank = nullptr;
   double* leaf_values_dev = nullptr;  // [K][L] for add_leaf_outputs
   double* score_scratch = nullptr;  // host gradients staged for train (2 x num_data floats)
   double* score_stage = nullptr;    // host scores staged for add_leaf_outputs (num_data doubles)
@@ -309,6 +311,9 @@ struct LgbmB200Learner {
 
 
 namespace lgbm_b200 {
+// Warps of the leaf renewal's sum kernel (4 CTAs of 8 warps per SM); its
+// partial sums are laid out by warp.
+inline int32_t leaf_sum_warps(const LgbmB200Learner* h) { return h->num_sms * 4 * 8; }
 // One tree per slot from the given gradients (class-major [K x n]); NULL
 // gradients reuse the slots' interleaved buffers filled by the caller.
 Status train(LgbmB200Learner* h, const float* grad, const float* hess, int32_t location);

@@ -2434,47 +2434,76 @@ __device__ __forceinline__ void walk_leaf_positions(const LeafTable& t, Visit vi
 }
 
 // FP64 (g, h) sums of each leaf's rows for the leaf renewal
-// (learner/mod.rs:736-747). Grid (G, 1, slots), 256 threads. A lane sums its
-// positions of the warp's current leaf in registers; the warp adds them to
-// the leaf's total when it leaves the leaf (positions of leaves shorter than
-// a step add theirs at once).
-__global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* sums /*[slots][leaves][2]*/) {
+// (learner/mod.rs:736-747), in a fixed order so that a tree's leaf values
+// are the same on every run. Grid (G, 1, slots), 256 threads. Warp w takes
+// the positions [w * per, (w + 1) * per) (per = the positions over the
+// warps, rounded up to 32) and visits the leaves its share meets in
+// position order. For each it sums the share's part of the leaf lane-wise
+// (position q to lane q mod 32, in order) and across lanes by a fixed
+// butterfly, and stores the pair at segment w + rank, where rank is the
+// leaf's place in position order. Along the positions both w and rank only
+// grow and one of them grows at every new segment, so no two segments share
+// an index. Block 0 also records each leaf's rank and the share size for
+// k_leaf_renew, which adds a leaf's segments in warp order.
+// partial: [slots][G * 8 + num_leaves][2]; rank: [slots][num_leaves + 1].
+__global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx c, double* partial, int32_t* rank) {
   extern __shared__ int32_t lt_smem[];
   const DSlot& s = c.slots[blockIdx.z];
   const int32_t nl = s.st->num_leaves_cur;
   const LeafTable t = build_leaf_table(s, nl, lt_smem);
   const int lane = threadIdx.x & 31;
-  double* base = sums + (size_t)blockIdx.z * c.p.num_leaves * 2;
-  double g = 0.0, h = 0.0;
-  walk_leaf_positions(
-      t,
-      [&](int32_t q, int32_t rank, bool same) {
-        const float2 v = s.gh[s.idx[t.side[rank]][q]];
-        if (same) {
-          g += (double)v.x;
-          h += (double)v.y;
-        } else {
-          atomicAdd(base + 2 * t.leaf[rank], (double)v.x);
-          atomicAdd(base + 2 * t.leaf[rank] + 1, (double)v.y);
-        }
-      },
-      [&](int32_t rank) {
-        const double sg = warp_sum_d(g), sh = warp_sum_d(h);
-        if (lane == 0) {
-          atomicAdd(base + 2 * t.leaf[rank], sg);
-          atomicAdd(base + 2 * t.leaf[rank] + 1, sh);
-        }
-        g = 0.0;
-        h = 0.0;
-      });
+  const int32_t nwarps = (int32_t)(gridDim.x * (blockDim.x >> 5));
+  const int32_t gw = (int32_t)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+  const int32_t per = ((t.total + nwarps - 1) / nwarps + 31) & ~31;
+  int32_t* rk = rank + (size_t)blockIdx.z * (c.p.num_leaves + 1);
+  if (blockIdx.x == 0) {
+    for (int32_t r = threadIdx.x; r < t.n; r += blockDim.x) rk[t.leaf[r]] = r;
+    if (threadIdx.x == 0) rk[c.p.num_leaves] = per;
+  }
+  const int32_t p0 = min(t.total, gw * per), p1 = min(t.total, p0 + per);
+  if (p0 >= p1 || t.n == 0) return;
+  double* base = partial + (size_t)blockIdx.z * (nwarps + c.p.num_leaves) * 2;
+  int32_t r = leaf_rank_of(t, p0);
+  for (int32_t q0 = p0; q0 < p1; ++r) {
+    const int32_t end = min(p1, r + 1 < t.n ? t.begin[r + 1] : t.total);
+    const uint32_t* idx = s.idx[t.side[r]];
+    double g = 0.0, h = 0.0;
+    for (int32_t q = q0 + lane; q < end; q += 32) {
+      const float2 v = s.gh[idx[q]];
+      g += (double)v.x;
+      h += (double)v.y;
+    }
+    g = warp_sum_d(g);
+    h = warp_sum_d(h);
+    if (lane == 0) {
+      base[2 * (gw + r)] = g;
+      base[2 * (gw + r) + 1] = h;
+    }
+    q0 = end;
+  }
 }
 
-__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* sums) {
+// Leaf outputs from the segment sums of k_leaf_sums (grid (1, 1, slots)):
+// a leaf at rank r covering positions [b, e) adds segments w + r for
+// w = b / per ... (e - 1) / per, in that order.
+__global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* partial, const int32_t* rank,
+                             int32_t nwarps) {
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
+  const int32_t* rk = rank + (size_t)blockIdx.z * (c.p.num_leaves + 1);
+  const int32_t per = rk[c.p.num_leaves];
+  const double* base = partial + (size_t)blockIdx.z * (nwarps + c.p.num_leaves) * 2;
   for (int32_t leaf = threadIdx.x; leaf < st->num_leaves_cur; leaf += blockDim.x) {
-    const double* o = sums + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
-    s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(o[0], o[1], c.p, s.leaf_count[leaf]));
+    const int32_t cnt = s.leaf_count[leaf];
+    double g = 0.0, h = 0.0;
+    if (cnt > 0) {
+      const int32_t b = s.leaf_begin[leaf], r = rk[leaf];
+      for (int32_t w = b / per; w <= (b + cnt - 1) / per; ++w) {
+        g += base[2 * (w + r)];
+        h += base[2 * (w + r) + 1];
+      }
+    }
+    s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(g, h, c.p, cnt));
   }
 }
 

@@ -46,7 +46,10 @@ struct Dataset {
   std::vector<int32_t> num_bin, missing_type, default_bin, most_freq_bin, bin_type, real_index, bin_to_cat;
   std::vector<double> upper_bounds;
   std::vector<int64_t> ub_offsets, cat_offsets;
+  std::string feature_infos;  // built on request
   void fill_view(LgbmB200DatasetView* v);
+  // Dataset::feature_infos (dataset.rs:770-776), space-separated
+  const std::string& infos();
 };
 
 // device < 0: the rows are binned on the host; else on that CUDA device

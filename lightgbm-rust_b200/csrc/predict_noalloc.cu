@@ -21,7 +21,8 @@
 // The first call on a device, with that device current, resolves the array's
 // device address with cudaGetSymbolAddress (which also loads the library's
 // device code on that device); make that first call before capturing any
-// stream on the device.
+// stream on the device. The calling thread's current device is the same
+// before and after a call.
 #include <mutex>
 
 #include "learner_impl.h"
@@ -62,6 +63,22 @@ using namespace lgbm_b200;
 
 extern "C" {
 
+namespace {
+
+// Restores the calling thread's current device when the call returns, so a
+// serving thread that works on another device keeps it.
+struct DeviceRestore {
+  int prev = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceRestore() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
 int lgbm_b200_predict_noalloc(LgbmB200Forest* F, const float* X, int64_t nrow, int32_t ncol, double* out) {
   if (!F || !X || !out || nrow < 0 || ncol <= 0)
     return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "predict_noalloc: bad argument"));
@@ -79,6 +96,7 @@ int lgbm_b200_predict_noalloc(LgbmB200Forest* F, const float* X, int64_t nrow, i
                            " staging bytes (4 x ncol + 8 x num_tree_per_iteration); the static staging array "
                            "holds 16 MiB"));
   if (nrow == 0) return LGBM_B200_OK;
+  DeviceRestore restore;
   if (cudaSetDevice(device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
   unsigned char* stage;
   Status st = stage_address(device, &stage);
@@ -93,10 +111,7 @@ int lgbm_b200_predict_noalloc(LgbmB200Forest* F, const float* X, int64_t nrow, i
     // all three steps run in order on the forest's stream, so the next chunk's
     // rows overwrite the array only after this chunk's kernel and copy-out
     e = cudaMemcpyAsync(xs, X + r0 * ncol, x_bytes, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
-      launch_predict(*f, xs, m, ncol, os, s);
-      e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = launch_predict(*f, xs, m, ncol, os, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(out + r0 * ntpi, os, sizeof(double) * (size_t)m * ntpi, cudaMemcpyDeviceToHost, s);
   }

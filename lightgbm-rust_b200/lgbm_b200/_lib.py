@@ -81,7 +81,7 @@ class TreeView(C.Structure):
                 ("leaf_depth", P(i32)), ("internal_value", P(f64)), ("internal_weight", P(f64)),
                 ("internal_count", P(i32)), ("num_cat", i32), ("cat_boundaries", P(i32)),
                 ("cat_threshold", P(C.c_uint32)), ("cat_boundaries_inner", P(i32)),
-                ("cat_threshold_inner", P(C.c_uint32))]
+                ("cat_threshold_inner", P(C.c_uint32)), ("split_gain_f64", P(f64))]
 
 
 class ObjectiveConfig(C.Structure):
@@ -110,13 +110,14 @@ SIGNATURES = {
     "lgbm_b200_dataset_create_device": (C.c_int, [P(C.c_float), i64, i32, P(BinParams), i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_create_valid_device": (C.c_int, [P(C.c_float), i64, i32, C.c_void_p, i32, P(C.c_void_p)]),
     "lgbm_b200_dataset_view": (C.c_int, [C.c_void_p, P(DatasetView)]),
+    "lgbm_b200_dataset_feature_infos": (C.c_int, [C.c_void_p, P(C.c_char_p)]),
     "lgbm_b200_dataset_free": (None, [C.c_void_p]),
     "lgbm_b200_learner_create": (C.c_int, [P(LearnerConfig), u8p, i64, i32, P(FeatureMeta), P(f64), P(i64),
                                            P(i32), P(i64), P(C.c_void_p)]),
     "lgbm_b200_learner_destroy": (None, [C.c_void_p]),
     "lgbm_b200_learner_set_bagging": (C.c_int, [C.c_void_p, P(C.c_uint32), i64, i32]),
     "lgbm_b200_learner_set_feature_mask": (C.c_int, [C.c_void_p, i32, u8p]),
-    "lgbm_b200_learner_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, i32, P(TreeView)]),
+    "lgbm_b200_learner_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, i32, i32, P(TreeView)]),
     "lgbm_b200_learner_add_leaf_outputs": (C.c_int, [C.c_void_p, i32, P(f64), i32, C.c_void_p, i32]),
     "lgbm_b200_learner_get_partition": (C.c_int, [C.c_void_p, i32, P(i32), P(i32), P(C.c_uint32)]),
     "lgbm_b200_learner_get_launch_shape": (C.c_int, [C.c_void_p, P(LaunchShape)]),

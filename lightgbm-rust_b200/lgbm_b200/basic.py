@@ -10,6 +10,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib as L
+from . import model_text
 
 # config.rs:517-602 defaults for the parameters this path reads
 DEFAULTS = {
@@ -180,6 +181,7 @@ def tree_from_view(v):
     t["cat_boundaries_inner"] = arr(v.cat_boundaries_inner, nc + 1, np.int32)
     t["cat_threshold_inner"] = arr(v.cat_threshold_inner, int(t["cat_boundaries_inner"][-1]) if nc else 0,
                                    np.uint32)
+    t["split_gain_f64"] = arr(v.split_gain_f64, nn, np.float64) if v.split_gain_f64 else np.zeros(0)
     return t
 
 
@@ -242,12 +244,13 @@ class Learner:
         self.handle = h
         self.num_tree_slots = num_tree_slots
 
-    def train(self, grad, hess):
+    def train(self, grad, hess, is_first_tree=False):
         """SerialTreeLearner::train on host gradients; one tree dict per slot."""
         g = np.ascontiguousarray(grad, dtype=np.float32)
         h = np.ascontiguousarray(hess, dtype=np.float32)
         views = (L.TreeView * self.num_tree_slots)()
-        L.check(L.lib().lgbm_b200_learner_train(self.handle, g.ctypes.data, h.ctypes.data, L.HOST, views))
+        L.check(L.lib().lgbm_b200_learner_train(self.handle, g.ctypes.data, h.ctypes.data, int(bool(is_first_tree)),
+                                                L.HOST, views))
         return [tree_from_view(views[k]) for k in range(self.num_tree_slots)]
 
     def set_bagging(self, used):
@@ -446,9 +449,11 @@ class Booster:
         p = self.params
         self.num_class = int(p["num_class"]) if OBJECTIVES[p["objective"]] == L.OBJ_MULTICLASS else 1
         self.trees = []
+        self.shrinkages = []  # Tree::shrinkage of each tree (tree.rs:303-339)
         self._forest = None
         self.learner = None
         self._b = None
+        self._train_set = train_set
         if train_set is not None:
             self.learner = Learner(train_set, params, num_tree_slots=self.num_class)
             valid_bins = None
@@ -482,9 +487,40 @@ class Booster:
         L.check(L.lib().lgbm_b200_booster_train_iter(self._b, C.byref(stop), views))
         if stop.value:
             return True
-        self.trees.extend(tree_from_view(views[k]) for k in range(self.num_class))
+        first = not self.trees
+        if first:
+            init = np.zeros(self.num_class, np.float64)
+            L.check(L.lib().lgbm_b200_booster_init_scores(self._b, _ptr(init, C.c_double)))
+        for k in range(self.num_class):
+            t = tree_from_view(views[k])
+            self.trees.append(t)
+            # shrink() multiplies the shrinkage by the learning rate; add_bias
+            # (the first iteration's boost_from_average score) and a constant
+            # tree set it back to 1
+            if t["num_leaves"] <= 1 or (first and abs(init[k]) > model_text.K_EPSILON):
+                self.shrinkages.append(1.0)
+            else:
+                self.shrinkages.append(float(self.params["learning_rate"]))
         self._forest = None
         return False
+
+    def model_to_string(self):
+        """Gbdt::save_model_to_string (io.rs:13-85): the model text from the
+        header through the feature importances (model_text.py)."""
+        ds = self._train_set
+        if ds is None:
+            raise L.LightGBMError(L.ERR_INVALID_PARAMETER, "model_to_string needs the training Dataset")
+        ds.construct(self.params)
+        infos = C.c_char_p()
+        L.check(L.lib().lgbm_b200_dataset_feature_infos(ds._handle, C.byref(infos)))
+        mono = self.params.get("monotone_constraints")
+        return model_text.model_to_string(self.params, self.trees, self.shrinkages, self.num_class,
+                                          ds.data.shape[1], infos.value.decode().split(" "), mono)
+
+    def save_model(self, filename):
+        with open(filename, "w") as f:
+            f.write(self.model_to_string())
+        return self
 
     def scores(self, valid=False):
         n = self.num_valid if valid else self.num_train

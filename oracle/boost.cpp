@@ -4,6 +4,7 @@
 // (learner/col_sampler.rs), raw-value prediction (predict.rs) and metrics
 // (metric.rs), plus the C ABI the tests load with ctypes.
 // TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.
+#include <cstdio>
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -238,6 +239,7 @@ struct Booster {
   int32_t used_cnt_bytree = 0;
   int iter = 0;
   std::vector<std::vector<TreeTraceEntry>> traces;
+  std::string model_text;
 };
 
 static void add_const(std::vector<double>& s, int k, size_t n, double v) {
@@ -402,14 +404,7 @@ static SplitParams split_params(const OracleParams& p) {
 using namespace oracle;
 
 static thread_local std::string g_last_error;
-#define ORACLE_TRY(...)                  \
-  try {                                  \
-    __VA_ARGS__;                         \
-    return 0;                            \
-  } catch (const std::exception& e) {    \
-    g_last_error = e.what();             \
-    return -1;                           \
-  }
+void oracle::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" {
 
@@ -472,6 +467,17 @@ int oracle_train(const OracleParams* p, const OracleData* train, const float* la
     for (int32_t it = 0; it < p->num_iterations; ++it)
       if (train_one_iter(*b)) break;
     *out = reinterpret_cast<OracleBooster*>(b.release());
+  })
+}
+
+// One more boosting iteration of a booster made by oracle_train (which may
+// have run 0 iterations): Gbdt::train_one_iter (boosting.rs:957). *stop is 1
+// when the iteration found no split (training has finished).
+int oracle_booster_update(OracleBooster* h, int32_t* stop) {
+  ORACLE_TRY({
+    Booster* b = reinterpret_cast<Booster*>(h);
+    const bool finished = train_one_iter(*b);
+    if (stop) *stop = finished ? 1 : 0;
   })
 }
 
@@ -697,6 +703,30 @@ int oracle_hist(const OracleData* d, const uint32_t* rows, int64_t nrows, const 
   })
 }
 
+// histogram.rs:42-56 fix on one feature view: num_bin bins, the view
+// starting at bin `offset`, hist holding 2 * (num_bin - offset) values.
+int oracle_fix_hist(int32_t num_bin, int32_t offset, int32_t most_freq_bin, double sum_g, double sum_h,
+                    double* hist) {
+  ORACLE_TRY({
+    FeatureMeta m{};
+    m.num_bin = num_bin;
+    m.offset = offset;
+    m.most_freq_bin = (uint32_t)most_freq_bin;
+    if (offset == 0) fix_hist(m, sum_g, sum_h, hist);  // an offset view has no stored most-frequent bin to fix
+  })
+}
+
+// split.rs:114-121 SplitInfo::better_than of (gain_a, feature_a) against
+// (gain_b, feature_b); feature -1 is "no split".
+int32_t oracle_better_than(double gain_a, int32_t feature_a, double gain_b, int32_t feature_b) {
+  SplitInfo a, b;
+  a.gain = gain_a;
+  a.feature = feature_a;
+  b.gain = gain_b;
+  b.feature = feature_b;
+  return a.better_than(b) ? 1 : 0;
+}
+
 int oracle_find_best_threshold(const OracleFeature* f, const OracleParams* p, const double* hist,
                                const int64_t* ihist, double sum_g, double sum_h, int64_t int_sum, double gscale,
                                double hscale, int32_t num_data, double parent_output, OracleSplit* out) {
@@ -771,5 +801,110 @@ int oracle_block_info(int64_t threads, int64_t cnt, int64_t min_cnt, int64_t* ou
 }
 
 int8_t oracle_to_i8(double x) { return to_i8(x); }
+
+
+}  // extern "C"
+
+// ---- model text: io.rs:13-85 (save_model_to_string), tree.rs:718-773
+// (Tree::to_model_string) and fmt.rs (%g / %.17g) ---------------------------
+// The text stops after the feature importances: the "parameters:" block is
+// the Config's own text (config.rs:1169-1187), which is not on this path.
+static std::string fmt_g(double v, int prec) {  // fmt.rs fmt_g: C printf("%.{prec}g")
+  if (std::isnan(v)) return std::signbit(v) ? "-nan" : "nan";
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "%.*g", prec, v);
+  return buf;
+}
+
+template <class T, class F>
+static std::string join_arr(const T* a, size_t n, F f) {
+  std::string s;
+  for (size_t i = 0; i < n; ++i) {
+    if (i) s += ' ';
+    s += f(a[i]);
+  }
+  return s;
+}
+
+static std::string tree_text(const Tree& t) {  // tree.rs:718-773 (is_linear false)
+  const size_t n = (size_t)t.num_leaves, ni = n - 1;
+  auto i2s = [](auto x) { return std::to_string((long long)x); };
+  auto g6 = [](double x) { return fmt_g(x, 6); };
+  auto g17 = [](double x) { return fmt_g(x, 17); };
+  std::string s;
+  s += "num_leaves=" + std::to_string(n) + "\n";
+  s += "num_cat=" + std::to_string(t.num_cat) + "\n";
+  s += "split_feature=" + join_arr(t.split_feature.data(), ni, i2s) + "\n";
+  s += "split_gain=" + join_arr(t.split_gain.data(), ni, [&](float x) { return g6((double)x); }) + "\n";
+  s += "threshold=" + join_arr(t.threshold.data(), ni, g17) + "\n";
+  s += "decision_type=" + join_arr(t.decision_type.data(), ni, i2s) + "\n";
+  s += "left_child=" + join_arr(t.left_child.data(), ni, i2s) + "\n";
+  s += "right_child=" + join_arr(t.right_child.data(), ni, i2s) + "\n";
+  s += "leaf_value=" + join_arr(t.leaf_value.data(), n, g17) + "\n";
+  s += "leaf_weight=" + join_arr(t.leaf_weight.data(), std::min(n, t.leaf_weight.size()), g17) + "\n";
+  s += "leaf_count=" + join_arr(t.leaf_count.data(), n, i2s) + "\n";
+  s += "internal_value=" + join_arr(t.internal_value.data(), ni, g6) + "\n";
+  s += "internal_weight=" + join_arr(t.internal_weight.data(), ni, g6) + "\n";
+  s += "internal_count=" + join_arr(t.internal_count.data(), ni, i2s) + "\n";
+  if (t.num_cat > 0) {
+    s += "cat_boundaries=" + join_arr(t.cat_boundaries.data(), (size_t)t.num_cat + 1, i2s) + "\n";
+    s += "cat_threshold=" + join_arr(t.cat_threshold.data(), t.cat_threshold.size(), i2s) + "\n";
+  }
+  s += "is_linear=0\n";
+  s += "shrinkage=" + g6(t.shrinkage) + "\n";
+  s += "\n";
+  return s;
+}
+
+extern "C" {
+
+int oracle_model_to_string(OracleBooster* h, int32_t num_total_features, const char* feature_infos,
+                           const int8_t* monotone, int32_t num_monotone, const char** out) {
+  ORACLE_TRY({
+    Booster* b = reinterpret_cast<Booster*>(h);
+    const OracleParams& p = b->p;
+    std::string obj;  // the objectives' to_model_string
+    if (p.objective == 0) obj = "binary sigmoid:" + fmt_g(p.sigmoid, 6);  // binary.rs:168-170
+    else if (p.objective == 1) obj = "regression";                       // regression.rs:346-348
+    else if (p.objective == 2) obj = "multiclass num_class:" + std::to_string(p.num_class);  // multiclass.rs:169
+    else obj = "lambdarank";                                              // rank.rs:338-340
+    std::string s = "tree\nversion=v4\n";
+    s += "num_class=" + std::to_string(p.objective == 2 ? p.num_class : 1) + "\n";
+    s += "num_tree_per_iteration=" + std::to_string(b->ntpi) + "\n";
+    s += "label_index=0\n";
+    s += "max_feature_idx=" + std::to_string(num_total_features - 1) + "\n";
+    s += "objective=" + obj + "\n";
+    std::string names;
+    for (int32_t c = 0; c < num_total_features; ++c) names += (c ? " Column_" : "Column_") + std::to_string(c);
+    s += "feature_names=" + names + "\n";
+    if (monotone && num_monotone > 0)
+      s += "monotone_constraints=" + join_arr(monotone, (size_t)num_monotone, [](int8_t x) {
+             return std::to_string((int)x);
+           }) + "\n";
+    s += std::string("feature_infos=") + (feature_infos ? feature_infos : "") + "\n";
+    std::vector<std::string> trees;
+    for (size_t i = 0; i < b->models.size(); ++i)
+      trees.push_back("Tree=" + std::to_string(i) + "\n" + tree_text(b->models[i]) + "\n");
+    std::string sizes;
+    for (size_t i = 0; i < trees.size(); ++i) sizes += (i ? " " : "") + std::to_string(trees[i].size());
+    s += "tree_sizes=" + sizes + "\n\n";
+    for (const std::string& t : trees) s += t;
+    s += "end of trees\n";
+    // boosting.rs:1337-1360 split counts, importance_type 0; sorted by count,
+    // descending, stable
+    std::vector<long long> imp((size_t)num_total_features, 0);
+    for (const Tree& t : b->models)
+      for (int32_t k = 0; k + 1 < t.num_leaves; ++k)
+        if (t.split_gain[(size_t)k] > 0.0f) imp[(size_t)t.split_feature[(size_t)k]] += 1;
+    std::vector<int32_t> order;
+    for (int32_t c = 0; c < num_total_features; ++c)
+      if (imp[(size_t)c] > 0) order.push_back(c);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return imp[(size_t)a] > imp[(size_t)c]; });
+    s += "\nfeature_importances:\n";
+    for (int32_t c : order) s += "Column_" + std::to_string(c) + "=" + std::to_string(imp[(size_t)c]) + "\n";
+    b->model_text = s;
+    *out = b->model_text.c_str();
+  });
+}
 
 }  // extern "C"

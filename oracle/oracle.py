@@ -61,6 +61,13 @@ class OracleSplit(C.Structure):
                 ("left_sum_gh", i64), ("right_sum_gh", i64)]
 
 
+class OracleBinParams(C.Structure):
+    _fields_ = [("max_bin", i32), ("min_data_in_bin", i32), ("min_data_in_leaf", i32),
+                ("bin_construct_sample_cnt", i32), ("data_random_seed", i32), ("use_missing", i32),
+                ("zero_as_missing", i32), ("feature_pre_filter", i32), ("categorical", P(i32)),
+                ("num_categorical", i32)]
+
+
 _lib = None
 
 
@@ -78,6 +85,7 @@ def lib():
         L.oracle_train.argtypes = [P(OracleParams), P(OracleData), P(C.c_float), P(i32), i32, P(OracleData),
                                    P(C.c_void_p)]
         L.oracle_booster_free.argtypes = [C.c_void_p]
+        L.oracle_booster_update.argtypes = [C.c_void_p, P(i32)]
         L.oracle_train_tree.argtypes = [P(OracleParams), P(OracleData), P(C.c_float), P(C.c_float),
                                         P(C.c_uint32), i64, i32, P(C.c_uint8), P(C.c_void_p)]
         L.oracle_booster_partition.argtypes = [C.c_void_p, P(i32), P(i32), P(C.c_uint32)]
@@ -100,6 +108,16 @@ def lib():
         L.oracle_mt19937.argtypes = [C.c_uint32, i32, P(C.c_uint32)]
         L.oracle_lcg_sample.argtypes = [i32, i32, i32, P(i32), P(i32)]
         L.oracle_block_info.argtypes = [i64, i64, i64, P(i64)]
+        L.oracle_dataset_create.argtypes = [P(C.c_float), i64, i32, P(OracleBinParams), P(C.c_void_p)]
+        L.oracle_dataset_create_valid.argtypes = [P(C.c_float), i64, i32, C.c_void_p, P(C.c_void_p)]
+        L.oracle_dataset_view.argtypes = [C.c_void_p, P(OracleData), P(i32)]
+        L.oracle_dataset_feature_infos.restype = C.c_char_p
+        L.oracle_dataset_feature_infos.argtypes = [C.c_void_p]
+        L.oracle_dataset_free.argtypes = [C.c_void_p]
+        L.oracle_model_to_string.argtypes = [C.c_void_p, i32, C.c_char_p, P(C.c_int8), i32, P(C.c_char_p)]
+        L.oracle_fix_hist.argtypes = [i32, i32, i32, f64, f64, P(f64)]
+        L.oracle_better_than.restype = i32
+        L.oracle_better_than.argtypes = [f64, i32, f64, i32]
         L.oracle_to_i8.restype = C.c_int8
         L.oracle_to_i8.argtypes = [f64]
         _lib = L
@@ -224,6 +242,25 @@ class Model:
         _check(lib().oracle_predict_raw(self.h, _p(X, C.c_float), X.shape[0], X.shape[1], _p(out, f64)))
         return out.reshape(X.shape[0], self.ntpi)
 
+    def update(self):
+        """One more boosting iteration (Gbdt::train_one_iter); True when training stopped."""
+        stop = i32()
+        _check(lib().oracle_booster_update(self.h, C.byref(stop)))
+        L = lib()
+        for i in range(len(self.trees), L.oracle_booster_num_trees(self.h)):
+            v = OracleTreeView()
+            _check(L.oracle_booster_tree(self.h, i, C.byref(v)))
+            self.trees.append(_tree(v))
+        return bool(stop.value)
+
+    def model_to_string(self, num_total_features, feature_infos, monotone=None):
+        """Gbdt::save_model_to_string (io.rs:13-85) up to the feature importances."""
+        out = C.c_char_p()
+        mono = None if monotone is None else np.ascontiguousarray(monotone, dtype=np.int8)
+        _check(lib().oracle_model_to_string(self.h, int(num_total_features), " ".join(feature_infos).encode(),
+                                            _p(mono, C.c_int8), 0 if mono is None else len(mono), C.byref(out)))
+        return out.value.decode()
+
     def __del__(self):
         if getattr(self, "h", None) is not None and _lib is not None:
             _lib.oracle_booster_free(self.h)
@@ -245,7 +282,10 @@ def train(p, binned, label, num_iterations, valid_binned=None, group=None, monot
     _check(lib().oracle_train(C.byref(ps), C.byref(d.s), _p(label, C.c_float), _p(bnd, i32), nq,
                               C.byref(vd.s) if vd else None, C.byref(h)))
     ntpi = int(p["num_class"]) if OBJ[p["objective"]] == 2 else 1
-    return Model(h, ntpi, int(binned["num_data"]), int(valid_binned["num_data"]) if valid_binned else 0)
+    m = Model(h, ntpi, int(binned["num_data"]), int(valid_binned["num_data"]) if valid_binned else 0)
+    # the booster keeps pointers into the binned arrays: they live as long as the model
+    m.data, m.vdata = d, vd
+    return m
 
 
 def train_trees(p, binned, grad, hess, num_trees=1, bag=None, bytree=None, monotone=None):
@@ -318,3 +358,51 @@ def ndcg(label, score, group, ks):
     _check(lib().oracle_ndcg(_p(label, C.c_float), _p(score, f64), _p(bnd, i32), len(group), _p(ks, i32), len(ks),
                              _p(out, f64)))
     return out
+
+
+class Dataset:
+    """The oracle's own binning of a dense f32 matrix (Dataset::from_dense,
+    dataset.rs:355; binning.cpp). `binned()` has the layout of the product's
+    Dataset.binned(); `feature_infos` is Dataset::feature_infos (dataset.rs:770)."""
+
+    def __init__(self, X, params, categorical=None, reference=None):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        n, ncol = X.shape
+        h = C.c_void_p()
+        if reference is not None:
+            _check(lib().oracle_dataset_create_valid(_p(X, C.c_float), n, ncol, reference.h, C.byref(h)))
+        else:
+            cats = np.ascontiguousarray(sorted(set(categorical or [])), dtype=np.int32)
+            bp = OracleBinParams(int(params["max_bin"]), int(params["min_data_in_bin"]),
+                                 int(params["min_data_in_leaf"]), int(params["bin_construct_sample_cnt"]),
+                                 int(params["data_random_seed"]), int(bool(params["use_missing"])),
+                                 int(bool(params["zero_as_missing"])), int(bool(params["feature_pre_filter"])),
+                                 _p(cats, i32) if len(cats) else None, len(cats))
+            _check(lib().oracle_dataset_create(_p(X, C.c_float), n, ncol, C.byref(bp), C.byref(h)))
+        self.h = h
+        v = OracleData()
+        nt = i32()
+        _check(lib().oracle_dataset_view(h, C.byref(v), C.byref(nt)))
+        nf = v.num_features
+        nd = int(v.num_data)
+        b = {"num_data": nd, "num_features": nf, "num_total_features": int(nt.value),
+             "bins": np.ctypeslib.as_array(v.bins, shape=(nd * nf,)).reshape(nd, nf).copy()
+             if nf else np.zeros((nd, 0), np.uint8)}
+        for name in ("num_bin", "missing_type", "default_bin", "most_freq_bin", "bin_type", "real_index"):
+            b[name] = np.ctypeslib.as_array(getattr(v, name), shape=(nf,)).copy() if nf else np.zeros(0, np.int32)
+        b["ub_offsets"] = np.ctypeslib.as_array(v.ub_offsets, shape=(nf + 1,)).copy()
+        b["cat_offsets"] = np.ctypeslib.as_array(v.cat_offsets, shape=(nf + 1,)).copy()
+        nu, nc = int(b["ub_offsets"][-1]), int(b["cat_offsets"][-1])
+        b["upper_bounds"] = np.ctypeslib.as_array(v.upper_bounds, shape=(nu,)).copy() if nu else np.zeros(0)
+        b["bin_to_cat"] = (np.ctypeslib.as_array(v.bin_to_cat, shape=(nc,)).copy() if nc
+                           else np.zeros(0, np.int32))
+        self._binned = b
+        self.feature_infos = lib().oracle_dataset_feature_infos(h).decode().split(" ")
+
+    def binned(self):
+        return self._binned
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.oracle_dataset_free(self.h)
+            self.h = None

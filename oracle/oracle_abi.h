@@ -93,12 +93,33 @@ typedef struct {
   int64_t left_sum_gh, right_sum_gh;
 } OracleSplit;
 
+// Bin parameters of a dataset build (config.rs names).
+typedef struct {
+  int32_t max_bin, min_data_in_bin, min_data_in_leaf, bin_construct_sample_cnt, data_random_seed;
+  int32_t use_missing, zero_as_missing, feature_pre_filter;
+  const int32_t* categorical;  // column indices of categorical features
+  int32_t num_categorical;
+} OracleBinParams;
+
+typedef struct OracleDataset OracleDataset;
+
 const char* oracle_last_error(void);
+// Dataset::from_dense (dataset.rs:355) and from_dense_with_reference (:446):
+// the oracle's own bin finding and stored group values (binning.cpp).
+int oracle_dataset_create(const float* X, int64_t n, int32_t ncol, const OracleBinParams* p, OracleDataset** out);
+int oracle_dataset_create_valid(const float* X, int64_t n, int32_t ncol, const OracleDataset* ref,
+                                OracleDataset** out);
+// The binned matrix and per-feature metadata (valid until the dataset is freed).
+int oracle_dataset_view(OracleDataset* d, OracleData* out, int32_t* num_total_features);
+// Dataset::feature_infos (dataset.rs:770), space-separated.
+const char* oracle_dataset_feature_infos(OracleDataset* d);
+void oracle_dataset_free(OracleDataset* d);
 int oracle_train(const OracleParams* p, const OracleData* train, const float* label, const int32_t* query_boundaries,
                  int32_t num_queries, const OracleData* valid, OracleBooster** out);
 int oracle_train_tree(const OracleParams* p, const OracleData* train, const float* grad, const float* hess,
                       const uint32_t* bag, int64_t n_bag, int32_t num_trees, const uint8_t* bytree,
                       OracleBooster** out);
+int oracle_booster_update(OracleBooster* h, int32_t* stop);
 int oracle_booster_partition(OracleBooster* h, int32_t* leaf_begin, int32_t* leaf_count, uint32_t* indices);
 void oracle_booster_free(OracleBooster* h);
 int32_t oracle_booster_num_trees(OracleBooster* h);
@@ -106,6 +127,11 @@ int oracle_booster_tree(OracleBooster* h, int32_t i, OracleTreeView* out);
 int oracle_booster_trace(OracleBooster* h, int32_t i, int32_t* n, int32_t* leaf, int32_t* feature,
                          uint32_t* threshold, double* gain);
 int oracle_booster_scores(OracleBooster* h, int valid, double* out);
+// Gbdt::save_model_to_string (io.rs:13-85) up to the feature importances:
+// the header, every tree (tree.rs:718-773) and the split counts. The text
+// stays valid until the booster is freed or the next call.
+int oracle_model_to_string(OracleBooster* h, int32_t num_total_features, const char* feature_infos,
+                           const int8_t* monotone, int32_t num_monotone, const char** out);
 int oracle_predict_raw(OracleBooster* h, const float* X, int64_t nrow, int32_t ncol, double* out);
 double oracle_auc(const float* label, const double* score, int64_t n);
 int oracle_ndcg(const float* label, const double* score, const int32_t* bnd, int32_t nq, const int32_t* ks,
@@ -114,6 +140,9 @@ int oracle_gradients(int32_t objective, int32_t num_class, double sigmoid, const
                      int64_t n, const int32_t* bnd, int32_t nq, int32_t truncation, int32_t norm, float* g, float* h);
 int oracle_hist(const OracleData* d, const uint32_t* rows, int64_t nrows, const float* g, const float* h,
                 const int64_t* packed, double* out_f64, int64_t* out_int);
+int oracle_fix_hist(int32_t num_bin, int32_t offset, int32_t most_freq_bin, double sum_g, double sum_h,
+                    double* hist);
+int32_t oracle_better_than(double gain_a, int32_t feature_a, double gain_b, int32_t feature_b);
 int oracle_find_best_threshold(const OracleFeature* f, const OracleParams* p, const double* hist,
                                const int64_t* ihist, double sum_g, double sum_h, int64_t int_sum, double gscale,
                                double hscale, int32_t num_data, double parent_output, OracleSplit* out);

@@ -6,9 +6,22 @@
 #include <array>
 #include <cstddef>
 #include <memory>
+#include <stdexcept>
 #include <string>
 
 namespace oracle {
+
+// Error state of the C ABI: an entry point body runs inside ORACLE_TRY, which
+// returns 0, or -1 with the exception's message kept for oracle_last_error().
+void set_last_error(const std::string& msg);
+#define ORACLE_TRY(...)                       \
+  try {                                       \
+    __VA_ARGS__;                              \
+    return 0;                                 \
+  } catch (const std::exception& e) {         \
+    ::oracle::set_last_error(e.what());       \
+    return -1;                                \
+  }
 
 // split.cpp
 double threshold_l1(double s, double l1);

@@ -75,3 +75,52 @@ def binned_dataset(lgb, X, y=None, params=None, reference=None, categorical=None
     ds = lgb.Dataset(X, label=y, params=params, reference=reference, categorical_feature=categorical)
     ds.construct(params)
     return ds
+
+
+def tolerances():
+    """The parity bars of tests/tolerances.toml."""
+    import tomllib
+
+    with open(os.path.join(ROOT, "tests", "tolerances.toml"), "rb") as f:
+        return tomllib.load(f)
+
+
+TOL = tolerances()
+
+
+def within(got, want, section):
+    """|got - want| <= atol + rtol * |want| under TOL[section] (NaN == NaN)."""
+    t = TOL[section]
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    ok = np.abs(got - want) <= t.get("atol", 0.0) + t["rtol"] * np.abs(want)
+    return bool(np.all(ok | (np.isnan(got) & np.isnan(want))))
+
+
+def compare_boosted_trees(gpu_trees, oracle_model, leaf_section="leaf_value"):
+    """Walk two boosting runs tree by tree: the structure must be exact, the
+    FP64 split gains within TOL["split_gain"] of the oracle's trace and the
+    leaf values within TOL[leaf_section]. At the first split where the two
+    pick different candidates, the pick must be a gain tie (the two gains
+    within TOL["split_gain"]["tie_rtol"]); later trees legitimately differ
+    and are not compared. Returns (identical trees, tie or None) where tie =
+    (tree, node, gpu gain, oracle gain)."""
+    g = TOL["split_gain"]
+    for i, (a, o) in enumerate(zip(gpu_trees, oracle_model.trees)):
+        _, feat, thr, gains = oracle_model.trace(i)
+        nn = min(a["num_leaves"], o["num_leaves"]) - 1
+        for j in range(nn):
+            ga = float(a["split_gain_f64"][j])
+            same = a["split_feature"][j] == o["split_feature"][j] and a["threshold_in_bin"][j] == o["threshold_in_bin"][j]
+            if not same:
+                assert abs(ga - gains[j]) <= g["tie_rtol"] * abs(gains[j]), (
+                    f"tree {i} node {j}: different split without a gain tie", ga, gains[j])
+                return i, (i, j, ga, float(gains[j]))
+            assert abs(ga - gains[j]) <= g["atol"] + g["rtol"] * abs(gains[j]), (i, j, ga, gains[j])
+        assert a["num_leaves"] == o["num_leaves"], (i, a["num_leaves"], o["num_leaves"])
+        for k in ("split_feature", "threshold_in_bin", "decision_type", "left_child", "right_child", "leaf_count",
+                  "internal_count", "leaf_depth"):
+            assert np.array_equal(np.asarray(a[k]), np.asarray(o[k])), (i, k)
+        for k in ("leaf_value", "leaf_weight", "internal_value", "internal_weight"):
+            assert within(a[k], o[k], leaf_section), (i, k, np.max(np.abs(a[k] - o[k])))
+    return len(gpu_trees), None

@@ -10,7 +10,7 @@ Tolerances:
 import numpy as np
 import pytest
 
-from conftest import binned_dataset
+from conftest import TOL, binned_dataset, compare_boosted_trees, within
 
 pytestmark = pytest.mark.gpu
 
@@ -39,20 +39,36 @@ def _binary_data(n, f=28, seed=0, nan_frac=0.0):
     return X, y
 
 
+# Gain ties the device resolves differently from the oracle, by (tree, node):
+# two candidates whose FP64 gains agree within the [split_gain] tie_rtol. A
+# divergence not listed here fails its test.
+DOCUMENTED_TIES = {"binary_30_rounds": set(), "lambdarank_8_rounds": set()}
+
+
 def _grads(orc, p, y, scores=None):
     if scores is None:
         scores = np.zeros(len(y))
     return orc.gradients(p, y, scores)
 
 
-def assert_same_tree(a, b, leaf_rtol=1e-9, gain_rtol=1e-6, check_inner=True):
+def assert_same_tree(a, b, leaf_rtol=None, gain_rtol=None, gains=None):
+    """Structure exact; leaf values within leaf_rtol (tests/tolerances.toml
+    [leaf_value] by default); the FP64 split gains within gain_rtol
+    ([split_gain]) of the oracle's trace `gains`, and the stored f32 gains
+    within one f32 ulp (an FP64 gain within 1e-10 can round either way)."""
+    leaf_rtol = TOL["leaf_value"]["rtol"] if leaf_rtol is None else leaf_rtol
+    gain_rtol = TOL["split_gain"]["rtol"] if gain_rtol is None else gain_rtol
     assert a["num_leaves"] == b["num_leaves"], (a["num_leaves"], b["num_leaves"])
     for k in ("split_feature", "threshold_in_bin", "decision_type", "left_child", "right_child", "leaf_count",
               "internal_count", "leaf_depth"):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
     for k in ("leaf_value", "leaf_weight", "internal_value", "internal_weight"):
-        np.testing.assert_allclose(a[k], b[k], rtol=leaf_rtol, atol=1e-12, err_msg=k)
-    np.testing.assert_allclose(a["split_gain"], b["split_gain"], rtol=gain_rtol, err_msg="split_gain")
+        np.testing.assert_allclose(a[k], b[k], rtol=leaf_rtol, atol=TOL["leaf_value"]["atol"], err_msg=k)
+    if gains is not None:
+        np.testing.assert_allclose(a["split_gain_f64"], gains, rtol=gain_rtol, atol=0.0, err_msg="split_gain_f64")
+    ulps = np.abs(np.asarray(a["split_gain"], np.float32).view(np.int32).astype(np.int64) -
+                  np.asarray(b["split_gain"], np.float32).view(np.int32).astype(np.int64))
+    assert ulps.max(initial=0) <= (0 if gain_rtol == 0.0 else 1), "split_gain (f32)"
 
 
 @pytest.mark.parametrize("form", ["f64", "f32c"])
@@ -127,12 +143,12 @@ def test_single_tree_f64(lgb, orc, num_leaves):
     X, y = _binary_data(20000, seed=10)
     params = {"objective": "binary", "num_leaves": num_leaves, "min_data_in_leaf": 20}
     gt, ot, learner, om, b = _tree_pair(lgb, orc, X, y, params)
-    assert_same_tree(gt, ot)
-    # leaf row sets are exact
+    assert_same_tree(gt, ot, gains=om.trace(0)[3])
+    # leaf row lists are exact, in the reference's (ascending) order
     beg, cnt, idx = learner.partition(0, gt["num_leaves"])
     obeg, ocnt, oidx = orc.partition(om, ot["num_leaves"], len(y))
     for leaf in range(gt["num_leaves"]):
-        a = np.sort(idx[beg[leaf]: beg[leaf] + cnt[leaf]])
+        a = idx[beg[leaf]: beg[leaf] + cnt[leaf]]
         o = oidx[obeg[leaf]: obeg[leaf] + ocnt[leaf]]
         assert np.array_equal(a, o), leaf
 
@@ -141,15 +157,15 @@ def test_single_tree_nan_missing_and_regularisation(lgb, orc):
     X, y = _binary_data(30000, seed=11, nan_frac=0.05)
     params = {"objective": "binary", "num_leaves": 63, "min_data_in_leaf": 10, "lambda_l1": 0.5,
               "lambda_l2": 2.0, "max_delta_step": 0.7, "min_gain_to_split": 0.01}
-    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
-    assert_same_tree(gt, ot)
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, y, params)
+    assert_same_tree(gt, ot, gains=om.trace(0)[3])
 
 
 def test_single_tree_path_smooth_and_depth(lgb, orc):
     X, y = _binary_data(20000, seed=12)
     params = {"objective": "binary", "num_leaves": 63, "max_depth": 5, "path_smooth": 3.0}
-    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
-    assert_same_tree(gt, ot)
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, y, params)
+    assert_same_tree(gt, ot, gains=om.trace(0)[3])
 
 
 def test_single_tree_categorical(lgb, orc):
@@ -164,9 +180,9 @@ def test_single_tree_categorical(lgb, orc):
     y = (X[:, 0] + eff[X[:, 4].astype(int)] + 0.5 * (X[:, 5] == 1) + 0.3 * rng.standard_normal(n) > 0)
     params = {"objective": "binary", "num_leaves": 31, "max_cat_to_onehot": 4, "min_data_per_group": 50,
               "cat_smooth": 5.0}
-    gt, ot, *_ = _tree_pair(lgb, orc, X, y.astype(np.float32), params, categorical=[4, 5])
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, y.astype(np.float32), params, categorical=[4, 5])
     assert gt["num_cat"] > 0
-    assert_same_tree(gt, ot)
+    assert_same_tree(gt, ot, gains=om.trace(0)[3])
     assert np.array_equal(gt["cat_boundaries"], ot["cat_boundaries"])
     assert np.array_equal(gt["cat_threshold"], ot["cat_threshold"])
 
@@ -177,8 +193,9 @@ def test_single_tree_bagging_and_feature_mask(lgb, orc):
     bag = np.sort(rng.choice(len(y), 18000, replace=False)).astype(np.uint32)
     mask = (rng.random(X.shape[1]) < 0.7).astype(np.uint8)
     params = {"objective": "regression", "num_leaves": 127}
-    gt, ot, *_ = _tree_pair(lgb, orc, X, rng.standard_normal(len(y)).astype(np.float32), params, bag=bag, mask=mask)
-    assert_same_tree(gt, ot)
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, rng.standard_normal(len(y)).astype(np.float32), params, bag=bag,
+                                  mask=mask)
+    assert_same_tree(gt, ot, gains=om.trace(0)[3])
     assert set(gt["split_feature"]) <= set(np.nonzero(mask)[0])
 
 
@@ -192,8 +209,8 @@ def test_single_tree_monotone(lgb, orc):
     g, h = orc.gradients(p, y, np.zeros(len(y)))
     learner = lgb.Learner(ds, params)
     gt = learner.train(g, h)[0]
-    ot = orc.train_trees(p, b, g, h, monotone=mono).trees[0]
-    assert_same_tree(gt, ot)
+    om = orc.train_trees(p, b, g, h, monotone=mono)
+    assert_same_tree(gt, om.trees[0], gains=om.trace(0)[3])
 
 
 @pytest.mark.parametrize("renew", [False, True])
@@ -202,10 +219,11 @@ def test_single_tree_quantized_exact(lgb, orc, renew):
     params = {"objective": "binary", "num_leaves": 127, "use_quantized_grad": True, "num_threads": 16,
               "quant_train_renew_leaf": renew}
     gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
+    gains = om.trace(0)[3]
     if renew:  # leaf outputs re-fit from FP64 gradient sums (summation order differs)
-        assert_same_tree(gt, ot, leaf_rtol=1e-12)
+        assert_same_tree(gt, ot, leaf_rtol=1e-12, gain_rtol=0.0, gains=gains)
     else:
-        assert_same_tree(gt, ot, leaf_rtol=0.0, gain_rtol=0.0)
+        assert_same_tree(gt, ot, leaf_rtol=0.0, gain_rtol=0.0, gains=gains)
 
 
 def test_multiclass_slots_in_lockstep(lgb, orc):
@@ -223,7 +241,7 @@ def test_multiclass_slots_in_lockstep(lgb, orc):
     gts = learner.train(g, h)
     om = orc.train_trees(p, b, g, h, num_trees=3)
     for k in range(3):
-        assert_same_tree(gts[k], om.trees[k])
+        assert_same_tree(gts[k], om.trees[k], gains=om.trace(k)[3])
 
 
 def test_gradients(lgb, orc):
@@ -245,6 +263,10 @@ def test_gradients(lgb, orc):
 
 
 def test_boosting_matches_oracle(lgb, orc):
+    """30 rounds: every tree as the oracle's (structure exact, gains and leaf
+    values within tests/tolerances.toml) unless the device meets a gain tie,
+    which must be a tie within [split_gain] tie_rtol; with no tie the held-out
+    scores and AUC agree within the [predictions] / [metrics] bars."""
     X, y = _binary_data(12000, seed=20)
     Xv, yv = _binary_data(3000, seed=21)
     params = {"objective": "binary", "num_leaves": 31, "learning_rate": 0.1, "min_data_in_leaf": 20}
@@ -254,20 +276,15 @@ def test_boosting_matches_oracle(lgb, orc):
     bst = lgb.train(params, ds, rounds, valid_sets=[dv])
     om = orc.train(lgb.resolve_params(params), ds.binned(), y, rounds, valid_binned=dv.binned())
     assert bst.num_trees() == len(om.trees)
-    same = 0
-    for a, o in zip(bst.trees, om.trees):
-        if not (np.array_equal(a["split_feature"], o["split_feature"])
-                and np.array_equal(a["threshold_in_bin"], o["threshold_in_bin"])):
-            break
-        np.testing.assert_allclose(a["leaf_value"], o["leaf_value"], rtol=1e-7, atol=1e-12)
-        same += 1
-    assert same >= 10, same
-    auc_g = orc.auc(yv, bst.scores(valid=True)[0])
-    auc_o = orc.auc(yv, om.scores(valid=True)[0])
-    assert abs(auc_g - auc_o) < 1e-4
+    same, tie = compare_boosted_trees(bst.trees, om)
+    assert tie is None or tie[:2] in DOCUMENTED_TIES["binary_30_rounds"], tie
+    if tie is None:
+        assert same == rounds
+        assert within(bst.scores(valid=True)[0], om.scores(valid=True)[0], "predictions")
+        assert within(orc.auc(yv, bst.scores(valid=True)[0]), orc.auc(yv, om.scores(valid=True)[0]), "metrics")
     # batched prediction of the GPU model on raw features equals its binned valid scores
     raw = bst.predict(Xv, raw_score=True)
-    np.testing.assert_allclose(raw, bst.scores(valid=True)[0], rtol=1e-12, atol=1e-12)
+    assert within(raw, bst.scores(valid=True)[0], "predictions")
 
 
 def test_predict_matches_oracle(lgb, orc):
@@ -297,6 +314,8 @@ def _ranking_data(nq, f=16, seed=0):
 
 
 def test_lambdarank_boosting_matches_oracle(lgb, orc):
+    """8 lambdarank rounds: trees as the oracle's up to a documented gain tie,
+    NDCG@1/3/5/10 of the scores within the [metrics] bar when no tie."""
     X, y, group = _ranking_data(400, seed=30)
     params = {"objective": "lambdarank", "num_leaves": 31, "min_data_in_leaf": 20, "learning_rate": 0.1}
     rounds = 8
@@ -304,15 +323,52 @@ def test_lambdarank_boosting_matches_oracle(lgb, orc):
     bst = lgb.train(params, ds, rounds)
     om = orc.train(lgb.resolve_params(params), ds.binned(), y, rounds, group=group)
     assert bst.num_trees() == len(om.trees)
-    same = 0
-    for a, o in zip(bst.trees, om.trees):
-        if not (np.array_equal(a["split_feature"], o["split_feature"])
-                and np.array_equal(a["threshold_in_bin"], o["threshold_in_bin"])):
-            break
-        np.testing.assert_allclose(a["leaf_value"], o["leaf_value"], rtol=1e-6, atol=1e-12)
-        same += 1
-    assert same >= 4, same
-    ks = [1, 3, 5, 10]
-    got = orc.ndcg(y, bst.scores()[0], group, ks)
-    want = orc.ndcg(y, om.scores()[0], group, ks)
-    np.testing.assert_allclose(got, want, atol=1e-3)
+    same, tie = compare_boosted_trees(bst.trees, om)
+    assert tie is None or tie[:2] in DOCUMENTED_TIES["lambdarank_8_rounds"], tie
+    if tie is None:
+        assert same == rounds
+        ks = [1, 3, 5, 10]
+        got = orc.ndcg(y, bst.scores()[0], group, ks)
+        want = orc.ndcg(y, om.scores()[0], group, ks)
+        assert within(got, want, "metrics"), (got, want)
+
+
+def _multiclass_categorical(n, seed):
+    """The multiclass K=10 workload's generator (180 N(0,1) + 20 categorical
+    features, Zipf s=1.2 over 50 categories), reduced to n rows."""
+    from lgbm_b200 import synthetic
+
+    d = synthetic.config3(scale=n / 2_000_000, seed=seed)
+    return d["X"], d["y"], d["categorical"]
+
+
+@pytest.mark.parametrize("renew", [False, True])
+def test_quantized_categorical_multiclass_matches_oracle(lgb, orc, renew, grow_mode):
+    """Config 3's form (quantized, K=10 trees per iteration, 20 Zipf
+    categorical features, max_cat_to_onehot 4) on 50k rows: three boosting
+    iterations. The integer histograms and the integer categorical scan
+    (split.rs:1190-1400) make every tree bit-exact with the oracle; with
+    FP64 leaf renewal the leaf values follow the leaf_value bar."""
+    from conftest import TOL
+
+    if grow_mode != "per_step":
+        pytest.skip("the booster runs the default launch strategy")
+    X, y, cats = _multiclass_categorical(50_000, seed=8)
+    params = {"objective": "multiclass", "num_class": 10, "num_leaves": 127, "max_cat_to_onehot": 4,
+              "use_quantized_grad": True, "num_grad_quant_bins": 4, "num_threads": 16, "seed": 11,
+              "quant_train_renew_leaf": renew}
+    ds = lgb.Dataset(X, y, params=params, categorical_feature=cats)
+    bst = lgb.train(params, ds, 3)
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, 3)
+    assert bst.num_trees() == len(om.trees) == 30
+    assert sum(t["num_cat"] for t in om.trees) > 0  # categorical splits are taken
+    for i, (a, o) in enumerate(zip(bst.trees, om.trees)):
+        for k in ("split_feature", "threshold_in_bin", "decision_type", "left_child", "right_child",
+                  "leaf_count", "cat_boundaries", "cat_threshold"):
+            assert np.array_equal(np.asarray(a[k]), np.asarray(o[k])), (i, k)
+        if renew:
+            tol = TOL["leaf_value"]
+            np.testing.assert_allclose(a["leaf_value"], o["leaf_value"], rtol=tol["rtol"], atol=tol["atol"])
+        else:
+            assert np.array_equal(a["leaf_value"], o["leaf_value"]), i
+            assert np.array_equal(a["split_gain"], o["split_gain"]), i

@@ -37,3 +37,50 @@ def test_predict_chunks_match_one_chunk_and_oracle(lgb, orc, monkeypatch, classe
     assert np.array_equal(whole, chunked)
     want = om.predict_raw(Xt)
     assert np.array_equal(np.asarray(chunked).reshape(want.shape), want)
+
+
+def test_predict_more_than_64_classes_matches_oracle(lgb, orc):
+    """num_tree_per_iteration above 64: every class sums its own trees in
+    model order (no fixed-size per-class array), bit-exact with the oracle."""
+    k = 70
+    rng = np.random.default_rng(33)
+    n = 7_000
+    X = rng.standard_normal((n, 6)).astype(np.float32)
+    y = rng.integers(0, k, n).astype(np.float32)
+    params = {"objective": "multiclass", "num_class": k, "num_leaves": 4, "min_data_in_leaf": 5}
+    ds = lgb.Dataset(X, y, params=params)
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, 2)
+    assert len(om.trees) == 2 * k
+    bst = lgb.Booster(params)
+    bst.trees = [dict(t, leaf_parent=np.zeros(t["num_leaves"], np.int32),
+                      cat_boundaries_inner=np.zeros(1, np.int32), cat_threshold_inner=np.zeros(0, np.uint32))
+                 for t in om.trees]
+    Xt = rng.standard_normal((3_000, 6)).astype(np.float32)
+    got = bst.predict(Xt, raw_score=True)
+    want = om.predict_raw(Xt)
+    assert got.shape == want.shape == (3_000, k)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("ncol", [3, 136, 300])
+def test_predict_row_staging_widths(lgb, orc, ncol):
+    """Rows staged in shared memory (up to 223 features, vector loads when
+    the row width is a multiple of 4) and read in place above that: all
+    bit-exact with the oracle."""
+    rng = np.random.default_rng(34 + ncol)
+    n = 4_000
+    X = rng.standard_normal((n, ncol)).astype(np.float32)
+    X[rng.random(X.shape) < 0.05] = np.nan
+    X[rng.random(X.shape) < 0.05] = 0.0
+    X[rng.random(X.shape) < 0.01] = 1e-38  # below the zero threshold: read as 0
+    z = np.nan_to_num(X[:, 0]) + np.nan_to_num(X[:, ncol - 1]) * np.nan_to_num(X[:, ncol // 2])
+    y = (z + 0.3 * rng.standard_normal(n) > 0).astype(np.float32)
+    params = {"objective": "binary", "num_leaves": 15, "min_data_in_leaf": 10}
+    ds = lgb.Dataset(X, y, params=params)
+    om = orc.train(lgb.resolve_params(params), ds.binned(), y, 6)
+    bst = lgb.Booster(params)
+    bst.trees = [dict(t, leaf_parent=np.zeros(t["num_leaves"], np.int32),
+                      cat_boundaries_inner=np.zeros(1, np.int32), cat_threshold_inner=np.zeros(0, np.uint32))
+                 for t in om.trees]
+    Xt = X[:1_537]  # a partial last CTA of rows
+    assert np.array_equal(bst.predict(Xt, raw_score=True), om.predict_raw(Xt)[:, 0])

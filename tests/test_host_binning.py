@@ -94,3 +94,44 @@ def test_bundleable_features_rejected(lgb):
     X[100:200, 1] = 2.0
     with pytest.raises(lgb.LightGBMError):
         binned_dataset(lgb, X, np.zeros(2000, np.float32), {"min_data_in_leaf": 1})
+
+
+@pytest.mark.parametrize("cfg,scale", [("config0", 1.0), ("config1", 0.02), ("config2", 0.003), ("config3", 0.005),
+                                       ("config4", 0.003)])
+def test_product_binning_equals_the_oracle_restatement(lgb, orc, cfg, scale):
+    """The product's host binning (host_dataset.cpp) and the oracle's own
+    restatement of binning.rs / dataset.rs (oracle/binning.cpp) give the same
+    bin matrix, bin mappers and thresholds on each workload's generator, and
+    the same for the held-out rows binned with the training mappers."""
+    from lgbm_b200 import synthetic as syn
+
+    d = getattr(syn, cfg)(scale=scale)
+    params = d["params"]
+    cats = d.get("categorical")
+    p = lgb.resolve_params(params)
+    ds = lgb.Dataset(d["X"], d["y"], params=params, categorical_feature=cats)
+    od = orc.Dataset(d["X"], p, categorical=cats)
+    b, ob = ds.binned(), od.binned()
+    assert set(b) == set(ob)
+    for k in b:
+        assert np.array_equal(np.asarray(b[k]), np.asarray(ob[k]), equal_nan=True), k
+    if "X_valid" in d:
+        dv = lgb.Dataset(d["X_valid"], d["y_valid"], params=params, reference=ds)
+        odv = orc.Dataset(d["X_valid"], p, reference=od)
+        assert np.array_equal(dv.binned()["bins"], odv.binned()["bins"])
+
+
+def test_oracle_feature_infos_format(orc, lgb):
+    """Dataset::feature_infos (dataset.rs:770): [min:max] with %.17g for a
+    numerical feature, the categories of each bin joined by ':' for a
+    categorical one, none for a feature left out as trivial."""
+    rng = np.random.default_rng(5)
+    n = 5000
+    X = np.stack([rng.standard_normal(n), np.full(n, 3.0), rng.integers(0, 4, n)], axis=1).astype(np.float32)
+    p = lgb.resolve_params({})
+    od = orc.Dataset(X, p, categorical=[2])
+    info = od.feature_infos
+    assert info[0] == "[%.17g:%.17g]" % (float(X[:, 0].min()), float(X[:, 0].max()))
+    assert info[1] == "none"
+    cats = info[2].split(":")
+    assert cats[0] == "-1" and sorted(cats[1:]) == ["0", "1", "2", "3"]

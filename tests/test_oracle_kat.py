@@ -6,7 +6,11 @@ import math
 import numpy as np
 import pytest
 
-from conftest import binned_dataset
+
+
+def _oracle_binned(orc, lgb, x, params):
+    """The oracle's own binning of x (binning.rs restated in oracle/binning.cpp)."""
+    return orc.Dataset(x, lgb.resolve_params(params)).binned()
 
 
 def _feature(orc, num_bin, missing_type, default_bin, mfb, bin_type, offset, penalty=1.0):
@@ -157,8 +161,7 @@ def test_first_split_separates_step(lgb, orc):  # learner/tests.rs:24-43
     n = 200
     x, y = _step_data(n)
     params = {"num_leaves": 2, "min_data_in_leaf": 5}
-    ds = binned_dataset(lgb, x.astype(np.float32), y, params)
-    b = ds.binned()
+    b = _oracle_binned(orc, lgb, x.astype(np.float32), params)
     grad = -y
     hess = np.ones(n, np.float32)
     t = orc_tree(lgb, orc, b, params, grad, hess)
@@ -173,7 +176,7 @@ def test_max_depth_and_min_data(lgb, orc):  # learner/tests.rs:64-78
     n = 300
     x, y = _step_data(n)
     params = {"num_leaves": 31, "max_depth": 2, "min_data_in_leaf": 40}
-    b = binned_dataset(lgb, x.astype(np.float32), y, params).binned()
+    b = _oracle_binned(orc, lgb, x.astype(np.float32), params)
     grad = np.sin(np.arange(n, dtype=np.float32) * np.float32(0.37)).astype(np.float32)
     t = orc_tree(lgb, orc, b, params, grad, np.ones(n, np.float32))
     assert t["num_leaves"] <= 4
@@ -184,7 +187,7 @@ def test_max_depth_and_min_data(lgb, orc):  # learner/tests.rs:64-78
 def test_constant_gradient_single_leaf(lgb, orc):  # learner/tests.rs:80-89
     n = 100
     x, y = _step_data(n)
-    b = binned_dataset(lgb, x.astype(np.float32), y, {}).binned()
+    b = _oracle_binned(orc, lgb, x.astype(np.float32), {})
     t = orc_tree(lgb, orc, b, {}, np.full(n, 0.5, np.float32), np.ones(n, np.float32))
     assert t["num_leaves"] == 1
 
@@ -192,3 +195,71 @@ def test_constant_gradient_single_leaf(lgb, orc):  # learner/tests.rs:80-89
 def orc_tree(lgb, orc, b, params, grad, hess):
     """One tree of the oracle learner on given gradients (a custom-objective iteration)."""
     return orc.train_trees(lgb.resolve_params(params), b, grad, hess).trees[0]
+
+
+def test_fix_recovers_most_frequent_bin(orc):  # histogram.rs:91-97
+    # bins 0,1,1,2 with gradients 1,2,3,4 and mfb = 1: bin 1 is not stored
+    hist = np.array([1.0, 1.0, 0.0, 0.0, 4.0, 1.0])
+    assert orc.lib().oracle_fix_hist(3, 0, 1, 10.0, 4.0, hist.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert list(hist) == [1.0, 1.0, 5.0, 2.0, 4.0, 1.0]
+
+
+def test_offset_one_leaves_the_histogram_alone(orc):  # histogram.rs:99-106
+    hist = np.array([2.0, 1.0, 3.0, 1.0])  # 2 * (num_bin - offset) values
+    assert orc.lib().oracle_fix_hist(3, 1, 0, 7.0, 3.0, hist.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert list(hist) == [2.0, 1.0, 3.0, 1.0]
+
+
+def test_tie_break_prefers_smaller_feature(orc):  # split.rs:1476-1484
+    L = orc.lib()
+    assert L.oracle_better_than(1.0, 1, 1.0, 3) == 1  # b (feature 1) beats a (feature 3) at equal gain
+    assert L.oracle_better_than(1.0, 3, 1.0, 1) == 0
+    assert L.oracle_better_than(1.0, 3, -math.inf, -1) == 1  # any split beats the default (none)
+
+
+def test_partition_is_stable(lgb, orc):  # learner/tests.rs:45-63
+    n = 100
+    x, y = _step_data(n)
+    params = {"num_leaves": 4, "min_data_in_leaf": 3}
+    b = _oracle_binned(orc, lgb, x.astype(np.float32), params)
+    grad = np.array([((i * 7919) % 13) - 6.0 for i in range(n)], np.float32)
+    m = orc.train_trees(lgb.resolve_params(params), b, grad, np.ones(n, np.float32))
+    t = m.trees[0]
+    beg, cnt, idx = orc.partition(m, t["num_leaves"], n)
+    seen = 0
+    for leaf in range(t["num_leaves"]):
+        rows = idx[beg[leaf]: beg[leaf] + cnt[leaf]].astype(np.int64)
+        assert np.all(np.diff(rows) > 0), f"leaf {leaf} indices not increasing"
+        seen += len(rows)
+    assert seen == n
+
+
+def bin_rs_histogram_case():
+    """bin.rs:762-788: 300 rows, stored value 1 + i % 3 on every 7th row and
+    0 (the most frequent bin, not stored) elsewhere; gradients and hessians
+    i * 0.5; the rows with i % 3 != 1. Returns (binned, g, rows, want): a
+    one-feature binned dataset holding those stored values (num_bin 4, most
+    frequent bin 0) and the (g, h) sums of stored values 1..3."""
+    n = 300
+    vals = np.array([(1 + i % 3) if i % 7 == 0 else 0 for i in range(n)], np.uint8)
+    g = (np.arange(n, dtype=np.float32) * np.float32(0.5)).astype(np.float32)
+    rows = np.array([i for i in range(n) if i % 3 != 1], np.uint32)
+    want = np.zeros(8)
+    for i in rows:
+        v = int(vals[i])
+        if v != 0:
+            want[2 * v] += float(g[i])
+            want[2 * v + 1] += float(g[i])
+    b = {"num_data": n, "num_features": 1, "num_total_features": 1, "bins": vals.reshape(n, 1),
+         "num_bin": np.array([4], np.int32), "missing_type": np.array([0], np.int32),
+         "default_bin": np.array([0], np.int32), "most_freq_bin": np.array([0], np.int32),
+         "bin_type": np.array([0], np.int32), "real_index": np.array([0], np.int32),
+         "upper_bounds": np.array([1e-35, 1.5, 2.5, np.inf]), "ub_offsets": np.array([0, 4], np.int64),
+         "bin_to_cat": np.zeros(0, np.int32), "cat_offsets": np.array([0, 0], np.int64)}
+    return b, g, rows, want[2:]
+
+
+def test_bin_histogram_matches_dense_reference(orc):  # bin.rs:762-788 (the histogram part)
+    b, g, rows, want = bin_rs_histogram_case()
+    got = orc.hist(b, rows, g, g)
+    assert list(got) == list(want)

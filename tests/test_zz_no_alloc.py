@@ -2,6 +2,7 @@
 device array) against lgbm_b200_predict with host buffers, both through the C
 ABI. Collected last so it also runs after every other test in one process."""
 import ctypes as C
+import gc
 
 import numpy as np
 import pytest
@@ -70,3 +71,42 @@ def test_noalloc_rejects_rows_above_the_staging_size(lgb):
     # the entry point still works afterwards
     want, got = _both(lgb, bst, _rows(100, 4, 7))
     assert np.array_equal(got[0], want)
+
+
+def test_noalloc_allocates_nothing_and_keeps_the_current_device(lgb):
+    """The point of the entry point: a call on a forest the array has not
+    served yet leaves the device's free memory unchanged, and the calling
+    thread's current device is the same after the call. Two different
+    forests use the shared array one after the other."""
+    import torch
+
+    X = _rows(6000, 8, 11)
+    y = (np.nan_to_num(X[:, 0]) - np.nan_to_num(X[:, 2]) > 0).astype(np.float32)
+    a = lgb.train({"objective": "binary", "num_leaves": 15}, lgb.Dataset(X, y), num_boost_round=6)
+    b = lgb.train({"objective": "binary", "num_leaves": 31, "learning_rate": 0.3}, lgb.Dataset(X, y),
+                  num_boost_round=9)
+    L = lgb._lib
+    Xt = _rows(20000, 8, 12)
+    out = np.zeros(20000, np.float64)
+    # warm-up with forest a: loads the kernel and resolves the array's address
+    L.check(L.lib().lgbm_b200_predict_noalloc(a._forest_handle(), Xt.ctypes.data, 20000, 8, out.ctypes.data))
+    hb = b._forest_handle()  # forest b's own arrays are allocated here, before the measurement
+    torch.cuda.synchronize()
+    before_dev = torch.cuda.current_device()
+    gc.collect()  # no unrelated object may free device memory inside the window
+    gc.disable()
+    try:
+        free0, _ = torch.cuda.mem_get_info()
+        rc = L.lib().lgbm_b200_predict_noalloc(hb, Xt.ctypes.data, 20000, 8, out.ctypes.data)
+        free1, _ = torch.cuda.mem_get_info()
+    finally:
+        gc.enable()
+    L.check(rc)
+    assert free1 == free0
+    assert torch.cuda.current_device() == before_dev
+    want_b, got_b = _both(lgb, b, Xt)
+    assert np.array_equal(out, want_b)
+    for g in got_b:
+        assert np.array_equal(g, want_b)
+    want_a, got_a = _both(lgb, a, Xt)  # back to forest a after b used the array
+    assert np.array_equal(got_a[1], want_a)
