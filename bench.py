@@ -138,6 +138,40 @@ def hist_bytes_per_row(nf, form):
     return nf * 1 + (4 if form == "quantized" else 8) + 4
 
 
+def hist_rows_by_step(t):
+    """Rows each split step's histogram launch reads: step 0 the root (every
+    row of the tree), step s the smaller child of split s - 1 (the split
+    order is the node order)."""
+    def count(c):
+        return int(t["internal_count"][c]) if c >= 0 else int(t["leaf_count"][~c])
+
+    nl = int(t["num_leaves"])
+    if nl < 2:
+        return []
+    out = [int(np.sum(t["leaf_count"]))]
+    for k in range(nl - 2):
+        out.append(min(count(int(t["left_child"][k])), count(int(t["right_child"][k]))))
+    return out
+
+
+def hist_by_rows(step_rows, step_ms, bytes_per_row):
+    """Histogram launches binned by the rows they read: launches, mean us per
+    launch, and GB/s of algorithmic bytes (rows x bytes per row) per bin."""
+    edges = [0, 1_000, 10_000, 100_000, 1_000_000, 10**12]
+    out = []
+    r = np.asarray(step_rows, np.float64)
+    ms = np.asarray(step_ms, np.float64)
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        sel = (r >= lo) & (r < hi)
+        if not np.any(sel):
+            continue
+        t = float(ms[sel].sum()) / 1000.0
+        out.append({"rows_from": lo, "rows_to": hi if hi < 10**12 else None, "launches": int(sel.sum()),
+                    "us_per_launch": 1e6 * t / int(sel.sum()),
+                    "gbs": float(r[sel].sum()) * bytes_per_row / t / 1e9 if t > 0 else None})
+    return out
+
+
 def _shape_key(args, form):
     """Key of a workload's tuned launch shape: workload, scale, histogram form."""
     return f"{args.workload}{'' if args.scale == 1.0 else '@' + format(args.scale, 'g')}/{form}"
@@ -203,6 +237,7 @@ def run_form(lgb, data, ds, dv, form, args, device):
     rows = prows = 0
     launches = 0
     fused = False
+    step_rows, step_hist_ms = [], []
     for _ in range(args.steps):
         bst.update()
         t, r, nl = L.last_timing()
@@ -213,6 +248,11 @@ def run_form(lgb, data, ds, dv, form, args, device):
         rows += r
         prows += pr
         launches = nl
+        if not fused:
+            st = L.step_times()
+            rr = hist_rows_by_step(bst.trees[-1])
+            step_rows.extend(rr)
+            step_hist_ms.extend(st[: len(rr), 0])
     L.set_timing(False)
     done = args.warmup + extra + 2 * args.steps
     for _ in range(max(0, args.rounds - done)):
@@ -247,6 +287,7 @@ def run_form(lgb, data, ds, dv, form, args, device):
         "part_ms_per_launch": part_ms / (args.steps * steps_per_tree),
         "hist_ms_per_step": hist_ms / args.steps, "kernel_launches_per_tree": launches, "clocks": clk,
         "num_trees": bst.num_trees(), "nf": nf, "launch_shape": shape, "launch_shape_source": shape_src,
+        "hist_by_rows": hist_by_rows(step_rows, step_hist_ms, hist_bytes_per_row(nf, form)),
     }
 
 
@@ -782,7 +823,8 @@ def main():
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
                       "hist_rows_per_tree": v["hist_rows_per_tree"], "fused": v["fused"], "part_gbs": v["part_gbs"],
                       "part_rows_per_tree": v["part_rows_per_tree"], "launch_shape": v["launch_shape"],
-                      "launch_shape_source": v["launch_shape_source"]} for k, v in res.items()},
+                      "launch_shape_source": v["launch_shape_source"], "hist_by_rows": v["hist_by_rows"]}
+                  for k, v in res.items()},
         "roofline": ({"bound": "hbm", "kernel": "k_partition_fused (row partition + both children's histograms)",
                       "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s", "frac": r["part_gbs"] / peak,
                       "peak_kind": peak_kind, "traffic": None,
@@ -806,6 +848,9 @@ def main():
         "clocks": r["clocks"],
     }
     if not r["fused"]:
+        # the histogram's achieved fraction of the HBM roofline by leaf size
+        line["roofline"]["by_rows"] = [dict(b, frac=(b["gbs"] / peak if b["gbs"] else None))
+                                       for b in r["hist_by_rows"]]
         # the row partition, the largest share of device time (its launches are
         # latency-bound: most leaves are small)
         line["roofline_partition"] = {

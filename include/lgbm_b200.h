@@ -296,6 +296,12 @@ int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_
  * partitioned (in the fused quantized form, where *fused is 1, the partition
  * also builds both children's histograms from the rows it moves). For the
  * bench's bandwidth figures; no counterpart in the reference. */
+/* With timing on (lgbm_b200_learner_set_timing), the device time of the
+ * histogram, scan and partition launches of every split step of the last
+ * train call: ms[3 * step + {0, 1, 2}] for step < min(*steps, capacity).
+ * Histogram step s builds the smaller child of split s - 1 (step 0: the
+ * root). A diagnostic with no counterpart in the reference. */
+int lgbm_b200_learner_step_times(LgbmB200Learner* h, float* ms, int32_t capacity, int32_t* steps);
 int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows, int32_t* fused);
 
 /* Diagnostics for the parity tests. lgbm_b200_learner_histogram runs the

@@ -635,6 +635,7 @@ Status train_collect(LgbmB200Learner* h) {
     // phase times seen by the first CTA: histogram, scan, partition, bookkeeping
     for (int i = 0; i < 4; ++i) h->last_ms[i] = (double)ph[i] / 1e6;
   } else if (h->timing) {  // per-kernel-family device time of this tree
+    h->last_step_ms.assign((size_t)3 * (h->L - 1), 0.0f);
     for (int step = 0; step < h->L - 1; ++step) {
       cudaEvent_t* ev = &h->ev[(size_t)4 * step];
       float a, b, d;
@@ -644,6 +645,9 @@ Status train_collect(LgbmB200Learner* h) {
       h->last_ms[0] += a;
       h->last_ms[1] += b;
       h->last_ms[2] += d;
+      h->last_step_ms[(size_t)3 * step] = a;
+      h->last_step_ms[(size_t)3 * step + 1] = b;
+      h->last_step_ms[(size_t)3 * step + 2] = d;
     }
   }
   h->last_hist_rows = 0;
@@ -1036,6 +1040,15 @@ int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_
     for (int i = 0; i < 4; ++i) ms[i] = h->last_ms[i];
   if (hist_rows) *hist_rows = h->last_hist_rows;
   if (launches) *launches = h->last_launches;
+  return LGBM_B200_OK;
+}
+
+int lgbm_b200_learner_step_times(LgbmB200Learner* h, float* ms, int32_t capacity, int32_t* steps) {
+  if (!h || !steps) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  const int32_t n = (int32_t)(h->last_step_ms.size() / 3);
+  *steps = n;
+  if (ms)
+    for (int32_t i = 0; i < std::min(n, capacity) * 3; ++i) ms[i] = h->last_step_ms[(size_t)i];
   return LGBM_B200_OK;
 }
 

@@ -279,6 +279,7 @@ struct LgbmB200Learner {
   std::vector<cudaEvent_t> ev;
   cudaEvent_t marks[16] = {};  // caller-placed timing marks on the learner's stream
   double last_ms[4] = {0, 0, 0, 0};
+  std::vector<float> last_step_ms;  // timing on: (histogram, scan, partition) ms of every split step
   int64_t last_hist_rows = 0;
   int64_t last_part_rows = 0;
   bool fused = false;  // partition builds both children's histograms

@@ -126,6 +126,7 @@ SIGNATURES = {
     "lgbm_b200_learner_set_timing": (C.c_int, [C.c_void_p, i32]),
     "lgbm_b200_learner_last_timing": (C.c_int, [C.c_void_p, P(f64), P(i64), P(i32)]),
     "lgbm_b200_learner_last_rows": (C.c_int, [C.c_void_p, P(i64), P(i64), P(i32)]),
+    "lgbm_b200_learner_step_times": (C.c_int, [C.c_void_p, P(C.c_float), i32, P(i32)]),
     "lgbm_b200_learner_record": (C.c_int, [C.c_void_p, i32]),
     "lgbm_b200_learner_elapsed": (C.c_int, [C.c_void_p, i32, i32, P(f64)]),
     "lgbm_b200_learner_histogram": (C.c_int, [C.c_void_p, i32, P(C.c_uint32), i64, C.c_void_p]),

@@ -343,6 +343,15 @@ class Learner:
         L.check(L.lib().lgbm_b200_learner_last_timing(self.handle, ms, C.byref(rows), C.byref(launches)))
         return list(ms), int(rows.value), int(launches.value)
 
+    def step_times(self):
+        """With timing on: (steps x 3) device ms of each split step's
+        histogram, scan and partition launches in the last train call."""
+        n = C.c_int32()
+        L.check(L.lib().lgbm_b200_learner_step_times(self.handle, None, 0, C.byref(n)))
+        ms = np.zeros(3 * n.value, np.float32)
+        L.check(L.lib().lgbm_b200_learner_step_times(self.handle, _ptr(ms, C.c_float), n.value, C.byref(n)))
+        return ms.reshape(-1, 3)
+
     def last_rows(self):
         """(rows histogrammed, rows partitioned, fused) of the last train call."""
         h, pr, f = C.c_int64(), C.c_int64(), C.c_int32()
