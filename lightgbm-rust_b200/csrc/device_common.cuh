@@ -128,7 +128,6 @@ struct DSlot {
   const float2* gh;        // this slot's interleaved (gradient, hessian) [num_data]
   int32_t* packed;         // quantized gradients per row: (g << 16) + h
   uint8_t* bytree;         // by-tree feature mask [num_features]
-  long long* pair_hist;    // fused form: [2 pairs][2 children][total_bins] packed sums
   double* root_partials;   // [2 x kRootBlocks] (g, h) partial sums
   long long* root_ipartials;
   int32_t* root_counter;
@@ -152,7 +151,7 @@ struct DCtx {
   DSlot slots[kMaxSlots];  // by value: read from the constant bank
   int32_t num_slots;
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
-  int32_t fused;           // 1: the partition also builds both children's histograms (quantized, <= 32 features)
+  int32_t fused;           // 1: the partition also builds one child's histogram (quantized, <= 32 features)
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

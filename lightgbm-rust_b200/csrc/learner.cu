@@ -132,10 +132,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   h->part_grid = h->num_sms * 3;  // 3 CTAs per SM measured best with 1024-row tiles (2 and 2.5 per SM are slower)
   // LGBM_B200_FUSED=1: the quantized form with at most 32 features builds
-  // both children's histograms inside the partition. Off by default: on the
-  // 10M-row binary workload it measured slower (the first, largest splits
-  // move every row of the parent through one CTA per SM, where the separate
-  // histogram kernel reads only the smaller child's rows).
+  // the estimated smaller child's histogram inside the partition, and no
+  // histogram launch follows a split.
   h->fused = false;
   if (const char* e = std::getenv("LGBM_B200_FUSED"))
     h->fused = std::atoi(e) != 0 && mode == LGBM_B200_HIST_QUANT && nf <= 32 && !cfg->persistent_grow;
@@ -238,7 +236,6 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     d.gh = nullptr;  // set below from the contiguous [K x n] buffer
     if (mode == LGBM_B200_HIST_QUANT) ALLOC(d.packed, n);
     ALLOC(d.bytree, nf);
-    if (h->fused) ALLOC(d.pair_hist, 4 * (size_t)h->total_bins);
     ALLOC(d.root_partials, 2 * kRootBlocks);
     ALLOC(d.root_ipartials, kRootBlocks);
     ALLOC(d.root_counter, 1);

@@ -282,7 +282,7 @@ struct LgbmB200Learner {
   std::vector<float> last_step_ms;  // timing on: (histogram, scan, partition) ms of every split step
   int64_t last_hist_rows = 0;
   int64_t last_part_rows = 0;
-  bool fused = false;  // partition builds both children's histograms
+  bool fused = false;  // the partition also builds the estimated smaller child's histogram
   int fused_grid = 0;
   bool scan_wide = false;  // the register-capped scan variant (many CTAs per step)
   bool scan_part = false;  // scans and partition of a step in one cooperative launch

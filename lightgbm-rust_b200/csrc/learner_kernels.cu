@@ -70,10 +70,9 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   // positions -> rows (identity, or the in-bag rows)
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + tid; i < n; i += (int64_t)gridDim.x * blockDim.x)
     s.idx[0][i] = bag ? bag[i] : (uint32_t)i;
-  // zero the root's histogram buffer (pool buffer 0; fused form: pair 1, child 0)
+  // zero the root's histogram buffer (pool buffer 0)
   size_t cells = (size_t)c.total_bins * (c.hist_mode == LGBM_B200_HIST_QUANT ? 1 : 2);
-  double* h0 = c.fused ? reinterpret_cast<double*>(s.pair_hist + 2 * (size_t)c.total_bins)
-                       : reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
+  double* h0 = reinterpret_cast<double*>(s.hist);  // cells are 8 bytes in every form
   for (size_t i = (size_t)blockIdx.x * blockDim.x + tid; i < cells; i += (size_t)gridDim.x * blockDim.x) h0[i] = 0.0;
 
   // deterministic partial sums over this block's contiguous chunk (a
@@ -339,10 +338,7 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   const uint32_t* idx = lr.idx + lr.begin;
   const size_t stride = (size_t)c.stride;
   double* outf = reinterpret_cast<double*>(s.hist) + (size_t)lr.buf * c.total_bins * 2;
-  // fused form: only the root is histogrammed here, into pair 1, child 0
-  unsigned long long* outi = c.fused ? reinterpret_cast<unsigned long long*>(s.pair_hist + 2 * (size_t)c.total_bins)
-                                     : reinterpret_cast<unsigned long long*>(s.hist) +
-                                           (size_t)lr.buf * c.total_bins;
+  unsigned long long* outi = reinterpret_cast<unsigned long long*>(s.hist) + (size_t)lr.buf * c.total_bins;
   // Adds cell i (over groups) of the CTAs `src` to the leaf histogram; cells
   // outside the features' views are skipped.
   auto emit = [&](int i, auto read_cell) {
@@ -1315,60 +1311,6 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
   const DFeature m = c.feats[f];
   const DParams& p = c.p;
   const int32_t nf = c.num_features;
-  if (kInt && c.fused) {
-    if (st->done) return;
-    const bool have_larger = st->larger.leaf >= 0;
-    const bool need = st->need_find != 0;
-    const int32_t L = st->left_leaf;
-    const bool used = need && s.bytree[f] && (!have_larger || s.splittable[L * nf + f]);
-    if (!(used && (side == 0 || have_larger))) return;
-    // both leaves' histograms were built directly by the previous partition
-    // (the root's by the histogram kernel): each view is fixed from its own
-    // leaf's sum (histogram.rs:42-56); no subtraction
-    const DLeafSplits ls = side == 0 ? st->smaller : st->larger;
-    const int len = m.view_len;
-    const int k = st->num_leaves_cur - 1;
-    const int child = ls.leaf == st->left_leaf ? 0 : 1;
-    const long long* hs = s.pair_hist + ((size_t)(((k - 1) & 1) * 2 + child)) * c.total_bins + m.view_start;
-    if (tid < len) sm.ig[tid] = (int64_t)__ldcg(hs + tid);
-    __syncthreads();
-    if (m.most_freq_bin > 0 && warp == 0) {
-      int64_t part = 0;
-      for (int i = lane; i < m.num_bin; i += 32)
-        if (i != m.most_freq_bin) part = (int64_t)((uint64_t)part + (uint64_t)sm.ig[i]);
-      for (int o = 16; o > 0; o >>= 1)
-        part = (int64_t)((uint64_t)part + (uint64_t)__shfl_xor_sync(0xffffffffu, part, o));
-      __syncwarp();
-      if (lane == 0) sm.ig[m.most_freq_bin] = (int64_t)((uint64_t)ls.int_sum - (uint64_t)part);
-    }
-    __syncthreads();
-    LeafCtx lc;
-    lc.sum_g = ls.sum_gradients;
-    lc.sum_h = ls.sum_hessians;
-    lc.int_sum = ls.int_sum;
-    lc.gs = st->grad_scale;
-    lc.hs = st->hess_scale;
-    lc.num_data = ls.num_data;
-    lc.parent_output = st->num_leaves_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data)
-                                                : ls.weight;
-    lc.mc = p.use_monotone != 0;
-    lc.cmin = s.cmin[ls.leaf];
-    lc.cmax = s.cmax[ls.leaf];
-    DSplit& out = sm.out;
-    bool ok = find_best_threshold_block<kInt>(sm, m, p, lc, out);
-    if (tid == 0) {
-      out.feature = m.real_index;
-      out.inner = f;
-      s.feat_ok[side * nf + f] = ok ? 1 : 0;
-    }
-    __syncthreads();
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
-    for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
-    // the partition's goes-left table for this candidate, ready if it wins
-    if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins);
-    return;
-  }
   // The loads run in two waves so that their latencies overlap: the slot
   // state, then everything that depends on it (the feature's flags, both
   // histogram views, the leaf's output bounds).
@@ -1526,10 +1468,11 @@ __global__ void __launch_bounds__(kScanThreads, kMinBlocks) k_scan(const __grid_
     st->part_ticket = 0;
     st->part_done = 0;
   }
-  if (kInt && c.fused && !st->done) {  // the pair this step's partition fills (read by the scan before last)
-    const int k = st->num_leaves_cur - 1;
-    long long* z = s.pair_hist + (size_t)(k & 1) * 2 * c.total_bins;
-    const size_t n = 2 * (size_t)c.total_bins;
+  if (kInt && c.fused && !st->done) {
+    // the pool buffer this step's partition builds its child's histogram in
+    // (the next new leaf's, num_leaves_cur: no leaf holds it yet)
+    long long* z = reinterpret_cast<long long*>(s.hist) + (size_t)st->num_leaves_cur * c.total_bins;
+    const size_t n = (size_t)c.total_bins;
     const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x, ctas = (size_t)gridDim.x * gridDim.y;
     for (size_t i = cta * blockDim.x + threadIdx.x; i < n; i += ctas * blockDim.x) z[i] = 0;
   }
@@ -1575,8 +1518,14 @@ __device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L,
   return f;
 }
 
+// built_left: -1 when the next histogram launch builds the smaller child
+// (chosen by the actual counts, learner/mod.rs:1200-1208); 0 / 1 when this
+// step's partition has already built the right / left child's histogram in
+// buffer R. That child then takes the "smaller" role (its histogram is built,
+// the other one's is parent - built). For integer histograms the two roles
+// give the same sums, so only which buffer holds which leaf changes.
 __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left,
-                                   const FinalizeIn& fin) {
+                                   const FinalizeIn& fin, int built_left = -1) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
   const int32_t begin = fin.begin, cnt = fin.cnt, side = fin.side, buf_L = fin.buf_L, depth = fin.depth;
@@ -1597,8 +1546,9 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int
   ls.num_data = nl;
   rs.num_data = nr;
   int32_t new_status = status;
-  const bool left_smaller = nl < nr;
-  if ((left_smaller ? nl : nr) <= 0 && status == kStatusOk) new_status = kStatusEmptyChild;
+  const bool left_smaller = built_left < 0 ? nl < nr : built_left != 0;
+  if (min(nl, nr) <= 0 && status == kStatusOk) new_status = kStatusEmptyChild;
+  if (built_left >= 0) st->hist_rows += left_smaller ? nl : nr;
   st->smaller = left_smaller ? ls : rs;
   st->larger = left_smaller ? rs : ls;
   if (new_status != kStatusOk) {
@@ -1784,7 +1734,7 @@ __device__ void decide_split(const DCtx& c, const DSlot& s, const StepHead& h, S
 // choice and before_find_best_split are recorded. Every other CTA of the
 // launch has exited, so none of them reads the state changed here.
 __device__ void finish_step(const DCtx& c, const DSlot& s, const StepHead& h, const SplitDecision& d, int32_t bl,
-                            int32_t R, int32_t cnt) {
+                            int32_t R, int32_t cnt, int built_left = -1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   DSlotState* st = s.st;
   const int32_t nf = c.num_features;
@@ -1852,7 +1802,7 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const StepHead& h, co
   if (tid == 0) {
     apply_split(c, s, bl, R, ain);
   } else if (tid == 32) {
-    partition_finalize(c, s, bl, R, total_left, fin);
+    partition_finalize(c, s, bl, R, total_left, fin, built_left);
     st->part_epoch += 1;
     // every CTA of the launch has passed its last use of the step counters
     st->part_ticket = 0;
@@ -1874,6 +1824,7 @@ struct PartShared {
 // The leaf a step splits: its rows and the feature its split tests.
 struct SplitLeaf {
   int32_t L, begin, cnt, side, inner;
+  bool est_left_smaller;  // the scan's estimated counts (split.rs:229-231): left < right
 };
 
 // Step prologue of a partition CTA: the split decision and, when a leaf is
@@ -1895,6 +1846,7 @@ __device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const Ste
   sl.cnt = s.leaf_count[L];
   sl.side = s.leaf_side[L];
   sl.inner = info.inner;
+  sl.est_left_smaller = info.left_count < info.right_count;
   if (threadIdx.x < kMaxBins / 16)
     reinterpret_cast<uint4*>(ps.lut)[threadIdx.x] = reinterpret_cast<const uint4*>(lut)[threadIdx.x];
   return sl;
@@ -1904,10 +1856,12 @@ __device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const Ste
 // the per-thread left counts, the decoupled look-back for the tile's prefix,
 // then the scatter (left rows ascending from the range start, right rows
 // descending from its end). The CTA of the last tile posts the left count.
+// excl_out / tile_left_out: the left rows of the tile before this thread's,
+// and in the whole tile.
 template <int kItems>
 __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32_t ntiles, uint32_t epoch, int32_t t0,
                              int32_t cnt, const uint32_t (&rows)[kItems], uint32_t flags, int32_t nleft,
-                             uint32_t* out) {
+                             uint32_t* out, int32_t* excl_out = nullptr, int32_t* tile_left_out = nullptr) {
   DSlotState* st = s.st;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // block exclusive scan of per-thread left counts
@@ -1992,6 +1946,8 @@ __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32
       }
     }
     if (tile == ntiles - 1 && tid == 0) st->part_left = prefix + tile_left;
+    if (excl_out) *excl_out = excl;
+    if (tile_left_out) *tile_left_out = tile_left;
 }
 
 // Row tiles of the split leaf L claimed in order by the CTAs (kItems rows
@@ -2143,32 +2099,31 @@ template __global__ void k_scan_partition<true>(const __grid_constant__ DCtx);
 
 
 // =====================================================================================
-// Fused partition and histograms (quantized form, at most 32 features): the
-// partition of the split leaf also accumulates the histograms of both
-// children, so no histogram launch follows and no larger = parent - smaller
-// subtraction is needed (integer sums: the direct sums equal the difference
-// exactly). Each row's 32-byte bin segment is read whole: it holds the split
+// Fused partition and histogram (quantized form, at most 32 features): the
+// partition of the split leaf also builds the histogram of the child the
+// scan's estimated counts make the smaller one (split.rs:229-231), into
+// pool buffer R (zeroed by the scan before this launch). No histogram launch
+// follows; the next scan reads the built child and forms the other as
+// parent - built (histogram.rs:59-63). With integer sums both are exact
+// whichever child is built, so a wrong estimate only swaps which child is
+// built. Each row's 32-byte bin segment is read whole: it holds the split
 // feature's value (no column-major gather) and every feature's bin.
-// The children's packed sums go to pair (step & 1) of the slot's pair
-// buffers, child 0 the left child (the split leaf's index) and child 1 the
-// right one; the scan of the next step reads them and zeroes the other pair.
 // =====================================================================================
 constexpr int kFusedThreads = 512;
 constexpr int kFusedItems = kPartTileRows / kFusedThreads;
-constexpr int kFusedCells = kMaxBins * 32;  // one group of 32 features, per child
+constexpr int kFusedCells = kMaxBins * 32;  // one group of 32 features
 
 size_t fused_smem_bytes() {
-  return (size_t)2 * kFusedCells * 4 + (size_t)kPartTileRows * 32 + (size_t)kPartTileRows * 4 + kPartTileRows;
+  return (size_t)kFusedCells * 4 + (size_t)kPartTileRows * 32 + (size_t)kPartTileRows * 4;
 }
 
 __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThreads, 1)
     k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows) {
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int32_t* cells = reinterpret_cast<int32_t*>(smem_raw);  // [child][raw][lane]
-  uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)2 * kFusedCells * 4);
+  int32_t* cells = reinterpret_cast<int32_t*>(smem_raw);  // [raw][lane]
+  uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)kFusedCells * 4);
   int32_t* sq = reinterpret_cast<int32_t*>(sbins + 2 * kPartTileRows);
-  uint8_t* sf = reinterpret_cast<uint8_t*>(sq + kPartTileRows);
   __shared__ PartShared ps;
   __shared__ int32_t s_vlen[32], s_vstart[32];
   const DSlot& s = c.slots[blockIdx.z];
@@ -2178,10 +2133,10 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
   if (hd.done) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t R = hd.R;
-  const int step = R - 1;
   const uint32_t epoch = hd.epoch;
   const SplitLeaf sl = partition_prologue(c, s, hd, ps);
   const int32_t L = sl.L;
+  // every CTA of a cluster takes the same decision, so all of them return here or none
   if (L < 0) {
     if (blockIdx.x == 0 && tid == 0) st->done = 1;
     return;
@@ -2194,28 +2149,28 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
   }
   {
     uint4* z = reinterpret_cast<uint4*>(cells);
-    for (int i = tid; i < 2 * kFusedCells * 4 / 16; i += kFusedThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = tid; i < kFusedCells * 4 / 16; i += kFusedThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
   }
   __syncthreads();  // cells zeroed, feature facts and the LUT complete
   const int32_t begin = sl.begin, cnt = sl.cnt, side = sl.side, inner = sl.inner;
+  const bool build_left = sl.est_left_smaller;
   if (blockIdx.x == 0 && tid == 0) st->part_rows += cnt;
   const uint32_t* in = s.idx[side] + begin;
   uint32_t* out = s.idx[1 - side] + begin;
   const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
   const size_t stride = (size_t)c.stride;
   const uint8_t* lut = ps.lut;
-  long long* pair = s.pair_hist + (size_t)(step & 1) * 2 * c.total_bins;
+  long long* dst = reinterpret_cast<long long*>(s.hist) + (size_t)R * c.total_bins;
+  // adds cell i ([raw][lane]) holding (g << 16) + h to the built child's histogram
+  auto emit = [&](int i, int64_t g, int64_t h) {
+    const int raw = i >> 5, fl = i & 31;
+    if (raw == 0 || raw > s_vlen[fl] || (g == 0 && h == 0)) return;
+    atomicAdd(reinterpret_cast<unsigned long long*>(dst + s_vstart[fl] + raw - 1),
+              (unsigned long long)((uint64_t)(g << 32) + (uint64_t)h));
+  };
   auto decode = [](int32_t cell, int64_t& g, int64_t& h) {
     h = (int64_t)(cell & 0xFFFF);
     g = (int64_t)((cell - (int32_t)h) >> 16);
-  };
-  // adds cell i ([child][raw][lane]) with sums (g, h) to the child's histogram
-  auto emit = [&](int i, int64_t g, int64_t h) {
-    const int child = i / kFusedCells, k = i - child * kFusedCells;
-    const int raw = k >> 5, fl = k & 31;
-    if (raw == 0 || raw > s_vlen[fl] || (g == 0 && h == 0)) return;
-    atomicAdd(reinterpret_cast<unsigned long long*>(pair + (size_t)child * c.total_bins + s_vstart[fl] + raw - 1),
-              (unsigned long long)((uint64_t)(g << 32) + (uint64_t)h));
   };
   int32_t since_flush = 0;
   while (cnt > 0) {
@@ -2254,30 +2209,36 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
         ++nleft;
       }
     }
-    tile_scatter<kFusedItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out);
-    // the tile's rows into the children's cells (rows past the leaf stage as
-    // zeros: value 0 lands in cells no feature view contains)
+    int32_t excl = 0, tile_left = 0;
+    tile_scatter<kFusedItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out, &excl, &tile_left);
+    // the built child's rows of the tile, compacted in tile order into shared
+    // memory: its rows before this thread's are the tile's left rows before
+    // them, or the rest of the positions before them
+    const int32_t valid = min(kPartTileRows, cnt - t0);
+    const int32_t nbuilt = build_left ? tile_left : valid - tile_left;
+    int32_t at = build_left ? excl : tid * kFusedItems - excl;
 #pragma unroll
     for (int k = 0; k < kFusedItems; ++k) {
-      const int r = tid * kFusedItems + k;
-      sbins[2 * r] = b0[k];
-      sbins[2 * r + 1] = b1[k];
-      sq[r] = q[k];
-      sf[r] = (uint8_t)((flags >> k) & 1u);
+      if (t0 + tid * kFusedItems + k >= cnt) continue;
+      if ((((flags >> k) & 1u) != 0) == build_left) {
+        sbins[2 * at] = b0[k];
+        sbins[2 * at + 1] = b1[k];
+        sq[at] = q[k];
+        ++at;
+      }
     }
     __syncthreads();
     {
-      constexpr int kRowsPerWarp = kPartTileRows / (kFusedThreads / 32);
+      // lane l adds feature l of 32 rows per pass: every shared atomic of a
+      // warp hits 32 distinct banks
       const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + lane;
-      for (int j0 = warp * kRowsPerWarp; j0 < (warp + 1) * kRowsPerWarp; j0 += 32) {
-        const int32_t myq = sq[j0 + lane];
-        const int32_t myc = sf[j0 + lane] ? 0 : kFusedCells;  // left child: cells 0, right: cells 1
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
+      for (int j0 = warp * 32; j0 < nbuilt; j0 += kFusedThreads) {
+        const int32_t myq = j0 + lane < nbuilt ? sq[j0 + lane] : 0;
+        const int jn = min(32, nbuilt - j0);
+        for (int j = 0; j < jn; ++j) {
           const int32_t qq = __shfl_sync(0xffffffffu, myq, j);
-          const int32_t cb = __shfl_sync(0xffffffffu, myc, j);
           const int raw = rowp[(j0 + j) * 32];
-          atomicAdd(cells + cb + raw * 32 + lane, qq);
+          atomicAdd(cells + raw * 32 + lane, qq);
         }
       }
     }
@@ -2285,7 +2246,7 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
     __syncthreads();
     // int32 cells hold at most sub_rows rows before their 16-bit halves could wrap
     if (since_flush + kPartTileRows > sub_rows) {
-      for (int i = tid; i < 2 * kFusedCells; i += kFusedThreads) {
+      for (int i = tid; i < kFusedCells; i += kFusedThreads) {
         int64_t g, h;
         decode(cells[i], g, h);
         emit(i, g, h);
@@ -2295,12 +2256,12 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
       __syncthreads();
     }
   }
-  // cluster reduction: CTA rank r adds slice r of both children's cells,
-  // summed over the cluster's CTAs in rank order
+  // cluster reduction: CTA rank r adds slice r of the cells, summed over the
+  // cluster's CTAs in rank order
   cg::cluster_group cluster = cg::this_cluster();
   cluster.sync();
   {
-    const int per = 2 * kFusedCells / kHistCluster;
+    const int per = kFusedCells / kHistCluster;
     const int lo = (int)cluster.block_rank() * per;
     for (int i = lo + tid; i < lo + per; i += kFusedThreads) {
       int64_t g = 0, h = 0;
@@ -2322,7 +2283,7 @@ __global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThr
   __syncthreads();
   if (ps.last) {
     __threadfence();
-    finish_step(c, s, hd, ps.dec, L, R, cnt);
+    finish_step(c, s, hd, ps.dec, L, R, cnt, build_left ? 1 : 0);
   }
 }
 

@@ -218,7 +218,7 @@ def test_single_tree_quantized_exact(lgb, orc, renew):
     X, y = _binary_data(40000, seed=17)
     params = {"objective": "binary", "num_leaves": 127, "use_quantized_grad": True, "num_threads": 16,
               "quant_train_renew_leaf": renew}
-    gt, ot, *_ = _tree_pair(lgb, orc, X, y, params)
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, y, params)
     gains = om.trace(0)[3]
     if renew:  # leaf outputs re-fit from FP64 gradient sums (summation order differs)
         assert_same_tree(gt, ot, leaf_rtol=1e-12, gain_rtol=0.0, gains=gains)
