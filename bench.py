@@ -236,23 +236,21 @@ def run_form(lgb, data, ds, dv, form, args, device):
     hist_ms = scan_ms = part_ms = 0.0
     rows = prows = 0
     launches = 0
-    fused = False
     step_rows, step_hist_ms = [], []
     for _ in range(args.steps):
         bst.update()
         t, r, nl = L.last_timing()
-        _, pr, fused = L.last_rows()
+        _, pr = L.last_rows()
         hist_ms += t[0]
         scan_ms += t[1]
         part_ms += t[2]
         rows += r
         prows += pr
         launches = nl
-        if not fused:
-            st = L.step_times()
-            rr = hist_rows_by_step(bst.trees[-1])
-            step_rows.extend(rr)
-            step_hist_ms.extend(st[: len(rr), 0])
+        st = L.step_times()
+        rr = hist_rows_by_step(bst.trees[-1])
+        step_rows.extend(rr)
+        step_hist_ms.extend(st[: len(rr), 0])
     L.set_timing(False)
     done = args.warmup + extra + 2 * args.steps
     for _ in range(max(0, args.rounds - done)):
@@ -269,19 +267,18 @@ def run_form(lgb, data, ds, dv, form, args, device):
     auc_device_ms = 1000 * (time.perf_counter() - t0)
     nf = ds.binned()["num_features"]
     steps_per_tree = int(params["num_leaves"]) - 1
-    hist_launches = args.steps * (1 if fused else steps_per_tree)
+    hist_launches = args.steps * steps_per_tree
     hist_bytes = rows * hist_bytes_per_row(nf, form)
     # the partition moves each row of the split leaf: index in, its byte of the
-    # split feature (column copy), index out; the fused form also adds the row to
-    # its child's histogram: index in, bin row, packed gradient, index out
-    part_bytes = prows * ((4 + nf + 4 + 4) if fused else (4 + 1 + 4))
+    # split feature (column copy), index out
+    part_bytes = prows * (4 + 1 + 4)
     return {
         "ms_per_step": ms, "wall_ms_per_step": 1000 * wall / args.steps, "s_per_500": ms * ROUNDS / 1000.0,
         "auc": auc, "auc_device": auc_device, "auc_device_ms": auc_device_ms, "auc_numpy_ms": auc_numpy_ms,
         "hist_ms_per_launch": hist_ms / hist_launches, "hist_gbs": hist_bytes / (hist_ms / 1000) / 1e9,
         "hist_bytes_per_launch": hist_bytes / hist_launches, "hist_rows_per_tree": rows / args.steps,
         "scan_ms_per_step": scan_ms / args.steps, "partition_ms_per_step": part_ms / args.steps,
-        "fused": fused, "part_rows_per_tree": prows / args.steps,
+        "part_rows_per_tree": prows / args.steps,
         "part_gbs": part_bytes / (part_ms / 1000) / 1e9 if part_ms > 0 else None,
         "part_bytes_per_launch": part_bytes / (args.steps * steps_per_tree),
         "part_ms_per_launch": part_ms / (args.steps * steps_per_tree),
@@ -823,21 +820,18 @@ def main():
                       "auc_numpy_ms": v["auc_numpy_ms"],
                       "hist_gbs": v["hist_gbs"], "hist_ms_per_step": v["hist_ms_per_step"],
                       "scan_ms_per_step": v["scan_ms_per_step"], "partition_ms_per_step": v["partition_ms_per_step"],
-                      "hist_rows_per_tree": v["hist_rows_per_tree"], "fused": v["fused"], "part_gbs": v["part_gbs"],
+                      "hist_rows_per_tree": v["hist_rows_per_tree"], "part_gbs": v["part_gbs"],
                       "part_rows_per_tree": v["part_rows_per_tree"], "launch_shape": v["launch_shape"],
                       "launch_shape_source": v["launch_shape_source"], "hist_by_rows": v["hist_by_rows"]}
                   for k, v in res.items()},
-        "roofline": ({"bound": "hbm", "kernel": "k_partition_fused (row partition + both children's histograms)",
-                      "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s", "frac": r["part_gbs"] / peak,
-                      "peak_kind": peak_kind, "traffic": None,
-                      "bytes_per_launch": r["part_bytes_per_launch"], "ms_per_launch": r["part_ms_per_launch"]}
-                     if r["fused"] else
-                     {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
-                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                      "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] /
-                                  (int(data["params"]["num_leaves"]) - 1) if head == "quantized" else None),
-                      "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
-                      "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"]}),
+        "roofline": {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] /
+                                 (int(data["params"]["num_leaves"]) - 1) if head == "quantized" else None),
+                     "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
+                     "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"],
+                     # the histogram's achieved fraction of the HBM roofline by leaf size
+                     "by_rows": [dict(b, frac=(b["gbs"] / peak if b["gbs"] else None)) for b in r["hist_by_rows"]]},
         "cpu_baseline": cpu, "e2e": e2e,
         # per iteration: the tree's launches (init, 3 per split, leaf renewal), then the
         # gradients, the quantization (max-abs, packing), the leaf shrinkage, the training
@@ -849,19 +843,15 @@ def main():
                          for k in ("hist", "scan", "partition")},
         "clocks": r["clocks"],
     }
-    if not r["fused"]:
-        # the histogram's achieved fraction of the HBM roofline by leaf size
-        line["roofline"]["by_rows"] = [dict(b, frac=(b["gbs"] / peak if b["gbs"] else None))
-                                       for b in r["hist_by_rows"]]
-        # the row partition, the largest share of device time (its launches are
-        # latency-bound: most leaves are small)
-        line["roofline_partition"] = {
-            "bound": "hbm", "kernel": "k_partition", "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s",
-            "frac": r["part_gbs"] / peak, "peak_kind": peak_kind,
-            "traffic": PART_DRAM_BYTES_PER_ROW * r["part_rows_per_tree"] / (int(data["params"]["num_leaves"]) - 1),
-            "traffic_note": "ncu DRAM bytes per row of the 5M-row root split x rows per launch (average)",
-            "bytes_per_row": 9, "bytes_per_launch": r["part_bytes_per_launch"],
-            "ms_per_launch": r["part_ms_per_launch"]}
+    # the row partition, the largest share of device time (its launches are
+    # latency-bound: most leaves are small)
+    line["roofline_partition"] = {
+        "bound": "hbm", "kernel": "k_partition", "achieved": r["part_gbs"], "peak": peak, "unit": "GB/s",
+        "frac": r["part_gbs"] / peak, "peak_kind": peak_kind,
+        "traffic": PART_DRAM_BYTES_PER_ROW * r["part_rows_per_tree"] / (int(data["params"]["num_leaves"]) - 1),
+        "traffic_note": "ncu DRAM bytes per row of the 5M-row root split x rows per launch (average)",
+        "bytes_per_row": 9, "bytes_per_launch": r["part_bytes_per_launch"],
+        "ms_per_launch": r["part_ms_per_launch"]}
     if "f64" in res and head in res:
         line["speedup_vs_f64"] = res["f64"]["ms_per_step"] / res[head]["ms_per_step"]
         line["auc_delta_vs_f64"] = res[head]["auc"] - res["f64"]["auc"]

@@ -259,6 +259,29 @@ int lgbm_b200_learner_add_leaf_outputs(LgbmB200Learner* h, int32_t slot, const d
 int lgbm_b200_learner_get_partition(LgbmB200Learner* h, int32_t slot, int32_t* leaf_begin, int32_t* leaf_count,
                                     uint32_t* indices);
 
+/* ------------------------------------------------------------------------
+ * Data-parallel growth: the rows are sharded over ranks (one learner per
+ * rank and GPU, each created on its own rows, all with the same bin
+ * mappers); the trees are the ones a single learner grows on all rows. The
+ * reference's learner is serial and has no counterpart; this follows the
+ * data-parallel scheme of its upstream (LightGBM's data-parallel tree
+ * learner: a histogram all-reduce per split). Per tree the ranks reduce:
+ * the quantization maxima (max), the root sums, each split step's smaller-
+ * leaf histogram, the rows each step sends left, and the leaf renewal sums
+ * (sums). The learner calls `fn` for each reduction, on a device buffer of
+ * its own device, after synchronising its stream; fn must reduce the buffer
+ * in place over every rank (same call order on every rank) and return 0
+ * once the result is in the buffer. One tree slot only (not multiclass); no
+ * bagging; growth runs step by step (no CUDA graph).
+ * ------------------------------------------------------------------------ */
+enum { LGBM_B200_DT_INT64 = 0, LGBM_B200_DT_FLOAT64 = 1, LGBM_B200_DT_INT32 = 2 };
+enum { LGBM_B200_OP_SUM = 0, LGBM_B200_OP_MAX = 1 };
+typedef int32_t (*LgbmB200AllReduceFn)(void* device_buf, int64_t count, int32_t dtype, int32_t op, void* user);
+/* row_offset: this rank's first row in the global row order; global_num_data:
+ * every rank's rows. Call once, after lgbm_b200_learner_create. */
+int lgbm_b200_learner_set_data_parallel(LgbmB200Learner* h, int64_t row_offset, int64_t global_num_data,
+                                        LgbmB200AllReduceFn fn, void* user);
+
 /* Launch shape of the per-split-step kernels (the default launch strategy;
  * the persistent one has none). No field changes a result: the shapes differ
  * only in speed. No counterpart in the reference, whose CPU learner has a
@@ -292,17 +315,16 @@ int lgbm_b200_learner_elapsed(LgbmB200Learner* h, int32_t a, int32_t b, double* 
 /* Device time of the last train call summed per kernel family, ms:
  * [histogram, scan, partition, other]; rows histogrammed; kernels launched. */
 int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_rows, int32_t* launches);
-/* Rows of the last train call: histogrammed by the histogram kernel, and
- * partitioned (in the fused quantized form, where *fused is 1, the partition
- * also builds both children's histograms from the rows it moves). For the
- * bench's bandwidth figures; no counterpart in the reference. */
 /* With timing on (lgbm_b200_learner_set_timing), the device time of the
  * histogram, scan and partition launches of every split step of the last
  * train call: ms[3 * step + {0, 1, 2}] for step < min(*steps, capacity).
  * Histogram step s builds the smaller child of split s - 1 (step 0: the
  * root). A diagnostic with no counterpart in the reference. */
 int lgbm_b200_learner_step_times(LgbmB200Learner* h, float* ms, int32_t capacity, int32_t* steps);
-int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows, int32_t* fused);
+/* Rows of the last train call: histogrammed by the histogram kernel, and
+ * moved by the partition. For the bench's bandwidth figures; no
+ * counterpart in the reference. */
+int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows);
 
 /* Diagnostics for the parity tests. lgbm_b200_learner_histogram runs the
  * learner's histogram kernel over `rows` (NULL: every row) of slot `slot`'s

@@ -620,6 +620,8 @@ int lgbm_b200_booster_create(LgbmB200Learner* learner, const LgbmB200BoostConfig
                              const int32_t* query_boundaries, int32_t num_queries, const uint8_t* valid_bins,
                              int64_t num_valid, LgbmB200Booster** out) {
   if (!learner || !cfg || !label || !out) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
+  if (learner->dp)  // its init score and metrics would need reductions over the ranks too
+    return fail(Status(LGBM_B200_ERR_UNSUPPORTED, "the device booster does not drive a data-parallel learner"));
   auto b = std::make_unique<LgbmB200Booster>();
   Status s = booster_create(b.get(), learner, cfg, label, query_boundaries, num_queries, valid_bins,
                             valid_bins ? num_valid : 0);

@@ -110,7 +110,8 @@ struct DSlot {
   DSlotState* st;
   uint32_t* idx[2];        // ping-pong row index buffers [num_data]
   int32_t* leaf_begin;
-  int32_t* leaf_count;
+  int32_t* leaf_count;     // this rank's rows of each leaf (the row ranges)
+  int32_t* leaf_gcount;    // every rank's rows of each leaf: the counts (leaf_count itself unless data-parallel)
   int32_t* leaf_side;      // which idx buffer holds the leaf's rows
   int32_t* buf_of;         // histogram buffer of each leaf
   DSplit* best;            // best_split_per_leaf [num_leaves]
@@ -132,9 +133,14 @@ struct DSlot {
   long long* root_ipartials;
   int32_t* root_counter;
   DTree tree;
+  // data-parallel growth: the split decision the partition leaves for the
+  // finishing launch, and this rank's rows sent left
+  unsigned char* dp_dec;
+  int32_t* dp_left;
 };
 
 constexpr int kRootBlocks = 296;
+constexpr int kDpDecBytes = 2048;  // a split decision kept between a data-parallel partition and its finish
 constexpr int kMaxSlots = 16;  // tree slots grown together (slot structs travel as kernel parameters)
 
 struct DCtx {
@@ -151,7 +157,7 @@ struct DCtx {
   DSlot slots[kMaxSlots];  // by value: read from the constant bank
   int32_t num_slots;
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
-  int32_t fused;           // 1: the partition also builds one child's histogram (quantized, <= 32 features)
+  int32_t dp;              // 1: rows sharded over ranks; the step's end waits for the global left count
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

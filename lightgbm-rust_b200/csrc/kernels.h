@@ -117,12 +117,14 @@ size_t grow_smem_bytes(int mode, int ng);
 cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
                         int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns);
 __global__ void k_partition(const __grid_constant__ DCtx c);
-__global__ void k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows);
-size_t fused_smem_bytes();
 __global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
 __global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* partial, int32_t* rank);
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* partial, const int32_t* rank,
-                             int32_t nwarps);
+                             int32_t nwarps, double* totals);
+__global__ void k_dp_leaf_apply(const __grid_constant__ DCtx c, const double* totals);
+__global__ void k_dp_finish(const __grid_constant__ DCtx c);
+__global__ void k_dp_root_pack(const __grid_constant__ DCtx c, double* f, long long* q);
+__global__ void k_dp_root_apply(const __grid_constant__ DCtx c, const double* f, const long long* q);
 __global__ void k_add_leaf_outputs(const __grid_constant__ DCtx c, const double* leaf_values, int32_t lv_stride, double* score,
                                    int64_t score_stride);
 __global__ void k_leaf_of_row(const __grid_constant__ DCtx c, int32_t* leaf_of_row);
@@ -138,10 +140,11 @@ __global__ void k_grad_softmax(const float* label, const double* score, int64_t 
                                int64_t gh_stride, float* g, float* h);
 __global__ void k_interleave(const float* g, const float* h, int64_t n, float2* gh);
 __global__ void k_quant_absmax(const float2* gh, int64_t n, unsigned long long* maxbits, int32_t* counter,
-                               DSlotState* st, int32_t bins, int32_t const_hess, int32_t num_blocks);
+                               DSlotState* st, int32_t bins, int32_t const_hess, int32_t num_blocks, int32_t derive);
+__global__ void k_quant_scales(unsigned long long* maxbits, DSlotState* st, int32_t bins, int32_t const_hess);
 __global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv,
                               const int64_t* start_dev, const DSlotState* st, int32_t const_hess, int32_t stochastic,
-                              int32_t* packed);
+                              int32_t* packed, int64_t row_offset, int64_t table_n);
 __global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag, int32_t* block_in);
 __global__ void k_bag_scan(const int32_t* block_in, int32_t nb, int64_t n, int32_t* block_base, int32_t* counts);
 __global__ void k_bag_scatter(const uint8_t* in_bag, int64_t n, const int32_t* block_base, uint32_t* bag,

@@ -131,23 +131,6 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     h->hist_grid = std::max(1, clusters / std::max(1, h->ntiles)) * cl;
   }
   h->part_grid = h->num_sms * 3;  // 3 CTAs per SM measured best with 1024-row tiles (2 and 2.5 per SM are slower)
-  // LGBM_B200_FUSED=1: the quantized form with at most 32 features builds
-  // the estimated smaller child's histogram inside the partition, and no
-  // histogram launch follows a split.
-  h->fused = false;
-  if (const char* e = std::getenv("LGBM_B200_FUSED"))
-    h->fused = std::atoi(e) != 0 && mode == LGBM_B200_HIST_QUANT && nf <= 32 && !cfg->persistent_grow;
-  if (h->fused) {
-    CU(cudaFuncSetAttribute(k_partition_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes()));
-    cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(kHistCluster * 32, 1, 1);
-    lc.blockDim = dim3(512, 1, 1);
-    lc.dynamicSmemBytes = fused_smem_bytes();
-    int clusters = 0;
-    CU(cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_partition_fused, &lc));
-    if (clusters < 1) return Status(LGBM_B200_ERR_CUDA, "fused partition cluster does not fit on the device");
-    h->fused_grid = clusters * kHistCluster;
-  }
   // LGBM_B200_PART_GRID sets the partition's CTA count (launch-shape sweeps)
   if (const char* e = std::getenv("LGBM_B200_PART_GRID")) h->part_grid = std::max(1, std::atoi(e));
   // LGBM_B200_SCANPART=1: the threshold scans and the partition of a step run
@@ -155,7 +138,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   // grid is what stays resident at once, shared by the tree slots
   h->scan_part = false;
   if (const char* e = std::getenv("LGBM_B200_SCANPART"))
-    h->scan_part = std::atoi(e) != 0 && !h->fused && !cfg->persistent_grow;
+    h->scan_part = std::atoi(e) != 0 && !cfg->persistent_grow;
   if (h->scan_part) {
     const void* k = mode == LGBM_B200_HIST_QUANT ? (const void*)k_scan_partition<true> : (const void*)k_scan_partition<false>;
     int per_sm = 0;
@@ -215,6 +198,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     ALLOC(d.idx[1], n);
     ALLOC(d.leaf_begin, L);
     ALLOC(d.leaf_count, L);
+    d.leaf_gcount = d.leaf_count;  // one learner holds every row: its counts are its ranges
     ALLOC(d.leaf_side, L);
     ALLOC(d.buf_of, L);
     ALLOC(d.best, L);
@@ -285,28 +269,7 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     if (!(s = A.alloc_n(&h->quant_counter, 1)).ok()) return s;
     CU(cudaMemset(h->maxbits, 0, 2 * sizeof(unsigned long long)));
     CU(cudaMemset(h->quant_counter, 0, sizeof(int32_t)));
-    // learner/quant.rs:364-398: per-block MT19937 tables (the block layout
-    // follows the reference's thread count)
-    if (cfg->stochastic_rounding) {
-      size_t nt = (size_t)std::max(1, cfg->quant_num_threads);
-      size_t nb = std::max<size_t>(1, std::min(nt, ((size_t)n + 511) / 512));
-      size_t bs = (size_t)n;
-      if (nb > 1) bs = (((size_t)n + nb - 1) / nb + 31) / 32 * 32;
-      std::vector<double> g(n), hh(n);
-      for (size_t b = 0; b < nb; ++b) {
-        size_t st = b * bs, en = std::min((size_t)n, st + bs);
-        Mt19937 ge((uint32_t)(cfg->seed + (int32_t)b));
-        Mt19937 he((uint32_t)(cfg->seed + (int32_t)b + (int32_t)nt));
-        for (size_t i = st; i < en; ++i) {
-          g[i] = ge.uniform01();
-          hh[i] = he.uniform01();
-        }
-      }
-      if (!(s = A.alloc_n(&h->grv, (size_t)n)).ok()) return s;
-      if (!(s = A.alloc_n(&h->hrv, (size_t)n)).ok()) return s;
-      CU(cudaMemcpy(h->grv, g.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-      CU(cudaMemcpy(h->hrv, hh.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-    }
+    if (cfg->stochastic_rounding && !(s = quant_tables(h, n)).ok()) return s;
     h->start_eng = std::make_unique<Mt19937>((uint32_t)cfg->seed);
     if (!(s = A.alloc_n(&h->start_dev, (size_t)K)).ok()) return s;
     CU(cudaHostAlloc(reinterpret_cast<void**>(&h->start_h), sizeof(int64_t) * K, cudaHostAllocDefault));
@@ -342,7 +305,6 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   for (int k = 0; k < K; ++k) c.slots[k] = h->slots_h[k];
   c.num_slots = K;
   c.rows_per_block = rpb;
-  c.fused = h->fused ? 1 : 0;
   h->n_used = (int32_t)n;
   h->st_h.resize(K);
   h->trees.resize(K);
@@ -353,6 +315,34 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     h->ev.push_back(e);
   }
   for (int i = 0; i < 16; ++i) CU(cudaEventCreate(&h->marks[i]));
+  return Status();
+}
+
+// learner/quant.rs:364-398: the stochastic-rounding tables of `rows` rows,
+// drawn per block by MT19937 (the block layout follows the reference's thread
+// count), uploaded to new device arrays.
+Status quant_tables(LgbmB200Learner* h, int64_t rows) {
+  const LgbmB200LearnerConfig* cfg = &h->cfg;
+  const size_t n = (size_t)rows;
+  size_t nt = (size_t)std::max(1, cfg->quant_num_threads);
+  size_t nb = std::max<size_t>(1, std::min(nt, (n + 511) / 512));
+  size_t bs = n;
+  if (nb > 1) bs = ((n + nb - 1) / nb + 31) / 32 * 32;
+  std::vector<double> g(n), hh(n);
+  for (size_t b = 0; b < nb; ++b) {
+    size_t st = b * bs, en = std::min(n, st + bs);
+    Mt19937 ge((uint32_t)(cfg->seed + (int32_t)b));
+    Mt19937 he((uint32_t)(cfg->seed + (int32_t)b + (int32_t)nt));
+    for (size_t i = st; i < en; ++i) {
+      g[i] = ge.uniform01();
+      hh[i] = he.uniform01();
+    }
+  }
+  Status s;
+  if (!(s = h->arena.alloc_n(&h->grv, n)).ok()) return s;
+  if (!(s = h->arena.alloc_n(&h->hrv, n)).ok()) return s;
+  CU(cudaMemcpy(h->grv, g.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(h->hrv, hh.data(), n * sizeof(double), cudaMemcpyHostToDevice));
   return Status();
 }
 
@@ -382,9 +372,7 @@ Status enqueue_tree(LgbmB200Learner* h) {
     // (not when events are recorded between them)
     const int pdl_edges = h->timing ? 0 : h->use_pdl;
     const bool pdl = (pdl_edges & 1) != 0, pdl_scan = (pdl_edges & 2) != 0, pdl_part = (pdl_edges & 4) != 0;
-    // fused form: only the root needs a histogram launch
-    if (!h->fused || step == 0)
-      CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
+    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
     if (h->scan_part) {  // scans and partition in one launch: the scan interval records as empty
       if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
@@ -404,25 +392,102 @@ Status enqueue_tree(LgbmB200Learner* h) {
       CU(launch_ex(k_scan<false, 1>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
     }
     if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
-    if (h->fused)
-      CU(launch_ex(k_partition_fused, dim3(h->fused_grid, 1, K), dim3(512), fused_smem_bytes(), s, pdl_part, c,
-                   h->sub_rows));
-    else CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl_part, c));
+    CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl_part, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
     k_leaf_sums<<<dim3(leaf_sum_warps(h) / 8, 1, K), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums, h->leaf_rank);
     CU_LAUNCH();
-    k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums, h->leaf_rank, leaf_sum_warps(h));
+    k_leaf_renew<<<dim3(1, 1, K), 256, 0, s>>>(c, h->leaf_sums, h->leaf_rank, leaf_sum_warps(h), nullptr);
     CU_LAUNCH();
   }
-  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : ((h->fused || h->scan_part) ? 2 * (L - 1) + (h->fused ? 1 : 0)
+  h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : (h->scan_part ? 2 * (L - 1)
                                                                                    : 3 * (L - 1))) +
                      ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
   return Status();
 }
 
+// Data-parallel growth: one reduction over the ranks, in place on a device
+// buffer, once this learner's stream has run up to here.
+Status dp_allreduce(LgbmB200Learner* h, void* buf, int64_t count, int32_t dtype, int32_t op) {
+  CU(cudaStreamSynchronize(h->stream));
+  const int32_t rc = h->dp_fn(buf, count, dtype, op, h->dp_user);
+  if (rc != 0) return Status(LGBM_B200_ERR_INTERNAL, "data-parallel all-reduce failed with " + std::to_string(rc));
+  return Status();
+}
+
+static Status launch_scan(LgbmB200Learner* h, bool pdl) {
+  const DCtx& c = h->ctx;
+  const dim3 g(h->nf, 2, h->K);
+  cudaStream_t s = h->stream;
+  if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT) {
+    if (h->scan_wide) CU(launch_ex(k_scan<true, kScanWideBlocks>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
+    else CU(launch_ex(k_scan<true, 1>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
+  } else if (h->scan_wide) {
+    CU(launch_ex(k_scan<false, kScanWideBlocks>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
+  } else {
+    CU(launch_ex(k_scan<false, 1>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
+  }
+  return Status();
+}
+
+// One tree grown data-parallel (one slot): the launches of enqueue_tree, with
+// the reductions over ranks between them. The host reads the slot state
+// after every step, which is what keeps every rank's calls in step: the
+// decisions come from the reduced histograms, so they are the same on every
+// rank.
+static Status run_tree_dp(LgbmB200Learner* h) {
+  const DCtx& c = h->ctx;
+  const int L = h->L;
+  const int mode = h->cfg.hist_precision;
+  cudaStream_t s = h->stream;
+  const DSlot& d = h->slots_h[0];
+  Status st;
+  k_tree_init<<<dim3(h->root_grid, 1, 1), 256, 0, s>>>(c, nullptr, h->n_used_dev);
+  CU_LAUNCH();
+  k_dp_root_pack<<<1, 1, 0, s>>>(c, h->dp_f64, h->dp_i64);
+  CU_LAUNCH();
+  if (!(st = dp_allreduce(h, h->dp_f64, 2, LGBM_B200_DT_FLOAT64, LGBM_B200_OP_SUM)).ok()) return st;
+  if (!(st = dp_allreduce(h, h->dp_i64, 2, LGBM_B200_DT_INT64, LGBM_B200_OP_SUM)).ok()) return st;
+  k_dp_root_apply<<<1, 1, 0, s>>>(c, h->dp_f64, h->dp_i64);
+  CU_LAUNCH();
+  const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
+  const dim3 hist_grid(h->hist_grid, h->ntiles, 1);
+  for (int step = 0; step < L - 1; ++step) {
+    DSlotState ss;
+    CU(cudaMemcpyAsync(&ss, d.st, sizeof(ss), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (ss.done) break;
+    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false));
+    if (ss.need_find) {  // the smaller leaf's histogram, summed over the ranks
+      void* buf = static_cast<char*>(d.hist) + (size_t)ss.s_buf * cells * 8;
+      const int32_t dt = mode == LGBM_B200_HIST_QUANT ? LGBM_B200_DT_INT64 : LGBM_B200_DT_FLOAT64;
+      if (!(st = dp_allreduce(h, buf, (int64_t)cells, dt, LGBM_B200_OP_SUM)).ok()) return st;
+    }
+    if (!(st = launch_scan(h, false)).ok()) return st;
+    CU(launch_ex(k_partition, dim3(h->part_grid, 1, 1), dim3(kPartThreads), 0, s, false, c));
+    CU(cudaMemcpyAsync(&ss, d.st, sizeof(ss), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (ss.done) break;  // no leaf had a positive gain: the tree is finished
+    if (!(st = dp_allreduce(h, d.dp_left, 1, LGBM_B200_DT_INT32, LGBM_B200_OP_SUM)).ok()) return st;
+    k_dp_finish<<<1, kPartThreads, 0, s>>>(c);
+    CU_LAUNCH();
+  }
+  if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
+    k_leaf_sums<<<dim3(leaf_sum_warps(h) / 8, 1, 1), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums, h->leaf_rank);
+    CU_LAUNCH();
+    k_leaf_renew<<<1, 256, 0, s>>>(c, h->leaf_sums, h->leaf_rank, leaf_sum_warps(h), h->dp_f64);
+    CU_LAUNCH();
+    if (!(st = dp_allreduce(h, h->dp_f64, 2 * (int64_t)L, LGBM_B200_DT_FLOAT64, LGBM_B200_OP_SUM)).ok()) return st;
+    k_dp_leaf_apply<<<1, 256, 0, s>>>(c, h->dp_f64);
+    CU_LAUNCH();
+  }
+  h->last_launches = 0;
+  return Status();
+}
+
 static Status run_tree(LgbmB200Learner* h) {
+  if (h->dp) return run_tree_dp(h);
   cudaStream_t s = h->stream;
   // a cooperative launch is enqueued directly rather than captured
   const bool graph = h->cfg.use_cuda_graph != 0 && !h->cfg.persistent_grow;
@@ -539,7 +604,8 @@ void draw_quant_starts(LgbmB200Learner* h, bool replay) {
   const int K = h->K;
   if (h->last_start.size() < (size_t)K) h->last_start.resize((size_t)K, 0);
   for (int k = 0; k < K; ++k) {
-    const int64_t start = replay ? h->last_start[k] : h->start_eng->uniform_int(0, (int32_t)h->n);
+    const int64_t rows = h->dp ? h->dp_global_n : h->n;  // the tables cover every rank's rows
+    const int64_t start = replay ? h->last_start[k] : h->start_eng->uniform_int(0, (int32_t)rows);
     h->last_start[k] = start;
     h->start_h[k] = start;
   }
@@ -552,15 +618,24 @@ void draw_quant_starts(LgbmB200Learner* h, bool replay) {
 Status enqueue_quant(LgbmB200Learner* h) {
   cudaStream_t s = h->stream;
   const int64_t n = h->n;
+  const int64_t offset = h->dp ? h->dp_offset : 0, table_n = h->dp ? h->dp_global_n : n;
   CU(cudaMemcpyAsync(h->start_dev, h->start_h, sizeof(int64_t) * h->K, cudaMemcpyHostToDevice, s));
   for (int k = 0; k < h->K; ++k) {
     int blocks = h->num_sms * 4;
     k_quant_absmax<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->maxbits, h->quant_counter, h->slots_h[k].st,
-                                          h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks);
+                                          h->cfg.num_grad_quant_bins, h->cfg.is_constant_hessian, blocks,
+                                          h->dp ? 0 : 1);
     CU_LAUNCH();
+    if (h->dp) {  // the scales from the maxima over every rank
+      Status st = dp_allreduce(h, h->maxbits, 2, LGBM_B200_DT_INT64, LGBM_B200_OP_MAX);
+      if (!st.ok()) return st;
+      k_quant_scales<<<1, 1, 0, s>>>(h->maxbits, h->slots_h[k].st, h->cfg.num_grad_quant_bins,
+                                     h->cfg.is_constant_hessian);
+      CU_LAUNCH();
+    }
     k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, h->start_dev + k, h->slots_h[k].st,
                                          h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
-                                         h->slots_h[k].packed);
+                                         h->slots_h[k].packed, offset, table_n);
     CU_LAUNCH();
   }
   return Status();
@@ -782,7 +857,6 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   // one slot only: a context whose slot array starts at `slot`
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
-  c.fused = 0;  // into the pool buffer 0
   dim3 grid(h->hist_grid, h->ntiles, 1);
   CU(launch_hist(mode, h->hist_ng, grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false));
   CU_LAUNCH();
@@ -1040,6 +1114,44 @@ int lgbm_b200_learner_last_timing(LgbmB200Learner* h, double* ms, int64_t* hist_
   return LGBM_B200_OK;
 }
 
+int lgbm_b200_learner_set_data_parallel(LgbmB200Learner* h, int64_t row_offset, int64_t global_num_data,
+                                        LgbmB200AllReduceFn fn, void* user) {
+  if (!h || !fn) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "set_data_parallel: null argument"));
+  if (h->dp) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "set_data_parallel: already set"));
+  if (h->K != 1)
+    return fail(Status(LGBM_B200_ERR_UNSUPPORTED, "data-parallel growth takes one tree slot (no multiclass)"));
+  if (h->bagging) return fail(Status(LGBM_B200_ERR_UNSUPPORTED, "data-parallel growth does not take bagging"));
+  if (row_offset < 0 || global_num_data < row_offset + h->n || global_num_data > INT32_MAX)
+    return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "set_data_parallel: rows outside [0, global_num_data)"));
+  if (cudaSetDevice(h->device) != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, "cudaSetDevice"));
+  DeviceArena& A = h->arena;
+  DSlot& d = h->slots_h[0];
+  Status s;
+  const int L = h->L;
+  if (!(s = A.alloc_n(&d.leaf_gcount, (size_t)L)).ok() || !(s = A.alloc_n(&d.dp_left, 2)).ok() ||
+      !(s = A.alloc_n(&h->dp_f64, (size_t)(2 * L + 4))).ok() || !(s = A.alloc_n(&h->dp_i64, 4)).ok())
+    return fail(s);
+  if (!(s = A.alloc(reinterpret_cast<void**>(&d.dp_dec), kDpDecBytes)).ok()) return fail(s);
+  if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT && h->cfg.stochastic_rounding &&
+      !(s = quant_tables(h, global_num_data)).ok())
+    return fail(s);
+  h->ctx.slots[0] = d;
+  h->ctx.dp = 1;
+  h->scan_part = false;
+  h->cfg.persistent_grow = 0;
+  h->cfg.use_cuda_graph = 0;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  h->dp = true;
+  h->dp_offset = row_offset;
+  h->dp_global_n = global_num_data;
+  h->dp_fn = fn;
+  h->dp_user = user;
+  return LGBM_B200_OK;
+}
+
 int lgbm_b200_learner_step_times(LgbmB200Learner* h, float* ms, int32_t capacity, int32_t* steps) {
   if (!h || !steps) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null argument"));
   const int32_t n = (int32_t)(h->last_step_ms.size() / 3);
@@ -1049,11 +1161,10 @@ int lgbm_b200_learner_step_times(LgbmB200Learner* h, float* ms, int32_t capacity
   return LGBM_B200_OK;
 }
 
-int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows, int32_t* fused) {
+int lgbm_b200_learner_last_rows(LgbmB200Learner* h, int64_t* hist_rows, int64_t* partition_rows) {
   if (!h) return fail(Status(LGBM_B200_ERR_INVALID_PARAMETER, "null handle"));
   if (hist_rows) *hist_rows = h->last_hist_rows;
   if (partition_rows) *partition_rows = h->last_part_rows;
-  if (fused) *fused = h->fused ? 1 : 0;
   return LGBM_B200_OK;
 }
 

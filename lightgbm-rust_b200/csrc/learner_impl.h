@@ -280,10 +280,15 @@ struct LgbmB200Learner {
   cudaEvent_t marks[16] = {};  // caller-placed timing marks on the learner's stream
   double last_ms[4] = {0, 0, 0, 0};
   std::vector<float> last_step_ms;  // timing on: (histogram, scan, partition) ms of every split step
+  // data-parallel growth (lgbm_b200_learner_set_data_parallel)
+  bool dp = false;
+  int64_t dp_offset = 0, dp_global_n = 0;
+  LgbmB200AllReduceFn dp_fn = nullptr;
+  void* dp_user = nullptr;
+  double* dp_f64 = nullptr;     // [2 * L + 4] root / renewal sums
+  long long* dp_i64 = nullptr;  // [4]
   int64_t last_hist_rows = 0;
   int64_t last_part_rows = 0;
-  bool fused = false;  // the partition also builds the estimated smaller child's histogram
-  int fused_grid = 0;
   bool scan_wide = false;  // the register-capped scan variant (many CTAs per step)
   bool scan_part = false;  // scans and partition of a step in one cooperative launch
   int scan_part_grid = 0;
@@ -326,6 +331,10 @@ Status train_collect(LgbmB200Learner* h);
 // quantization, and the launches of one tree
 void draw_quant_starts(LgbmB200Learner* h, bool replay);
 Status enqueue_quant(LgbmB200Learner* h);
+// the stochastic-rounding tables of `rows` rows (learner/quant.rs:364-398)
+Status quant_tables(LgbmB200Learner* h, int64_t rows);
+// data-parallel growth: one in-place reduction over the ranks of a device buffer
+Status dp_allreduce(LgbmB200Learner* h, void* buf, int64_t count, int32_t dtype, int32_t op);
 Status enqueue_tree(LgbmB200Learner* h);
 Status get_launch_shape(const LgbmB200Learner* h, LgbmB200LaunchShape* out);
 Status set_launch_shape(LgbmB200Learner* h, const LgbmB200LaunchShape& in);

@@ -47,8 +47,8 @@ __device__ bool before_find_best_split(const DCtx& c, const DSlot& s, int32_t le
     }
     return false;
   }
-  int32_t nl = left >= 0 ? s.leaf_count[left] : 0;
-  int32_t nr = right >= 0 ? s.leaf_count[right] : 0;
+  int32_t nl = left >= 0 ? s.leaf_gcount[left] : 0;
+  int32_t nr = right >= 0 ? s.leaf_gcount[right] : 0;
   int32_t min2 = p.min_data_in_leaf * 2;
   if (nr < min2 && nl < min2) {
     s.best[left].gain = -INFINITY;
@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
     s.buf_of[l] = l;
     s.leaf_begin[l] = 0;
     s.leaf_count[l] = 0;
+    s.leaf_gcount[l] = 0;
     s.leaf_side[l] = 0;
   }
   for (int f = tid; f < c.num_features; f += blockDim.x) s.splittable[f] = 1;
@@ -203,6 +204,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
     d += s.root_ipartials[k];
   }
   s.leaf_count[0] = (int32_t)n;
+  s.leaf_gcount[0] = (int32_t)n;  // data-parallel: the global count replaces it after the root sums' reduction
   st->num_used = (int32_t)n;
   st->num_leaves_cur = 1;
   st->done = 0;
@@ -1468,14 +1470,6 @@ __global__ void __launch_bounds__(kScanThreads, kMinBlocks) k_scan(const __grid_
     st->part_ticket = 0;
     st->part_done = 0;
   }
-  if (kInt && c.fused && !st->done) {
-    // the pool buffer this step's partition builds its child's histogram in
-    // (the next new leaf's, num_leaves_cur: no leaf holds it yet)
-    long long* z = reinterpret_cast<long long*>(s.hist) + (size_t)st->num_leaves_cur * c.total_bins;
-    const size_t n = (size_t)c.total_bins;
-    const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x, ctas = (size_t)gridDim.x * gridDim.y;
-    for (size_t i = cta * blockDim.x + threadIdx.x; i < n; i += ctas * blockDim.x) z[i] = 0;
-  }
   scan_item<kInt>(c, s, blockIdx.x, blockIdx.y, *reinterpret_cast<ScanSmem*>(smem_raw));
 }
 template __global__ void k_scan<false, 1>(const __grid_constant__ DCtx);
@@ -1501,7 +1495,7 @@ __device__ __forceinline__ unsigned long long pack_status(uint32_t epoch, unsign
 // What partition_finalize reads, loaded before apply_split runs so that the
 // two sets of loads overlap.
 struct FinalizeIn {
-  int32_t begin, cnt, side, buf_L, depth, status;
+  int32_t begin, cnt, gcnt, side, buf_L, depth, status;
   DLeafSplits ls0, rs0;
 };
 
@@ -1509,6 +1503,7 @@ __device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L,
   FinalizeIn f;
   f.begin = s.leaf_begin[L];
   f.cnt = s.leaf_count[L];
+  f.gcnt = s.leaf_gcount[L];
   f.side = s.leaf_side[L];
   f.buf_L = s.buf_of[L];
   f.depth = s.tree.leaf_depth[L] + 1;  // both children's depth after the split
@@ -1518,37 +1513,35 @@ __device__ __forceinline__ FinalizeIn finalize_inputs(const DSlot& s, int32_t L,
   return f;
 }
 
-// built_left: -1 when the next histogram launch builds the smaller child
-// (chosen by the actual counts, learner/mod.rs:1200-1208); 0 / 1 when this
-// step's partition has already built the right / left child's histogram in
-// buffer R. That child then takes the "smaller" role (its histogram is built,
-// the other one's is parent - built). For integer histograms the two roles
-// give the same sums, so only which buffer holds which leaf changes.
+// gleft: every rank's rows sent left (data-parallel growth), or -1: this
+// rank's total_left is the whole count.
 __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int32_t R, int32_t total_left,
-                                   const FinalizeIn& fin, int built_left = -1) {
+                                   const FinalizeIn& fin, int32_t gleft = -1) {
   DSlotState* st = s.st;
   const DParams& p = c.p;
   const int32_t begin = fin.begin, cnt = fin.cnt, side = fin.side, buf_L = fin.buf_L, depth = fin.depth;
   const DLeafSplits ls0 = fin.ls0, rs0 = fin.rs0;
   const int32_t status = fin.status;
-  const int32_t nl = total_left, nr = cnt - total_left;
+  const int32_t nl = total_left, nr = cnt - total_left;  // this rank's rows: the ranges
+  const int32_t gl = gleft >= 0 ? gleft : nl, gr = gleft >= 0 ? fin.gcnt - gleft : nr;  // the counts
   s.leaf_count[L] = nl;
   s.leaf_begin[R] = begin + nl;
   s.leaf_count[R] = nr;
+  s.leaf_gcount[L] = gl;
+  s.leaf_gcount[R] = gr;
   s.leaf_side[L] = 1 - side;
   s.leaf_side[R] = 1 - side;
   const DTree& t = s.tree;
   const int32_t node = R - 1;
-  t.leaf_count[L] = nl;
-  t.leaf_count[R] = nr;
-  t.internal_count[node] = nl + nr;
+  t.leaf_count[L] = gl;
+  t.leaf_count[R] = gr;
+  t.internal_count[node] = gl + gr;
   DLeafSplits ls = ls0, rs = rs0;
-  ls.num_data = nl;
-  rs.num_data = nr;
+  ls.num_data = gl;
+  rs.num_data = gr;
   int32_t new_status = status;
-  const bool left_smaller = built_left < 0 ? nl < nr : built_left != 0;
-  if (min(nl, nr) <= 0 && status == kStatusOk) new_status = kStatusEmptyChild;
-  if (built_left >= 0) st->hist_rows += left_smaller ? nl : nr;
+  const bool left_smaller = gl < gr;  // learner/mod.rs:1200-1208
+  if ((left_smaller ? gl : gr) <= 0 && status == kStatusOk) new_status = kStatusEmptyChild;
   st->smaller = left_smaller ? ls : rs;
   st->larger = left_smaller ? rs : ls;
   if (new_status != kStatusOk) {
@@ -1574,7 +1567,7 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int
   // before_find_best_split (learner/mod.rs:712-731) on the values just written
   bool need = true;
   if (p.max_depth > 0 && depth >= p.max_depth) need = false;
-  else if (nr < p.min_data_in_leaf * 2 && nl < p.min_data_in_leaf * 2) need = false;
+  else if (gr < p.min_data_in_leaf * 2 && gl < p.min_data_in_leaf * 2) need = false;
   if (!need) {
     s.best[L].gain = -INFINITY;
     s.bgain[L] = -INFINITY;
@@ -1611,6 +1604,8 @@ struct SplitDecision {
   int32_t wfeat[32], wleaf[32];
   int32_t bl;            // the leaf to split, -1: the tree is finished
 };
+static_assert(sizeof(SplitDecision) <= kDpDecBytes, "the data-parallel decision buffer is too small");
+
 
 // Best split of a new leaf over its features and its per-feature splittable
 // flags (learner/mod.rs:842-849, :1066-1086); one warp.
@@ -1734,7 +1729,7 @@ __device__ void decide_split(const DCtx& c, const DSlot& s, const StepHead& h, S
 // choice and before_find_best_split are recorded. Every other CTA of the
 // launch has exited, so none of them reads the state changed here.
 __device__ void finish_step(const DCtx& c, const DSlot& s, const StepHead& h, const SplitDecision& d, int32_t bl,
-                            int32_t R, int32_t cnt, int built_left = -1) {
+                            int32_t R, int32_t cnt, int32_t gleft = -1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   DSlotState* st = s.st;
   const int32_t nf = c.num_features;
@@ -1802,7 +1797,7 @@ __device__ void finish_step(const DCtx& c, const DSlot& s, const StepHead& h, co
   if (tid == 0) {
     apply_split(c, s, bl, R, ain);
   } else if (tid == 32) {
-    partition_finalize(c, s, bl, R, total_left, fin, built_left);
+    partition_finalize(c, s, bl, R, total_left, fin, gleft);
     st->part_epoch += 1;
     // every CTA of the launch has passed its last use of the step counters
     st->part_ticket = 0;
@@ -1824,7 +1819,6 @@ struct PartShared {
 // The leaf a step splits: its rows and the feature its split tests.
 struct SplitLeaf {
   int32_t L, begin, cnt, side, inner;
-  bool est_left_smaller;  // the scan's estimated counts (split.rs:229-231): left < right
 };
 
 // Step prologue of a partition CTA: the split decision and, when a leaf is
@@ -1846,7 +1840,6 @@ __device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const Ste
   sl.cnt = s.leaf_count[L];
   sl.side = s.leaf_side[L];
   sl.inner = info.inner;
-  sl.est_left_smaller = info.left_count < info.right_count;
   if (threadIdx.x < kMaxBins / 16)
     reinterpret_cast<uint4*>(ps.lut)[threadIdx.x] = reinterpret_cast<const uint4*>(lut)[threadIdx.x];
   return sl;
@@ -1856,12 +1849,10 @@ __device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const Ste
 // the per-thread left counts, the decoupled look-back for the tile's prefix,
 // then the scatter (left rows ascending from the range start, right rows
 // descending from its end). The CTA of the last tile posts the left count.
-// excl_out / tile_left_out: the left rows of the tile before this thread's,
-// and in the whole tile.
 template <int kItems>
 __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32_t ntiles, uint32_t epoch, int32_t t0,
                              int32_t cnt, const uint32_t (&rows)[kItems], uint32_t flags, int32_t nleft,
-                             uint32_t* out, int32_t* excl_out = nullptr, int32_t* tile_left_out = nullptr) {
+                             uint32_t* out) {
   DSlotState* st = s.st;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // block exclusive scan of per-thread left counts
@@ -1946,8 +1937,6 @@ __device__ void tile_scatter(const DSlot& s, PartShared& ps, int32_t tile, int32
       }
     }
     if (tile == ntiles - 1 && tid == 0) st->part_left = prefix + tile_left;
-    if (excl_out) *excl_out = excl;
-    if (tile_left_out) *tile_left_out = tile_left;
 }
 
 // Row tiles of the split leaf L claimed in order by the CTAs (kItems rows
@@ -2038,8 +2027,59 @@ __device__ __forceinline__ void partition_body(const DCtx& c, const DSlot& s, Pa
   __syncthreads();
   if (ps.last) {
     __threadfence();
-    finish_step(c, s, h, ps.dec, L, R, sl.cnt);
+    if (c.dp) {
+      // data-parallel: the step ends in k_dp_finish once the left rows of every
+      // rank are summed; the decision and this rank's left rows wait for it
+      const uint32_t* from = reinterpret_cast<const uint32_t*>(&ps.dec);
+      uint32_t* to = reinterpret_cast<uint32_t*>(s.dp_dec);
+      for (int i = tid; i < (int)(sizeof(SplitDecision) / 4); i += blockDim.x) to[i] = from[i];
+      if (tid == 0) s.dp_left[0] = sl.cnt > 0 ? *reinterpret_cast<volatile int32_t*>(&st->part_left) : 0;
+    } else {
+      finish_step(c, s, h, ps.dec, L, R, sl.cnt);
+    }
   }
+}
+
+// Data-parallel growth: the end of a split step (finish_step) after the
+// partition, with dp_left[0] holding the rows every rank sent left. Grid
+// (1, 1, slots), kPartThreads threads.
+__global__ void __launch_bounds__(kPartThreads) k_dp_finish(const __grid_constant__ DCtx c) {
+  const DSlot& s = c.slots[blockIdx.z];
+  __shared__ SplitDecision dec;
+  const StepHead h = load_step_head(s.st);
+  if (h.done) return;
+  const uint32_t* from = reinterpret_cast<const uint32_t*>(s.dp_dec);
+  uint32_t* to = reinterpret_cast<uint32_t*>(&dec);
+  for (int i = threadIdx.x; i < (int)(sizeof(SplitDecision) / 4); i += blockDim.x) to[i] = from[i];
+  __syncthreads();
+  const int32_t L = dec.bl;
+  if (L < 0) return;
+  finish_step(c, s, h, dec, L, h.R, s.leaf_count[L], s.dp_left[0]);
+}
+
+// Data-parallel growth: the root's sums of this rank out (sum_g, sum_h as
+// f64; the packed integer sum and the row count as i64), and back in once
+// summed over the ranks, with what k_tree_init derived from them. Grid (1, 1, slots).
+__global__ void k_dp_root_pack(const __grid_constant__ DCtx c, double* f, long long* q) {
+  const DSlotState* st = c.slots[blockIdx.z].st;
+  f[2 * blockIdx.z] = st->smaller.sum_gradients;
+  f[2 * blockIdx.z + 1] = st->smaller.sum_hessians;
+  q[2 * blockIdx.z] = (long long)st->smaller.int_sum;
+  q[2 * blockIdx.z + 1] = (long long)st->smaller.num_data;
+}
+
+__global__ void k_dp_root_apply(const __grid_constant__ DCtx c, const double* f, const long long* q) {
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  const double a = f[2 * blockIdx.z], b = f[2 * blockIdx.z + 1];
+  const int32_t n = (int32_t)q[2 * blockIdx.z + 1];
+  st->smaller.sum_gradients = a;
+  st->smaller.sum_hessians = b;
+  st->smaller.int_sum = (int64_t)q[2 * blockIdx.z];
+  st->smaller.num_data = n;
+  s.leaf_gcount[0] = n;
+  s.tree.leaf_value[0] = maybe_round_to_zero(root_output(a, b, c.p, n));
+  st->need_find = before_find_best_split(c, s, 0, -1) ? 1 : 0;
 }
 
 // Grid (G, 1, slots), kPartThreads threads. Every CTA first derives the
@@ -2097,195 +2137,6 @@ __global__ void __launch_bounds__(kPartThreads) k_scan_partition(const __grid_co
 template __global__ void k_scan_partition<false>(const __grid_constant__ DCtx);
 template __global__ void k_scan_partition<true>(const __grid_constant__ DCtx);
 
-
-// =====================================================================================
-// Fused partition and histogram (quantized form, at most 32 features): the
-// partition of the split leaf also builds the histogram of the child the
-// scan's estimated counts make the smaller one (split.rs:229-231), into
-// pool buffer R (zeroed by the scan before this launch). No histogram launch
-// follows; the next scan reads the built child and forms the other as
-// parent - built (histogram.rs:59-63). With integer sums both are exact
-// whichever child is built, so a wrong estimate only swaps which child is
-// built. Each row's 32-byte bin segment is read whole: it holds the split
-// feature's value (no column-major gather) and every feature's bin.
-// =====================================================================================
-constexpr int kFusedThreads = 512;
-constexpr int kFusedItems = kPartTileRows / kFusedThreads;
-constexpr int kFusedCells = kMaxBins * 32;  // one group of 32 features
-
-size_t fused_smem_bytes() {
-  return (size_t)kFusedCells * 4 + (size_t)kPartTileRows * 32 + (size_t)kPartTileRows * 4;
-}
-
-__global__ void __cluster_dims__(kHistCluster, 1, 1) __launch_bounds__(kFusedThreads, 1)
-    k_partition_fused(const __grid_constant__ DCtx c, int32_t sub_rows) {
-  namespace cg = cooperative_groups;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  int32_t* cells = reinterpret_cast<int32_t*>(smem_raw);  // [raw][lane]
-  uint4* sbins = reinterpret_cast<uint4*>(smem_raw + (size_t)kFusedCells * 4);
-  int32_t* sq = reinterpret_cast<int32_t*>(sbins + 2 * kPartTileRows);
-  __shared__ PartShared ps;
-  __shared__ int32_t s_vlen[32], s_vstart[32];
-  const DSlot& s = c.slots[blockIdx.z];
-  DSlotState* st = s.st;
-  // done changes during this launch only where every CTA returns here too
-  const StepHead hd = load_step_head(st);
-  if (hd.done) return;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int32_t R = hd.R;
-  const uint32_t epoch = hd.epoch;
-  const SplitLeaf sl = partition_prologue(c, s, hd, ps);
-  const int32_t L = sl.L;
-  // every CTA of a cluster takes the same decision, so all of them return here or none
-  if (L < 0) {
-    if (blockIdx.x == 0 && tid == 0) st->done = 1;
-    return;
-  }
-  const int32_t nf = c.num_features;
-  if (tid < 32) {
-    const bool ok = tid < nf;
-    s_vlen[tid] = ok ? c.feats[tid].view_len : 0;
-    s_vstart[tid] = ok ? c.feats[tid].view_start : 0;
-  }
-  {
-    uint4* z = reinterpret_cast<uint4*>(cells);
-    for (int i = tid; i < kFusedCells * 4 / 16; i += kFusedThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
-  }
-  __syncthreads();  // cells zeroed, feature facts and the LUT complete
-  const int32_t begin = sl.begin, cnt = sl.cnt, side = sl.side, inner = sl.inner;
-  const bool build_left = sl.est_left_smaller;
-  if (blockIdx.x == 0 && tid == 0) st->part_rows += cnt;
-  const uint32_t* in = s.idx[side] + begin;
-  uint32_t* out = s.idx[1 - side] + begin;
-  const int32_t ntiles = (cnt + kPartTileRows - 1) / kPartTileRows;
-  const size_t stride = (size_t)c.stride;
-  const uint8_t* lut = ps.lut;
-  long long* dst = reinterpret_cast<long long*>(s.hist) + (size_t)R * c.total_bins;
-  // adds cell i ([raw][lane]) holding (g << 16) + h to the built child's histogram
-  auto emit = [&](int i, int64_t g, int64_t h) {
-    const int raw = i >> 5, fl = i & 31;
-    if (raw == 0 || raw > s_vlen[fl] || (g == 0 && h == 0)) return;
-    atomicAdd(reinterpret_cast<unsigned long long*>(dst + s_vstart[fl] + raw - 1),
-              (unsigned long long)((uint64_t)(g << 32) + (uint64_t)h));
-  };
-  auto decode = [](int32_t cell, int64_t& g, int64_t& h) {
-    h = (int64_t)(cell & 0xFFFF);
-    g = (int64_t)((cell - (int32_t)h) >> 16);
-  };
-  int32_t since_flush = 0;
-  while (cnt > 0) {
-    __syncthreads();
-    if (tid == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
-    __syncthreads();
-    const int32_t tile = ps.tile;
-    if (tile >= ntiles) break;
-    const int32_t t0 = tile * kPartTileRows;
-    uint32_t rows[kFusedItems];
-    int32_t q[kFusedItems];
-    uint4 b0[kFusedItems], b1[kFusedItems];
-    uint32_t flags = 0;
-    int32_t nleft = 0;
-#pragma unroll
-    for (int k = 0; k < kFusedItems; ++k) {
-      const int32_t pos = t0 + tid * kFusedItems + k;
-      rows[k] = pos < cnt ? __ldcg(in + pos) : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < kFusedItems; ++k) {
-      const bool live = t0 + tid * kFusedItems + k < cnt;
-      const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)rows[k] * stride);
-      q[k] = live ? __ldg(s.packed + rows[k]) : 0;
-      b0[k] = live ? __ldg(src) : make_uint4(0u, 0u, 0u, 0u);
-      b1[k] = live ? __ldg(src + 1) : make_uint4(0u, 0u, 0u, 0u);
-    }
-#pragma unroll
-    for (int k = 0; k < kFusedItems; ++k) {
-      if (t0 + tid * kFusedItems + k >= cnt) continue;
-      const uint4 v = inner < 16 ? b0[k] : b1[k];
-      const int wsel = (inner >> 2) & 3;
-      const uint32_t w = wsel == 0 ? v.x : (wsel == 1 ? v.y : (wsel == 2 ? v.z : v.w));
-      if (lut[(w >> ((inner & 3) * 8)) & 0xFFu]) {
-        flags |= 1u << k;
-        ++nleft;
-      }
-    }
-    int32_t excl = 0, tile_left = 0;
-    tile_scatter<kFusedItems>(s, ps, tile, ntiles, epoch, t0, cnt, rows, flags, nleft, out, &excl, &tile_left);
-    // the built child's rows of the tile, compacted in tile order into shared
-    // memory: its rows before this thread's are the tile's left rows before
-    // them, or the rest of the positions before them
-    const int32_t valid = min(kPartTileRows, cnt - t0);
-    const int32_t nbuilt = build_left ? tile_left : valid - tile_left;
-    int32_t at = build_left ? excl : tid * kFusedItems - excl;
-#pragma unroll
-    for (int k = 0; k < kFusedItems; ++k) {
-      if (t0 + tid * kFusedItems + k >= cnt) continue;
-      if ((((flags >> k) & 1u) != 0) == build_left) {
-        sbins[2 * at] = b0[k];
-        sbins[2 * at + 1] = b1[k];
-        sq[at] = q[k];
-        ++at;
-      }
-    }
-    __syncthreads();
-    {
-      // lane l adds feature l of 32 rows per pass: every shared atomic of a
-      // warp hits 32 distinct banks
-      const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + lane;
-      for (int j0 = warp * 32; j0 < nbuilt; j0 += kFusedThreads) {
-        const int32_t myq = j0 + lane < nbuilt ? sq[j0 + lane] : 0;
-        const int jn = min(32, nbuilt - j0);
-        for (int j = 0; j < jn; ++j) {
-          const int32_t qq = __shfl_sync(0xffffffffu, myq, j);
-          const int raw = rowp[(j0 + j) * 32];
-          atomicAdd(cells + raw * 32 + lane, qq);
-        }
-      }
-    }
-    since_flush += kPartTileRows;
-    __syncthreads();
-    // int32 cells hold at most sub_rows rows before their 16-bit halves could wrap
-    if (since_flush + kPartTileRows > sub_rows) {
-      for (int i = tid; i < kFusedCells; i += kFusedThreads) {
-        int64_t g, h;
-        decode(cells[i], g, h);
-        emit(i, g, h);
-        cells[i] = 0;
-      }
-      since_flush = 0;
-      __syncthreads();
-    }
-  }
-  // cluster reduction: CTA rank r adds slice r of the cells, summed over the
-  // cluster's CTAs in rank order
-  cg::cluster_group cluster = cg::this_cluster();
-  cluster.sync();
-  {
-    const int per = kFusedCells / kHistCluster;
-    const int lo = (int)cluster.block_rank() * per;
-    for (int i = lo + tid; i < lo + per; i += kFusedThreads) {
-      int64_t g = 0, h = 0;
-#pragma unroll
-      for (int r = 0; r < kHistCluster; ++r) {
-        int64_t a, b;
-        decode(cluster.map_shared_rank(cells, r)[i], a, b);
-        g += a;
-        h += b;
-      }
-      emit(i, g, h);
-    }
-  }
-  cluster.sync();  // no CTA leaves while another may still read its cells
-  if (tid == 0) {
-    __threadfence();
-    ps.last = atomicAdd(&st->part_done, 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (ps.last) {
-    __threadfence();
-    finish_step(c, s, hd, ps.dec, L, R, cnt, build_left ? 1 : 0);
-  }
-}
 
 // Column-major copy of the bin matrix (the partition reads one feature of the
 // rows of a leaf, which are ascending, so neighbouring rows share sectors).
@@ -2448,7 +2299,7 @@ __global__ void __launch_bounds__(256) k_leaf_sums(const __grid_constant__ DCtx 
 // a leaf at rank r covering positions [b, e) adds segments w + r for
 // w = b / per ... (e - 1) / per, in that order.
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* partial, const int32_t* rank,
-                             int32_t nwarps) {
+                             int32_t nwarps, double* totals) {
   const DSlot& s = c.slots[blockIdx.z];
   DSlotState* st = s.st;
   const int32_t* rk = rank + (size_t)blockIdx.z * (c.p.num_leaves + 1);
@@ -2464,7 +2315,21 @@ __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* parti
         h += base[2 * (w + r) + 1];
       }
     }
-    s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(g, h, c.p, cnt));
+    if (totals) {  // data-parallel: this rank's sums, refit after the reduction over ranks
+      totals[((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2] = g;
+      totals[((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2 + 1] = h;
+    } else {
+      s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(g, h, c.p, s.leaf_gcount[leaf]));
+    }
+  }
+}
+
+// Data-parallel growth: leaf outputs from the per-leaf sums over every rank.
+__global__ void k_dp_leaf_apply(const __grid_constant__ DCtx c, const double* totals) {
+  const DSlot& s = c.slots[blockIdx.z];
+  for (int32_t leaf = threadIdx.x; leaf < s.st->num_leaves_cur; leaf += blockDim.x) {
+    const double* o = totals + ((size_t)blockIdx.z * c.p.num_leaves + leaf) * 2;
+    s.tree.leaf_value[leaf] = maybe_round_to_zero(refit_leaf_output(o[0], o[1], c.p, s.leaf_gcount[leaf]));
   }
 }
 

@@ -70,9 +70,11 @@ __global__ void __launch_bounds__(256) k_interleave(const float* g, const float*
 
 // max |g| and |h| (order-independent, exact); the last block derives the
 // scales exactly as quant.rs:429-430 does.
+// derive 0 (data-parallel): the last block leaves the maxima in maxbits for
+// the reduction over ranks; k_quant_scales derives the scales after it.
 __global__ void __launch_bounds__(256) k_quant_absmax(const float2* gh, int64_t n, unsigned long long* maxbits,
                                                       int32_t* counter, DSlotState* st, int32_t bins,
-                                                      int32_t const_hess, int32_t num_blocks) {
+                                                      int32_t const_hess, int32_t num_blocks, int32_t derive) {
   double mg = 0.0, mh = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float2 v = gh[i];
@@ -96,6 +98,10 @@ __global__ void __launch_bounds__(256) k_quant_absmax(const float2* gh, int64_t 
   __syncthreads();
   if (!last || threadIdx.x != 0) return;
   __threadfence();
+  if (!derive) {
+    *counter = 0;
+    return;
+  }
   double max_g = __longlong_as_double((long long)atomicAdd(&maxbits[0], 0ull));
   double max_h = __longlong_as_double((long long)atomicAdd(&maxbits[1], 0ull));
   st->grad_scale = max_g / (double)(bins / 2);
@@ -103,6 +109,17 @@ __global__ void __launch_bounds__(256) k_quant_absmax(const float2* gh, int64_t 
   maxbits[0] = 0;
   maxbits[1] = 0;
   *counter = 0;
+}
+
+// The scales from maxima taken over every rank, as the last
+// block of k_quant_absmax derives them (quant.rs:429-430). One thread.
+__global__ void k_quant_scales(unsigned long long* maxbits, DSlotState* st, int32_t bins, int32_t const_hess) {
+  const double max_g = __longlong_as_double((long long)maxbits[0]);
+  const double max_h = __longlong_as_double((long long)maxbits[1]);
+  st->grad_scale = max_g / (double)(bins / 2);
+  st->hess_scale = const_hess ? max_h : max_h / (double)bins;
+  maxbits[0] = 0;
+  maxbits[1] = 0;
 }
 
 // quant.rs:355-359 static_cast<int8_t>(double) as x86-64 compiles it.
@@ -117,7 +134,7 @@ __device__ __forceinline__ int32_t to_i8(double x) {
 __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n, const double* grv,
                                                      const double* hrv, const int64_t* start_dev,
                                                      const DSlotState* st, int32_t const_hess, int32_t stochastic,
-                                                     int32_t* packed) {
+                                                     int32_t* packed, int64_t row_offset, int64_t table_n) {
   const int64_t start = *start_dev;
   const double inv_g = 1.0 / st->grad_scale;
   const double inv_h = 1.0 / st->hess_scale;
@@ -126,8 +143,10 @@ __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n
     double g = (double)v.x;
     double rg = 0.5, rh = 0.5;
     if (stochastic) {
-      int64_t pos = i + start;  // (i + start) mod n, with i, start < n
-      if (pos >= n) pos -= n;
+      // (global row + start) mod the table length, with both below it
+      // (data-parallel: row_offset is this rank's first global row)
+      int64_t pos = row_offset + i + start;
+      if (pos >= table_n) pos -= table_n;
       rg = grv[pos];
       rh = hrv[pos];
     }

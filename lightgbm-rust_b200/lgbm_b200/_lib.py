@@ -99,6 +99,11 @@ class LaunchShape(C.Structure):
     _fields_ = [("partition_ctas", i32), ("hist_ctas", i32), ("hist_rows_per_block", i32)]
 
 
+# the data-parallel reduction callback: (device buffer, count, dtype, op, user) -> 0 on success
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, i64, i32, i32, C.c_void_p)
+DT_INT64, DT_FLOAT64, DT_INT32 = 0, 1, 2
+OP_SUM, OP_MAX = 0, 1
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "lgbm_b200_last_error": (C.c_char_p, []),
@@ -125,8 +130,9 @@ SIGNATURES = {
     "lgbm_b200_learner_autotune": (C.c_int, [C.c_void_p, P(LaunchShape), i32, i32, P(i32), P(f64)]),
     "lgbm_b200_learner_set_timing": (C.c_int, [C.c_void_p, i32]),
     "lgbm_b200_learner_last_timing": (C.c_int, [C.c_void_p, P(f64), P(i64), P(i32)]),
-    "lgbm_b200_learner_last_rows": (C.c_int, [C.c_void_p, P(i64), P(i64), P(i32)]),
+    "lgbm_b200_learner_last_rows": (C.c_int, [C.c_void_p, P(i64), P(i64)]),
     "lgbm_b200_learner_step_times": (C.c_int, [C.c_void_p, P(C.c_float), i32, P(i32)]),
+    "lgbm_b200_learner_set_data_parallel": (C.c_int, [C.c_void_p, i64, i64, ALLREDUCE_FN, C.c_void_p]),
     "lgbm_b200_learner_record": (C.c_int, [C.c_void_p, i32]),
     "lgbm_b200_learner_elapsed": (C.c_int, [C.c_void_p, i32, i32, P(f64)]),
     "lgbm_b200_learner_histogram": (C.c_int, [C.c_void_p, i32, P(C.c_uint32), i64, C.c_void_p]),

@@ -343,6 +343,26 @@ class Learner:
         L.check(L.lib().lgbm_b200_learner_last_timing(self.handle, ms, C.byref(rows), C.byref(launches)))
         return list(ms), int(rows.value), int(launches.value)
 
+    def set_data_parallel(self, row_offset, global_num_data, allreduce):
+        """Grow trees data-parallel: this learner holds rows [row_offset,
+        row_offset + its rows) of `global_num_data`, and allreduce(ptr, count,
+        dtype, op) reduces a device buffer of this learner's device in place
+        over every rank (dtype: L.DT_INT64 / DT_FLOAT64 / DT_INT32; op:
+        L.OP_SUM / OP_MAX). See data_parallel.py for torch.distributed ones."""
+        def cb(ptr, count, dtype, op, _user):
+            try:
+                allreduce(ptr, int(count), int(dtype), int(op))
+                return 0
+            except Exception:  # an exception must not cross the C boundary
+                import traceback
+
+                traceback.print_exc()
+                return 1
+
+        self._allreduce_cb = L.ALLREDUCE_FN(cb)  # kept alive with the learner
+        L.check(L.lib().lgbm_b200_learner_set_data_parallel(self.handle, int(row_offset), int(global_num_data),
+                                                            self._allreduce_cb, None))
+
     def step_times(self):
         """With timing on: (steps x 3) device ms of each split step's
         histogram, scan and partition launches in the last train call."""
@@ -353,10 +373,10 @@ class Learner:
         return ms.reshape(-1, 3)
 
     def last_rows(self):
-        """(rows histogrammed, rows partitioned, fused) of the last train call."""
-        h, pr, f = C.c_int64(), C.c_int64(), C.c_int32()
-        L.check(L.lib().lgbm_b200_learner_last_rows(self.handle, C.byref(h), C.byref(pr), C.byref(f)))
-        return int(h.value), int(pr.value), bool(f.value)
+        """(rows histogrammed, rows partitioned) of the last train call."""
+        h, pr = C.c_int64(), C.c_int64()
+        L.check(L.lib().lgbm_b200_learner_last_rows(self.handle, C.byref(h), C.byref(pr)))
+        return int(h.value), int(pr.value)
 
     def __del__(self):
         if getattr(self, "handle", None) is not None and L._lib is not None:

@@ -15,16 +15,14 @@ from conftest import TOL, binned_dataset, compare_boosted_trees, within
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(autouse=True, params=["per_step", "persistent", "fused", "scan_part"])
+@pytest.fixture(autouse=True, params=["per_step", "persistent", "scan_part"])
 def grow_mode(request, lgb, monkeypatch):
     """Every test runs with each launch strategy: the per-step graph (the
-    default), persistent growth, the fused partition + histograms (used by
-    the quantized form with at most 32 features), and the scans and the
-    partition of a step in one cooperative launch."""
+    default), persistent growth, and the scans and the partition of a step
+    in one cooperative launch."""
     from lgbm_b200 import basic
 
     monkeypatch.setitem(basic.DEFAULTS, "persistent_grow", request.param == "persistent")
-    monkeypatch.setenv("LGBM_B200_FUSED", "1" if request.param == "fused" else "0")
     monkeypatch.setenv("LGBM_B200_SCANPART", "1" if request.param == "scan_part" else "0")
     yield request.param
 
