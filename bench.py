@@ -744,6 +744,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--predict-trees", type=int, default=None,
+                    help="c4: train the model to this many trees before the batched prediction (the config's 300)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the AUC seeds, precision report, the 20k-row workload and the other workloads")
     ap.add_argument("--rounds", type=int, default=ROUNDS, help="rounds trained per form (AUC after these)")
@@ -757,7 +759,7 @@ def main():
     if args.autotune and int(os.environ.get("WORLD_SIZE", "1")) > 1:
         ap.error("--autotune records one device's choice: run it with one process")
     if args.workload != "c2":
-        print(json.dumps(run_workload(args)), flush=True)
+        print(json.dumps(run_workload(args, predict_trees=args.predict_trees)), flush=True)
         return
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
