@@ -79,6 +79,8 @@ struct DSlotState {
   double grad_scale, hess_scale;  // quantized gradients
   DLeafSplits smaller, larger;
   int32_t s_begin, s_side, s_buf;  // the smaller leaf's range start, index buffer and histogram buffer
+  int32_t s_count;                 // the smaller leaf's rows in this learner's range (data-parallel: this
+                                   // rank's; smaller.num_data counts every rank's)
   int32_t l_buf;                   // the larger leaf's histogram buffer
   int64_t hist_rows;       // rows histogrammed in this tree (statistics)
   int64_t part_rows;       // rows partitioned in this tree (statistics)

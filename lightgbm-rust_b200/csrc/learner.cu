@@ -847,6 +847,7 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   ss.need_find = 1;
   ss.smaller.leaf = 0;
   ss.smaller.num_data = (int32_t)cnt;
+  ss.s_count = (int32_t)cnt;
   ss.s_begin = 0;
   ss.s_side = 0;
   ss.s_buf = 0;

@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->smaller.leaf = 0;
   st->smaller.num_data = (int32_t)n;
   st->s_begin = 0;
+  st->s_count = (int32_t)n;
   st->s_side = 0;
   st->s_buf = 0;
   st->l_buf = -1;
@@ -255,7 +256,7 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int ra
                                            int64_t& r0, int64_t& r1) {
   DSlotState* st = s.st;
   // every field read at once
-  const int32_t done = st->done, need = st->need_find, count_s = st->smaller.num_data, begin_s = st->s_begin,
+  const int32_t done = st->done, need = st->need_find, count_s = st->s_count, begin_s = st->s_begin,
                 side_s = st->s_side, buf_s = st->s_buf;
   if (done || !need) return false;
   lr.buf = buf_s;
@@ -1559,6 +1560,7 @@ __device__ void partition_finalize(const DCtx& c, const DSlot& s, int32_t L, int
   }
   // the next step's histogram and scan read these instead of the leaf arrays
   st->s_begin = left_smaller ? begin : begin + nl;
+  st->s_count = left_smaller ? nl : nr;
   st->s_side = 1 - side;
   st->s_buf = R;
   st->l_buf = buf_L;

@@ -12,9 +12,7 @@
 // Each thread sums, per class k, the leaf values of trees k, k + ntpi, ... in
 // model order, which is the reference's summation order for that class
 // (predict.rs:231-339), so the FP64 sums are the reference's. Any number of
-// classes works: no per-class array is kept. A thread walks kWalk trees of
-// its class together, so that their node loads (each depends on the last of
-// its own tree) are in flight at the same time.
+// classes works: no per-class array is kept.
 #include <mutex>
 
 #include "predict.h"
@@ -24,7 +22,6 @@ namespace lgbm_b200 {
 constexpr int kPredictThreads = 128;
 constexpr int kStageMaxCols = 223;  // 128 rows x 224 floats = 112 KiB of shared memory
 constexpr int kMaxPredictDevices = 64;
-constexpr int kWalk = 4;  // trees a thread walks at once
 
 __device__ __forceinline__ bool find_in_bitset(const uint32_t* bits, int32_t n, int32_t pos) {  // tree.rs:46-52
   int32_t i1 = pos / 32;
@@ -113,26 +110,14 @@ __global__ void __launch_bounds__(kPredictThreads) k_predict(DForest f, const fl
   const int ntpi = f.ntpi;
   for (int k = 0; k < ntpi; ++k) {
     double acc = 0.0;
-    // kWalk trees of class k at once: their dependent node loads overlap;
-    // the leaf values are then added in model order
-    for (int32_t t0 = k; t0 < f.num_trees; t0 += kWalk * ntpi) {
-      int4 tt[kWalk];
-      int32_t node[kWalk];
-#pragma unroll
-      for (int j = 0; j < kWalk; ++j) {
-        const int32_t t = t0 + j * ntpi;
-        tt[j] = t < f.num_trees ? f.tree[t] : make_int4(0, 0, 1, 0);  // first node, first leaf, num_leaves
-        node[j] = tt[j].z > 1 ? 0 : ~0;                              // a one-leaf tree is leaf 0
-      }
-      bool more = true;
-      while (more) {
-        more = false;
-#pragma unroll
-        for (int j = 0; j < kWalk; ++j) {
-          if (node[j] < 0) continue;
+    for (int32_t t = k; t < f.num_trees; t += ntpi) {
+      const int4 tt = f.tree[t];  // first node, first leaf, num_leaves
+      int32_t node = 0;
+      if (tt.z > 1) {
+        while (node >= 0) {
           double thr;
           int32_t fd, l, rc;
-          load_node(nodes, tt[j].x + node[j], thr, fd, l, rc);
+          load_node(nodes, tt.x + node, thr, fd, l, rc);
           const int32_t feat = fd & ((1 << kNodeFeatureBits) - 1);
           // features past the row read 0.0
           double v = 0.0;
@@ -143,13 +128,11 @@ __global__ void __launch_bounds__(kPredictThreads) k_predict(DForest f, const fl
               v = (double)drop_tiny(row[feat]);
             }
           }
-          node[j] = goes_left(f, thr, (int8_t)(fd >> kNodeFeatureBits), v) ? l : rc;
-          more |= node[j] >= 0;
+          node = goes_left(f, thr, (int8_t)(fd >> kNodeFeatureBits), v) ? l : rc;
         }
+        node = ~node;
       }
-#pragma unroll
-      for (int j = 0; j < kWalk; ++j)
-        if (t0 + j * ntpi < f.num_trees) acc += f.leaf_value[tt[j].y + ~node[j]];
+      acc += f.leaf_value[tt.y + node];
     }
     out[r * ntpi + k] = acc;
   }
