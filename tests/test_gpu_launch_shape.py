@@ -172,3 +172,21 @@ def test_wide_scan_grows_the_same_trees(lgb, monkeypatch, form):
         _same(a, b, exact=form == "quantized")
         categorical |= bool(np.any(np.asarray(a["decision_type"]) & 1))
     assert categorical  # the categorical scan ran in both variants
+
+
+@pytest.mark.parametrize("groups", ["2", "3", "4"])
+def test_lane_groups_per_tile_grow_the_same_trees(lgb, monkeypatch, groups):
+    """The quantized histogram's 32-feature lane groups per feature tile
+    (LGBM_B200_HIST_GROUPS; default 1) change the tiling only: 150 features
+    in 5 tiles of one group, or 3 / 2 / 2 tiles of several, grow the same
+    trees, exactly."""
+    X, y = _data(60_000, f=150, seed=4)
+    params = _params("quantized")
+    ds = binned_dataset(lgb, X, y, params)
+    monkeypatch.setenv("LGBM_B200_HIST_GROUPS", "1")
+    base = lgb.Learner(ds, params)
+    monkeypatch.setenv("LGBM_B200_HIST_GROUPS", groups)
+    other = lgb.Learner(ds, params)
+    for it in range(2):
+        g, h = _grads(lgb, params, y, 1, 200 + it)
+        _same(base.train(g, h)[0], other.train(g, h)[0], exact=True)
