@@ -82,6 +82,15 @@ struct DSlotState {
   int32_t s_count;                 // the smaller leaf's rows in this learner's range (data-parallel: this
                                    // rank's; smaller.num_data counts every rank's)
   int32_t l_buf;                   // the larger leaf's histogram buffer
+  // A split step whose end (finish_step) runs beside the next histogram
+  // launch's row CTAs: the partition posts the split leaf's rows and the
+  // decision here. The histogram's row CTAs derive the smaller child's range
+  // from them and the left count, and read nothing the step's end writes.
+  int32_t pending;                 // 1: the posted step has not been finished
+  int32_t pd_bl, pd_begin, pd_cnt, pd_side, pd_depth;  // the split leaf, its rows, its children's depth
+  int32_t pd_need, pd_S, pd_G, pd_Lft, pd_R;            // the step's head
+  int32_t pd_bf[2];                // the new leaves' best candidates (inner feature, -1 none)
+  double pd_bg[2];                 // and their penalized gains
   int64_t hist_rows;       // rows histogrammed in this tree (statistics)
   int64_t part_rows;       // rows partitioned in this tree (statistics)
 };
@@ -160,6 +169,7 @@ struct DCtx {
   int32_t num_slots;
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
   int32_t dp;              // 1: rows sharded over ranks; the step's end waits for the global left count
+  int32_t defer;           // 1: a partition posts its step's end for the next histogram launch to run
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

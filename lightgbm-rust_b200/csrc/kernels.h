@@ -53,12 +53,14 @@ struct ScanSmem {
 
 __global__ void k_tree_init(const __grid_constant__ DCtx c, const uint32_t* bag, const int32_t* n_used);
 template <int kMode, int kNG>
-__global__ void k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows);
+__global__ void k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows, int32_t lead);
 // dynamic shared memory, kernel and launch of the histogram for a form and groups per tile
 size_t hist_smem_bytes(int mode, int ng);
 const void* hist_kernel(int mode, int ng);
+// finish: one more cluster whose first CTA runs the previous split step's end,
+// which the partition posted (DCtx::defer)
 cudaError_t launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
-                        int32_t sub_rows, bool pdl);
+                        int32_t sub_rows, bool pdl, bool finish);
 
 // A kernel launch, optionally with programmatic stream serialisation (the
 // kernel may start launching while its predecessor in the stream runs; it
@@ -117,6 +119,9 @@ size_t grow_smem_bytes(int mode, int ng);
 cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
                         int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns);
 __global__ void k_partition(const __grid_constant__ DCtx c);
+// the last split step's end, when the partitions post theirs (DCtx::defer);
+// grid (1, 1, slots), kPartThreads threads
+__global__ void k_finish(const __grid_constant__ DCtx c);
 __global__ void k_transpose_bins(const uint8_t* bins, int64_t n, int32_t stride, int32_t nf, uint8_t* colbins);
 __global__ void k_leaf_sums(const __grid_constant__ DCtx c, double* partial, int32_t* rank);
 __global__ void k_leaf_renew(const __grid_constant__ DCtx c, const double* partial, const int32_t* rank,

@@ -294,6 +294,11 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   c.total_bins = h->total_bins;
   c.hist_mode = mode;
   c.bagging = 0;
+  // each partition posts its step's end for the next histogram launch (one
+  // leading CTA) to run beside the row CTAs, off the step's critical path
+  c.defer = 1;
+  // LGBM_B200_DEFER=0: the partition's last CTA ends the step itself (A/B)
+  if (const char* e = std::getenv("LGBM_B200_DEFER")) c.defer = std::atoi(e) != 0;
   c.feats = feats_d;
   DParams& p = c.p;
   p.lambda_l1 = cfg->lambda_l1;
@@ -382,7 +387,8 @@ Status enqueue_tree(LgbmB200Learner* h) {
     // (not when events are recorded between them)
     const int pdl_edges = h->timing ? 0 : h->use_pdl;
     const bool pdl = (pdl_edges & 1) != 0, pdl_scan = (pdl_edges & 2) != 0, pdl_part = (pdl_edges & 4) != 0;
-    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0));
+    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, pdl && step > 0,
+                   c.defer && step > 0));
     if (ev) CU(cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal));
     if (h->scan_part) {  // scans and partition in one launch: the scan interval records as empty
       if (ev) CU(cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal));
@@ -405,6 +411,12 @@ Status enqueue_tree(LgbmB200Learner* h) {
     CU(launch_ex(k_partition, part_grid, dim3(256), 0, s, pdl_part, c));
     if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
   }
+  // the last split step's end (the earlier ones ran beside the histograms)
+  const bool tail = c.defer && !h->cfg.persistent_grow && L > 1;
+  if (tail) {
+    k_finish<<<dim3(1, 1, K), kPartThreads, 0, s>>>(c);
+    CU_LAUNCH();
+  }
   if (mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) {
     k_leaf_sums<<<dim3(leaf_sum_warps(h) / 8, 1, K), 256, 16 * (size_t)L, s>>>(c, h->leaf_sums, h->leaf_rank);
     CU_LAUNCH();
@@ -413,7 +425,7 @@ Status enqueue_tree(LgbmB200Learner* h) {
   }
   h->last_launches = 1 + (h->cfg.persistent_grow ? 1 : (h->scan_part ? 2 * (L - 1)
                                                                                    : 3 * (L - 1))) +
-                     ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
+                     (tail ? 1 : 0) + ((mode == LGBM_B200_HIST_QUANT && h->cfg.quant_train_renew_leaf) ? 2 : 0);
   return Status();
 }
 
@@ -468,7 +480,7 @@ static Status run_tree_dp(LgbmB200Learner* h) {
     CU(cudaMemcpyAsync(&ss, d.st, sizeof(ss), cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (ss.done) break;
-    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false));
+    CU(launch_hist(mode, h->hist_ng, hist_grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false, false));
     if (ss.need_find) {  // the smaller leaf's histogram, summed over the ranks
       void* buf = static_cast<char*>(d.hist) + (size_t)ss.s_buf * cells * 8;
       const int32_t dt = mode == LGBM_B200_HIST_QUANT ? LGBM_B200_DT_INT64 : LGBM_B200_DT_FLOAT64;
@@ -861,6 +873,7 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   ss.s_begin = 0;
   ss.s_side = 0;
   ss.s_buf = 0;
+  ss.pending = 0;
   CU(cudaMemcpyAsync(d.st, &ss, sizeof(ss), cudaMemcpyHostToDevice, s));
   const int mode = h->cfg.hist_precision;
   const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
@@ -869,7 +882,7 @@ Status histogram_of_rows(LgbmB200Learner* h, int slot, const uint32_t* rows, int
   DCtx c = h->ctx;
   c.slots[0] = h->ctx.slots[slot];
   dim3 grid(h->hist_grid, h->ntiles, 1);
-  CU(launch_hist(mode, h->hist_ng, grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false));
+  CU(launch_hist(mode, h->hist_ng, grid, h->hist_smem, s, c, h->tiles, h->sub_rows, false, false));
   CU_LAUNCH();
   CU(cudaMemcpyAsync(out, d.hist, cells * 8, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
@@ -1148,6 +1161,7 @@ int lgbm_b200_learner_set_data_parallel(LgbmB200Learner* h, int64_t row_offset, 
     return fail(s);
   h->ctx.slots[0] = d;
   h->ctx.dp = 1;
+  h->ctx.defer = 0;  // the step's end waits for the left count summed over the ranks
   h->scan_part = false;
   h->cfg.persistent_grow = 0;
   h->cfg.use_cuda_graph = 0;

@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(256) k_tree_init(const __grid_constant__ DCtx 
   st->scan_done = 0;
   st->part_ticket = 0;
   st->part_done = 0;
+  st->pending = 0;
   st->hist_rows = 0;
   st->part_rows = 0;
   st->smaller.leaf = 0;
@@ -258,11 +259,31 @@ __device__ __forceinline__ bool hist_setup(const DCtx& c, const DSlot& s, int ra
   // every field read at once
   const int32_t done = st->done, need = st->need_find, count_s = st->s_count, begin_s = st->s_begin,
                 side_s = st->s_side, buf_s = st->s_buf;
-  if (done || !need) return false;
-  lr.buf = buf_s;
-  lr.count = count_s;
-  lr.begin = begin_s;
-  lr.idx = side_s == 0 ? s.idx[0] : s.idx[1];
+  const int32_t pending = st->pending, pbegin = st->pd_begin, pcnt = st->pd_cnt, pside = st->pd_side,
+                pdepth = st->pd_depth, pR = st->pd_R, status = st->status, left = st->part_left;
+  if (pending) {
+    // The previous step's end runs beside this launch: the smaller child's
+    // range and before_find_best_split as partition_finalize derives them.
+    // (A step end that records a status sets done; either value read here
+    // leads to the same skip.)
+    if (done || status != kStatusOk) return false;
+    const int32_t nl = pcnt > 0 ? left : 0, nr = pcnt - nl;
+    const bool left_smaller = nl < nr;
+    const int32_t sc = left_smaller ? nl : nr;
+    if (sc <= 0) return false;
+    if (c.p.max_depth > 0 && pdepth >= c.p.max_depth) return false;
+    if (nr < c.p.min_data_in_leaf * 2 && nl < c.p.min_data_in_leaf * 2) return false;
+    lr.buf = pR;
+    lr.count = sc;
+    lr.begin = left_smaller ? pbegin : pbegin + nl;
+    lr.idx = pside == 0 ? s.idx[1] : s.idx[0];
+  } else {
+    if (done || !need) return false;
+    lr.buf = buf_s;
+    lr.count = count_s;
+    lr.begin = begin_s;
+    lr.idx = side_s == 0 ? s.idx[0] : s.idx[1];
+  }
   int64_t per = c.rows_per_block;
   int64_t active = min((int64_t)count, (lr.count + per - 1) / per);
   active = (active + kCl - 1) / kCl * kCl;
@@ -616,22 +637,32 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   }
 }
 
+__device__ void deferred_finish(const DCtx& c, const DSlot& s, void* dec_smem);
+
+// Grid (lead + row CTAs, feature tiles, slots). With lead > 0 (one cluster)
+// the first CTA of each slot runs the previous split step's end, which its
+// partition posted, while the row CTAs build the histogram.
 template <int kMode, int kNG>
 __global__ void __cluster_dims__(hist_cluster(kMode), 1, 1) __launch_bounds__(kHistThreads, 2)
-    k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows) {
+    k_hist(const __grid_constant__ DCtx c, DTileTable tt, int32_t sub_rows, int32_t lead) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_wait();
   pdl_trigger();
   const DSlot& s = c.slots[blockIdx.z];
+  if ((int)blockIdx.x < lead) {
+    if (blockIdx.x == 0 && blockIdx.y == 0) deferred_finish(c, s, smem_raw);
+    return;
+  }
+  const int rank = (int)blockIdx.x - lead;
   LeafRows lr;
   int64_t r0, r1;
-  if (!hist_setup<hist_cluster(kMode)>(c, s, blockIdx.x, gridDim.x, lr, r0, r1)) return;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) s.st->hist_rows += lr.count;
+  if (!hist_setup<hist_cluster(kMode)>(c, s, rank, (int)gridDim.x - lead, lr, r0, r1)) return;
+  if (rank == 0 && blockIdx.y == 0 && threadIdx.x == 0) s.st->hist_rows += lr.count;
   hist_body<kMode, kNG, hist_cluster(kMode)>(c, s, tt, blockIdx.y, lr, r0, r1, sub_rows, smem_raw);
 }
 
 #define LGBM_B200_HIST_INST(M, G) \
-  template __global__ void k_hist<M, G>(const __grid_constant__ DCtx, DTileTable, int32_t);
+  template __global__ void k_hist<M, G>(const __grid_constant__ DCtx, DTileTable, int32_t, int32_t);
 LGBM_B200_HIST_INST(0, 1)
 LGBM_B200_HIST_INST(1, 1)
 LGBM_B200_HIST_INST(2, 1)
@@ -657,13 +688,16 @@ const void* hist_kernel(int mode, int ng) {
 }
 
 cudaError_t launch_hist(int mode, int ng, dim3 grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
-                        int32_t sub_rows, bool pdl) {
-  if (mode == 0) return launch_ex(k_hist<0, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
-  if (mode == 1) return launch_ex(k_hist<1, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
-  if (ng == 1) return launch_ex(k_hist<2, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
-  if (ng == 2) return launch_ex(k_hist<2, 2>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
-  if (ng == 3) return launch_ex(k_hist<2, 3>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
-  return launch_ex(k_hist<2, 4>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows);
+                        int32_t sub_rows, bool pdl, bool finish) {
+  // the step-end CTA leads as one whole cluster, so the row CTAs' clusters keep their alignment
+  const int32_t lead = finish ? hist_cluster(mode) : 0;
+  grid.x += (unsigned)lead;
+  if (mode == 0) return launch_ex(k_hist<0, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
+  if (mode == 1) return launch_ex(k_hist<1, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
+  if (ng == 1) return launch_ex(k_hist<2, 1>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
+  if (ng == 2) return launch_ex(k_hist<2, 2>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
+  if (ng == 3) return launch_ex(k_hist<2, 3>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
+  return launch_ex(k_hist<2, 4>, grid, dim3(kHistThreads), smem, st, pdl, c, tt, sub_rows, lead);
 }
 
 // =====================================================================================
@@ -1821,6 +1855,7 @@ struct PartShared {
 // The leaf a step splits: its rows and the feature its split tests.
 struct SplitLeaf {
   int32_t L, begin, cnt, side, inner;
+  int32_t depth;  // the children's depth (CTA 0 of a deferring launch only)
 };
 
 // Step prologue of a partition CTA: the split decision and, when a leaf is
@@ -1842,6 +1877,7 @@ __device__ SplitLeaf partition_prologue(const DCtx& c, const DSlot& s, const Ste
   sl.cnt = s.leaf_count[L];
   sl.side = s.leaf_side[L];
   sl.inner = info.inner;
+  sl.depth = (c.defer && blockIdx.x == 0) ? s.tree.leaf_depth[L] + 1 : 0;
   if (threadIdx.x < kMaxBins / 16)
     reinterpret_cast<uint4*>(ps.lut)[threadIdx.x] = reinterpret_cast<const uint4*>(lut)[threadIdx.x];
   return sl;
@@ -2015,12 +2051,35 @@ __device__ __forceinline__ void partition_body(const DCtx& c, const DSlot& s, Pa
   const SplitLeaf sl = partition_prologue(c, s, h, ps);
   const int32_t L = sl.L;
   if (L < 0) {
-    if (blockIdx.x == 0 && tid == 0) st->done = 1;
+    if (blockIdx.x == 0 && tid == 0) {
+      st->done = 1;
+      st->pending = 0;
+    }
     return;
+  }
+  if (c.defer && blockIdx.x == 0 && tid == 0) {
+    // the step's end is left to the next histogram launch: post what it and
+    // the histogram's row CTAs need (the left count follows from the tiles)
+    st->pd_bl = L;
+    st->pd_begin = sl.begin;
+    st->pd_cnt = sl.cnt;
+    st->pd_side = sl.side;
+    st->pd_depth = sl.depth;
+    st->pd_need = h.need;
+    st->pd_S = h.S;
+    st->pd_G = h.G;
+    st->pd_Lft = h.Lft;
+    st->pd_R = R;
+    for (int k = 0; k < 2; ++k) {
+      st->pd_bf[k] = ps.dec.side_bf[k];
+      st->pd_bg[k] = ps.dec.side_bg[k];
+    }
+    st->pending = 1;
   }
   zero_hist_buffer(c, s, R, blockIdx.x, gridDim.x);
   if (blockIdx.x == 0 && tid == 0) st->part_rows += sl.cnt;
   partition_rows<kPartTileRows / kPartThreads>(c, s, ps, sl, h.epoch, true);
+  if (c.defer) return;
   __syncthreads();
   if (tid == 0) {
     __threadfence();
@@ -2097,8 +2156,47 @@ __global__ void __launch_bounds__(kPartThreads) k_partition(const __grid_constan
   // before every partition of a live tree)
   const StepHead h = load_step_head(s.st);
   if (threadIdx.x == 0) ps.tile = atomicAdd(&s.st->part_ticket, 1);
-  if (h.done) return;
+  if (h.done) {
+    // a step end that finished the tree ran beside the last histogram launch
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.st->pending = 0;
+    return;
+  }
   partition_body(c, s, ps, h);
+}
+
+// The end of a split step that a partition posted (finish_step with the
+// posted head and decision), by one whole CTA of at least kPartThreads
+// threads; dec_smem holds a SplitDecision. Nothing else of the launch reads
+// what it writes.
+__device__ void deferred_finish(const DCtx& c, const DSlot& s, void* dec_smem) {
+  DSlotState* st = s.st;
+  SplitDecision& d = *static_cast<SplitDecision*>(dec_smem);
+  // every field read at once (the same addresses in every thread)
+  const int32_t pending = st->pending, bl = st->pd_bl, cnt = st->pd_cnt;
+  StepHead h;
+  h.done = 0;
+  h.need = st->pd_need;
+  h.S = st->pd_S;
+  h.G = st->pd_G;
+  h.Lft = st->pd_Lft;
+  h.R = st->pd_R;
+  h.epoch = 0;
+  if (threadIdx.x < 2) {
+    d.side_bf[threadIdx.x] = st->pd_bf[threadIdx.x];
+    d.side_bg[threadIdx.x] = st->pd_bg[threadIdx.x];
+  }
+  if (threadIdx.x == 0) d.bl = bl;
+  __syncthreads();
+  if (!pending) return;
+  finish_step(c, s, h, d, bl, h.R, cnt);
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_finish(const __grid_constant__ DCtx c) {
+  __shared__ SplitDecision dec;
+  const DSlot& s = c.slots[blockIdx.z];
+  deferred_finish(c, s, &dec);
+  __syncthreads();
+  if (threadIdx.x == 0) s.st->pending = 0;
 }
 
 // Threshold scans, then the partition, of one step (one cooperative launch):
@@ -2114,7 +2212,10 @@ __global__ void __launch_bounds__(kPartThreads) k_scan_partition(const __grid_co
   __shared__ PartShared ps;
   const StepHead h = load_step_head(st);
   if (threadIdx.x == 0) ps.tile = atomicAdd(&st->part_ticket, 1);
-  if (h.done) return;  // no CTA of this launch sets done before every CTA has passed the wait below
+  if (h.done) {  // no CTA of this launch sets done before every CTA has passed the wait below
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->pending = 0;
+    return;
+  }
   const int nitems = 2 * c.num_features;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     scan_item<kInt>(c, s, it >> 1, it & 1, *reinterpret_cast<ScanSmem*>(smem_raw));
