@@ -170,6 +170,7 @@ struct DCtx {
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
   int32_t dp;              // 1: rows sharded over ranks; the step's end waits for the global left count
   int32_t defer;           // 1: a partition posts its step's end for the next histogram launch to run
+  int32_t hist_direct;     // 1: the quantized one-group histogram adds each row from registers (no staging)
 };
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

@@ -299,6 +299,10 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   c.defer = 1;
   // LGBM_B200_DEFER=0: the partition's last CTA ends the step itself (A/B)
   if (const char* e = std::getenv("LGBM_B200_DEFER")) c.defer = std::atoi(e) != 0;
+  // LGBM_B200_HIST_DIRECT=0: the quantized one-group histogram stages each
+  // tile of rows in shared memory first (A/B)
+  c.hist_direct = 1;
+  if (const char* e = std::getenv("LGBM_B200_HIST_DIRECT")) c.hist_direct = std::atoi(e) != 0;
   c.feats = feats_d;
   DParams& p = c.p;
   p.lambda_l1 = cfg->lambda_l1;

@@ -402,148 +402,244 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
       hv = (double)fl[2 * kGroupCells + k] + (double)fl[3 * kGroupCells + k];
     }
   };
-  // registers of the next tile: this thread's row of it
-  uint32_t nrow = 0;
-  int32_t nq = 0;
-  float2 ngh = make_float2(0.f, 0.f);
-  uint4 nb[2 * kNG];
-  // row indices run one tile ahead of the gathers that use them
-  auto load_idx = [&](int64_t pos) { return pos < r1 ? __ldcg(idx + pos) : 0u; };  // written by the partition
-  uint32_t idx_ahead = 0;
-  auto fetch = [&](int64_t pos, uint32_t row) {
-    const bool live = pos < r1;
-    nrow = row;
-    if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
-    else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
-    const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
+  bool direct = false;
+  if constexpr (kMode == 2 && kNG == 1) {
+    direct = c.hist_direct != 0;
+    if (direct) {
+      // Direct row loop (quantized, one lane group): no staging and no tile
+      // barriers. A warp takes its rows four at a time: lane l loads word
+      // a = l & 7 (features f0 + 4a .. f0 + 4a + 3) of row j = l >> 3 and in
+      // pass k (0..3) adds byte b = (k + j) & 3 of it, feature 4a + b, whose
+      // cell raw * 32 + 4a + b lies in bank 4a + b: the 32 lanes of every
+      // warp-wide atomic touch 32 different banks. A warp's batch is kU row
+      // quads; the next batch's words and gradients are in flight while this
+      // one is added, and the row indices one batch further ahead.
+      if (threadIdx.x < 32) {
+        s_vlen[threadIdx.x] = my_vlen;
+        s_vstart[threadIdx.x] = my_vstart;
+      }
+      constexpr int kU = 4;
+      constexpr int kBatch = 4 * kU;                   // rows per warp and batch
+      constexpr int64_t kStep = (int64_t)kWarps * kBatch;  // rows per CTA and batch
+      const int j = lane >> 3, a = lane & 7;
+      int32_t* icells = reinterpret_cast<int32_t*>(cells);
+      const uint32_t* wbase = reinterpret_cast<const uint32_t*>(c.bins + f0) + a;
+      const size_t wstride = stride / 4;  // the row stride is a multiple of 32 bytes
+      int fk[4], sk[4];
 #pragma unroll
-    for (int k = 0; k < 2 * kNG; ++k)
-      nb[k] = (live && (k >> 1) < ngroups) ? __ldg(src + k) : make_uint4(0u, 0u, 0u, 0u);
-  };
-  {
-    const uint32_t first = load_idx(r0 + threadIdx.x);
-    idx_ahead = load_idx(r0 + kHistTileRows + threadIdx.x);
-    fetch(r0 + threadIdx.x, first);
-  }
-  if (threadIdx.x < 32 * kNG) {
-    s_vlen[threadIdx.x] = my_vlen;
-    s_vstart[threadIdx.x] = my_vstart;
-  }
-  int32_t since_flush = 0;
-  __syncthreads();
-  for (int64_t t0 = r0; t0 < r1; t0 += kHistTileRows) {
-    const int tile_rows = (int)min((int64_t)kHistTileRows, r1 - t0);
-    // stage this tile (the previous tile's accumulation has finished); rows
-    // past the range stage as zeros and add nothing
+      for (int k = 0; k < 4; ++k) {
+        const int b = (k + j) & 3;
+        fk[k] = 4 * a + b;
+        sk[k] = 8 * b;
+      }
+      for (int64_t seg0 = r0; seg0 < r1;) {
+        // int32 cells hold at most sub_rows rows of this CTA before their
+        // 16-bit halves could wrap
+        const int64_t seg1 = min(r1, seg0 + (int64_t)sub_rows);
+        int64_t b = seg0 + (int64_t)warp * kBatch;
+        uint32_t rid[kU], wn[kU];
+        int32_t qn[kU];
 #pragma unroll
-    for (int k = 0; k < 2 * kNG; ++k) sbins[threadIdx.x * 2 * kNG + k] = nb[k];
-    if (kMode == 2) sq[threadIdx.x] = nq;
-    else sgh[threadIdx.x] = ngh;
-    __syncthreads();
-    // the next tile's gathers run while this one is accumulated
-    if (t0 + kHistTileRows < r1) {
-      fetch(t0 + kHistTileRows + threadIdx.x, idx_ahead);
-      idx_ahead = load_idx(t0 + 2 * kHistTileRows + threadIdx.x);
-    }
-    const int rw0 = warp * kRowsPerWarp;
-    if (rw0 < tile_rows) {
-      // this warp's 32 staged rows; lane l adds feature f0 + 32 g + l of
-      // each row. The gradients of two or four rows arrive in one broadcast
-      // load.
-      const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + rw0 * kRowBytes + lane;
-      auto rows = [&](auto groups) {
-        constexpr int kG = decltype(groups)::value;
-        // rows per batch: every byte of a batch is loaded before its first
-        // atomic (the compiler cannot move loads past shared atomics that may
-        // alias them), so a batch waits for one shared-load latency
-        constexpr int kB = kG == 1 ? 8 : 4;
-#pragma unroll
-        for (int jb = 0; jb < kRowsPerWarp / kB; ++jb) {
-          int raw[kB][kG];
-#pragma unroll
-          for (int u = 0; u < kB; ++u)
-#pragma unroll
-            for (int g = 0; g < kG; ++g) raw[u][g] = (int)rowp[(kB * jb + u) * kRowBytes + 32 * g];
-          if constexpr (kMode == 2) {
-            int32_t qs[kB];
-#pragma unroll
-            for (int v = 0; v < kB / 4; ++v) {
-              const int4 q4 = reinterpret_cast<const int4*>(sq + rw0 + kB * jb)[v];
-              qs[4 * v] = q4.x;
-              qs[4 * v + 1] = q4.y;
-              qs[4 * v + 2] = q4.z;
-              qs[4 * v + 3] = q4.w;
-            }
-#pragma unroll
-            for (int u = 0; u < kB; ++u)
-#pragma unroll
-              for (int g = 0; g < kG; ++g)
-                atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + raw[u][g] * 32 + lane, qs[u]);
-          } else {
-            float gs[kB], hs[kB];
-#pragma unroll
-            for (int v = 0; v < kB / 2; ++v) {
-              const float4 t = reinterpret_cast<const float4*>(sgh + rw0 + kB * jb)[v];
-              gs[2 * v] = t.x;
-              hs[2 * v] = t.y;
-              gs[2 * v + 1] = t.z;
-              hs[2 * v + 1] = t.w;
-            }
-#pragma unroll
-            for (int u = 0; u < kB; ++u)
-#pragma unroll
-              for (int g = 0; g < kG; ++g) {
-                // float cells take a compare-and-swap loop per add: skip value 0
-                if (raw[u][g] == 0) continue;
-                const int k = raw[u][g] * 32 + lane;
-                const float gv = gs[u], hv = hs[u];
-                if constexpr (kMode == 0) {
-                  double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
-                  atomicAdd(d + k, (double)gv);
-                  atomicAdd(d + kGroupCells + k, (double)hv);
-                } else {
-                  float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
-                  float og = atomicAdd(fl + k, gv);
-                  float sg = __fadd_rn(og, gv);
-                  float bg = __fsub_rn(sg, og);
-                  atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv, bg)));
-                  float oh = atomicAdd(fl + 2 * kGroupCells + k, hv);
-                  float s2 = __fadd_rn(oh, hv);
-                  float bh = __fsub_rn(s2, oh);
-                  atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv, bh)));
-                }
-              }
-          }
+        for (int u = 0; u < kU; ++u) {
+          const int64_t pos = b + 4 * u + j;
+          rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
         }
-      };
-      // the group count is a compile-time constant inside the row loop
-      if (ngroups == kNG) {
-        rows(std::integral_constant<int, kNG>{});
-      } else {
-        if constexpr (kNG > 1) {
-          if (ngroups == 1) rows(std::integral_constant<int, 1>{});
-          else if constexpr (kNG > 2) {
-            if (ngroups == 2) rows(std::integral_constant<int, 2>{});
-            else if constexpr (kNG > 3) {
-              if (ngroups == 3) rows(std::integral_constant<int, 3>{});
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const bool v = b + 4 * u + j < seg1;
+          wn[u] = v ? __ldg(wbase + (size_t)rid[u] * wstride) : 0u;
+          qn[u] = v ? __ldg(s.packed + rid[u]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int64_t pos = b + kStep + 4 * u + j;
+          rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
+        }
+        // every cell is zeroed (above, or by the last flush) before the first add
+        if (seg0 == r0) __syncthreads();
+        for (; b < seg1; b += kStep) {
+          uint32_t w[kU];
+          int32_t q[kU];
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            w[u] = wn[u];
+            q[u] = qn[u];
+          }
+          const int64_t bn = b + kStep;
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const bool v = bn + 4 * u + j < seg1;
+            wn[u] = v ? __ldg(wbase + (size_t)rid[u] * wstride) : 0u;
+            qn[u] = v ? __ldg(s.packed + rid[u]) : 0;
+          }
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int64_t pos = bn + kStep + 4 * u + j;
+            rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
+          }
+          // rows past the segment hold word 0 and gradient 0: they add 0 to
+          // cell 0, which no feature view contains
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int u = 0; u < kU; ++u) atomicAdd(icells + ((w[u] >> sk[k]) & 0xFFu) * 32 + fk[k], q[u]);
+        }
+        seg0 = seg1;
+        if (seg0 < r1) {
+          __syncthreads();
+          for (int i = threadIdx.x; i < kGroupCells; i += kHistThreads) {
+            emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
+            icells[i] = 0;
+          }
+          __syncthreads();
+        }
+      }
+    }
+  }
+  if (!direct) {
+    // registers of the next tile: this thread's row of it
+    uint32_t nrow = 0;
+    int32_t nq = 0;
+    float2 ngh = make_float2(0.f, 0.f);
+    uint4 nb[2 * kNG];
+    // row indices run one tile ahead of the gathers that use them
+    auto load_idx = [&](int64_t pos) { return pos < r1 ? __ldcg(idx + pos) : 0u; };  // written by the partition
+    uint32_t idx_ahead = 0;
+    auto fetch = [&](int64_t pos, uint32_t row) {
+      const bool live = pos < r1;
+      nrow = row;
+      if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
+      else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
+      const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
+  #pragma unroll
+      for (int k = 0; k < 2 * kNG; ++k)
+        nb[k] = (live && (k >> 1) < ngroups) ? __ldg(src + k) : make_uint4(0u, 0u, 0u, 0u);
+    };
+    {
+      const uint32_t first = load_idx(r0 + threadIdx.x);
+      idx_ahead = load_idx(r0 + kHistTileRows + threadIdx.x);
+      fetch(r0 + threadIdx.x, first);
+    }
+    if (threadIdx.x < 32 * kNG) {
+      s_vlen[threadIdx.x] = my_vlen;
+      s_vstart[threadIdx.x] = my_vstart;
+    }
+    int32_t since_flush = 0;
+    __syncthreads();
+    for (int64_t t0 = r0; t0 < r1; t0 += kHistTileRows) {
+      const int tile_rows = (int)min((int64_t)kHistTileRows, r1 - t0);
+      // stage this tile (the previous tile's accumulation has finished); rows
+      // past the range stage as zeros and add nothing
+  #pragma unroll
+      for (int k = 0; k < 2 * kNG; ++k) sbins[threadIdx.x * 2 * kNG + k] = nb[k];
+      if (kMode == 2) sq[threadIdx.x] = nq;
+      else sgh[threadIdx.x] = ngh;
+      __syncthreads();
+      // the next tile's gathers run while this one is accumulated
+      if (t0 + kHistTileRows < r1) {
+        fetch(t0 + kHistTileRows + threadIdx.x, idx_ahead);
+        idx_ahead = load_idx(t0 + 2 * kHistTileRows + threadIdx.x);
+      }
+      const int rw0 = warp * kRowsPerWarp;
+      if (rw0 < tile_rows) {
+        // this warp's 32 staged rows; lane l adds feature f0 + 32 g + l of
+        // each row. The gradients of two or four rows arrive in one broadcast
+        // load.
+        const unsigned char* rowp = reinterpret_cast<const unsigned char*>(sbins) + rw0 * kRowBytes + lane;
+        auto rows = [&](auto groups) {
+          constexpr int kG = decltype(groups)::value;
+          // rows per batch: every byte of a batch is loaded before its first
+          // atomic (the compiler cannot move loads past shared atomics that may
+          // alias them), so a batch waits for one shared-load latency
+          constexpr int kB = kG == 1 ? 8 : 4;
+  #pragma unroll
+          for (int jb = 0; jb < kRowsPerWarp / kB; ++jb) {
+            int raw[kB][kG];
+  #pragma unroll
+            for (int u = 0; u < kB; ++u)
+  #pragma unroll
+              for (int g = 0; g < kG; ++g) raw[u][g] = (int)rowp[(kB * jb + u) * kRowBytes + 32 * g];
+            if constexpr (kMode == 2) {
+              int32_t qs[kB];
+  #pragma unroll
+              for (int v = 0; v < kB / 4; ++v) {
+                const int4 q4 = reinterpret_cast<const int4*>(sq + rw0 + kB * jb)[v];
+                qs[4 * v] = q4.x;
+                qs[4 * v + 1] = q4.y;
+                qs[4 * v + 2] = q4.z;
+                qs[4 * v + 3] = q4.w;
+              }
+  #pragma unroll
+              for (int u = 0; u < kB; ++u)
+  #pragma unroll
+                for (int g = 0; g < kG; ++g)
+                  atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + raw[u][g] * 32 + lane, qs[u]);
+            } else {
+              float gs[kB], hs[kB];
+  #pragma unroll
+              for (int v = 0; v < kB / 2; ++v) {
+                const float4 t = reinterpret_cast<const float4*>(sgh + rw0 + kB * jb)[v];
+                gs[2 * v] = t.x;
+                hs[2 * v] = t.y;
+                gs[2 * v + 1] = t.z;
+                hs[2 * v + 1] = t.w;
+              }
+  #pragma unroll
+              for (int u = 0; u < kB; ++u)
+  #pragma unroll
+                for (int g = 0; g < kG; ++g) {
+                  // float cells take a compare-and-swap loop per add: skip value 0
+                  if (raw[u][g] == 0) continue;
+                  const int k = raw[u][g] * 32 + lane;
+                  const float gv = gs[u], hv = hs[u];
+                  if constexpr (kMode == 0) {
+                    double* d = reinterpret_cast<double*>(cells + (size_t)g * kGroupCells * 16);
+                    atomicAdd(d + k, (double)gv);
+                    atomicAdd(d + kGroupCells + k, (double)hv);
+                  } else {
+                    float* fl = reinterpret_cast<float*>(cells + (size_t)g * kGroupCells * 16);
+                    float og = atomicAdd(fl + k, gv);
+                    float sg = __fadd_rn(og, gv);
+                    float bg = __fsub_rn(sg, og);
+                    atomicAdd(fl + kGroupCells + k, __fadd_rn(__fsub_rn(og, __fsub_rn(sg, bg)), __fsub_rn(gv, bg)));
+                    float oh = atomicAdd(fl + 2 * kGroupCells + k, hv);
+                    float s2 = __fadd_rn(oh, hv);
+                    float bh = __fsub_rn(s2, oh);
+                    atomicAdd(fl + 3 * kGroupCells + k, __fadd_rn(__fsub_rn(oh, __fsub_rn(s2, bh)), __fsub_rn(hv, bh)));
+                  }
+                }
+            }
+          }
+        };
+        // the group count is a compile-time constant inside the row loop
+        if (ngroups == kNG) {
+          rows(std::integral_constant<int, kNG>{});
+        } else {
+          if constexpr (kNG > 1) {
+            if (ngroups == 1) rows(std::integral_constant<int, 1>{});
+            else if constexpr (kNG > 2) {
+              if (ngroups == 2) rows(std::integral_constant<int, 2>{});
+              else if constexpr (kNG > 3) {
+                if (ngroups == 3) rows(std::integral_constant<int, 3>{});
+              }
             }
           }
         }
       }
-    }
-    since_flush += tile_rows;
-    __syncthreads();
-    // int32 cells hold at most sub_rows rows before their 16-bit halves could
-    // wrap: this CTA adds its own cells to the histogram and clears them
-    if constexpr (kMode == 2) {
-      if (t0 + kHistTileRows < r1 && since_flush + kHistTileRows > sub_rows) {
-        const int total = ngroups * kGroupCells;
-        for (int i = threadIdx.x; i < total; i += kHistThreads) {
-          emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
-          reinterpret_cast<int32_t*>(cells)[i] = 0;
+      since_flush += tile_rows;
+      __syncthreads();
+      // int32 cells hold at most sub_rows rows before their 16-bit halves could
+      // wrap: this CTA adds its own cells to the histogram and clears them
+      if constexpr (kMode == 2) {
+        if (t0 + kHistTileRows < r1 && since_flush + kHistTileRows > sub_rows) {
+          const int total = ngroups * kGroupCells;
+          for (int i = threadIdx.x; i < total; i += kHistThreads) {
+            emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
+            reinterpret_cast<int32_t*>(cells)[i] = 0;
+          }
+          since_flush = 0;
+          __syncthreads();
         }
-        since_flush = 0;
-        __syncthreads();
       }
     }
   }
