@@ -303,6 +303,8 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   // tile of rows in shared memory first (A/B)
   c.hist_direct = 1;
   if (const char* e = std::getenv("LGBM_B200_HIST_DIRECT")) c.hist_direct = std::atoi(e) != 0;
+  // the direct loop addresses row words with 32-bit offsets
+  if ((uint64_t)n * (uint64_t)h->stride >= (1ull << 34)) c.hist_direct = 0;
   c.feats = feats_d;
   DParams& p = c.p;
   p.lambda_l1 = cfg->lambda_l1;

@@ -419,44 +419,47 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
         s_vstart[threadIdx.x] = my_vstart;
       }
       constexpr int kU = 4;
-      constexpr int kBatch = 4 * kU;                   // rows per warp and batch
-      constexpr int64_t kStep = (int64_t)kWarps * kBatch;  // rows per CTA and batch
+      constexpr int kBatch = 4 * kU;              // rows per warp and batch
+      constexpr int32_t kStep = kWarps * kBatch;  // rows per CTA and batch
       const int j = lane >> 3, a = lane & 7;
       int32_t* icells = reinterpret_cast<int32_t*>(cells);
+      // word offsets of a row fit 32 bits (the host allows this loop for bin
+      // matrices under 16 GiB only); positions in the leaf fit 31 bits
       const uint32_t* wbase = reinterpret_cast<const uint32_t*>(c.bins + f0) + a;
-      const size_t wstride = stride / 4;  // the row stride is a multiple of 32 bytes
-      int fk[4], sk[4];
+      const uint32_t wstride = (uint32_t)(stride / 4);  // the row stride is a multiple of 32 bytes
+      const int32_t R0 = (int32_t)r0, R1 = (int32_t)r1;
+      // pass k: the byte selector of this lane's byte and the shared address
+      // of its feature's cell of stored value 0 (value v adds v * 128 bytes)
+      uint32_t sel[4], cb[4];
+      const uint32_t cells_s = (uint32_t)__cvta_generic_to_shared(icells);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const int b = (k + j) & 3;
-        fk[k] = 4 * a + b;
-        sk[k] = 8 * b;
+        const uint32_t b = (uint32_t)((k + j) & 3);
+        sel[k] = 0x4440u | b;  // byte b of the word, zero-extended
+        cb[k] = cells_s + 4u * (4u * (uint32_t)a + b);
       }
-      for (int64_t seg0 = r0; seg0 < r1;) {
+      for (int32_t seg0 = R0; seg0 < R1;) {
         // int32 cells hold at most sub_rows rows of this CTA before their
         // 16-bit halves could wrap
-        const int64_t seg1 = min(r1, seg0 + (int64_t)sub_rows);
-        int64_t b = seg0 + (int64_t)warp * kBatch;
+        const int32_t seg1 = seg0 + min(R1 - seg0, sub_rows);
+        int32_t b = seg0 + warp * kBatch;
         uint32_t rid[kU], wn[kU];
         int32_t qn[kU];
+        {
+          const int32_t lim = seg1 - b - j;  // quad u is live when 4u < lim
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const int64_t pos = b + 4 * u + j;
-          rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
-        }
+          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim ? __ldcg(idx + b + j + 4 * u) : 0u;
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const bool v = b + 4 * u + j < seg1;
-          wn[u] = v ? __ldg(wbase + (size_t)rid[u] * wstride) : 0u;
-          qn[u] = v ? __ldg(s.packed + rid[u]) : 0;
-        }
+          for (int u = 0; u < kU; ++u) {
+            wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
+            qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
+          }
+          const int32_t lim2 = lim - kStep;
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const int64_t pos = b + kStep + 4 * u + j;
-          rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
+          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + kStep + j + 4 * u) : 0u;
         }
         // every cell is zeroed (above, or by the last flush) before the first add
-        if (seg0 == r0) __syncthreads();
+        if (seg0 == R0) __syncthreads();
         for (; b < seg1; b += kStep) {
           uint32_t w[kU];
           int32_t q[kU];
@@ -465,27 +468,27 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
             w[u] = wn[u];
             q[u] = qn[u];
           }
-          const int64_t bn = b + kStep;
+          const int32_t lim = seg1 - (b + kStep) - j;  // the next batch's live quads
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
-            const bool v = bn + 4 * u + j < seg1;
-            wn[u] = v ? __ldg(wbase + (size_t)rid[u] * wstride) : 0u;
-            qn[u] = v ? __ldg(s.packed + rid[u]) : 0;
+            wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
+            qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
           }
+          const int32_t lim2 = lim - kStep;
 #pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            const int64_t pos = bn + kStep + 4 * u + j;
-            rid[u] = pos < seg1 ? __ldcg(idx + pos) : 0u;
-          }
+          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + 2 * kStep + j + 4 * u) : 0u;
           // rows past the segment hold word 0 and gradient 0: they add 0 to
           // cell 0, which no feature view contains
 #pragma unroll
           for (int k = 0; k < 4; ++k)
 #pragma unroll
-            for (int u = 0; u < kU; ++u) atomicAdd(icells + ((w[u] >> sk[k]) & 0xFFu) * 32 + fk[k], q[u]);
+            for (int u = 0; u < kU; ++u) {
+              const uint32_t addr = cb[k] + (__byte_perm(w[u], 0u, sel[k]) << 7);
+              asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(q[u]) : "memory");
+            }
         }
         seg0 = seg1;
-        if (seg0 < r1) {
+        if (seg0 < R1) {
           __syncthreads();
           for (int i = threadIdx.x; i < kGroupCells; i += kHistThreads) {
             emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
