@@ -149,7 +149,8 @@ __global__ void k_quant_absmax(const float2* gh, int64_t n, unsigned long long* 
 __global__ void k_quant_scales(unsigned long long* maxbits, DSlotState* st, int32_t bins, int32_t const_hess);
 __global__ void k_quant_apply(const float2* gh, int64_t n, const double* grv, const double* hrv,
                               const int64_t* start_dev, const DSlotState* st, int32_t const_hess, int32_t stochastic,
-                              int32_t* packed, int64_t row_offset, int64_t table_n);
+                              int32_t* packed, int64_t row_offset, int64_t table_n, uint8_t* row_q,
+                              int32_t row_stride);
 __global__ void k_bagging(uint32_t* rng_state, int64_t n, double fraction, uint8_t* in_bag, int32_t* block_in);
 __global__ void k_bag_scan(const int32_t* block_in, int32_t nb, int64_t n, int32_t* block_base, int32_t* counts);
 __global__ void k_bag_scatter(const uint8_t* in_bag, int64_t n, const int32_t* block_base, uint32_t* bag,

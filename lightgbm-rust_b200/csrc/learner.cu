@@ -102,7 +102,9 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   if (mode == LGBM_B200_HIST_QUANT) {
     int32_t half = std::max(1, cfg->num_grad_quant_bins / 2);
     int64_t lim = std::min<int64_t>(32767 / half, 65535 / std::max(1, cfg->num_grad_quant_bins));
-    h->sub_rows = (int32_t)std::min<int64_t>(8192, lim);
+    // a cell packs (g << 16) + h: per-row |g| <= bins / 2 and h <= bins keep
+    // both 16-bit halves exact over `lim` rows
+    h->sub_rows = (int32_t)lim;
     if (cfg->num_grad_quant_bins < 2 || cfg->num_grad_quant_bins > 64)
       return Status(LGBM_B200_ERR_UNSUPPORTED, "num_grad_quant_bins must be in [2, 64]");
   }
@@ -305,6 +307,13 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   if (const char* e = std::getenv("LGBM_B200_HIST_DIRECT")) c.hist_direct = std::atoi(e) != 0;
   // the direct loop addresses row words with 32-bit offsets
   if ((uint64_t)n * (uint64_t)h->stride >= (1ull << 34)) c.hist_direct = 0;
+  // One slot and a single 32-byte row of at most 28 features: the packed
+  // gradient of a row rides in its row's padding, so the direct histogram
+  // loop reads one sector per row instead of two. LGBM_B200_Q_IN_ROW=0 keeps
+  // it in its own array only (A/B).
+  c.q_in_row = (mode == LGBM_B200_HIST_QUANT && K == 1 && h->ntiles == 1 && nf <= 28 && c.hist_direct) ? 1 : 0;
+  if (const char* e = std::getenv("LGBM_B200_Q_IN_ROW"))
+    if (std::atoi(e) == 0) c.q_in_row = 0;
   c.feats = feats_d;
   DParams& p = c.p;
   p.lambda_l1 = cfg->lambda_l1;
@@ -663,7 +672,9 @@ Status enqueue_quant(LgbmB200Learner* h) {
     }
     k_quant_apply<<<blocks, 256, 0, s>>>(h->slots_h[k].gh, n, h->grv, h->hrv, h->start_dev + k, h->slots_h[k].st,
                                          h->cfg.is_constant_hessian, h->cfg.stochastic_rounding && h->grv,
-                                         h->slots_h[k].packed, offset, table_n);
+                                         h->slots_h[k].packed, offset, table_n,
+                                         h->ctx.q_in_row ? const_cast<uint8_t*>(h->ctx.bins) + 28 : nullptr,
+                                         h->stride);
     CU_LAUNCH();
   }
   return Status();

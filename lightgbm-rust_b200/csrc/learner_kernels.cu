@@ -438,65 +438,76 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
         sel[k] = 0x4440u | b;  // byte b of the word, zero-extended
         cb[k] = cells_s + 4u * (4u * (uint32_t)a + b);
       }
-      for (int32_t seg0 = R0; seg0 < R1;) {
-        // int32 cells hold at most sub_rows rows of this CTA before their
-        // 16-bit halves could wrap
-        const int32_t seg1 = seg0 + min(R1 - seg0, sub_rows);
-        int32_t b = seg0 + warp * kBatch;
-        uint32_t rid[kU], wn[kU];
-        int32_t qn[kU];
-        {
-          const int32_t lim = seg1 - b - j;  // quad u is live when 4u < lim
+      // kQ: the packed gradient comes with the row (its padding bytes 28..31)
+      auto rows = [&](auto q_in_row) {
+        constexpr bool kQ = decltype(q_in_row)::value;
+        for (int32_t seg0 = R0; seg0 < R1;) {
+          // int32 cells hold at most sub_rows rows of this CTA before their
+          // 16-bit halves could wrap
+          const int32_t seg1 = seg0 + min(R1 - seg0, sub_rows);
+          int32_t b = seg0 + warp * kBatch;
+          uint32_t rid[kU], wn[kU];
+          int32_t qn[kU] = {};
+          {
+            const int32_t lim = seg1 - b - j;  // quad u is live when 4u < lim
 #pragma unroll
-          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim ? __ldcg(idx + b + j + 4 * u) : 0u;
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
-            qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
-          }
-          const int32_t lim2 = lim - kStep;
-#pragma unroll
-          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + kStep + j + 4 * u) : 0u;
-        }
-        // every cell is zeroed (above, or by the last flush) before the first add
-        if (seg0 == R0) __syncthreads();
-        for (; b < seg1; b += kStep) {
-          uint32_t w[kU];
-          int32_t q[kU];
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            w[u] = wn[u];
-            q[u] = qn[u];
-          }
-          const int32_t lim = seg1 - (b + kStep) - j;  // the next batch's live quads
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
-            qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
-          }
-          const int32_t lim2 = lim - kStep;
-#pragma unroll
-          for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + 2 * kStep + j + 4 * u) : 0u;
-          // rows past the segment hold word 0 and gradient 0: they add 0 to
-          // cell 0, which no feature view contains
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
+            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim ? __ldcg(idx + b + j + 4 * u) : 0u;
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-              const uint32_t addr = cb[k] + (__byte_perm(w[u], 0u, sel[k]) << 7);
-              asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(q[u]) : "memory");
+              wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
+              if constexpr (!kQ) qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
             }
-        }
-        seg0 = seg1;
-        if (seg0 < R1) {
-          __syncthreads();
-          for (int i = threadIdx.x; i < kGroupCells; i += kHistThreads) {
-            emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
-            icells[i] = 0;
+            const int32_t lim2 = lim - kStep;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + kStep + j + 4 * u) : 0u;
           }
-          __syncthreads();
+          // every cell is zeroed (above, or by the last flush) before the first add
+          if (seg0 == R0) __syncthreads();
+          for (; b < seg1; b += kStep) {
+            uint32_t w[kU];
+            int32_t q[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+              w[u] = wn[u];
+              if constexpr (!kQ) q[u] = qn[u];
+            }
+            const int32_t lim = seg1 - (b + kStep) - j;  // the next batch's live quads
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+              wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
+              if constexpr (!kQ) qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
+            }
+            const int32_t lim2 = lim - kStep;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + 2 * kStep + j + 4 * u) : 0u;
+            // the gradient in the row's padding (word 7), from the row's lane 7
+            if constexpr (kQ) {
+#pragma unroll
+              for (int u = 0; u < kU; ++u) q[u] = (int32_t)__shfl_sync(0xffffffffu, w[u], (lane & 24) | 7);
+            }
+            // rows past the segment hold word 0 and gradient 0: they add 0 to
+            // cell 0, which no feature view contains
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+              for (int u = 0; u < kU; ++u) {
+                const uint32_t addr = cb[k] + (__byte_perm(w[u], 0u, sel[k]) << 7);
+                asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(q[u]) : "memory");
+              }
+          }
+          seg0 = seg1;
+          if (seg0 < R1) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < kGroupCells; i += kHistThreads) {
+              emit(i, [&](int ii, int64_t& gv, int64_t& hv) { cell_of(cells, ii, gv, hv); });
+              icells[i] = 0;
+            }
+            __syncthreads();
+          }
         }
-      }
+      };
+      if (c.q_in_row) rows(std::true_type{});
+      else rows(std::false_type{});
     }
   }
   if (!direct) {
@@ -514,7 +525,7 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
       if (kMode == 2) nq = live ? __ldg(s.packed + nrow) : 0;
       else ngh = live ? s.gh[nrow] : make_float2(0.f, 0.f);
       const uint4* src = reinterpret_cast<const uint4*>(c.bins + (size_t)nrow * stride + f0);
-  #pragma unroll
+#pragma unroll
       for (int k = 0; k < 2 * kNG; ++k)
         nb[k] = (live && (k >> 1) < ngroups) ? __ldg(src + k) : make_uint4(0u, 0u, 0u, 0u);
     };
@@ -533,7 +544,7 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
       const int tile_rows = (int)min((int64_t)kHistTileRows, r1 - t0);
       // stage this tile (the previous tile's accumulation has finished); rows
       // past the range stage as zeros and add nothing
-  #pragma unroll
+#pragma unroll
       for (int k = 0; k < 2 * kNG; ++k) sbins[threadIdx.x * 2 * kNG + k] = nb[k];
       if (kMode == 2) sq[threadIdx.x] = nq;
       else sgh[threadIdx.x] = ngh;
@@ -555,16 +566,16 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
           // atomic (the compiler cannot move loads past shared atomics that may
           // alias them), so a batch waits for one shared-load latency
           constexpr int kB = kG == 1 ? 8 : 4;
-  #pragma unroll
+#pragma unroll
           for (int jb = 0; jb < kRowsPerWarp / kB; ++jb) {
             int raw[kB][kG];
-  #pragma unroll
+#pragma unroll
             for (int u = 0; u < kB; ++u)
-  #pragma unroll
+#pragma unroll
               for (int g = 0; g < kG; ++g) raw[u][g] = (int)rowp[(kB * jb + u) * kRowBytes + 32 * g];
             if constexpr (kMode == 2) {
               int32_t qs[kB];
-  #pragma unroll
+#pragma unroll
               for (int v = 0; v < kB / 4; ++v) {
                 const int4 q4 = reinterpret_cast<const int4*>(sq + rw0 + kB * jb)[v];
                 qs[4 * v] = q4.x;
@@ -572,14 +583,14 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
                 qs[4 * v + 2] = q4.z;
                 qs[4 * v + 3] = q4.w;
               }
-  #pragma unroll
+#pragma unroll
               for (int u = 0; u < kB; ++u)
-  #pragma unroll
+#pragma unroll
                 for (int g = 0; g < kG; ++g)
                   atomicAdd(reinterpret_cast<int32_t*>(cells) + g * kGroupCells + raw[u][g] * 32 + lane, qs[u]);
             } else {
               float gs[kB], hs[kB];
-  #pragma unroll
+#pragma unroll
               for (int v = 0; v < kB / 2; ++v) {
                 const float4 t = reinterpret_cast<const float4*>(sgh + rw0 + kB * jb)[v];
                 gs[2 * v] = t.x;
@@ -587,9 +598,9 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
                 gs[2 * v + 1] = t.z;
                 hs[2 * v + 1] = t.w;
               }
-  #pragma unroll
+#pragma unroll
               for (int u = 0; u < kB; ++u)
-  #pragma unroll
+#pragma unroll
                 for (int g = 0; g < kG; ++g) {
                   // float cells take a compare-and-swap loop per add: skip value 0
                   if (raw[u][g] == 0) continue;

@@ -134,7 +134,8 @@ __device__ __forceinline__ int32_t to_i8(double x) {
 __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n, const double* grv,
                                                      const double* hrv, const int64_t* start_dev,
                                                      const DSlotState* st, int32_t const_hess, int32_t stochastic,
-                                                     int32_t* packed, int64_t row_offset, int64_t table_n) {
+                                                     int32_t* packed, int64_t row_offset, int64_t table_n,
+                                                     uint8_t* row_q, int32_t row_stride) {
   const int64_t start = *start_dev;
   const double inv_g = 1.0 / st->grad_scale;
   const double inv_h = 1.0 / st->hess_scale;
@@ -152,7 +153,10 @@ __global__ void __launch_bounds__(256) k_quant_apply(const float2* gh, int64_t n
     }
     int32_t gq = g >= 0.0 ? to_i8(g * inv_g + rg) : to_i8(g * inv_g - rg);
     int32_t hq = const_hess ? 1 : to_i8((double)v.y * inv_h + rh);
-    packed[i] = gq * 65536 + (int32_t)(uint8_t)hq;
+    const int32_t pq = gq * 65536 + (int32_t)(uint8_t)hq;
+    packed[i] = pq;
+    // the copy in the row's padding, read with the row's bins
+    if (row_q) *reinterpret_cast<int32_t*>(row_q + i * row_stride) = pq;
   }
 }
 
