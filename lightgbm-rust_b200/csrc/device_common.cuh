@@ -170,7 +170,8 @@ struct DCtx {
   int32_t rows_per_block;  // histogram rows per CTA (minimum)
   int32_t dp;              // 1: rows sharded over ranks; the step's end waits for the global left count
   int32_t defer;           // 1: a partition posts its step's end for the next histogram launch to run
-  int32_t hist_direct;     // 1: the quantized one-group histogram adds each row from registers (no staging)
+  int32_t hist_direct;     // 1: the quantized one-group histogram runs the direct loop (asynchronous
+                           // copies per warp, no tile barriers)
   int32_t q_in_row;        // 1: each row's packed gradient also fills its bin row's padding bytes 28..31
                            // (one tree slot, one feature tile of at most 28 features)
 };

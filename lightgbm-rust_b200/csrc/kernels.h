@@ -9,6 +9,7 @@ namespace lgbm_b200 {
 
 constexpr int kHistThreads = 512;
 constexpr int kHistTileRows = kHistThreads;  // rows staged per histogram tile: one per thread
+constexpr int kHistAsyncStages = 4;  // stages of each warp's copy ring (asynchronously staged histogram rows)
 constexpr int kPartThreads = 256;             // threads of a partition CTA
 #ifndef LGBM_B200_PART_TILE_ROWS
 #define LGBM_B200_PART_TILE_ROWS 1024

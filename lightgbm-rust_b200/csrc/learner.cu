@@ -301,12 +301,10 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   c.defer = 1;
   // LGBM_B200_DEFER=0: the partition's last CTA ends the step itself (A/B)
   if (const char* e = std::getenv("LGBM_B200_DEFER")) c.defer = std::atoi(e) != 0;
-  // LGBM_B200_HIST_DIRECT=0: the quantized one-group histogram stages each
-  // tile of rows in shared memory first (A/B)
+  // LGBM_B200_HIST_DIRECT=0: the quantized one-group histogram runs the
+  // tile loop with block barriers instead of the direct loop (A/B)
   c.hist_direct = 1;
   if (const char* e = std::getenv("LGBM_B200_HIST_DIRECT")) c.hist_direct = std::atoi(e) != 0;
-  // the direct loop addresses row words with 32-bit offsets
-  if ((uint64_t)n * (uint64_t)h->stride >= (1ull << 34)) c.hist_direct = 0;
   // One slot and a single 32-byte row of at most 28 features: the packed
   // gradient of a row rides in its row's padding, so the direct histogram
   // loop reads one sector per row instead of two. LGBM_B200_Q_IN_ROW=0 keeps

@@ -406,95 +406,110 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
   if constexpr (kMode == 2 && kNG == 1) {
     direct = c.hist_direct != 0;
     if (direct) {
-      // Direct row loop (quantized, one lane group): no staging and no tile
-      // barriers. A warp takes its rows four at a time: lane l loads word
-      // a = l & 7 (features f0 + 4a .. f0 + 4a + 3) of row j = l >> 3 and in
-      // pass k (0..3) adds byte b = (k + j) & 3 of it, feature 4a + b, whose
-      // cell raw * 32 + 4a + b lies in bank 4a + b: the 32 lanes of every
-      // warp-wide atomic touch 32 different banks. A warp's batch is kU row
-      // quads; the next batch's words and gradients are in flight while this
-      // one is added, and the row indices one batch further ahead.
+      // Direct row loop (quantized, one lane group), without tile barriers.
+      // A warp adds its rows four at a time: lane l takes word a = l & 7
+      // (features f0 + 4a .. f0 + 4a + 3) of row j = l >> 3 and in pass k
+      // (0..3) adds byte b = (k + j) & 3 of it, feature 4a + b, whose cell
+      // raw * 32 + 4a + b lies in bank 4a + b: the 32 lanes of every
+      // warp-wide atomic touch 32 different banks.
       if (threadIdx.x < 32) {
         s_vlen[threadIdx.x] = my_vlen;
         s_vstart[threadIdx.x] = my_vstart;
       }
-      constexpr int kU = 4;
-      constexpr int kBatch = 4 * kU;              // rows per warp and batch
-      constexpr int32_t kStep = kWarps * kBatch;  // rows per CTA and batch
       const int j = lane >> 3, a = lane & 7;
       int32_t* icells = reinterpret_cast<int32_t*>(cells);
-      // word offsets of a row fit 32 bits (the host allows this loop for bin
-      // matrices under 16 GiB only); positions in the leaf fit 31 bits
-      const uint32_t* wbase = reinterpret_cast<const uint32_t*>(c.bins + f0) + a;
-      const uint32_t wstride = (uint32_t)(stride / 4);  // the row stride is a multiple of 32 bytes
+      // positions in the leaf fit 31 bits
       const int32_t R0 = (int32_t)r0, R1 = (int32_t)r1;
-      // pass k: the byte selector of this lane's byte and the shared address
-      // of its feature's cell of stored value 0 (value v adds v * 128 bytes)
-      uint32_t sel[4], cb[4];
+      // pass k: the shared address of the cell of stored value 0 of this
+      // lane's feature (value v adds v * 128 bytes); the word is rotated by
+      // j bytes once, so that pass k takes its byte k
+      uint32_t cb[4];
       const uint32_t cells_s = (uint32_t)__cvta_generic_to_shared(icells);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const uint32_t b = (uint32_t)((k + j) & 3);
-        sel[k] = 0x4440u | b;  // byte b of the word, zero-extended
-        cb[k] = cells_s + 4u * (4u * (uint32_t)a + b);
-      }
-      // kQ: the packed gradient comes with the row (its padding bytes 28..31)
-      auto rows = [&](auto q_in_row) {
+      for (int k = 0; k < 4; ++k) cb[k] = cells_s + 4u * (4u * (uint32_t)a + (uint32_t)((k + j) & 3));
+      const uint32_t rot = 8u * (uint32_t)j;
+      // The rows are staged by asynchronous copies: each warp keeps a private
+      // ring of kS stages of 16 rows (their 32-byte bin segments, and their
+      // gradients when these do not ride in the rows) in shared memory and
+      // copies kS - 1 batches ahead of the one it adds, so the bytes in flight
+      // take no registers. kQ: the packed gradient is the row's word 7.
+      auto rows_async = [&](auto q_in_row) {
         constexpr bool kQ = decltype(q_in_row)::value;
+        constexpr int kS = kHistAsyncStages;
+        constexpr int kRowsB = 16;                  // rows per warp and batch
+        constexpr int32_t kStep = kWarps * kRowsB;  // rows per CTA and batch
+        constexpr uint32_t kStageBytes = kRowsB * 32 + kRowsB * 4;
+        const uint32_t ring = (uint32_t)__cvta_generic_to_shared(smem_raw + (size_t)kGroupCells * 4) +
+                              (uint32_t)warp * kS * kStageBytes;
+        const unsigned char* rowsrc = c.bins + f0 + 16 * (lane & 1);  // lane l copies half (l & 1) of row l >> 1
         for (int32_t seg0 = R0; seg0 < R1;) {
-          // int32 cells hold at most sub_rows rows of this CTA before their
-          // 16-bit halves could wrap
           const int32_t seg1 = seg0 + min(R1 - seg0, sub_rows);
-          int32_t b = seg0 + warp * kBatch;
-          uint32_t rid[kU], wn[kU];
-          int32_t qn[kU] = {};
-          {
-            const int32_t lim = seg1 - b - j;  // quad u is live when 4u < lim
-#pragma unroll
-            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim ? __ldcg(idx + b + j + 4 * u) : 0u;
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-              wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
-              if constexpr (!kQ) qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
+          const int32_t b0 = seg0 + warp * kRowsB;
+          auto load_rid = [&](int32_t bt) {
+            const int32_t pos = bt + (lane >> 1);
+            return pos < seg1 ? __ldcg(idx + pos) : 0u;
+          };
+          auto issue = [&](int32_t bt, int stage, uint32_t rid) {
+            const uint32_t st_addr = ring + (uint32_t)stage * kStageBytes;
+            if (bt + (lane >> 1) < seg1) {
+              const unsigned char* src = rowsrc + (size_t)rid * stride;
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(st_addr + 16u * (uint32_t)lane), "l"(src)
+                           : "memory");
             }
-            const int32_t lim2 = lim - kStep;
+            if constexpr (!kQ) {
+              const uint32_t ridq = __shfl_sync(0xffffffffu, rid, (lane * 2) & 31);  // row `lane`'s index
+              if (lane < kRowsB && bt + lane < seg1)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(st_addr + kRowsB * 32 + 4u * (uint32_t)lane),
+                             "l"(s.packed + ridq)
+                             : "memory");
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+          };
+          // batches 0 .. kS - 2 in flight, the indices of batch kS - 1 loaded
+          {
+            uint32_t r[kS - 1];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + kStep + j + 4 * u) : 0u;
+            for (int t = 0; t < kS - 1; ++t) r[t] = load_rid(b0 + t * kStep);
+#pragma unroll
+            for (int t = 0; t < kS - 1; ++t) issue(b0 + t * kStep, t, r[t]);
           }
+          uint32_t rid_next = load_rid(b0 + (kS - 1) * kStep);
           // every cell is zeroed (above, or by the last flush) before the first add
           if (seg0 == R0) __syncthreads();
-          for (; b < seg1; b += kStep) {
-            uint32_t w[kU];
-            int32_t q[kU];
+          int stage = 0;
+          for (int32_t bt = b0; bt < seg1; bt += kStep) {
+            issue(bt + (kS - 1) * kStep, stage == 0 ? kS - 1 : stage - 1, rid_next);
+            rid_next = load_rid(bt + kS * kStep);
+            asm volatile("cp.async.wait_group %0;" ::"n"(kS - 1) : "memory");
+            __syncwarp();
+            const uint32_t st_addr = ring + (uint32_t)stage * kStageBytes;
+            uint32_t w[4];
+            int32_t q[4];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-              w[u] = wn[u];
-              if constexpr (!kQ) q[u] = qn[u];
+            for (int u = 0; u < 4; ++u) {
+              const int rr = 4 * u + j;
+              const bool live = bt + rr < seg1;
+              uint32_t x, y;
+              asm volatile("ld.shared.u32 %0, [%1];" : "=r"(x) : "r"(st_addr + 32u * rr + 4u * a) : "memory");
+              if constexpr (kQ) {
+                asm volatile("ld.shared.u32 %0, [%1];" : "=r"(y) : "r"(st_addr + 32u * rr + 28u) : "memory");
+              } else {
+                asm volatile("ld.shared.u32 %0, [%1];" : "=r"(y) : "r"(st_addr + kRowsB * 32 + 4u * rr) : "memory");
+              }
+              w[u] = __funnelshift_r(x, x, rot);  // byte k is the row's byte (k + j) & 3
+              q[u] = live ? (int32_t)y : 0;       // a dead row adds 0 wherever its stale word points
             }
-            const int32_t lim = seg1 - (b + kStep) - j;  // the next batch's live quads
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-              wn[u] = 4 * u < lim ? __ldg(wbase + rid[u] * wstride) : 0u;
-              if constexpr (!kQ) qn[u] = 4 * u < lim ? __ldg(s.packed + rid[u]) : 0;
-            }
-            const int32_t lim2 = lim - kStep;
-#pragma unroll
-            for (int u = 0; u < kU; ++u) rid[u] = 4 * u < lim2 ? __ldcg(idx + b + 2 * kStep + j + 4 * u) : 0u;
-            // the gradient in the row's padding (word 7), from the row's lane 7
-            if constexpr (kQ) {
-#pragma unroll
-              for (int u = 0; u < kU; ++u) q[u] = (int32_t)__shfl_sync(0xffffffffu, w[u], (lane & 24) | 7);
-            }
-            // rows past the segment hold word 0 and gradient 0: they add 0 to
-            // cell 0, which no feature view contains
 #pragma unroll
             for (int k = 0; k < 4; ++k)
 #pragma unroll
-              for (int u = 0; u < kU; ++u) {
-                const uint32_t addr = cb[k] + (__byte_perm(w[u], 0u, sel[k]) << 7);
+              for (int u = 0; u < 4; ++u) {
+                const uint32_t addr = cb[k] + (__byte_perm(w[u], 0u, 0x4440u | k) << 7);
                 asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(q[u]) : "memory");
               }
+            __syncwarp();  // the stage is refilled by the next batch's copies
+            stage = stage == kS - 1 ? 0 : stage + 1;
           }
+          asm volatile("cp.async.wait_all;" ::: "memory");
           seg0 = seg1;
           if (seg0 < R1) {
             __syncthreads();
@@ -506,8 +521,8 @@ __device__ void hist_body(const DCtx& c, const DSlot& s, const DTileTable& tt, i
           }
         }
       };
-      if (c.q_in_row) rows(std::true_type{});
-      else rows(std::false_type{});
+      if (c.q_in_row) rows_async(std::true_type{});
+      else rows_async(std::false_type{});
     }
   }
   if (!direct) {
@@ -783,7 +798,12 @@ LGBM_B200_HIST_INST(2, 4)
 
 size_t hist_smem_bytes(int mode, int ng) {
   const size_t cell = mode == 2 ? 4 : 16;
-  return (size_t)ng * kMaxBins * 32 * cell + (size_t)kHistTileRows * 32 * ng + (size_t)kHistTileRows * 8;
+  const size_t staged = (size_t)ng * kMaxBins * 32 * cell + (size_t)kHistTileRows * 32 * ng + (size_t)kHistTileRows * 8;
+  if (mode == 2 && ng == 1) {  // or the cells and every warp's ring of asynchronous copies
+    const size_t ring = (size_t)(kHistThreads / 32) * kHistAsyncStages * (16 * 32 + 16 * 4);
+    return std::max(staged, (size_t)kMaxBins * 32 * 4 + ring);
+  }
+  return staged;
 }
 
 const void* hist_kernel(int mode, int ng) {
