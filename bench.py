@@ -32,10 +32,14 @@ import numpy as np  # noqa: E402
 WORKLOAD = ("binary 10M train + 1M held-out x 28 (21 N(0,1) + 7 heavy-tailed), max_bin 255, 255 leaves, lr 0.1, "
             "500 rounds; forms FP64, FP32-compensated, quantized (int8 g/h, 4 bins, stochastic rounding, FP64 leaf "
             "renewal)")
-# DRAM bytes per histogrammed row of the quantized histogram kernel, from the
-# ncu capture of a 5M-row root launch (summarised under profiles/);
-# traffic grows with the rows of a launch, so a launch's traffic is this times its rows
-HIST_DRAM_BYTES_PER_ROW = 40.8
+# DRAM bytes (read + write) per histogrammed row of the quantized histogram
+# kernel, from one ncu capture of a 5M-row run (summarised under profiles/):
+# the root launch, whose rows are in order, and the next launch, whose rows are
+# scattered (each 32-byte row segment then comes with its neighbour sector).
+# Traffic grows with the rows of a launch, so a tree's traffic is the root's
+# rows times the first plus every other histogrammed row times the second.
+HIST_DRAM_BYTES_PER_ROW_ROOT = 36.9
+HIST_DRAM_BYTES_PER_ROW_SCATTERED = 69.6
 # DRAM bytes per moved row of the partition kernel, from the ncu capture of its
 # first launch in a 5M-row run (the root split: every row; summarised under profiles/).
 # The index writes stay in L2 during the launch, so this is below the 9 algorithmic bytes.
@@ -828,9 +832,11 @@ def main():
                   for k, v in res.items()},
         "roofline": {"bound": "hbm", "kernel": f"k_hist ({head})", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (HIST_DRAM_BYTES_PER_ROW * r["hist_rows_per_tree"] /
+                     "traffic": ((HIST_DRAM_BYTES_PER_ROW_ROOT * len(data["y"]) + HIST_DRAM_BYTES_PER_ROW_SCATTERED *
+                                  (r["hist_rows_per_tree"] - len(data["y"]))) /
                                  (int(data["params"]["num_leaves"]) - 1) if head == "quantized" else None),
-                     "traffic_note": "ncu DRAM bytes per row of a 5M-row launch x rows per launch (average)",
+                     "traffic_note": ("ncu DRAM bytes per row of a 5M-row run (root launch: rows in order; next "
+                                      "launch: scattered rows) x the rows of an average launch"),
                      "bytes_per_launch": r["hist_bytes_per_launch"], "ms_per_launch": r["hist_ms_per_launch"],
                      # the histogram's achieved fraction of the HBM roofline by leaf size
                      "by_rows": [dict(b, frac=(b["gbs"] / peak if b["gbs"] else None)) for b in r["hist_by_rows"]]},
