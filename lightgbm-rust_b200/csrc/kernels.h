@@ -120,6 +120,10 @@ size_t grow_smem_bytes(int mode, int ng);
 cudaError_t launch_grow(int mode, int ng, int grid, size_t smem, cudaStream_t st, const DCtx& c, const DTileTable& tt,
                         int32_t sub_rows, int32_t ntiles, GrowSync* gs, int32_t num_steps, long long* phase_ns);
 __global__ void k_partition(const __grid_constant__ DCtx c);
+// the quantized threshold scan by one warp per (feature, side) item;
+// grid (CTAs, 1, slots), kScanThreads threads
+template <int kMinBlocks>
+__global__ void k_scan_warp(const __grid_constant__ DCtx c, const int32_t* items);
 // the last split step's end, when the partitions post theirs (DCtx::defer);
 // grid (1, 1, slots), kPartThreads threads
 __global__ void k_finish(const __grid_constant__ DCtx c);

@@ -197,6 +197,39 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   if (!(s = A.alloc_n(&feats_d, (size_t)nf)).ok()) return s;
   CU(cudaMemcpy(feats_d, h->feats.data(), sizeof(DFeature) * nf, cudaMemcpyHostToDevice));
   const int K = h->K, L = h->L;
+  // The quantized scan by one warp per (feature, side) item, for steps whose
+  // block scans would run in waves (many features or tree slots): there the
+  // scan is bound by throughput, and eight items share a CTA without block
+  // barriers (multiclass K=10 x 200 features: 29.6 -> 25.1 ms per iteration).
+  // With few items each item's latency counts, and the block scan's 256
+  // threads per item are faster (binary x 28 features: 7.39 against 8.54 ms;
+  // lambdarank x 136: 29.9 against 31.1). Each CTA takes up to `per` items,
+  // at most one of them categorical (the CTA's scratch holds its sort).
+  // LGBM_B200_SCAN_WARP=0/1 forces either; LGBM_B200_SCAN_PER=<1..8> sets the
+  // items per CTA.
+  h->scan_warp = mode == LGBM_B200_HIST_QUANT && h->scan_wide;
+  if (const char* e = std::getenv("LGBM_B200_SCAN_WARP"))
+    h->scan_warp = mode == LGBM_B200_HIST_QUANT && std::atoi(e) != 0;
+  if (h->scan_warp) {
+    constexpr int kWarps = kScanThreads / 32;
+    std::vector<int32_t> numer, cats;
+    for (int f = 0; f < nf; ++f)
+      for (int side = 0; side < 2; ++side) (h->feats[f].bin_type == 1 ? cats : numer).push_back(f * 2 + side);
+    const int64_t items = (int64_t)numer.size() + (int64_t)cats.size();
+    int per = (int)std::min<int64_t>(kWarps, std::max<int64_t>(1, (items * K + h->num_sms - 1) / h->num_sms));
+    if (const char* e = std::getenv("LGBM_B200_SCAN_PER")) per = std::max(1, std::min(kWarps, std::atoi(e)));
+    const int64_t ctas = std::max<int64_t>((items + per - 1) / per, (int64_t)cats.size());
+    std::vector<int32_t> table((size_t)ctas * kWarps, -1);
+    size_t next = 0;
+    for (int64_t b = 0; b < ctas; ++b) {
+      int used = 0;
+      if ((size_t)b < cats.size()) table[(size_t)b * kWarps + used++] = cats[(size_t)b];
+      while (used < per && next < numer.size()) table[(size_t)b * kWarps + used++] = numer[next++];
+    }
+    if (!(s = A.alloc_n(&h->scan_items, table.size())).ok()) return s;
+    CU(cudaMemcpy(h->scan_items, table.data(), sizeof(int32_t) * table.size(), cudaMemcpyHostToDevice));
+    h->scan_warp_grid = (int)ctas;
+  }
   const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
   const size_t max_tiles = ((size_t)n + kPartTileRows - 1) / kPartTileRows + 1;
   h->slots_h.resize(K);
@@ -411,7 +444,13 @@ Status enqueue_tree(LgbmB200Learner* h) {
       if (ev) CU(cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal));
       continue;
     }
-    if (mode == LGBM_B200_HIST_QUANT) {
+    if (mode == LGBM_B200_HIST_QUANT && h->scan_warp) {
+      const dim3 g(h->scan_warp_grid, 1, K);
+      if (h->scan_wide)
+        CU(launch_ex(k_scan_warp<kScanWideBlocks>, g, dim3(kScanThreads), 0, s, pdl_scan, c,
+                     (const int32_t*)h->scan_items));
+      else CU(launch_ex(k_scan_warp<2>, g, dim3(kScanThreads), 0, s, pdl_scan, c, (const int32_t*)h->scan_items));
+    } else if (mode == LGBM_B200_HIST_QUANT) {
       if (h->scan_wide)
         CU(launch_ex(k_scan<true, kScanWideBlocks>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
       else CU(launch_ex(k_scan<true, 1>, scan_grid, dim3(kScanThreads), h->scan_smem, s, pdl_scan, c));
@@ -455,7 +494,12 @@ static Status launch_scan(LgbmB200Learner* h, bool pdl) {
   const DCtx& c = h->ctx;
   const dim3 g(h->nf, 2, h->K);
   cudaStream_t s = h->stream;
-  if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT) {
+  if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT && h->scan_warp) {
+    const dim3 gw(h->scan_warp_grid, 1, h->K);
+    if (h->scan_wide)
+      CU(launch_ex(k_scan_warp<kScanWideBlocks>, gw, dim3(kScanThreads), 0, s, pdl, c, (const int32_t*)h->scan_items));
+    else CU(launch_ex(k_scan_warp<2>, gw, dim3(kScanThreads), 0, s, pdl, c, (const int32_t*)h->scan_items));
+  } else if (h->cfg.hist_precision == LGBM_B200_HIST_QUANT) {
     if (h->scan_wide) CU(launch_ex(k_scan<true, kScanWideBlocks>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
     else CU(launch_ex(k_scan<true, 1>, g, dim3(kScanThreads), h->scan_smem, s, pdl, c));
   } else if (h->scan_wide) {

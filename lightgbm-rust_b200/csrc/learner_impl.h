@@ -290,6 +290,12 @@ struct LgbmB200Learner {
   int64_t last_hist_rows = 0;
   int64_t last_part_rows = 0;
   bool scan_wide = false;  // the register-capped scan variant (many CTAs per step)
+  // the quantized scan by one warp per (feature, side): the item of each
+  // warp of each CTA (feature * 2 + side, -1 none; at most one categorical
+  // item per CTA) and the CTAs per slot
+  bool scan_warp = false;
+  int32_t* scan_items = nullptr;
+  int scan_warp_grid = 0;
   bool scan_part = false;  // scans and partition of a step in one cooperative launch
   int scan_part_grid = 0;
   int scan_part_max = 0;  // CTAs of that launch resident at once, shared by the slots

@@ -1361,11 +1361,12 @@ __device__ __forceinline__ bool split_better(const DSplit& a, const DSplit& b) {
 // Partition LUT over stored group values (learner/mod.rs:1313-1329): one
 // goes-left flag per value a row of the split feature can hold; thread t
 // of the CTA writes value t.
-__device__ void build_partition_lut(const DFeature& m, const DSplit& info, uint8_t* lut) {
+__device__ void build_partition_lut(const DFeature& m, const DSplit& info, uint8_t* lut, int32_t first,
+                                    int32_t step) {
   const bool numerical = m.bin_type == 0;
   const bool default_left = numerical ? info.default_left != 0 : false;
   const int32_t ntb = m.view_len + 1;
-  for (int32_t raw = threadIdx.x; raw < kMaxBins; raw += blockDim.x) {
+  for (int32_t raw = first; raw < kMaxBins; raw += step) {
     uint8_t left = 0;
     if (raw < ntb) {
       uint32_t b = decode_bin((uint32_t)raw, m);
@@ -1614,9 +1615,312 @@ __device__ void scan_item(const DCtx& c, const DSlot& s, int f, int side, ScanSm
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
     for (int i = tid; i < (int)(sizeof(DSplit) / 4); i += blockDim.x) dst[i] = src[i];
     // the partition's goes-left table for this candidate, ready if it wins
-    if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins);
+    if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins, tid, (int32_t)blockDim.x);
   }
 }
+
+// =====================================================================================
+// Quantized threshold scan, one warp per (feature, side): the same search as
+// scan_item / find_best_threshold_block / scan_direction_block for packed
+// integer sums, with lane l holding stored bins 8l .. 8l + 7 in registers.
+// Integer cumulative sums are exact in any order, and every per-candidate
+// value comes from the same expressions, so the results are the block
+// version's bit for bit; candidates reduce with the same tie rules. No block
+// barrier is involved, so a CTA runs eight items side by side.
+// =====================================================================================
+
+// One direction of the quantized scan by one warp. vw[32 j + lane] is stored
+// bin 8 * lane + j of the leaf's view (the most frequent bin fixed, the
+// larger leaf's view already formed), in this warp's shared memory.
+__device__ __noinline__ bool scan_direction_warp(const int64_t* vw, const DFeature& m, const DParams& p, const LeafCtx& lc,
+                                    double min_gain_shift, double cnt_factor, bool reverse, bool skip_default,
+                                    bool na_as_missing, DSplit& out) {
+  const int lane = threadIdx.x & 31;
+  const int offset = m.offset;
+  const int len = m.view_len;
+  int32_t t_lo, t_hi;
+  if (reverse) {
+    t_hi = m.num_bin - 1 - offset - (int32_t)na_as_missing;
+    t_lo = 1 - offset;
+  } else {
+    t_lo = 0;
+    t_hi = m.num_bin - 2 - offset;
+  }
+  const int32_t skip_t = skip_default ? m.default_bin - offset : INT32_MIN;
+  auto visited = [&](int t) { return t >= t_lo && t <= t_hi && t != skip_t && t < len; };
+  const bool first_extra = !reverse && na_as_missing && offset == 1;
+  const int32_t nstored = m.num_bin - offset;
+  // cumulative sums in scan order: ascending, the visited bins up to t;
+  // reverse, the visited bins from t up (the total minus those below t)
+  uint64_t pre = 0, all = 0;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int t = lane * kPer + j;
+    const uint64_t x = (uint64_t)vw[32 * j + lane];
+    if (visited(t)) pre += x;
+    if (first_extra && t < len && t < nstored) all += x;
+  }
+  uint64_t incl = pre;  // inclusive over lanes of this lane's visited sum
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t other = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += other;
+    all += __shfl_xor_sync(0xffffffffu, all, o);
+  }
+  const uint64_t total = __shfl_sync(0xffffffffu, incl, 31);
+  const uint64_t base = first_extra ? (uint64_t)lc.int_sum - all : 0ull;
+  const uint64_t run0 = incl - pre;  // visited bins below this lane's first
+  // visits this lane's visited candidates with their cumulative packed sum
+  // and count estimate, recomputed on each walk (no per-bin arrays live)
+  auto walk = [&](auto fn) {
+    uint64_t run = run0;
+#pragma unroll 1
+    for (int j = 0; j < kPer; ++j) {
+      const int t = lane * kPer + j;
+      const bool vis = visited(t);
+      const uint64_t below = run;  // visited bins below t
+      if (vis) {
+        run += (uint64_t)vw[32 * j + lane];
+        const int64_t q = (int64_t)(reverse ? total - below : base + run);
+        fn(t, round_int((double)int_hess(q) * cnt_factor), q);
+      }
+    }
+  };
+  // the extra candidate t = -1 (lane 0)
+  const int64_t eq = (int64_t)base;
+  const int32_t ec = round_int((double)int_hess(eq) * cnt_factor);
+  const int32_t min_data = p.min_data_in_leaf;
+  const double min_hess = p.min_sum_hessian_in_leaf;
+  const bool plain = plain_split(p, lc.mc);
+  const bool extra = lane == 0 && first_extra;
+  auto hsides = [&](int64_t aq, double& ha, double& hr) {
+    ha = (double)int_hess(aq) * lc.hs;
+    hr = (double)int_hess((int64_t)((uint64_t)lc.int_sum - (uint64_t)aq)) * lc.hs;
+  };
+  // pass 1: the first break in scan order
+  int32_t brk = reverse ? INT32_MIN : INT32_MAX;
+  auto break_at = [&](int t, int32_t ac, int64_t aq) {
+    double ha, hr;
+    hsides(aq, ha, hr);
+    const bool skip1 = ac < min_data || ha < min_hess;
+    if (!skip1 && (lc.num_data - ac < min_data || hr < min_hess)) brk = reverse ? max(brk, t) : min(brk, t);
+  };
+  walk(break_at);
+  if (extra) break_at(-1, ec, eq);
+  for (int o = 16; o > 0; o >>= 1) {
+    const int32_t ob = __shfl_xor_sync(0xffffffffu, brk, o);
+    brk = reverse ? max(brk, ob) : min(brk, ob);
+  }
+  // pass 2: gains of the candidates before the break
+  double best_gain = -INFINITY;
+  int32_t best_t = INT32_MIN;
+  bool splittable = false;
+  int64_t wq = 0;  // this lane's best candidate's cumulative values
+  int32_t wc = 0;
+  auto consider = [&](int t, int32_t ac, int64_t aq) {
+    if (t >= 0 ? (reverse ? t <= brk : t >= brk) : !(brk > -1)) return;
+    double ha, hr;
+    hsides(aq, ha, hr);
+    if (ac < min_data || ha < min_hess) return;
+    const int64_t rest = (int64_t)((uint64_t)lc.int_sum - (uint64_t)aq);
+    const double ga = (double)int_grad(aq) * lc.gs, gr = (double)int_grad(rest) * lc.gs;
+    ha += kEpsilon;
+    hr += kEpsilon;
+    const int32_t rc = lc.num_data - ac;
+    // the left child is the rest when scanning in reverse
+    const double g1 = reverse ? gr : ga, h1 = reverse ? hr : ha, g2 = reverse ? ga : gr, h2 = reverse ? ha : hr;
+    const int32_t c1 = reverse ? rc : ac, c2 = reverse ? ac : rc;
+    const double gain = split_gain_hot(plain, g1, h1, g2, h2, p, c1, c2, lc.parent_output, lc.mc, lc.cmin, lc.cmax,
+                                       m.monotone_type);
+    if (gain <= min_gain_shift) return;
+    splittable = true;
+    if (gain > best_gain || (gain == best_gain && best_t != INT32_MIN && (reverse ? t > best_t : t < best_t))) {
+      best_gain = gain;
+      best_t = t;
+      wq = aq;
+      wc = ac;
+    }
+  };
+  walk(consider);
+  if (extra) consider(-1, ec, eq);
+  warp_pick(reverse, best_gain, best_t);
+  const bool any = __any_sync(0xffffffffu, splittable);
+  ScanBest r;
+  r.splittable = any;
+  r.gain = best_gain;
+  r.t = best_t;
+  r.acc_g = r.acc_h = 0.0;
+  // the winner's cumulative values, from the lane whose best it was (the
+  // extra candidate t = -1 is lane 0's)
+  const int src = best_t >= 0 ? best_t / kPer : 0;
+  wq = (int64_t)__shfl_sync(0xffffffffu, (unsigned long long)wq, src);
+  wc = __shfl_sync(0xffffffffu, wc, src);
+  r.acc_q = best_t == INT32_MIN ? 0 : wq;
+  r.acc_c = best_t == INT32_MIN ? 0 : wc;
+  apply_direction<true>(r, m, p, lc.sum_g, lc.sum_h, lc.int_sum, lc.gs, lc.hs, lc.num_data, lc.parent_output, lc.mc,
+                        lc.cmin, lc.cmax, min_gain_shift, cnt_factor, reverse, out);
+  __syncwarp();
+  return any;
+}
+
+// find_best_threshold (split.rs:246-271, :930-950) of the quantized form for
+// one leaf and feature, by one warp; cat: the CTA's scratch, for a
+// categorical feature (its view is copied there first).
+__device__ bool find_best_threshold_warp(const int64_t* vw, ScanSmem* cat, const DFeature& m,
+                                         const DParams& p, const LeafCtx& lc, DSplit& out) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    out.default_left = 1;
+    out.gain = -INFINITY;
+    out.num_cat = 0;
+    out.monotone_type = 0;
+  }
+  __syncwarp();
+  bool ok = false;
+  if (m.bin_type == 1) {
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) cat->ig[lane * kPer + j] = vw[32 * j + lane];
+    __syncwarp();
+    ok = scan_categorical<true>(*cat, m, p, lc, out);
+  } else {
+    if (lane == 0) out.monotone_type = m.monotone_type;
+    const double sg = (double)int_grad(lc.int_sum) * lc.gs;
+    const double sh = (double)int_hess(lc.int_sum) * lc.hs;
+    const double min_gain_shift =
+        leaf_gain_hot(plain_split(p, lc.mc), sg, sh, p, lc.num_data, lc.parent_output) + p.min_gain_to_split;
+    const double cnt_factor = (double)lc.num_data / (double)int_hess(lc.int_sum);
+    // split.rs:426-439: the directions scanned and their missing-value rules
+    const bool two = m.num_bin > 2 && m.missing_type != 0;
+    const bool skip_default = two && m.missing_type == 1;
+    const bool na_missing = two && m.missing_type == 2;
+#pragma unroll 1
+    for (int d = 0; d < (two ? 2 : 1); ++d)
+      ok |= scan_direction_warp(vw, m, p, lc, min_gain_shift, cnt_factor, d == 0, skip_default, na_missing, out);
+    if (!two && lane == 0 && m.missing_type == 2) out.default_left = 0;
+  }
+  __syncwarp();
+  if (lane == 0) out.gain *= m.penalty;
+  __syncwarp();
+  return ok;
+}
+
+// scan_item for the quantized form by one warp: feature f, side (0 smaller,
+// 1 larger) of slot s. vw: this warp's view in shared memory ([kPer][32]);
+// out: its result in shared memory.
+__device__ void scan_item_warp(const DCtx& c, const DSlot& s, int f, int side, ScanSmem* cat, int64_t* vw,
+                               DSplit& out) {
+  DSlotState* st = s.st;
+  const int lane = threadIdx.x & 31;
+  const DFeature m = c.feats[f];
+  const DParams& p = c.p;
+  const int32_t nf = c.num_features;
+  // two waves of loads, as in the block version: the slot state, then what
+  // depends on it
+  const int32_t larger_leaf = st->larger.leaf, L = st->left_leaf, s_buf = st->s_buf, l_buf = st->l_buf;
+  const bool need = st->need_find != 0 && st->done == 0;
+  const int32_t nl_cur = st->num_leaves_cur;
+  const DLeafSplits sl = st->smaller;
+  const DLeafSplits ls = side == 0 ? sl : st->larger;
+  const double gsc = st->grad_scale, hsc = st->hess_scale;
+  const bool have_larger = larger_leaf >= 0;
+  const bool live = need && (side == 0 || have_larger);
+  const int len = m.view_len;
+  const size_t sbase = (size_t)s_buf * c.total_bins + m.view_start;
+  const size_t lbase = (size_t)l_buf * c.total_bins + m.view_start;
+  const long long* hsrc = reinterpret_cast<const long long*>(s.hist);
+  int64_t v[kPer], pv[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int i = lane * kPer + j;
+    // histogram cells are written by other CTAs' atomics: loaded through L2
+    v[j] = (live && i < len) ? (int64_t)__ldcg(hsrc + sbase + i) : 0;
+    pv[j] = (live && side == 1 && i < len) ? (int64_t)__ldcg(hsrc + lbase + i) : 0;
+  }
+  const uint8_t in_tree = s.bytree[f];
+  const uint8_t split_ok = have_larger ? s.splittable[L * nf + f] : (uint8_t)1;
+  const double cmin = live ? s.cmin[ls.leaf] : 0.0, cmax = live ? s.cmax[ls.leaf] : 0.0;
+  if (!(live && in_tree && split_ok)) return;
+  int64_t* hdst = reinterpret_cast<int64_t*>(s.hist);
+  // the smaller leaf's view with its most frequent bin fixed (histogram.rs:42-56; exact in any order)
+  if (m.most_freq_bin > 0) {
+    uint64_t part = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = lane * kPer + j;
+      if (i < m.num_bin && i != m.most_freq_bin) part += (uint64_t)v[j];
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    const int64_t fixed = (int64_t)((uint64_t)sl.int_sum - part);
+#pragma unroll
+    for (int j = 0; j < kPer; ++j)
+      if (lane * kPer + j == m.most_freq_bin) {
+        v[j] = fixed;
+        if (side == 0) hdst[sbase + m.most_freq_bin] = fixed;
+      }
+  }
+  if (side == 1) {  // larger = parent - smaller, in the parent's buffer (histogram.rs:59-63)
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = lane * kPer + j;
+      if (i < len) {
+        v[j] = (int64_t)((uint64_t)pv[j] - (uint64_t)v[j]);
+        hdst[lbase + i] = v[j];
+      }
+    }
+  }
+  LeafCtx lc;
+  lc.sum_g = ls.sum_gradients;
+  lc.sum_h = ls.sum_hessians;
+  lc.int_sum = ls.int_sum;
+  lc.gs = gsc;
+  lc.hs = hsc;
+  lc.num_data = ls.num_data;
+  // learner/mod.rs:1303-1309 parent output
+  lc.parent_output = nl_cur == 1 ? root_output(ls.sum_gradients, ls.sum_hessians, p, ls.num_data) : ls.weight;
+  lc.mc = p.use_monotone != 0;
+  lc.cmin = cmin;
+  lc.cmax = cmax;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) vw[32 * j + lane] = v[j];
+  __syncwarp();
+  const bool ok = find_best_threshold_warp(vw, cat, m, p, lc, out);
+  if (lane == 0) {
+    out.feature = m.real_index;
+    out.inner = f;
+    s.feat_ok[side * nf + f] = ok ? 1 : 0;
+  }
+  __syncwarp();
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(&out);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s.feat_res[side * nf + f]);
+  for (int i = lane; i < (int)(sizeof(DSplit) / 4); i += 32) dst[i] = src[i];
+  // the partition's goes-left table for this candidate, ready if it wins
+  if (ok) build_partition_lut(m, out, s.lut_cand + ((size_t)side * nf + f) * kMaxBins, lane, 32);
+}
+
+// Grid (CTAs, 1, slots), kScanThreads threads: warp w of CTA b scans item
+// items[8b + w] (feature * 2 + side, or -1 for none) of slot z. The host
+// gives each CTA at most one categorical item, which uses the CTA's scratch.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kScanThreads, kMinBlocks) k_scan_warp(const __grid_constant__ DCtx c,
+                                                                        const int32_t* items) {
+  __shared__ ScanSmem cat;
+  __shared__ DSplit outs[kScanThreads / 32];
+  __shared__ int64_t views[kScanThreads / 32][kPer * 32];
+  pdl_wait();
+  pdl_trigger();
+  const DSlot& s = c.slots[blockIdx.z];
+  DSlotState* st = s.st;
+  const int warp = threadIdx.x >> 5;
+  // the partition that follows claims its row tiles from this counter
+  if (blockIdx.x == 0 && threadIdx.x == 0 && !st->done) {
+    st->part_ticket = 0;
+    st->part_done = 0;
+  }
+  const int32_t it = items[blockIdx.x * (kScanThreads / 32) + warp];
+  if (it < 0) return;
+  scan_item_warp(c, s, it >> 1, it & 1, &cat, views[warp], outs[warp]);
+}
+template __global__ void k_scan_warp<2>(const __grid_constant__ DCtx, const int32_t*);
+template __global__ void k_scan_warp<kScanWideBlocks>(const __grid_constant__ DCtx, const int32_t*);
 
 // kMinBlocks: CTAs the compiler keeps resident per SM (registers capped to
 // fit). 1 for a step of few features, where each CTA's latency is what counts;

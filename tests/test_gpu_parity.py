@@ -224,6 +224,31 @@ def test_single_tree_quantized_exact(lgb, orc, renew):
         assert_same_tree(gt, ot, leaf_rtol=0.0, gain_rtol=0.0, gains=gains)
 
 
+@pytest.mark.parametrize("per", [1, 8])
+def test_single_tree_quantized_warp_scan(lgb, orc, grow_mode, monkeypatch, per):
+    """The quantized scan by one warp per (feature, side), forced on a step of
+    few items (by default it runs only when the block scans would take several
+    waves): NaN missing values in both scan directions, L1/L2, max_delta_step
+    and two categorical features (one-hot and sorted). Integer sums make it
+    bit-exact with the oracle, as the block scan is; `per` items share a CTA."""
+    if grow_mode != "per_step":
+        pytest.skip("the warp scan is a launch of the per-step graph")
+    monkeypatch.setenv("LGBM_B200_SCAN_WARP", "1")
+    monkeypatch.setenv("LGBM_B200_SCAN_PER", str(per))
+    rng = np.random.default_rng(21)
+    X, y = _binary_data(30000, f=12, seed=21, nan_frac=0.05)
+    pz = 1.0 / np.arange(1, 41) ** 1.1
+    X[:, 10] = rng.choice(40, len(y), p=pz / pz.sum())
+    X[:, 11] = rng.integers(0, 3, len(y))
+    params = {"objective": "binary", "num_leaves": 63, "use_quantized_grad": True, "num_threads": 16,
+              "lambda_l1": 0.3, "lambda_l2": 1.5, "max_delta_step": 0.8, "max_cat_to_onehot": 4,
+              "min_data_per_group": 50, "cat_smooth": 5.0}
+    gt, ot, _, om, _ = _tree_pair(lgb, orc, X, y, params, categorical=[10, 11])
+    assert_same_tree(gt, ot, leaf_rtol=0.0, gain_rtol=0.0, gains=om.trace(0)[3])
+    assert np.array_equal(gt["cat_boundaries"], ot["cat_boundaries"])
+    assert np.array_equal(gt["cat_threshold"], ot["cat_threshold"])
+
+
 def test_multiclass_slots_in_lockstep(lgb, orc):
     rng = np.random.default_rng(18)
     n = 15000
