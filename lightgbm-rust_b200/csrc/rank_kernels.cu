@@ -116,7 +116,7 @@ constexpr int kRankWarps = 8;  // queries per CTA (one warp each)
 // LambdarankNDCG::one_query (rank.rs:192-262) for every query, one warp
 // each. Writes g/h (class-major float arrays) and/or the interleaved pairs.
 __global__ void __launch_bounds__(kRankWarps * 32) k_lambdarank(DRank r, float* g, float* h, float2* gh) {
-  __shared__ double chain[kRankWarps][32];
+  __shared__ __align__(16) double chain[kRankWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int32_t T = r.truncation_level;
   for (int64_t q = (int64_t)blockIdx.x * kRankWarps + wib; q < r.nq; q += (int64_t)gridDim.x * kRankWarps) {
@@ -181,8 +181,14 @@ __global__ void __launch_bounds__(kRankWarps * 32) k_lambdarank(DRank r, float* 
         chain[wib][lane] = val;
         __syncwarp();
         if (lane == 0) {
-          const int32_t m = min(32, cnt - jb);
-          for (int32_t k = 0; k < m; ++k) sum_lambdas -= chain[wib][k];
+          // all 32 in order: the slots past the query hold +0.0, which
+          // changes no sum; unrolled, the loads go in pairs
+#pragma unroll
+          for (int32_t k = 0; k < 32; k += 2) {
+            const double2 two = *reinterpret_cast<const double2*>(&chain[wib][k]);
+            sum_lambdas -= two.x;
+            sum_lambdas -= two.y;
+          }
         }
         __syncwarp();
       }
