@@ -1101,6 +1101,17 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
   const int khi = len > 0 ? (len - 1) / kPer : -1;
   if (!kInt) {
     if (warp == 0) {
+      // this lane's bins in registers first, so that no shared load sits on
+      // the chain's critical path
+      double gv[kPer], hv[kPer];
+      int32_t cv[kPer];
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int t = lane * kPer + j;
+        gv[j] = t < len ? sm.g[t] : 0.0;
+        hv[j] = t < len ? sm.h[t] : 0.0;
+        cv[j] = t < len ? sm.ce[t] : 0;
+      }
       double a = 0.0, b = kEpsilon;
       int32_t c = 0;
       if (first_extra) {  // split.rs:787-800: the leaf sums minus every stored bin, ascending
@@ -1110,9 +1121,9 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
         carry_chain(false, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
           int t = lane * kPer + j;
           if (t < nstored && t < len) {
-            x -= sm.g[t];
-            y -= sm.h[t];
-            z -= sm.ce[t];
+            x -= gv[j];
+            y -= hv[j];
+            z -= cv[j];
           }
         });
         if (lane == 0) {
@@ -1124,9 +1135,9 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
       carry_chain(reverse, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
         int t = lane * kPer + j;
         if (visited(t)) {
-          x += sm.g[t];
-          y += sm.h[t];
-          z += sm.ce[t];
+          x += gv[j];
+          y += hv[j];
+          z += cv[j];
           sm.cg[t] = x;
           sm.ch[t] = y;
           sm.cc[t] = z;
