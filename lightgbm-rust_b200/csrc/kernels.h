@@ -37,6 +37,8 @@ struct ScanSmem {
   double g[kMaxBins], h[kMaxBins];        // this leaf's feature view
   double cg[kMaxBins], ch[kMaxBins];      // cumulative sums in scan order
   int32_t cc[kMaxBins];                   // cumulative count estimates
+  double cg2[kMaxBins], ch2[kMaxBins];    // the forward direction's, formed beside the reverse one's
+  int32_t cc2[kMaxBins];
   int32_t ce[kMaxBins];                   // count estimate of each bin
   int64_t ig[kMaxBins];                   // quantized view
   int64_t cq[kMaxBins];                   // quantized cumulative sums in scan order

@@ -1071,6 +1071,76 @@ __device__ __noinline__ bool scan_categorical(ScanSmem& sm, const DFeature& m, c
   return is_splittable;
 }
 
+// The FP64 cumulative sums of one scan direction in the reference's order
+// (split.rs:676-891): a lane carry chain by one warp, one add per visited
+// bin in scan order, into chain set `set` of `sm` (0: cg/ch/cc, 1:
+// cg2/ch2/cc2); the forward direction's extra candidate (NaN missing, no
+// stored bin 0) into eg/eh/ec.
+__device__ void fp64_direction_chain(ScanSmem& sm, const DFeature& m, const LeafCtx& lc, bool reverse,
+                                     bool skip_default, bool na_as_missing, int set) {
+  const int lane = threadIdx.x & 31;
+  const int offset = m.offset;
+  const int len = m.view_len;
+  int32_t t_lo, t_hi;
+  if (reverse) {
+    t_hi = m.num_bin - 1 - offset - (int32_t)na_as_missing;
+    t_lo = 1 - offset;
+  } else {
+    t_lo = 0;
+    t_hi = m.num_bin - 2 - offset;
+  }
+  const int32_t skip_t = skip_default ? m.default_bin - offset : INT32_MIN;
+  auto visited = [&](int t) { return t >= t_lo && t <= t_hi && t != skip_t && t < len; };
+  const bool first_extra = !reverse && na_as_missing && offset == 1;
+  const int32_t nstored = m.num_bin - offset;
+  const int khi = len > 0 ? (len - 1) / kPer : -1;
+  double* cg = set ? sm.cg2 : sm.cg;
+  double* ch = set ? sm.ch2 : sm.ch;
+  int32_t* cc = set ? sm.cc2 : sm.cc;
+  // this lane's bins in registers first, so that no shared load sits on the
+  // chain's critical path
+  double gv[kPer], hv[kPer];
+  int32_t cv[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int t = lane * kPer + j;
+    gv[j] = t < len ? sm.g[t] : 0.0;
+    hv[j] = t < len ? sm.h[t] : 0.0;
+    cv[j] = t < len ? sm.ce[t] : 0;
+  }
+  double a = 0.0, b = kEpsilon;
+  int32_t c = 0;
+  if (first_extra) {  // split.rs:787-800: the leaf sums minus every stored bin, ascending
+    a = lc.sum_g;
+    b = lc.sum_h - kEpsilon;
+    c = lc.num_data;
+    carry_chain(false, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
+      int t = lane * kPer + j;
+      if (t < nstored && t < len) {
+        x -= gv[j];
+        y -= hv[j];
+        z -= cv[j];
+      }
+    });
+    if (lane == 0) {
+      sm.eg = a;
+      sm.eh = b;
+      sm.ec = c;
+    }
+  }
+  carry_chain(reverse, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
+    int t = lane * kPer + j;
+    if (visited(t)) {
+      x += gv[j];
+      y += hv[j];
+      z += cv[j];
+      cg[t] = x;
+      ch[t] = y;
+      cc[t] = z;
+    }
+  });
+}
+
 // One direction of FindBestThresholdSequentially (split.rs:676-891 and
 // :995-1190) over the view in `sm`, by the whole CTA. Warp 0 forms the
 // cumulative sums in the reference's order (FP64: a lane carry chain, one
@@ -1081,7 +1151,7 @@ __device__ __noinline__ bool scan_categorical(ScanSmem& sm, const DFeature& m, c
 template <bool kInt>
 __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DParams& p, const LeafCtx& lc,
                                      double min_gain_shift, double cnt_factor, bool reverse, bool skip_default,
-                                     bool na_as_missing, DSplit& out) {
+                                     bool na_as_missing, DSplit& out, int chain = -1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int offset = m.offset;
   const int len = m.view_len;
@@ -1098,53 +1168,10 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
   // extra candidate t = -1 (forward with NaN missing and no stored bin 0)
   const bool first_extra = !reverse && na_as_missing && offset == 1;
   const int32_t nstored = m.num_bin - offset;
-  const int khi = len > 0 ? (len - 1) / kPer : -1;
   if (!kInt) {
-    if (warp == 0) {
-      // this lane's bins in registers first, so that no shared load sits on
-      // the chain's critical path
-      double gv[kPer], hv[kPer];
-      int32_t cv[kPer];
-#pragma unroll
-      for (int j = 0; j < kPer; ++j) {
-        const int t = lane * kPer + j;
-        gv[j] = t < len ? sm.g[t] : 0.0;
-        hv[j] = t < len ? sm.h[t] : 0.0;
-        cv[j] = t < len ? sm.ce[t] : 0;
-      }
-      double a = 0.0, b = kEpsilon;
-      int32_t c = 0;
-      if (first_extra) {  // split.rs:787-800: the leaf sums minus every stored bin, ascending
-        a = lc.sum_g;
-        b = lc.sum_h - kEpsilon;
-        c = lc.num_data;
-        carry_chain(false, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
-          int t = lane * kPer + j;
-          if (t < nstored && t < len) {
-            x -= gv[j];
-            y -= hv[j];
-            z -= cv[j];
-          }
-        });
-        if (lane == 0) {
-          sm.eg = a;
-          sm.eh = b;
-          sm.ec = c;
-        }
-      }
-      carry_chain(reverse, 0, khi, a, b, c, [&](int j, double& x, double& y, int32_t& z) {
-        int t = lane * kPer + j;
-        if (visited(t)) {
-          x += gv[j];
-          y += hv[j];
-          z += cv[j];
-          sm.cg[t] = x;
-          sm.ch[t] = y;
-          sm.cc[t] = z;
-        }
-      });
-      if (lane == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
-    }
+    const bool own = chain < 0;  // form the chain here (warp 0), or use the one formed before
+    if (own && warp == 0) fp64_direction_chain(sm, m, lc, reverse, skip_default, na_as_missing, 0);
+    if (tid == 0) sm.brk = reverse ? INT32_MIN : INT32_MAX;
   } else {
     // exact packed sums (any order): thread u holds scan position u, a block
     // scan over the threads in scan order gives every cumulative sum
@@ -1190,9 +1217,9 @@ __device__ bool scan_direction_block(ScanSmem& sm, const DFeature& m, const DPar
       ac = sm.ec;
       aq = sm.eq;
     } else {
-      ag = kInt ? 0.0 : sm.cg[t];
-      ah = kInt ? 0.0 : sm.ch[t];
-      ac = sm.cc[t];
+      ag = kInt ? 0.0 : (chain == 1 ? sm.cg2[t] : sm.cg[t]);
+      ah = kInt ? 0.0 : (chain == 1 ? sm.ch2[t] : sm.ch[t]);
+      ac = (!kInt && chain == 1) ? sm.cc2[t] : sm.cc[t];
       aq = kInt ? sm.cq[t] : 0;
     }
   };
@@ -1347,10 +1374,22 @@ __device__ bool find_best_threshold_block(ScanSmem& sm, const DFeature& m, const
     const bool skip_default = two && m.missing_type == 1;
     const bool na_missing = two && m.missing_type == 2;
     ok = false;
+    if (!kInt && two) {
+      // both directions' chains at once (warp 0 reverse, warp 1 forward): they
+      // read the same view and write separate sums; each direction's scan
+      // then reads its own (the barrier at its start orders them)
+      const int warp = tid >> 5;
+      if (warp < 2) fp64_direction_chain(sm, m, lc, warp == 0, skip_default, na_missing, warp);
+      ok |= scan_direction_block<kInt>(sm, m, p, lc, min_gain_shift, cnt_factor, true, skip_default, na_missing, out,
+                                        0);
+      ok |= scan_direction_block<kInt>(sm, m, p, lc, min_gain_shift, cnt_factor, false, skip_default, na_missing, out,
+                                        1);
+    } else {
 #pragma unroll 1
-    for (int d = 0; d < (two ? 2 : 1); ++d)
-      ok |= scan_direction_block<kInt>(sm, m, p, lc, min_gain_shift, cnt_factor, d == 0, skip_default, na_missing,
-                                        out);
+      for (int d = 0; d < (two ? 2 : 1); ++d)
+        ok |= scan_direction_block<kInt>(sm, m, p, lc, min_gain_shift, cnt_factor, d == 0, skip_default, na_missing,
+                                          out);
+    }
     if (!two && tid == 0 && m.missing_type == 2) out.default_left = 0;
   }
   if (tid == 0) out.gain *= m.penalty;
