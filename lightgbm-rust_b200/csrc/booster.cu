@@ -401,7 +401,8 @@ struct GradWorkspace {
   cudaStream_t stream = nullptr;
   ChunkStreams chunks;  // row chunks of the elementwise objectives
   DeviceArena arena;
-  size_t cap = 0;
+  size_t cap = 0;       // values (rows x classes) of score, g and h
+  size_t cap_rows = 0;  // rows of label
   float* label = nullptr;
   double* score = nullptr;
   float* g = nullptr;
@@ -474,21 +475,27 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
   if (w.device != device) {
     w.arena.free_all();
     w.cap = 0;
+    w.cap_rows = 0;
     if (w.stream) cudaStreamDestroy(w.stream);
     w.chunks.release();
     if (cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess || !w.chunks.init())
       return fail(Status(LGBM_B200_ERR_CUDA, "stream"));
     w.device = device;
   }
-  if (w.cap < nk) {
+  // both capacities are checked: a call with more rows but fewer values than
+  // an earlier multiclass one needs a larger label buffer
+  if (w.cap < nk || w.cap_rows < n) {
     w.arena.free_all();
+    const size_t rows = std::max(n, w.cap_rows), vals = std::max(nk, w.cap);
     Status s;
-    if (!(s = w.arena.alloc_n(&w.label, n)).ok() || !(s = w.arena.alloc_n(&w.score, nk)).ok() ||
-        !(s = w.arena.alloc_n(&w.g, nk)).ok() || !(s = w.arena.alloc_n(&w.h, nk)).ok()) {
+    if (!(s = w.arena.alloc_n(&w.label, rows)).ok() || !(s = w.arena.alloc_n(&w.score, vals)).ok() ||
+        !(s = w.arena.alloc_n(&w.g, vals)).ok() || !(s = w.arena.alloc_n(&w.h, vals)).ok()) {
       w.cap = 0;
+      w.cap_rows = 0;
       return fail(s);
     }
-    w.cap = nk;
+    w.cap = vals;
+    w.cap_rows = rows;
   }
   cudaStream_t s = w.stream;
   if (k == 1 && (cfg->objective == LGBM_B200_OBJ_BINARY || cfg->objective == LGBM_B200_OBJ_REGRESSION)) {
@@ -496,26 +503,38 @@ int lgbm_b200_gradients(const LgbmB200ObjectiveConfig* cfg, const float* label, 
     // copies out on one of three streams, so that copies in and out of
     // different chunks overlap
     cudaError_t e = cudaSuccess;
+    const char* where = "";
     for (int64_t r0 = 0, c = 0; r0 < num_data && e == cudaSuccess; r0 += ChunkStreams::kRows, ++c) {
       const int64_t m = std::min<int64_t>(ChunkStreams::kRows, num_data - r0);
       cudaStream_t cs = w.chunks.s[c % ChunkStreams::kN];
+      where = "labels in";
       e = cudaMemcpyAsync(w.label + r0, label + r0, sizeof(float) * m, cudaMemcpyHostToDevice, cs);
-      if (e == cudaSuccess)
+      if (e == cudaSuccess) {
+        where = "scores in";
         e = cudaMemcpyAsync(w.score + r0, scores + r0, sizeof(double) * m, cudaMemcpyHostToDevice, cs);
+      }
       if (e == cudaSuccess) {
         Status st = launch_gradients(*cfg, w.label + r0, w.score + r0, m, nullptr, w.g + r0, w.h + r0, current_device_sms(), cs, rk);
         if (!st.ok()) {
           w.chunks.sync();
           return fail(st);
         }
+        where = "gradient launch";
         e = cudaGetLastError();
       }
-      if (e == cudaSuccess) e = cudaMemcpyAsync(grad + r0, w.g + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) {
+        where = "gradients out";
+        e = cudaMemcpyAsync(grad + r0, w.g + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
+      }
       if (e == cudaSuccess) e = cudaMemcpyAsync(hess + r0, w.h + r0, sizeof(float) * m, cudaMemcpyDeviceToHost, cs);
     }
     cudaError_t e2 = w.chunks.sync();
-    if (e == cudaSuccess) e = e2;
-    if (e != cudaSuccess) return fail(Status(LGBM_B200_ERR_CUDA, cudaGetErrorString(e)));
+    if (e == cudaSuccess && e2 != cudaSuccess) {
+      e = e2;
+      where = "chunk sync";
+    }
+    if (e != cudaSuccess)
+      return fail(Status(LGBM_B200_ERR_CUDA, std::string("gradients (") + where + "): " + cudaGetErrorString(e)));
     return LGBM_B200_OK;
   }
   cudaMemcpyAsync(w.label, label, sizeof(float) * n, cudaMemcpyHostToDevice, s);
@@ -613,6 +632,7 @@ void lgbm_b200_objective_free(LgbmB200Objective* o) {
   if (o) {
     cudaSetDevice(o->device);
     delete o;
+    teardown_done("lgbm_b200_objective_free");
   }
 }
 
@@ -634,6 +654,7 @@ void lgbm_b200_booster_destroy(LgbmB200Booster* b) {
   if (b) {
     cudaSetDevice(b->L->device);
     delete b;
+    teardown_done("lgbm_b200_booster_destroy");
   }
 }
 
@@ -792,6 +813,7 @@ void lgbm_b200_forest_destroy(LgbmB200Forest* f) {
   if (f) {
     cudaSetDevice(f->device);
     delete f;
+    teardown_done("lgbm_b200_forest_destroy");
   }
 }
 

@@ -1010,7 +1010,10 @@ int lgbm_b200_dataset_create_valid_device(const float* X, int64_t n, int32_t nco
   return LGBM_B200_OK;
 }
 
-void lgbm_b200_dataset_free(LgbmB200Dataset* ds) { delete reinterpret_cast<Dataset*>(ds); }
+void lgbm_b200_dataset_free(LgbmB200Dataset* ds) {
+  delete reinterpret_cast<Dataset*>(ds);
+  teardown_done("lgbm_b200_dataset_free");
+}
 
 int lgbm_b200_learner_create(const LgbmB200LearnerConfig* cfg, const uint8_t* bins, int64_t num_data,
                              int32_t num_features, const LgbmB200FeatureMeta* metas, const double* upper_bounds,
@@ -1035,6 +1038,7 @@ void lgbm_b200_learner_destroy(LgbmB200Learner* h) {
   if (h) {
     cudaSetDevice(h->device);
     delete h;
+    teardown_done("lgbm_b200_learner_destroy");
   }
 }
 

@@ -2,6 +2,8 @@
 // units (learner.cu, booster.cu).
 #pragma once
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -30,6 +32,16 @@ namespace lgbm_b200 {
 inline int fail(const Status& s) {
   set_last_error(s.msg);
   return s.code;
+}
+
+// The end of a void teardown entry point (destroy / free): it cannot report
+// a CUDA error, so it consumes any its calls left as the thread's last
+// error; otherwise the next, unrelated call that checks cudaGetLastError
+// would return it. LGBM_B200_DEBUG_TEARDOWN=1 prints what was consumed.
+inline void teardown_done(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess && std::getenv("LGBM_B200_DEBUG_TEARDOWN"))
+    std::fprintf(stderr, "lgbm_b200: %s left %s\n", what, cudaGetErrorString(e));
 }
 
 // ------------------------------------------------------------------------------------------

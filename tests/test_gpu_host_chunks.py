@@ -74,3 +74,26 @@ def test_objective_handle_matches_stateless_gradients(lgb):
             g, h = obj.gradients(s)
             g0, h0 = lgb.gradients(params, y, s, group=grp)
             assert np.array_equal(g, g0) and np.array_equal(h, h0), params["objective"]
+
+
+def test_gradients_workspace_after_a_multiclass_call(lgb, orc):
+    """The stateless gradient call keeps its device buffers between calls.
+    A multiclass call on few rows (rows x classes values) followed by a
+    binary call on more rows, but fewer values, must grow the label buffer:
+    once the cache compared only the value count, and the second call's
+    label copy overran the buffer ("invalid argument")."""
+    rng = np.random.default_rng(43)
+    n_mc, k, n_bin = 50_000, 10, 120_000
+    ymc = rng.integers(0, k, n_mc).astype(np.float32)
+    pmc = {"objective": "multiclass", "num_class": k}
+    g, h = lgb.gradients(pmc, ymc, rng.standard_normal(n_mc * k))
+    assert g.shape == (n_mc * k,) or g.size == n_mc * k
+    yb = (rng.random(n_bin) < 0.3).astype(np.float32)
+    s = rng.standard_normal(n_bin)
+    pb = {"objective": "binary"}
+    g, h = lgb.gradients(pb, yb, s)
+    og, oh = orc.gradients(lgb.resolve_params(pb), yb, s)
+    for a, o in ((g, og), (h, oh)):
+        u = _ulps(np.asarray(a, np.float32).ravel(), np.asarray(o, np.float32).ravel())
+        assert u.max() <= 1
+        assert np.mean(u == 0) > 0.99
