@@ -232,13 +232,47 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
   }
   const size_t cells = (size_t)h->total_bins * (mode == LGBM_B200_HIST_QUANT ? 1 : 2);
   const size_t max_tiles = ((size_t)n + kPartTileRows - 1) / kPartTileRows + 1;
+  {
+    // the readback block: each slot's state, then its tree arrays, each
+    // piece on a 256-byte boundary
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+      const size_t o = off;
+      off += (bytes + 255) / 256 * 256;
+      return o;
+    };
+    auto& rb = h->rb;
+    const size_t Ls = (size_t)L;
+    rb.st = take(sizeof(DSlotState));
+    rb.sfi = take(4 * Ls);
+    rb.sf = take(4 * Ls);
+    rb.sg = take(4 * Ls);
+    rb.tib = take(4 * Ls);
+    rb.dt = take(Ls);
+    rb.lc = take(4 * Ls);
+    rb.rc = take(4 * Ls);
+    rb.lp = take(4 * Ls);
+    rb.lv = take(8 * Ls);
+    rb.lw = take(8 * Ls);
+    rb.lcnt = take(4 * Ls);
+    rb.ld = take(4 * Ls);
+    rb.iv = take(8 * Ls);
+    rb.iw = take(8 * Ls);
+    rb.ic = take(4 * Ls);
+    rb.cb = take(4 * Ls * kCatWords);
+    rb.ng = take(8 * Ls);
+    h->rb_slot = off;
+    if (!(s = A.alloc(reinterpret_cast<void**>(&h->rb_dev), off * (size_t)K)).ok()) return s;
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&h->rb_host), off * (size_t)K, cudaHostAllocDefault));
+  }
   h->slots_h.resize(K);
   for (int k = 0; k < K; ++k) {
     DSlot& d = h->slots_h[k];
     std::memset(&d, 0, sizeof(d));
 #define ALLOC(ptr, count)                                  \
   if (!(s = A.alloc_n(&(ptr), (size_t)(count))).ok()) return s;
-    ALLOC(d.st, 1);
+    unsigned char* rbk = h->rb_dev + (size_t)k * h->rb_slot;
+    d.st = reinterpret_cast<DSlotState*>(rbk + h->rb.st);
     ALLOC(d.idx[0], n);
     ALLOC(d.idx[1], n);
     ALLOC(d.leaf_begin, L);
@@ -269,23 +303,24 @@ static Status setup_learner(LgbmB200Learner* h, const LgbmB200LearnerConfig* cfg
     ALLOC(d.root_ipartials, kRootBlocks);
     ALLOC(d.root_counter, 1);
     DTree& t = d.tree;
-    ALLOC(t.split_feature_inner, L);
-    ALLOC(t.split_feature, L);
-    ALLOC(t.split_gain, L);
-    ALLOC(t.threshold_in_bin, L);
-    ALLOC(t.decision_type, L);
-    ALLOC(t.left_child, L);
-    ALLOC(t.right_child, L);
-    ALLOC(t.leaf_parent, L);
-    ALLOC(t.leaf_value, L);
-    ALLOC(t.leaf_weight, L);
-    ALLOC(t.leaf_count, L);
-    ALLOC(t.leaf_depth, L);
-    ALLOC(t.internal_value, L);
-    ALLOC(t.internal_weight, L);
-    ALLOC(t.internal_count, L);
-    ALLOC(t.cat_bits, (size_t)L * kCatWords);
-    ALLOC(t.node_gain, L);
+    const auto& rb = h->rb;
+    t.split_feature_inner = reinterpret_cast<int32_t*>(rbk + rb.sfi);
+    t.split_feature = reinterpret_cast<int32_t*>(rbk + rb.sf);
+    t.split_gain = reinterpret_cast<float*>(rbk + rb.sg);
+    t.threshold_in_bin = reinterpret_cast<uint32_t*>(rbk + rb.tib);
+    t.decision_type = reinterpret_cast<int8_t*>(rbk + rb.dt);
+    t.left_child = reinterpret_cast<int32_t*>(rbk + rb.lc);
+    t.right_child = reinterpret_cast<int32_t*>(rbk + rb.rc);
+    t.leaf_parent = reinterpret_cast<int32_t*>(rbk + rb.lp);
+    t.leaf_value = reinterpret_cast<double*>(rbk + rb.lv);
+    t.leaf_weight = reinterpret_cast<double*>(rbk + rb.lw);
+    t.leaf_count = reinterpret_cast<int32_t*>(rbk + rb.lcnt);
+    t.leaf_depth = reinterpret_cast<int32_t*>(rbk + rb.ld);
+    t.internal_value = reinterpret_cast<double*>(rbk + rb.iv);
+    t.internal_weight = reinterpret_cast<double*>(rbk + rb.iw);
+    t.internal_count = reinterpret_cast<int32_t*>(rbk + rb.ic);
+    t.cat_bits = reinterpret_cast<uint32_t*>(rbk + rb.cb);
+    t.node_gain = reinterpret_cast<double*>(rbk + rb.ng);
     CU(cudaMemset(d.st, 0, sizeof(DSlotState)));
     CU(cudaMemset(d.tile_status, 0, max_tiles * sizeof(unsigned long long)));
     CU(cudaMemset(d.root_counter, 0, sizeof(int32_t)));
@@ -594,39 +629,39 @@ static Status run_tree(LgbmB200Learner* h) {
   return Status();
 }
 
-// Copies one slot's device tree back and rebuilds the reference's arrays.
+// Rebuilds one slot's tree as the reference's arrays, from the readback
+// block's pinned mirror.
 static Status read_tree(LgbmB200Learner* h, int k) {
-  const DSlot& d = h->slots_h[k];
   const DSlotState& st = h->st_h[k];
   HostTree& t = h->trees[k];
   const int nl = std::max(1, st.num_leaves_cur);
   const int nn = nl - 1;
   t.num_leaves = nl;
-  auto get = [&](auto& vec, const auto* src, int count) -> Status {
+  // the slot's tree arrays from the pinned mirror of the readback block
+  // (train_collect copied every slot's in one transfer)
+  const unsigned char* base = h->rb_host + (size_t)k * h->rb_slot;
+  const auto& rb = h->rb;
+  auto get = [&](auto& vec, size_t offset, int count) {
     vec.resize((size_t)std::max(count, 0));
-    if (count > 0)
-      CU(cudaMemcpyAsync(vec.data(), src, sizeof(vec[0]) * count, cudaMemcpyDeviceToHost, h->stream));
-    return Status();
+    if (count > 0) std::memcpy(vec.data(), base + offset, sizeof(vec[0]) * (size_t)count);
   };
-  Status s;
-  if (!(s = get(t.split_feature_inner, d.tree.split_feature_inner, nn)).ok()) return s;
-  if (!(s = get(t.split_feature, d.tree.split_feature, nn)).ok()) return s;
-  if (!(s = get(t.split_gain, d.tree.split_gain, nn)).ok()) return s;
-  if (!(s = get(t.threshold_in_bin, d.tree.threshold_in_bin, nn)).ok()) return s;
-  if (!(s = get(t.decision_type, d.tree.decision_type, nn)).ok()) return s;
-  if (!(s = get(t.left_child, d.tree.left_child, nn)).ok()) return s;
-  if (!(s = get(t.right_child, d.tree.right_child, nn)).ok()) return s;
-  if (!(s = get(t.leaf_parent, d.tree.leaf_parent, nl)).ok()) return s;
-  if (!(s = get(t.leaf_value, d.tree.leaf_value, nl)).ok()) return s;
-  if (!(s = get(t.leaf_weight, d.tree.leaf_weight, nl)).ok()) return s;
-  if (!(s = get(t.leaf_count, d.tree.leaf_count, nl)).ok()) return s;
-  if (!(s = get(t.leaf_depth, d.tree.leaf_depth, nl)).ok()) return s;
-  if (!(s = get(t.internal_value, d.tree.internal_value, nn)).ok()) return s;
-  if (!(s = get(t.internal_weight, d.tree.internal_weight, nn)).ok()) return s;
-  if (!(s = get(t.internal_count, d.tree.internal_count, nn)).ok()) return s;
-  if (!(s = get(t.cat_bits, d.tree.cat_bits, nn * kCatWords)).ok()) return s;
-  if (!(s = get(t.node_gain, d.tree.node_gain, nn)).ok()) return s;
-  CU(cudaStreamSynchronize(h->stream));
+  get(t.split_feature_inner, rb.sfi, nn);
+  get(t.split_feature, rb.sf, nn);
+  get(t.split_gain, rb.sg, nn);
+  get(t.threshold_in_bin, rb.tib, nn);
+  get(t.decision_type, rb.dt, nn);
+  get(t.left_child, rb.lc, nn);
+  get(t.right_child, rb.rc, nn);
+  get(t.leaf_parent, rb.lp, nl);
+  get(t.leaf_value, rb.lv, nl);
+  get(t.leaf_weight, rb.lw, nl);
+  get(t.leaf_count, rb.lcnt, nl);
+  get(t.leaf_depth, rb.ld, nl);
+  get(t.internal_value, rb.iv, nn);
+  get(t.internal_weight, rb.iw, nn);
+  get(t.internal_count, rb.ic, nn);
+  get(t.cat_bits, rb.cb, nn * kCatWords);
+  get(t.node_gain, rb.ng, nn);
   // real-valued thresholds and category bitsets (learner/mod.rs:1132-1165)
   t.threshold.assign((size_t)nn, 0.0);
   t.num_cat = 0;
@@ -775,9 +810,11 @@ Status train_collect(LgbmB200Learner* h) {
   const int K = h->K;
   cudaStream_t s = h->stream;
   Status st;
-  for (int k = 0; k < K; ++k)
-    CU(cudaMemcpyAsync(&h->st_h[k], h->slots_h[k].st, sizeof(DSlotState), cudaMemcpyDeviceToHost, s));
+  // every slot's state and tree arrays in one transfer
+  CU(cudaMemcpyAsync(h->rb_host, h->rb_dev, h->rb_slot * (size_t)K, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
+  for (int k = 0; k < K; ++k)
+    std::memcpy(&h->st_h[k], h->rb_host + (size_t)k * h->rb_slot + h->rb.st, sizeof(DSlotState));
   if (h->cfg.persistent_grow) {
     GrowSync gsh;
     long long ph[4] = {0, 0, 0, 0};

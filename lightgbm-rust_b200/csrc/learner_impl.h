@@ -284,6 +284,15 @@ struct LgbmB200Learner {
   ChunkStreams chunks;              // add_leaf_outputs from host buffers
   // readback
   std::vector<DSlotState> st_h;
+  // Every slot's state and tree arrays in one device block (rb_slot bytes
+  // per slot, at the offsets in rb), so that one copy into the pinned mirror
+  // reads a whole tree set back.
+  struct ReadbackLayout {
+    size_t st, sfi, sf, sg, tib, dt, lc, rc, lp, lv, lw, lcnt, ld, iv, iw, ic, cb, ng;
+  } rb{};
+  unsigned char* rb_dev = nullptr;
+  unsigned char* rb_host = nullptr;
+  size_t rb_slot = 0;
   std::vector<HostTree> trees;
   std::vector<int32_t> tmp_i32;
   // timing
@@ -329,6 +338,7 @@ struct LgbmB200Learner {
     arena.free_all();
     chunks.release();
     if (start_h) cudaFreeHost(start_h);
+    if (rb_host) cudaFreeHost(rb_host);
     if (stream) cudaStreamDestroy(stream);
   }
 };
